@@ -1,0 +1,145 @@
+/*
+ * wamgpu.h - C ABI of the B200 (sm_100a) implementation of WAM Cycle 7's
+ * per-time-step hot path: the implicit source-term integration IMPLSCH
+ * (ST4 / IPHYS=1 and ST6 / IPHYS=2, with the DIA nonlinear transfer) and the
+ * spectral propagation PROPAGS with depth and current refraction.
+ *
+ * The Fortran driver binds these entry points through ISO_C_BINDING behind
+ * the reference's own module procedure names.  Every
+ * entry point that replaces a reference procedure cites it; references are
+ * myWAveModel/WAM file:line.
+ *
+ * Conventions
+ *  - Spectra use the reference layout FL3(IJ,K,M): sea point fastest, then
+ *    direction K (1..KL), then frequency M (1..ML), single precision.
+ *  - Index tables keep the reference convention: 1-based sea point numbers,
+ *    0 for a land neighbour (KLAT, KLON), 1-based depth-table index (INDEP).
+ *  - Every call returns 0 on success and a negative WAMGPU_E* code on
+ *    failure; wamgpu_last_error() then holds a message.  There is no CPU
+ *    fallback: without a usable CUDA device every call fails.
+ *  - One context per rank/thread; work is ordered on the context's CUDA
+ *    stream.  *_host calls are synchronous; *_dev calls are asynchronous on the
+ *    stream passed (NULL = the context stream).
+ */
+#ifndef WAMGPU_H
+#define WAMGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define WAMGPU_API __attribute__((visibility("default")))
+#else
+#define WAMGPU_API
+#endif
+
+#define WAMGPU_OK 0
+#define WAMGPU_E_ARG -1       /* invalid argument or unsupported option      */
+#define WAMGPU_E_CUDA -2      /* CUDA runtime error                           */
+#define WAMGPU_E_STATE -3     /* call out of order (e.g. no grid yet)         */
+#define WAMGPU_E_CFL -4       /* negative propagation coefficient (CHECK_CFL) */
+#define WAMGPU_E_NOMEM -5     /* device allocation failed                     */
+#define WAMGPU_E_NUMERIC -6   /* non-finite values detected in outputs        */
+#define WAMGPU_E_TIMEOUT -7   /* a bounded device wait expired                */
+
+typedef struct wamgpu_ctx wamgpu_ctx;
+
+/* Model configuration.  Field meaning follows the reference module variables
+ * after INITMDL (initmdl.f90:137-212): effective BETAMAX, ZALP, ALPHA and
+ * TAUWSHELTER after the ST4 swap and the ML<=30 ALPHA rule (initmdl.f90:153-160).
+ * Layout is shared with the Fortran shim (BIND(C) derived type). */
+typedef struct wamgpu_config {
+  int kl, ml;                 /* KL directions, ML frequencies (wam_fre_dir_module.f90:38-39) */
+  double fr1; int iref;       /* SET_FRE_DIR(N_DIR,N_FRE,FR1,IREF), fre_dir:122 */
+  int iphys;                  /* 1 = ST4 (Ardhuin), 2 = ST6 */
+  int shallow_run, spherical_run, refraction_d_run, refraction_c_run, reduced_grid;
+  int isnonlin, lcflx;        /* SNL depth scaling option; compute surface fluxes */
+  int idelt, idelpro;         /* source and propagation time steps [s] */
+  double betamax, zalp, alpha, tauwshelter, cdfac;
+  int ndepth; double deptha, depthd;  /* shallow-water table (wam_tables_module.f90:76-79) */
+  double delphi;              /* latitude increment [m] (wam_grid_module DELPHI) */
+  int precision;              /* 4 = FP32 (production), 8 = FP64 reference run of the same kernels */
+  int device;                 /* CUDA device ordinal */
+} wamgpu_config;
+
+/* Creates a context and builds the static spectral tables on the host:
+ * MAKE_FRE_DIR (wam_fre_dir_module.f90:297-459), MAKE_SHALLOW_TABLES
+ * (wam_tables_module.f90:388-464), MIN_ENERGY (:315-384), NLWEIGT and
+ * INIT_SNONLIN (wam_source_module.f90:1056-1523), TABU_SWELLFT (:3360),
+ * INIT_SDISSP_ARD (:3419), INIT_X0TAUHF (:3784); then uploads them.
+ * Replaces the table part of PREPARE_SOURCE (wam_source_module.f90:704). */
+WAMGPU_API int wamgpu_create(const wamgpu_config* cfg, wamgpu_ctx** out);
+WAMGPU_API int wamgpu_destroy(wamgpu_ctx* ctx);
+WAMGPU_API const char* wamgpu_last_error(const wamgpu_ctx* ctx);
+WAMGPU_API int wamgpu_config_size(void);
+
+/* Reference-convention copy of a host table (names as in the reference,
+ * e.g. "FR", "TFAK", "IKP", "K1W", "INDICESSAT"); returns the element count
+ * when out is NULL.  Float tables go to fout, integer tables to iout. */
+WAMGPU_API int wamgpu_get_table(const wamgpu_ctx* ctx, const char* name, float* fout, int* iout);
+
+/* The same tables computed on the host without a context or a GPU (for a
+ * driver that checks its own PREPARE_SOURCE tables against the library's). */
+WAMGPU_API int wamgpu_host_table(const wamgpu_config* cfg, const char* name, float* fout, int* iout);
+
+/* Grid module arrays for this rank's NSEA sea points (wam_grid_module.f90:
+ * KLAT(NSEA,2,2), KLON(NSEA,2), WLAT(NSEA,2), KFROMIJ(NSEA)) and the
+ * per-latitude SINPH, COSPH, DELLAM of the NY rows; computes DCO and DPSN
+ * (wam_initial_module.f90:204-214). */
+WAMGPU_API int wamgpu_set_grid(wamgpu_ctx* ctx, int nsea, const int* klat, const int* klon, const float* wlat,
+                    const int* kfromij, int ny, const float* sinph, const float* cosph, const float* dellam);
+
+/* Sea-point water depth [m] (WAM_MODEL_MODULE DEPTH) and currents U, V
+ * [m/s] (NULL = zero).  Take effect at the next wamgpu_prepare_propagation. */
+WAMGPU_API int wamgpu_set_depth(wamgpu_ctx* ctx, const float* depth);
+WAMGPU_API int wamgpu_set_current(wamgpu_ctx* ctx, const float* u, const float* v);
+
+/* PREPARE_PROPAGATION (wam_propagation_module.f90:279-598): INDEP, CGOND,
+ * depth/current gradients, refraction terms, the propagation coefficients
+ * and CHECK_CFL (:1917-2138) with COUNTER sub-stepping.  Returns
+ * WAMGPU_E_CFL where the reference calls ABORT1 (negative coefficient). */
+WAMGPU_API int wamgpu_prepare_propagation(wamgpu_ctx* ctx, float* total_cfl, int* counter);
+
+/* MAKE_SHALLOW_SNL (wam_source_module.f90:975-1048) for ISNONLIN != 0 and the
+ * remaining per-point source preparation; call after set_depth. */
+WAMGPU_API int wamgpu_prepare_source(wamgpu_ctx* ctx);
+
+/* INDEP(NSEA) as computed by prepare_propagation (propagation:327-332). */
+WAMGPU_API int wamgpu_get_indep(const wamgpu_ctx* ctx, int* indep);
+
+/* IMPLSCH(FL3, U10, UDIR, TAUW, USTAR, Z0, ROAIRN, WSTAR, DEPTH, INDEP)
+ * (wam_source_module.f90:374-700) on host buffers: copies in, integrates one
+ * source step of IDELT seconds on the device, copies FL3, TAUW, USTAR, Z0
+ * back.  nsea must equal the grid's NSEA; depth/indep may be NULL to use the
+ * context's own.  When LCFLX is set the flux-module arrays (wam_flux_module
+ * PHIOC, TAUOC_X, TAUOC_Y, PHIBOT, TAUBOT_X, TAUBOT_Y, PHIAW) are kept on the
+ * device; read them with wamgpu_get_fluxes. */
+WAMGPU_API int wamgpu_implsch_host(wamgpu_ctx* ctx, float* fl3, const float* u10, const float* udir, float* tauw, float* ustar,
+                        float* z0, const float* roairn, const float* wstar, const float* depth, const int* indep);
+
+/* PROPAGS(F3) (wam_propagation_module.f90:635-829) on a host buffer: COUNTER
+ * upwind sub-steps of IDELPRO/COUNTER seconds each. */
+WAMGPU_API int wamgpu_propags_host(wamgpu_ctx* ctx, float* f3);
+
+/* Device-pointer forms for callers that keep the model state resident on the
+ * GPU.  fl3 has leading dimension ld >= NSEA (elements); pointer element type
+ * is float for precision 4 and double for precision 8.  stream is a
+ * cudaStream_t (NULL = context stream).  wamgpu_propags_dev takes an
+ * optional scratch spectrum of the same shape (NULL = context-owned). */
+WAMGPU_API int wamgpu_implsch_dev(wamgpu_ctx* ctx, void* fl3, int ld, const void* u10, const void* udir, void* tauw, void* ustar,
+                       void* z0, const void* roairn, const void* wstar, void* stream);
+WAMGPU_API int wamgpu_propags_dev(wamgpu_ctx* ctx, void* f3, int ld, void* scratch, void* stream);
+
+/* Flux-module arrays of the last LCFLX step, 7 blocks of NSEA in the order
+ * PHIOC, TAUOC_X, TAUOC_Y, PHIBOT, TAUBOT_X, TAUBOT_Y, PHIAW (host copy). */
+WAMGPU_API int wamgpu_get_fluxes(wamgpu_ctx* ctx, float* out7);
+
+/* Synchronises the context stream; returns WAMGPU_E_NUMERIC if a kernel
+ * reported non-finite output since the last call. */
+WAMGPU_API int wamgpu_sync(wamgpu_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* WAMGPU_H */

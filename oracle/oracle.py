@@ -1,0 +1,190 @@
+"""ctypes wrapper around the CPU oracle (oracle/liboracle.so).
+
+ORACLE — test infrastructure only.  Imported by tests/ and by bench.py's
+CPU-baseline leg; never by the wam_b200 package.  The oracle is a
+statement-order C++ restatement of WAM Cycle 7's IMPLSCH/PROPAGS path and its
+table builders (wam_source_module.f90, wam_propagation_module.f90,
+wam_fre_dir_module.f90, wam_tables_module.f90, preproc_module.f90).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+class OracleConfig(ctypes.Structure):
+    _fields_ = [("kl", ctypes.c_int), ("ml", ctypes.c_int), ("fr1", ctypes.c_double), ("iref", ctypes.c_int),
+                ("iphys", ctypes.c_int), ("shallow_run", ctypes.c_int), ("spherical_run", ctypes.c_int),
+                ("refraction_d_run", ctypes.c_int), ("refraction_c_run", ctypes.c_int), ("reduced_grid", ctypes.c_int),
+                ("isnonlin", ctypes.c_int), ("lcflx", ctypes.c_int), ("idelt", ctypes.c_int), ("idelpro", ctypes.c_int),
+                ("betamax", ctypes.c_double), ("zalp", ctypes.c_double), ("alpha", ctypes.c_double),
+                ("tauwshelter", ctypes.c_double), ("cdfac", ctypes.c_double), ("ndepth", ctypes.c_int),
+                ("deptha", ctypes.c_double), ("depthd", ctypes.c_double), ("delphi", ctypes.c_double)]
+
+
+class GridDef(ctypes.Structure):
+    _fields_ = [("NX", ctypes.c_int), ("NY", ctypes.c_int), ("AMOSOP", ctypes.c_int), ("AMOWEP", ctypes.c_int),
+                ("AMOEAP", ctypes.c_int), ("XDELLA", ctypes.c_int), ("XDELLO", ctypes.c_int),
+                ("reduced_grid", ctypes.c_int)]
+
+
+def build():
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        vp, ip, dp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)
+        L.oracle_create.restype = vp
+        L.oracle_create.argtypes = [ctypes.POINTER(OracleConfig), ctypes.c_int]
+        L.oracle_destroy.argtypes = [vp]
+        L.oracle_get_table.argtypes = [vp, ctypes.c_char_p, dp]
+        L.oracle_get_itable.argtypes = [vp, ctypes.c_char_p, ip]
+        L.oracle_set_grid.argtypes = [vp, ctypes.c_int, ip, ip, dp, ip, ctypes.c_int, dp, dp, dp, ctypes.c_double]
+        L.oracle_set_fields.argtypes = [vp, dp, dp, dp]
+        L.oracle_prepare_propagation.argtypes = [vp, dp, ip]
+        L.oracle_prepare_source.argtypes = [vp]
+        L.oracle_get_indep.argtypes = [vp, ip]
+        L.oracle_get_coef.argtypes = [vp, ctypes.c_char_p, dp]
+        L.oracle_implsch.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, ip, dp,
+                                     ctypes.c_int]
+        L.oracle_propags.argtypes = [vp, dp]
+        L.oracle_grid_create.restype = vp
+        L.oracle_grid_create.argtypes = [ctypes.POINTER(GridDef), ctypes.c_char_p]
+        L.oracle_grid_destroy.argtypes = [vp]
+        L.oracle_grid_nsea.argtypes = [vp]
+        L.oracle_grid_get.argtypes = [vp, ip, ip, dp, ip, dp, dp, dp, dp, ip, ip, ip]
+        assert L.oracle_sizeof_config() == ctypes.sizeof(OracleConfig)
+        assert L.oracle_sizeof_griddef() == ctypes.sizeof(GridDef)
+        _LIB = L
+    return _LIB
+
+
+def _d(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if a is not None else None
+
+
+def _i(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int)) if a is not None else None
+
+
+def build_grid(nx, ny, amosop, amowep, amoeap, xdella, xdello, mask, reduced=False):
+    """Reference neighbour tables for a land-sea mask[nx, ny] (True = sea)."""
+    L = lib()
+    g = GridDef(nx, ny, amosop, amowep, amoeap, xdella, xdello, int(reduced))
+    m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8).T)  # (ny, nx) rows -> i fastest
+    h = L.oracle_grid_create(ctypes.byref(g), m.tobytes())
+    try:
+        n = L.oracle_grid_nsea(h)
+        out = dict(klat=np.zeros(4 * n, np.int32), klon=np.zeros(2 * n, np.int32), wlat=np.zeros(2 * n),
+                   kfromij=np.zeros(n, np.int32), sinph=np.zeros(ny), cosph=np.zeros(ny), dellam=np.zeros(ny),
+                   ixlg=np.zeros(n, np.int32), kxlt=np.zeros(n, np.int32))
+        delphi = ctypes.c_double()
+        iper = ctypes.c_int()
+        L.oracle_grid_get(h, _i(out["klat"]), _i(out["klon"]), _d(out["wlat"]), _i(out["kfromij"]), _d(out["sinph"]),
+                          _d(out["cosph"]), _d(out["dellam"]), ctypes.byref(delphi), _i(out["ixlg"]), _i(out["kxlt"]),
+                          ctypes.byref(iper))
+        out["delphi"] = delphi.value
+        out["iper"] = iper.value
+        out["nsea"] = n
+        return out
+    finally:
+        L.oracle_grid_destroy(h)
+
+
+class Oracle:
+    """One model configuration of the CPU oracle, FP32 (precision=4) or FP64 (8)."""
+
+    def __init__(self, cfg: dict, precision=4):
+        self.L = lib()
+        fields = {f for f, _ in OracleConfig._fields_}
+        c = OracleConfig(**{k: v for k, v in cfg.items() if k in fields})
+        self.cfg = dict(cfg)
+        self.h = self.L.oracle_create(ctypes.byref(c), precision)
+        if not self.h:
+            raise RuntimeError("oracle_create failed")
+        self.kl, self.ml = cfg["kl"], cfg["ml"]
+        self.nsea = 0
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.oracle_destroy(self.h)
+            self.h = None
+
+    def table(self, name):
+        n = self.L.oracle_get_table(self.h, name.encode(), None)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n)
+        self.L.oracle_get_table(self.h, name.encode(), _d(out))
+        return out
+
+    def itable(self, name):
+        n = self.L.oracle_get_itable(self.h, name.encode(), None)
+        if n < 0:
+            raise KeyError(name)
+        out = np.zeros(n, np.int32)
+        self.L.oracle_get_itable(self.h, name.encode(), _i(out))
+        return out
+
+    def set_grid(self, g):
+        self.nsea = g["nsea"]
+        self.L.oracle_set_grid(self.h, g["nsea"], _i(np.ascontiguousarray(g["klat"], np.int32)),
+                               _i(np.ascontiguousarray(g["klon"], np.int32)), _d(np.ascontiguousarray(g["wlat"], float)),
+                               _i(np.ascontiguousarray(g["kfromij"], np.int32)), len(g["sinph"]),
+                               _d(np.ascontiguousarray(g["sinph"], float)), _d(np.ascontiguousarray(g["cosph"], float)),
+                               _d(np.ascontiguousarray(g["dellam"], float)), float(g["delphi"]))
+
+    def set_fields(self, depth, u=None, v=None):
+        d = np.ascontiguousarray(depth, float)
+        uu = None if u is None else np.ascontiguousarray(u, float)
+        vv = None if v is None else np.ascontiguousarray(v, float)
+        self.L.oracle_set_fields(self.h, _d(d), _d(uu), _d(vv))
+
+    def prepare_propagation(self):
+        cfl = ctypes.c_double()
+        cnt = ctypes.c_int()
+        rc = self.L.oracle_prepare_propagation(self.h, ctypes.byref(cfl), ctypes.byref(cnt))
+        return rc, cfl.value, cnt.value
+
+    def prepare_source(self):
+        self.L.oracle_prepare_source(self.h)
+
+    def indep(self):
+        out = np.zeros(self.nsea, np.int32)
+        self.L.oracle_get_indep(self.h, _i(out))
+        return out
+
+    def coef(self, name):
+        n = self.L.oracle_get_coef(self.h, name.encode(), None)
+        out = np.zeros(n)
+        self.L.oracle_get_coef(self.h, name.encode(), _d(out))
+        return out
+
+    def implsch(self, fl3, u10, udir, tauw, ustar, z0, roairn, wstar, depth, indep, lcflx=False, nthreads=0):
+        """One IMPLSCH step in place on float64 copies; returns (fl3, tauw, ustar, z0, fluxes)."""
+        nsea = fl3.shape[0]
+        f = np.array(fl3, dtype=float, order="F")
+        tw, us, zz = (np.array(a, dtype=float) for a in (tauw, ustar, z0))
+        fl = np.zeros(7 * nsea) if lcflx else None
+        self.L.oracle_implsch(self.h, nsea, nsea, _d(f), _d(np.ascontiguousarray(u10, float)),
+                              _d(np.ascontiguousarray(udir, float)), _d(tw), _d(us), _d(zz),
+                              _d(np.ascontiguousarray(roairn, float)), _d(np.ascontiguousarray(wstar, float)),
+                              _d(np.ascontiguousarray(depth, float)), _i(np.ascontiguousarray(indep, np.int32)), _d(fl),
+                              nthreads)
+        return f, tw, us, zz, (fl.reshape(7, nsea) if fl is not None else None)
+
+    def propags(self, fl3):
+        f = np.array(fl3, dtype=float, order="F")
+        self.L.oracle_propags(self.h, _d(f))
+        return f

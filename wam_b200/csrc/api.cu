@@ -1,0 +1,689 @@
+// C ABI of libwamgpu (declarations and reference citations in include/wamgpu.h).
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+#include "../../include/wamgpu.h"
+#include "wamgpu_config.hpp"
+#include "spectral_tables.hpp"
+#include "propags.cuh"
+#include "kernels.hpp"
+
+using namespace wamgpu;
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t n = 0;
+  ~DevBuf() { if (p) cudaFree(p); }
+  cudaError_t ensure(size_t bytes) {
+    if (bytes <= n && p) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr; n = 0;
+    cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+    if (e == cudaSuccess) n = bytes;
+    return e;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+struct ImplBase {
+  virtual ~ImplBase() {}
+};
+
+}  // namespace
+
+struct wamgpu_ctx {
+  Config cfg{};
+  std::string err;
+  cudaStream_t stream = nullptr;
+  int nsm = 148;
+  int P = 8;  // sea points per IMPLSCH CTA
+  // grid (reference convention, host)
+  int nsea = 0, ny = 0, n_ext = 0;
+  std::vector<int> klat, klon, kfromij;
+  std::vector<float> wlat, sinph, cosph, dellam;
+  std::vector<float> depth, u, v;
+  std::vector<int> indep;
+  bool have_grid = false, prepared = false;
+  int counter = 1; double total_cfl = 0, cfl_min = 0; int variant = 0;
+  std::unique_ptr<ImplBase> impl;
+  // precision-specific part
+  virtual ~wamgpu_ctx() {}
+};
+
+namespace {
+
+template <typename R> struct Impl : ImplBase {
+  TableSet<R> tab;
+  DevTables<R> dt{};
+  PropArgs<R> pa{};
+  DevBuf small, ismall, tfak, tcgond, tsihkd, flminfr, enh, gom, fr, sinth, costh;
+  // per-point metadata
+  DevBuf d_klat, d_klon, d_wlat, d_dpsn, d_della0, d_drgm, d_indep, d_indep_g, d_ddphi, d_ddlam, d_duphi, d_dulam,
+      d_dvphi, d_dvlam, d_u, d_v, d_depth;
+  // model state used by the host-buffer entry points
+  DevBuf fl3, scratch, u10, udir, tauw, ustar, z0, roairn, wstar, fluxes, status, cflext;
+  std::vector<R> dco, dpsn;  // host
+};
+
+int fail(wamgpu_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+int cuda_fail(wamgpu_ctx* c, cudaError_t e, const char* where) {
+  return fail(c, WAMGPU_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CK(call, where)                                 \
+  do {                                                  \
+    cudaError_t e_ = (call);                            \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, where); \
+  } while (0)
+
+template <typename T> cudaError_t upload(DevBuf& b, const std::vector<T>& h, cudaStream_t s) {
+  cudaError_t e = b.ensure(h.size() * sizeof(T) + 16);
+  if (e != cudaSuccess) return e;
+  if (h.empty()) return cudaSuccess;
+  return cudaMemcpyAsync(b.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
+  const Config& c = ctx->cfg;
+  TableSet<R>& t = I.tab;
+  t.build(c);
+  // packed small tables
+  SmallLayout L{};
+  std::vector<R> sr;
+  auto putr = [&](int& off, const std::vector<R>& v) { off = (int)sr.size(); sr.insert(sr.end(), v.begin(), v.end()); };
+  std::vector<R> delfl(t.ML);
+  for (int m = 0; m < t.ML; ++m) delfl[m] = R(5.0E-07) * Phys<R>::G / powi(t.FR[m], 4) * R(c.idelt);
+  putr(L.FR, t.FR); putr(L.DF, t.DF); putr(L.DFIM, t.DFIM); putr(L.DFIMOFR, t.DFIMOFR); putr(L.FR5, t.FR5);
+  putr(L.FRM5, t.FRM5); putr(L.RHOWG_DFIM, t.RHOWG_DFIM); putr(L.TH, t.TH); putr(L.COSTH, t.COSTH);
+  putr(L.SINTH, t.SINTH); putr(L.DELFL, delfl); putr(L.AF11, t.AF11); putr(L.RNLCOEF, t.RNLCOEF);
+  putr(L.SATW, t.SATWEIGHTS); putr(L.WTAUHF, t.WTAUHF); putr(L.SWELLFT, t.SWELLFT);
+  L.nreal = (int)sr.size();
+  std::vector<int> si;
+  auto puti = [&](int& off, const std::vector<int>& v) { off = (int)si.size(); si.insert(si.end(), v.begin(), v.end()); };
+  puti(L.K1W, t.K1W); puti(L.K2W, t.K2W); puti(L.K11W, t.K11W); puti(L.K21W, t.K21W); puti(L.INLCOEF, t.INLCOEF);
+  puti(L.IKP, t.IKP); puti(L.IKP1, t.IKP1); puti(L.IKM, t.IKM); puti(L.IKM1, t.IKM1); puti(L.INDSAT, t.INDICESSAT);
+  L.nint = (int)si.size();
+  cudaStream_t s = ctx->stream;
+  CK(upload(I.small, sr, s), "upload tables");
+  CK(upload(I.ismall, si, s), "upload tables");
+  CK(upload(I.tfak, t.TFAK, s), "upload tables");
+  CK(upload(I.tcgond, t.TCGOND, s), "upload tables");
+  CK(upload(I.tsihkd, t.TSIHKD, s), "upload tables");
+  CK(upload(I.flminfr, t.FLMINFR, s), "upload tables");
+  CK(upload(I.gom, t.GOM, s), "upload tables");
+  CK(upload(I.fr, t.FR, s), "upload tables");
+  CK(upload(I.sinth, t.SINTH, s), "upload tables");
+  CK(upload(I.costh, t.COSTH, s), "upload tables");
+  DevTables<R>& d = I.dt;
+  d.KL = t.KL; d.ML = t.ML; d.NS = t.KL * t.ML; d.NDEPTH = t.NDEPTH; d.MFRSTLW = t.MFRSTLW; d.MLSTHG = t.MLSTHG;
+  d.KFRH = t.KFRH; d.NSDSNTH = t.NSDSNTH;
+  {
+    const R sig1 = Phys<R>::ZPI * t.FR[0];
+    int nk10 = (int)std::ceil(std::log(R(10.) / (sig1 / Phys<R>::ZPI)) / std::log(Phys<R>::CO)) + 1;
+    d.NK10 = std::max(t.ML, nk10);
+  }
+  d.iphys = c.iphys; d.shallow = c.shallow_run; d.isnonlin = c.isnonlin; d.lcflx = c.lcflx;
+  d.DELTH = t.DELTH; d.DELTR = t.DELTR; d.INV_LOG_CO = t.INV_LOG_CO; d.MO_TAIL = t.MO_TAIL; d.MM1_TAIL = t.MM1_TAIL;
+  d.DELU = t.DELU; d.DAL1 = t.DAL1; d.DAL2 = t.DAL2; d.X0TAUHF = t.X0TAUHF;
+  d.BETAMAX = R(c.betamax); d.ZALP = R(c.zalp); d.ALPHA = R(c.alpha); d.TAUWSHELTER = R(c.tauwshelter);
+  d.CDFAC = R(c.cdfac); d.DELT = R(c.idelt);
+  d.lay = L;
+  d.small = I.small.template as<R>(); d.ismall = I.ismall.template as<int>();
+  d.TFAK = I.tfak.template as<R>(); d.TCGOND = I.tcgond.template as<R>(); d.FLMINFR = I.flminfr.template as<R>();
+  d.ENH = nullptr; d.enh_ld = 0;
+  if (d.NK10 > MAX_NK10) return fail(ctx, WAMGPU_E_ARG, "frequency grid too low: 10 Hz extension exceeds kernel bound");
+  // every DIA gather row and scatter target the kernel can touch lies inside the spectrum
+  {
+    const int ML = t.ML, KL = t.KL, mfr1 = -t.MFRSTLW + 1, mfrl = ML - t.KFRH + mfr1;
+    for (int v : t.K1W) if (v < 1 || v > KL) return fail(ctx, WAMGPU_E_ARG, "DIA angular index out of range");
+    for (int v : t.K2W) if (v < 1 || v > KL) return fail(ctx, WAMGPU_E_ARG, "DIA angular index out of range");
+    for (int v : t.K11W) if (v < 1 || v > KL) return fail(ctx, WAMGPU_E_ARG, "DIA angular index out of range");
+    for (int v : t.K21W) if (v < 1 || v > KL) return fail(ctx, WAMGPU_E_ARG, "DIA angular index out of range");
+    for (int v : t.INLCOEF) if (v < 1 || v > ML) return fail(ctx, WAMGPU_E_ARG, "DIA frequency index out of range");
+    for (int v : t.INDICESSAT) if (v < 1 || v > KL) return fail(ctx, WAMGPU_E_ARG, "saturation index out of range");
+    auto in = [&](int m) { return m >= 1 && m <= ML; };
+    for (int mc = 1; mc <= t.MLSTHG; ++mc) {
+      int i = mc - t.MFRSTLW, MP = t.IKP[i], MP1 = t.IKP1[i], MM = t.IKM[i], MM1 = t.IKM1[i];
+      bool ok = true;
+      if (mc > mfr1 && mc < mfrl) ok = in(mc) && in(MM) && in(MM1) && in(MP) && in(MP1);
+      else if (mc >= mfrl) ok = in(MM) && (MM1 > ML || (in(MM1) && (mc > ML || (in(mc) && (MP > ML || (in(MP) && (MP1 > ML || in(MP1))))))));
+      else ok = (MM1 < 1 || in(MM1)) && in(mc) && in(MP) && in(MP1);
+      if (!ok) return fail(ctx, WAMGPU_E_ARG, "DIA scatter target outside the spectrum");
+    }
+  }
+  // CTA shape: the largest of 8/4/2 points whose workspace fits the opt-in shared memory
+  int dev = c.device;
+  int maxsm = 0;
+  CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device attribute");
+  int choices[3] = {8, 4, 2};
+  ctx->P = 0;
+  for (int P : choices) {
+    if (sizeof(R) == 8 && P == 8) continue;
+    if (sizeof(R) == 4 && P == 2) continue;
+    size_t need = implsch_smem_bytes(d, P);
+    if ((int)need <= maxsm) { ctx->P = P; CK(implsch_set_max_smem<R>(P, need), "smem attribute"); break; }
+  }
+  if (!ctx->P) return fail(ctx, WAMGPU_E_ARG, "spectrum too large for the shared-memory workspace");
+  CK(cudaStreamSynchronize(s), "table upload");
+  return WAMGPU_OK;
+}
+
+template <typename R> R rf(float x) { return R(x); }
+
+// PREPARE_PROPAGATION host part: INDEP, DCO/DPSN, gradients, INDEP_G and
+// the variant metric factors; the coefficients themselves live in the kernels.
+template <typename R> int prepare_prop(wamgpu_ctx* ctx, Impl<R>& I, float* total_cfl, int* counter) {
+  const Config& c = ctx->cfg;
+  const TableSet<R>& t = I.tab;
+  const int n = ctx->nsea, KL = t.KL, ML = t.ML, ND = t.NDEPTH;
+  auto KLAT = [&](int ij1, int ic, int j) { return ctx->klat[(ij1 - 1) + n * ((ic - 1) + 2 * (j - 1))]; };
+  auto KLON = [&](int ij1, int d) { return ctx->klon[(ij1 - 1) + n * (d - 1)]; };
+  auto WLAT = [&](int ij1, int ic) { return R(ctx->wlat[(ij1 - 1) + n * (ic - 1)]); };
+  std::vector<R> D(n + 1, R(999.0)), U(n + 1, R(0)), V(n + 1, R(0));
+  for (int i = 0; i < n; ++i) { D[i + 1] = R(ctx->depth[i]); U[i + 1] = R(ctx->u[i]); V[i + 1] = R(ctx->v[i]); }
+  // INDEP (:327-332)
+  ctx->indep.assign(n, 1);
+  if (c.shallow_run)
+    for (int i = 0; i < n; ++i) {
+      int v = f_nint(std::log(D[i + 1] / t.DEPTHA) / std::log(t.DEPTHD) + R(1.));
+      ctx->indep[i] = std::min(std::max(v, 1), ND);
+    }
+  const bool refr = c.refraction_d_run || c.refraction_c_run;
+  // GRADIENT (:182-275) on 1-based fields with land slot 0
+  const R delphi = R(c.delphi);
+  auto gradient = [&](const std::vector<R>& Fd, std::vector<R>& dlat, std::vector<R>& dlon) {
+    dlat.assign(n, R(0)); dlon.assign(n, R(0));
+    for (int ij = 1; ij <= n; ++ij) {
+      int ip = KLAT(ij, 2, 1), im = KLAT(ij, 1, 1);
+      if (c.reduced_grid) {
+        int ip2 = KLAT(ij, 2, 2), im2 = KLAT(ij, 1, 2);
+        if (ip && im && ip2 && im2)
+          dlat[ij - 1] = (WLAT(ij, 2) * Fd[ip] + (R(1.) - WLAT(ij, 2)) * Fd[ip2] - WLAT(ij, 1) * Fd[im] -
+                          (R(1.) - WLAT(ij, 1)) * Fd[im2]) / (R(2.) * delphi);
+        else if (ip && im) dlat[ij - 1] = (Fd[ip] - Fd[im]) / (R(2.) * delphi);
+        else if (ip2 && im2) dlat[ij - 1] = (Fd[ip2] - Fd[im2]) / (R(2.) * delphi);
+      } else if (ip && im) dlat[ij - 1] = (Fd[ip] - Fd[im]) / (R(2.) * delphi);
+      int ie = KLON(ij, 2), iw = KLON(ij, 1);
+      if (ie && iw) dlon[ij - 1] = (Fd[ie] - Fd[iw]) / (R(2.) * R(ctx->dellam[ctx->kfromij[ij - 1] - 1]));
+    }
+  };
+  std::vector<R> ddphi(n, 0), ddlam(n, 0), duphi(n, 0), dulam(n, 0), dvphi(n, 0), dvlam(n, 0);
+  std::vector<int> indep_g(n, 1);
+  if (refr) {
+    if (c.shallow_run) {
+      gradient(D, ddphi, ddlam);
+      if (c.spherical_run) for (int i = 0; i < n; ++i) ddlam[i] = ddlam[i] * I.dco[i + 1];
+    }
+    if (c.refraction_c_run) {
+      gradient(U, duphi, dulam); gradient(V, dvphi, dvlam);
+      if (c.spherical_run)
+        for (int i = 0; i < n; ++i) { dulam[i] = dulam[i] * I.dco[i + 1]; dvlam[i] = dvlam[i] * I.dco[i + 1]; }
+    }
+    if (c.shallow_run)  // INDEP_G (:413-475)
+      for (int ij = 1; ij <= n; ++ij) {
+        R dm = R(4.) * D[ij]; int iz = 4;
+        int ip = KLAT(ij, 2, 1), im = KLAT(ij, 1, 1);
+        if (c.reduced_grid) {
+          int ip2 = KLAT(ij, 2, 2), im2 = KLAT(ij, 1, 2);
+          if (ip && im && ip2 && im2) {
+            dm = dm + WLAT(ij, 2) * D[ip] + (R(1.) - WLAT(ij, 2)) * D[ip2] + WLAT(ij, 1) * D[im] + (R(1.) - WLAT(ij, 1)) * D[im2];
+            iz += 2;
+          } else if (ip && im) { dm = dm + D[ip] + D[im]; iz += 2; }
+          else if (ip2 && im2) { dm = dm + D[ip2] + D[im2]; iz += 2; }
+        } else if (ip && im) { dm = dm + D[ip] + D[im]; iz += 2; }
+        int ie = KLON(ij, 2), iw = KLON(ij, 1);
+        if (ie && iw) { dm = dm + D[ie] + D[iw]; iz += 2; }
+        dm = dm / R(iz);
+        int v = f_nint(std::log(dm / t.DEPTHA) / std::log(t.DEPTHD) + R(1.));
+        indep_g[ij - 1] = std::min(std::max(v, 1), ND);
+      }
+  }
+  // variant and metric factors (PREPARE_PROPAGATION_COEF :837-917)
+  int var;
+  if (!c.spherical_run) var = c.refraction_c_run ? (c.shallow_run ? V_CART_SHALLOW_CUR : V_CART_DEEP_CUR) : (c.shallow_run ? V_CART_SHALLOW : V_CART_DEEP);
+  else var = c.refraction_c_run ? (c.shallow_run ? V_SPHER_SHALLOW_CURR : V_SPHER_DEEP_CURR) : (c.shallow_run ? V_SPHER_SHALLOW : V_SPHER_DEEP);
+  ctx->variant = var;
+  const R delpro = R(c.idelpro);
+  std::vector<R> della0(n), drgm(n, R(0));
+  for (int i = 0; i < n; ++i) {
+    R dl = R(ctx->dellam[ctx->kfromij[i] - 1]);
+    if (var == V_CART_DEEP) della0[i] = delpro / dl;
+    else if (var == V_SPHER_DEEP) della0[i] = delpro * I.dco[i + 1] / dl;
+    else if (c.spherical_run) della0[i] = R(0.5) * delpro * I.dco[i + 1] / dl;
+    else della0[i] = R(0.5) * delpro / dl;
+    if (c.spherical_run) drgm[i] = R(ctx->sinph[ctx->kfromij[i] - 1]) * I.dco[i + 1];
+  }
+  PropArgs<R>& A = I.pa;
+  A.nsea = n; A.KL = KL; A.ML = ML; A.variant = var; A.reduced = c.reduced_grid; A.refr_d = c.refraction_d_run;
+  A.spherical = c.spherical_run; A.counter = 1; A.rcounter = R(1); A.NDEPTH = ND;
+  A.DELPH0 = (var == V_CART_DEEP) ? delpro / delphi : R(0.5) * delpro / delphi;
+  A.DELTH0 = R(0.5) * delpro / t.DELTR;
+  A.DELTHR = R(0.5) * delpro / t.DELTH;
+  A.DELFR0 = c.shallow_run ? R(0.5) * delpro / (R(0.1) * Phys<R>::ZPI) : R(0.5) * delpro * R(2.1) / R(0.2);
+  cudaStream_t s = ctx->stream;
+  std::vector<R> wl(ctx->wlat.begin(), ctx->wlat.end());
+  CK(upload(I.d_klat, ctx->klat, s), "upload grid");
+  CK(upload(I.d_klon, ctx->klon, s), "upload grid");
+  CK(upload(I.d_wlat, wl, s), "upload grid");
+  CK(upload(I.d_dpsn, I.dpsn, s), "upload grid");
+  CK(upload(I.d_della0, della0, s), "upload grid");
+  CK(upload(I.d_drgm, drgm, s), "upload grid");
+  CK(upload(I.d_indep, ctx->indep, s), "upload grid");
+  CK(upload(I.d_indep_g, indep_g, s), "upload grid");
+  CK(upload(I.d_ddphi, ddphi, s), "upload grid"); CK(upload(I.d_ddlam, ddlam, s), "upload grid");
+  CK(upload(I.d_duphi, duphi, s), "upload grid"); CK(upload(I.d_dulam, dulam, s), "upload grid");
+  CK(upload(I.d_dvphi, dvphi, s), "upload grid"); CK(upload(I.d_dvlam, dvlam, s), "upload grid");
+  std::vector<R> uu(U.begin() + 1, U.end()), vv(V.begin() + 1, V.end()), dd(D.begin() + 1, D.end());
+  CK(upload(I.d_u, uu, s), "upload grid"); CK(upload(I.d_v, vv, s), "upload grid");
+  CK(upload(I.d_depth, dd, s), "upload grid");
+  A.klat = I.d_klat.template as<int>(); A.klon = I.d_klon.template as<int>(); A.wlat = I.d_wlat.template as<R>();
+  A.dpsn = I.d_dpsn.template as<R>(); A.della0 = I.d_della0.template as<R>(); A.drgm = I.d_drgm.template as<R>();
+  A.indep = I.d_indep.template as<int>(); A.indep_g = I.d_indep_g.template as<int>();
+  A.ddphi = I.d_ddphi.template as<R>(); A.ddlam = I.d_ddlam.template as<R>();
+  A.duphi = I.d_duphi.template as<R>(); A.dulam = I.d_dulam.template as<R>();
+  A.dvphi = I.d_dvphi.template as<R>(); A.dvlam = I.d_dvlam.template as<R>();
+  A.u = I.d_u.template as<R>(); A.v = I.d_v.template as<R>();
+  A.TCGOND = I.tcgond.template as<R>(); A.TSIHKD = I.tsihkd.template as<R>(); A.TFAK = I.tfak.template as<R>();
+  A.GOM = I.gom.template as<R>(); A.FR = I.fr.template as<R>(); A.SINTH = I.sinth.template as<R>(); A.COSTH = I.costh.template as<R>();
+  // CHECK_CFL (:1917-2138) from the extrema of the recomputed coefficients
+  CK(I.cflext.ensure(2 * CFL_NCLASS * sizeof(long long)), "alloc");
+  CK(launch_cfl_extrema<R>(A, I.cflext.template as<long long>(), ctx->nsm, s), "cfl kernel");
+  long long ext[2 * CFL_NCLASS];
+  CK(cudaMemcpyAsync(ext, I.cflext.p, sizeof(ext), cudaMemcpyDeviceToHost, s), "cfl copy");
+  CK(cudaStreamSynchronize(s), "cfl sync");
+  auto mx = [&](int q) { return (R)cfl_decode(ext[2 * q], sizeof(R)); };
+  auto mn = [&](int q) { return (R)cfl_decode(ext[2 * q + 1], sizeof(R)); };
+  const bool cur = c.refraction_c_run;
+  const bool has_theta = c.spherical_run || cur || (c.shallow_run && c.refraction_d_run);
+  R lat11max = cur ? std::max(mx(CFL_LAT11), mx(CFL_LAT21)) : mx(CFL_LAT11);
+  R lat11min = cur ? std::min(mn(CFL_LAT11), mn(CFL_LAT21)) : mn(CFL_LAT11);
+  R lat12max = R(0.1), lat12min = R(0.1);
+  if (c.reduced_grid) {
+    lat12max = cur ? std::max(mx(CFL_LAT12), mx(CFL_LAT22)) : mx(CFL_LAT12);
+    lat12min = cur ? std::min(mn(CFL_LAT12), mn(CFL_LAT22)) : mn(CFL_LAT12);
+  }
+  R lon11max = mx(CFL_LON1);
+  R lon12max = cur ? mx(CFL_LON2) : R(0.1), lon12min = cur ? mn(CFL_LON2) : R(0.1);
+  R th1max = has_theta ? mx(CFL_TH1) : R(0.1), th1min = has_theta ? mn(CFL_TH1) : R(0.1);
+  R th2max = has_theta ? mx(CFL_TH2) : R(0.1), th2min = has_theta ? mn(CFL_TH2) : R(0.1);
+  R sg1max = cur ? mx(CFL_SG1) : R(0.1), sg1min = cur ? mn(CFL_SG1) : R(0.1);
+  R sg2max = cur ? mx(CFL_SG2) : R(0.1), sg2min = cur ? mn(CFL_SG2) : R(0.1);
+  R summax = R(1.) - mn(CFL_SUM), summin = R(1.) - mx(CFL_SUM);
+  R cmax = std::max({lat11max, lat12max, lon11max, lon12max, th1max, th2max, sg1max, sg2max, summax});
+  R cmin = std::min({lat11min, lat12min, lon12min, lon12min, th1min, th2min, sg1min, sg2min, summin});
+  ctx->cfl_min = cmin;
+  if (cmin < R(0.)) {
+    ctx->total_cfl = cmin;
+    if (total_cfl) *total_cfl = (float)cmin;
+    return fail(ctx, WAMGPU_E_CFL, "negative propagation coefficient (CHECK_CFL): reduce IDELPRO");
+  }
+  R tc = cmax;
+  int cnt = 1;
+  if (tc > R(0.999)) { cnt = (int)std::ceil(tc); tc = tc / R(cnt); }
+  A.counter = cnt; A.rcounter = R(cnt);
+  ctx->counter = cnt; ctx->total_cfl = tc;
+  if (total_cfl) *total_cfl = (float)tc;
+  if (counter) *counter = cnt;
+  // per-point source inputs for the host entry points
+  I.dt.ENH = nullptr;
+  ctx->prepared = true;
+  return WAMGPU_OK;
+}
+
+template <typename R> int set_grid_t(wamgpu_ctx* ctx, Impl<R>& I) {
+  const int n = ctx->nsea;
+  I.dco.assign(n + 1, R(0)); I.dpsn.assign((size_t)2 * n, R(1.));
+  if (ctx->cfg.spherical_run) {  // wam_initial_module.f90:204-214
+    for (int i = 0; i < n; ++i) I.dco[i + 1] = R(1.) / R(ctx->cosph[ctx->kfromij[i] - 1]);
+    for (int i = 0; i < n; ++i)
+      for (int ic = 0; ic < 2; ++ic) {
+        int nb = ctx->klat[i + n * ic];
+        if (nb != 0) I.dpsn[i + (size_t)n * ic] = I.dco[i + 1] / I.dco[nb];
+      }
+  }
+  return WAMGPU_OK;
+}
+
+// MAKE_SHALLOW_SNL (:975-1048)
+template <typename R> int prepare_source_t(wamgpu_ctx* ctx, Impl<R>& I) {
+  const Config& c = ctx->cfg;
+  I.dt.ENH = nullptr; I.dt.enh_ld = 0;
+  if (!(c.shallow_run && c.isnonlin != 0)) return WAMGPU_OK;
+  const TableSet<R>& t = I.tab;
+  const int n = ctx->nsea, mlsthg = t.MLSTHG;
+  std::vector<R> enh((size_t)n * mlsthg);
+  for (int m = 1; m <= mlsthg; ++m)
+    for (int i = 0; i < n; ++i) {
+      R d = R(ctx->depth[i]);
+      R om = (m <= t.ML) ? Phys<R>::ZPI * t.FR[m - 1] : Phys<R>::ZPI * t.FR[t.ML - 1] * powi(Phys<R>::CO, m - t.ML);
+      enh[i + (size_t)n * (m - 1)] = std::min(R(10.), transf(aki(om, d), d));
+    }
+  CK(upload(I.enh, enh, ctx->stream), "upload ENH");
+  I.dt.ENH = I.enh.template as<R>(); I.dt.enh_ld = n;
+  CK(cudaStreamSynchronize(ctx->stream), "ENH");
+  return WAMGPU_OK;
+}
+
+template <typename R>
+int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u10, const void* udir, void* tauw,
+                  void* ustar, void* z0, const void* roairn, const void* wstar, cudaStream_t s) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first (INDEP)");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  if (ctx->cfg.shallow_run && ctx->cfg.isnonlin != 0 && !I.dt.ENH)
+    return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_source first (ISNONLIN table)");
+  if (!I.status.p) { CK(I.status.ensure(16), "alloc"); CK(cudaMemsetAsync(I.status.p, 0, 16, s), "memset"); }
+  if (ctx->cfg.lcflx) CK(I.fluxes.ensure((size_t)7 * ctx->nsea * sizeof(R) + 16), "alloc");
+  ImplArgs<R> a;
+  a.nsea = ctx->nsea; a.ld = ld;
+  a.fl3 = (R*)fl3; a.u10 = (const R*)u10; a.udir = (const R*)udir; a.roairn = (const R*)roairn; a.wstar = (const R*)wstar;
+  a.depth = I.d_depth.template as<R>(); a.indep = I.d_indep.template as<int>();
+  a.tauw = (R*)tauw; a.ustar = (R*)ustar; a.z0 = (R*)z0;
+  a.fluxes = ctx->cfg.lcflx ? I.fluxes.template as<R>() : nullptr;
+  a.status = I.status.template as<int>();
+  CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch");
+  return WAMGPU_OK;
+}
+
+template <typename R> int propags_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* f3v, int ld, void* scratch, cudaStream_t s) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  R* f3 = (R*)f3v;
+  const size_t bytes = (size_t)ld * ctx->cfg.kl * ctx->cfg.ml * sizeof(R);
+  R* sc = (R*)scratch;
+  if (!sc) { CK(I.scratch.ensure(bytes), "alloc scratch"); sc = I.scratch.template as<R>(); }
+  // ping-pong over COUNTER sub-steps so that the last one writes f3
+  const int cnt = ctx->counter;
+  R* src = f3; R* dst = sc;
+  if (cnt % 2 == 1) { CK(cudaMemcpyAsync(sc, f3, bytes, cudaMemcpyDeviceToDevice, s), "copy F1"); src = sc; dst = f3; }
+  for (int it = 0; it < cnt; ++it) {
+    CK(launch_propags<R>(I.pa, src, ld, dst, ld, s), "propags launch");
+    std::swap(src, dst);
+  }
+  return WAMGPU_OK;
+}
+
+template <typename R> std::vector<R> to_r(const float* p, size_t n) {
+  std::vector<R> v(n);
+  for (size_t i = 0; i < n; ++i) v[i] = R(p[i]);
+  return v;
+}
+
+template <typename R>
+int implsch_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, const float* u10, const float* udir, float* tauw, float* ustar,
+                   float* z0, const float* roairn, const float* wstar, const float* depth, const int* indep) {
+  const int n = ctx->nsea;
+  const size_t nb = (size_t)n * ctx->cfg.kl * ctx->cfg.ml;
+  cudaStream_t s = ctx->stream;
+  CK(I.fl3.ensure(nb * sizeof(R)), "alloc");
+  for (DevBuf* b : {&I.u10, &I.udir, &I.tauw, &I.ustar, &I.z0, &I.roairn, &I.wstar}) CK(b->ensure((size_t)n * sizeof(R) + 16), "alloc");
+  if (depth) { std::vector<R> d = to_r<R>(depth, n); CK(upload(I.d_depth, d, s), "upload depth"); CK(cudaStreamSynchronize(s), "sync"); }
+  if (indep) { CK(cudaMemcpyAsync(I.d_indep.p, indep, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, s), "upload indep"); }
+  struct Up { void* d; const float* h; size_t n; };
+  Up ups[] = {{I.fl3.p, fl3, nb}, {I.u10.p, u10, (size_t)n}, {I.udir.p, udir, (size_t)n}, {I.tauw.p, tauw, (size_t)n},
+              {I.ustar.p, ustar, (size_t)n}, {I.z0.p, z0, (size_t)n}, {I.roairn.p, roairn, (size_t)n}, {I.wstar.p, wstar, (size_t)n}};
+  std::vector<std::vector<R>> keep;
+  for (auto& u : ups) {
+    if (sizeof(R) == 4) CK(cudaMemcpyAsync(u.d, u.h, u.n * 4, cudaMemcpyHostToDevice, s), "H2D");
+    else { keep.push_back(to_r<R>(u.h, u.n)); CK(cudaMemcpyAsync(u.d, keep.back().data(), u.n * sizeof(R), cudaMemcpyHostToDevice, s), "H2D"); }
+  }
+  int rc = implsch_dev_t<R>(ctx, I, I.fl3.p, n, I.u10.p, I.udir.p, I.tauw.p, I.ustar.p, I.z0.p, I.roairn.p, I.wstar.p, s);
+  if (rc) return rc;
+  struct Dn { float* h; void* d; size_t n; };
+  Dn dns[] = {{fl3, I.fl3.p, nb}, {tauw, I.tauw.p, (size_t)n}, {ustar, I.ustar.p, (size_t)n}, {z0, I.z0.p, (size_t)n}};
+  for (auto& d : dns) {
+    if (sizeof(R) == 4) CK(cudaMemcpyAsync(d.h, d.d, d.n * 4, cudaMemcpyDeviceToHost, s), "D2H");
+    else {
+      std::vector<R> tmp(d.n);
+      CK(cudaMemcpyAsync(tmp.data(), d.d, d.n * sizeof(R), cudaMemcpyDeviceToHost, s), "D2H");
+      CK(cudaStreamSynchronize(s), "sync");
+      for (size_t i = 0; i < d.n; ++i) d.h[i] = (float)tmp[i];
+    }
+  }
+  CK(cudaStreamSynchronize(s), "implsch sync");
+  return wamgpu_sync(ctx);
+}
+
+template <typename R> int propags_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* f3) {
+  const size_t nb = (size_t)ctx->nsea * ctx->cfg.kl * ctx->cfg.ml;
+  cudaStream_t s = ctx->stream;
+  CK(I.fl3.ensure(nb * sizeof(R)), "alloc");
+  std::vector<R> tmp;
+  if (sizeof(R) == 4) CK(cudaMemcpyAsync(I.fl3.p, f3, nb * 4, cudaMemcpyHostToDevice, s), "H2D");
+  else { tmp = to_r<R>(f3, nb); CK(cudaMemcpyAsync(I.fl3.p, tmp.data(), nb * sizeof(R), cudaMemcpyHostToDevice, s), "H2D"); }
+  int rc = propags_dev_t<R>(ctx, I, I.fl3.p, ctx->nsea, nullptr, s);
+  if (rc) return rc;
+  if (sizeof(R) == 4) CK(cudaMemcpyAsync(f3, I.fl3.p, nb * 4, cudaMemcpyDeviceToHost, s), "D2H");
+  else {
+    CK(cudaMemcpyAsync(tmp.data(), I.fl3.p, nb * sizeof(R), cudaMemcpyDeviceToHost, s), "D2H");
+    CK(cudaStreamSynchronize(s), "sync");
+    for (size_t i = 0; i < nb; ++i) f3[i] = (float)tmp[i];
+  }
+  CK(cudaStreamSynchronize(s), "propags sync");
+  return WAMGPU_OK;
+}
+
+template <typename R> int get_table_t(const wamgpu_ctx* ctx, const Impl<R>& I, const std::string& n, float* fo, int* io) {
+  const TableSet<R>& t = I.tab;
+  const std::vector<R>* f = nullptr; const std::vector<int>* iv = nullptr;
+  std::vector<R> tmp; std::vector<int> itmp;
+  if (n == "FR") f = &t.FR; else if (n == "DF") f = &t.DF; else if (n == "DFIM") f = &t.DFIM; else if (n == "GOM") f = &t.GOM;
+  else if (n == "C") f = &t.C; else if (n == "TH") f = &t.TH; else if (n == "COSTH") f = &t.COSTH; else if (n == "SINTH") f = &t.SINTH;
+  else if (n == "DFIMOFR") f = &t.DFIMOFR; else if (n == "FR5") f = &t.FR5; else if (n == "FRM5") f = &t.FRM5;
+  else if (n == "RHOWG_DFIM") f = &t.RHOWG_DFIM; else if (n == "TFAK") f = &t.TFAK; else if (n == "TCGOND") f = &t.TCGOND;
+  else if (n == "TSIHKD") f = &t.TSIHKD; else if (n == "FLMINFR") f = &t.FLMINFR; else if (n == "AF11") f = &t.AF11;
+  else if (n == "FKLAP") f = &t.FKLAP; else if (n == "FKLAP1") f = &t.FKLAP1; else if (n == "FKLAM") f = &t.FKLAM;
+  else if (n == "FKLAM1") f = &t.FKLAM1; else if (n == "FRH") f = &t.FRH; else if (n == "RNLCOEF") f = &t.RNLCOEF;
+  else if (n == "SWELLFT") f = &t.SWELLFT; else if (n == "SATWEIGHTS") f = &t.SATWEIGHTS; else if (n == "WTAUHF") f = &t.WTAUHF;
+  else if (n == "SCALARS") {
+    tmp = {t.DELTH, t.DELTR, t.INV_LOG_CO, t.MO_TAIL, t.MM1_TAIL, t.MP1_TAIL, R(0), R(0), t.DELU, t.ACL1, t.ACL2, t.CL11,
+           t.CL21, t.DAL1, t.DAL2, t.X0TAUHF};
+    f = &tmp;
+  } else if (n == "IKP") iv = &t.IKP; else if (n == "IKP1") iv = &t.IKP1; else if (n == "IKM") iv = &t.IKM;
+  else if (n == "IKM1") iv = &t.IKM1; else if (n == "K1W") iv = &t.K1W; else if (n == "K2W") iv = &t.K2W;
+  else if (n == "K11W") iv = &t.K11W; else if (n == "K21W") iv = &t.K21W; else if (n == "INLCOEF") iv = &t.INLCOEF;
+  else if (n == "INDICESSAT") iv = &t.INDICESSAT;
+  else if (n == "DIA_SCALARS") { itmp = {t.MFRSTLW, t.MLSTHG, t.KFRH, 0, 0, t.NSDSNTH}; iv = &itmp; }
+  else if (n == "INDEP") iv = &ctx->indep;
+  if (f) { if (fo) for (size_t i = 0; i < f->size(); ++i) fo[i] = (float)(*f)[i]; return (int)f->size(); }
+  if (iv) { if (io) std::memcpy(io, iv->data(), iv->size() * sizeof(int)); return (int)iv->size(); }
+  return WAMGPU_E_ARG;
+}
+
+#define DISPATCH_CTX(ctx, FN, ...)                                                              \
+  ((ctx)->cfg.precision == 8 ? FN<double>((ctx), *static_cast<Impl<double>*>((ctx)->impl.get()), ##__VA_ARGS__) \
+                             : FN<float>((ctx), *static_cast<Impl<float>*>((ctx)->impl.get()), ##__VA_ARGS__))
+
+}  // namespace
+
+extern "C" {
+
+int wamgpu_config_size(void) { return (int)sizeof(wamgpu_config); }
+
+int wamgpu_create(const wamgpu_config* cfg, wamgpu_ctx** out) {
+  if (!cfg || !out) return WAMGPU_E_ARG;
+  *out = nullptr;
+  auto* ctx = new wamgpu_ctx();
+  ctx->cfg = *cfg;
+  const Config& c = ctx->cfg;
+  auto bail = [&](int rc) { if (rc) { /* keep ctx for wamgpu_last_error */ *out = ctx; } return rc; };
+  if (c.kl < 4 || c.kl > MAX_KL || c.ml < 4 || c.ml > MAX_ML) return bail(fail(ctx, WAMGPU_E_ARG, "KL/ML outside supported range"));
+  if (c.iphys != 1 && c.iphys != 2) return bail(fail(ctx, WAMGPU_E_ARG, "only IPHYS=1 (ST4) and IPHYS=2 (ST6) are implemented"));
+  if (c.precision != 4 && c.precision != 8) return bail(fail(ctx, WAMGPU_E_ARG, "precision must be 4 or 8"));
+  if (c.idelt <= 0 || c.idelpro <= 0) return bail(fail(ctx, WAMGPU_E_ARG, "time steps must be positive"));
+  if (c.refraction_c_run && !c.refraction_d_run && c.shallow_run)
+    return bail(fail(ctx, WAMGPU_E_ARG, "current refraction requires depth refraction (SET_MODEL_OPTION)"));
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) return bail(fail(ctx, WAMGPU_E_CUDA, "no CUDA device: libwamgpu has no CPU path"));
+  if (c.device < 0 || c.device >= ndev) return bail(fail(ctx, WAMGPU_E_ARG, "device ordinal out of range"));
+  if ((e = cudaSetDevice(c.device)) != cudaSuccess) return bail(cuda_fail(ctx, e, "cudaSetDevice"));
+  if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(cuda_fail(ctx, e, "stream"));
+  cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, c.device);
+  int rc;
+  if (c.precision == 8) { auto* I = new Impl<double>(); ctx->impl.reset(I); rc = build_tables<double>(ctx, *I); }
+  else { auto* I = new Impl<float>(); ctx->impl.reset(I); rc = build_tables<float>(ctx, *I); }
+  if (rc) return bail(rc);
+  *out = ctx;
+  return WAMGPU_OK;
+}
+
+int wamgpu_destroy(wamgpu_ctx* ctx) {
+  if (!ctx) return WAMGPU_OK;
+  if (ctx->stream) { cudaSetDevice(ctx->cfg.device); cudaStreamSynchronize(ctx->stream); }
+  ctx->impl.reset();
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return WAMGPU_OK;
+}
+
+const char* wamgpu_last_error(const wamgpu_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int wamgpu_get_table(const wamgpu_ctx* ctx, const char* name, float* fout, int* iout) {
+  if (!ctx || !name || !ctx->impl) return WAMGPU_E_ARG;
+  std::string n(name);
+  if (ctx->cfg.precision == 8) return get_table_t<double>(ctx, *static_cast<Impl<double>*>(ctx->impl.get()), n, fout, iout);
+  return get_table_t<float>(ctx, *static_cast<Impl<float>*>(ctx->impl.get()), n, fout, iout);
+}
+
+int wamgpu_host_table(const wamgpu_config* cfg, const char* name, float* fout, int* iout) {
+  if (!cfg || !name) return WAMGPU_E_ARG;
+  if (cfg->kl < 4 || cfg->kl > MAX_KL || cfg->ml < 4 || cfg->ml > MAX_ML) return WAMGPU_E_ARG;
+  wamgpu_ctx tmp;
+  tmp.cfg = *cfg;
+  std::string n(name);
+  if (cfg->precision == 8) {
+    Impl<double> I; I.tab.build(*cfg);
+    return get_table_t<double>(&tmp, I, n, fout, iout);
+  }
+  Impl<float> I; I.tab.build(*cfg);
+  return get_table_t<float>(&tmp, I, n, fout, iout);
+}
+
+int wamgpu_set_grid(wamgpu_ctx* ctx, int nsea, const int* klat, const int* klon, const float* wlat, const int* kfromij,
+                    int ny, const float* sinph, const float* cosph, const float* dellam) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (nsea < 0 || ny <= 0 || (nsea > 0 && (!klat || !klon || !wlat || !kfromij)) || !sinph || !cosph || !dellam)
+    return fail(ctx, WAMGPU_E_ARG, "invalid grid arguments");
+  for (int i = 0; i < 4 * nsea; ++i) if (klat[i] < 0 || klat[i] > nsea) return fail(ctx, WAMGPU_E_ARG, "KLAT index out of range");
+  for (int i = 0; i < 2 * nsea; ++i) if (klon[i] < 0 || klon[i] > nsea) return fail(ctx, WAMGPU_E_ARG, "KLON index out of range");
+  for (int i = 0; i < nsea; ++i) if (kfromij[i] < 1 || kfromij[i] > ny) return fail(ctx, WAMGPU_E_ARG, "KFROMIJ out of range");
+  ctx->nsea = nsea; ctx->ny = ny; ctx->n_ext = nsea;
+  ctx->klat.assign(klat, klat + 4 * (size_t)nsea); ctx->klon.assign(klon, klon + 2 * (size_t)nsea);
+  ctx->wlat.assign(wlat, wlat + 2 * (size_t)nsea); ctx->kfromij.assign(kfromij, kfromij + nsea);
+  ctx->sinph.assign(sinph, sinph + ny); ctx->cosph.assign(cosph, cosph + ny); ctx->dellam.assign(dellam, dellam + ny);
+  ctx->depth.assign(nsea, 999.0f); ctx->u.assign(nsea, 0.f); ctx->v.assign(nsea, 0.f);
+  ctx->have_grid = true; ctx->prepared = false;
+  cudaSetDevice(ctx->cfg.device);
+  return DISPATCH_CTX(ctx, set_grid_t);
+}
+
+int wamgpu_set_depth(wamgpu_ctx* ctx, const float* depth) {
+  if (!ctx || !ctx->have_grid || !depth) return ctx ? fail(ctx, WAMGPU_E_STATE, "set_grid first") : WAMGPU_E_ARG;
+  for (int i = 0; i < ctx->nsea; ++i)
+    if (!(depth[i] > 0.f) || !std::isfinite(depth[i])) return fail(ctx, WAMGPU_E_ARG, "depth must be positive and finite");
+  ctx->depth.assign(depth, depth + ctx->nsea);
+  ctx->prepared = false;
+  return WAMGPU_OK;
+}
+
+int wamgpu_set_current(wamgpu_ctx* ctx, const float* u, const float* v) {
+  if (!ctx || !ctx->have_grid) return ctx ? fail(ctx, WAMGPU_E_STATE, "set_grid first") : WAMGPU_E_ARG;
+  if (u) ctx->u.assign(u, u + ctx->nsea); else ctx->u.assign(ctx->nsea, 0.f);
+  if (v) ctx->v.assign(v, v + ctx->nsea); else ctx->v.assign(ctx->nsea, 0.f);
+  ctx->prepared = false;
+  return WAMGPU_OK;
+}
+
+int wamgpu_prepare_propagation(wamgpu_ctx* ctx, float* total_cfl, int* counter) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!ctx->have_grid) return fail(ctx, WAMGPU_E_STATE, "set_grid first");
+  cudaSetDevice(ctx->cfg.device);
+  return DISPATCH_CTX(ctx, prepare_prop, total_cfl, counter);
+}
+
+int wamgpu_prepare_source(wamgpu_ctx* ctx) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!ctx->have_grid) return fail(ctx, WAMGPU_E_STATE, "set_grid first");
+  cudaSetDevice(ctx->cfg.device);
+  return DISPATCH_CTX(ctx, prepare_source_t);
+}
+
+int wamgpu_get_indep(const wamgpu_ctx* ctx, int* indep) {
+  if (!ctx || !indep || !ctx->prepared) return WAMGPU_E_STATE;
+  std::memcpy(indep, ctx->indep.data(), ctx->indep.size() * sizeof(int));
+  return WAMGPU_OK;
+}
+
+int wamgpu_implsch_host(wamgpu_ctx* ctx, float* fl3, const float* u10, const float* udir, float* tauw, float* ustar,
+                        float* z0, const float* roairn, const float* wstar, const float* depth, const int* indep) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!fl3 || !u10 || !udir || !tauw || !ustar || !z0 || !roairn || !wstar) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  cudaSetDevice(ctx->cfg.device);
+  return DISPATCH_CTX(ctx, implsch_host_t, fl3, u10, udir, tauw, ustar, z0, roairn, wstar, depth, indep);
+}
+
+int wamgpu_propags_host(wamgpu_ctx* ctx, float* f3) {
+  if (!ctx || !ctx->impl || !f3) return WAMGPU_E_ARG;
+  cudaSetDevice(ctx->cfg.device);
+  return DISPATCH_CTX(ctx, propags_host_t, f3);
+}
+
+int wamgpu_implsch_dev(wamgpu_ctx* ctx, void* fl3, int ld, const void* u10, const void* udir, void* tauw, void* ustar,
+                       void* z0, const void* roairn, const void* wstar, void* stream) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!fl3 || !u10 || !udir || !tauw || !ustar || !z0 || !roairn || !wstar) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, implsch_dev_t, fl3, ld, u10, udir, tauw, ustar, z0, roairn, wstar, s);
+}
+
+int wamgpu_propags_dev(wamgpu_ctx* ctx, void* f3, int ld, void* scratch, void* stream) {
+  if (!ctx || !ctx->impl || !f3) return WAMGPU_E_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, propags_dev_t, f3, ld, scratch, s);
+}
+
+int wamgpu_get_fluxes(wamgpu_ctx* ctx, float* out7) {
+  if (!ctx || !ctx->impl || !out7) return WAMGPU_E_ARG;
+  if (!ctx->cfg.lcflx) return fail(ctx, WAMGPU_E_STATE, "LCFLX is off");
+  size_t n = (size_t)7 * ctx->nsea;
+  cudaSetDevice(ctx->cfg.device);
+  if (ctx->cfg.precision == 8) {
+    auto* I = static_cast<Impl<double>*>(ctx->impl.get());
+    std::vector<double> t(n);
+    CK(cudaMemcpyAsync(t.data(), I->fluxes.p, n * 8, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+    for (size_t i = 0; i < n; ++i) out7[i] = (float)t[i];
+  } else {
+    auto* I = static_cast<Impl<float>*>(ctx->impl.get());
+    CK(cudaMemcpyAsync(out7, I->fluxes.p, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
+    CK(cudaStreamSynchronize(ctx->stream), "sync");
+  }
+  return WAMGPU_OK;
+}
+
+int wamgpu_sync(wamgpu_ctx* ctx) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  cudaSetDevice(ctx->cfg.device);
+  CK(cudaStreamSynchronize(ctx->stream), "sync");
+  DevBuf* st = ctx->cfg.precision == 8 ? &static_cast<Impl<double>*>(ctx->impl.get())->status
+                                       : &static_cast<Impl<float>*>(ctx->impl.get())->status;
+  if (st->p) {
+    int flag = 0;
+    CK(cudaMemcpy(&flag, st->p, sizeof(int), cudaMemcpyDeviceToHost), "status");
+    if (flag) {
+      CK(cudaMemset(st->p, 0, sizeof(int)), "status");
+      return fail(ctx, WAMGPU_E_NUMERIC, "non-finite values in IMPLSCH output");
+    }
+  }
+  return WAMGPU_OK;
+}
+
+}  // extern "C"

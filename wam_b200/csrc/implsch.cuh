@@ -1,0 +1,814 @@
+// IMPLSCH on sm_100a: one warp integrates one sea point.  A CTA stages the
+// spectra of P consecutive sea points (32-byte sectors of the FL3(IJ,K,M)
+// layout) into shared memory together with the static tables, and each warp
+// then runs the reference's per-point statement sequence with its 32 lanes
+// spread over directions, frequencies or spectral bins; spectral integrals
+// and stresses are warp-shuffle reductions.  The DIA runs quadruplet by
+// quadruplet with lanes over directions: for fixed (MC,KH) the nine target
+// bins of different lanes are distinct (K1W..K21W are rotations), so each
+// target update is one conflict-free shared-memory step followed by
+// __syncwarp.
+//
+// Routine map (myWAveModel/WAM wam_source_module.f90 unless noted):
+//   IMPLSCH :374-700        implsch_point
+//   SINPUT_ARD :2312-2738   sinput_ard        SINPUT_ST6 :4704-4925   sinput_st6
+//   LFACTOR :4465-4700      st6_lfactor       TAU_WAVE_ATMOS :5258    st6_taunw
+//   SDISSIP_ARD :1704-1962  sdissip_ard       SDISSIP_ST6 :4929-5102  sdissip_st6
+//   W3SWL6 :5106-5252       w3swl6            SNONLIN :2742-3047      snonlin
+//   STRESSO :3164-3356      stresso           TAU_PHI_HF :3853-3966   tau_phi_hf
+//   AIRSEA :868-971         airsea            W3FLX4 :5372-5443       w3flx4
+//   WSIGSTAR :4250-4339     wsigstar          WAVNU2 :4343-4461       wavnu2
+//   FRCUTINDEX :3569, FRCUTINDEX_ST6 :5447    IMPHFTAIL :3651-3731
+//   SBOTTOM :1527-1589      WNFLUXES :3970-4054
+//   TOTAL_ENERGY/FEMEAN/WM1 wam_interface_module.f90:1342,207,1591
+#pragma once
+#include <cstdint>
+#include <cfloat>
+#include "wamgpu_config.hpp"
+#include "spectral_tables.hpp"
+#include "devmath.cuh"
+
+namespace wamgpu {
+
+// Shared-memory view of the small tables.
+template <typename R> struct STabs {
+  const R *FR, *DF, *DFIM, *DFIMOFR, *FR5, *FRM5, *RHOWG, *TH, *COSTH, *SINTH, *DELFL, *AF11, *RNL, *SATW, *WTAUHF, *SWELLFT;
+  const int *K1W, *K2W, *K11W, *K21W, *INL, *IKP, *IKP1, *IKM, *IKM1, *INDSAT;
+  __device__ void bind(const R* r, const int* i, const SmallLayout& L) {
+    FR = r + L.FR; DF = r + L.DF; DFIM = r + L.DFIM; DFIMOFR = r + L.DFIMOFR; FR5 = r + L.FR5; FRM5 = r + L.FRM5;
+    RHOWG = r + L.RHOWG_DFIM; TH = r + L.TH; COSTH = r + L.COSTH; SINTH = r + L.SINTH; DELFL = r + L.DELFL;
+    AF11 = r + L.AF11; RNL = r + L.RNLCOEF; SATW = r + L.SATW; WTAUHF = r + L.WTAUHF; SWELLFT = r + L.SWELLFT;
+    K1W = i + L.K1W; K2W = i + L.K2W; K11W = i + L.K11W; K21W = i + L.K21W; INL = i + L.INLCOEF;
+    IKP = i + L.IKP; IKP1 = i + L.IKP1; IKM = i + L.IKM; IKM1 = i + L.IKM1; INDSAT = i + L.INDSAT;
+  }
+};
+
+// Per-warp (per sea point) shared-memory workspace.
+template <typename R> struct WarpWS {
+  R *F, *SL, *FL, *SP;  // spectrum, source, diagonal derivative, positive input (later SMIN)
+  R* T;                 // 8 x SCR per-frequency / per-direction scratch
+  uint8_t* LL;          // LLWS mask
+  __device__ R* t(int i) const { return T + i * SCR; }
+};
+
+template <typename R> __host__ __device__ inline size_t warp_ws_bytes(int NS) {
+  size_t b = (size_t)(4 * NS + 8 * SCR) * sizeof(R) + (size_t)NS;
+  return (b + 15) & ~size_t(15);
+}
+
+// Per-point outputs of IMPLSCH beyond the spectrum.
+template <typename R> struct PointState {
+  R TAUW, USTAR, Z0;
+  R flx[7];  // PHIOC, TAUOC_X, TAUOC_Y, PHIBOT, TAUBOT_X, TAUBOT_Y, PHIAW
+};
+
+template <typename R> struct Src {
+  using P_ = Phys<R>;
+  const DevTables<R>& T;
+  const STabs<R>& S;
+  WarpWS<R>& w;
+  const int lane, ij, INDEP;
+  const R U10, UDIR, ROAIRN, WSTAR, DEPTH;
+  __device__ Src(const DevTables<R>& t, const STabs<R>& s, WarpWS<R>& ws, int l, int ij_, int indep, R u10, R udir,
+                 R roairn, R wstar, R depth)
+      : T(t), S(s), w(ws), lane(l), ij(ij_), INDEP(indep), U10(u10), UDIR(udir), ROAIRN(roairn), WSTAR(wstar), DEPTH(depth) {}
+
+  __device__ int KL() const { return T.KL; }
+  __device__ int ML() const { return T.ML; }
+  __device__ R tfak(int m) const { return __ldg(&T.TFAK[(INDEP - 1) + T.NDEPTH * m]); }
+  __device__ R tcgond(int m) const { return __ldg(&T.TCGOND[(INDEP - 1) + T.NDEPTH * m]); }
+
+  // TOTAL_ENERGY + FEMEAN (+ WM1 for AKMEAN); masked when mask != null.
+  __device__ void integrals(const uint8_t* mask, R& emean, R& fmean, R* akmean) const {
+    const int kl = KL(), ml = ML();
+    R pe = 0, pf = 0, pa = 0, tail = 0;
+    const R DEL2 = dsqrt(P_::G) / P_::ZPI;
+    for (int m = lane; m < ml; m += 32) {
+      R t = 0;
+      const R* f = w.F + kl * m;
+      if (mask) { const uint8_t* mk = mask + kl * m; for (int k = 0; k < kl; ++k) if (mk[k]) t = t + f[k]; }
+      else for (int k = 0; k < kl; ++k) t = t + f[k];
+      pe = pe + t * S.DFIM[m];
+      pf = pf + t * S.DFIMOFR[m];
+      if (akmean) pa = pa + (T.shallow ? t / dsqrt(tfak(m)) * S.DFIM[m] : t * S.DFIMOFR[m] * DEL2);
+      if (m == ml - 1) tail = t;
+    }
+    pe = warp_sum(pe); pf = warp_sum(pf);
+    tail = __shfl_sync(0xffffffffu, tail, (ml - 1) & 31);
+    emean = dmax(T.MO_TAIL * tail + pe, R(1.0E-12));
+    fmean = emean / dmax(T.MM1_TAIL * tail + pf, R(1.0E-12));
+    if (akmean) {
+      pa = warp_sum(pa);
+      R wm = T.MM1_TAIL * DEL2 * tail + pa;
+      *akmean = (emean > R(1.0E-12)) ? (emean / wm) * (emean / wm) : R(1.);
+    }
+  }
+
+  // AIRSEA: u* and z0 from U10 and the wave stress (15 Newton steps).
+  __device__ void airsea(R TAUW, R& USTAR, R& Z0) const {
+    const R EPS1 = R(0.00001);
+    R xlogxl = dlog(P_::XNLEV), alphaog = T.ALPHA / P_::G, xkutop = P_::XKAPPA * U10;
+    R ustold = U10 * dsqrt(R(8.0E-4) + R(8.0E-5) * U10);
+    R tauold = dmax(ustold * ustold, TAUW + EPS1);
+    USTAR = dsqrt(tauold);
+    R ustm1 = R(1.0) / dmax(USTAR, R(1.0E-6));
+    R z0ch = 0;
+    for (int it = 0; it < 15; ++it) {
+      R x = TAUW / tauold;
+      z0ch = alphaog * tauold / dsqrt(dmax(R(1.0) - x, EPS1));
+      R z0vis = P_::RNUAIRM * ustm1, z0tot = z0ch + z0vis;
+      R xologz0 = R(1.0) / (xlogxl - dlog(z0tot));
+      R f = USTAR - xkutop * xologz0;
+      R zz = ustm1 * (z0ch * (R(2.0) - R(3.0) * x) / (R(1.0) - x) - z0vis) / z0tot;
+      R delf = R(1.0) - xkutop * (xologz0 * xologz0) * zz;
+      USTAR = USTAR - f / delf;
+      R taunew = dmax(USTAR * USTAR, TAUW + EPS1);
+      USTAR = dsqrt(taunew);
+      if (taunew == tauold) break;
+      ustm1 = R(1.0) / dmax(USTAR, R(1.0E-6));
+      tauold = taunew;
+    }
+    Z0 = z0ch;
+  }
+
+  __device__ void w3flx4(R& UST, R& Z0) const {
+    R cd;
+    if (U10 >= R(50.33)) { UST = R(2.026) * dsqrt(T.CDFAC); cd = (UST / U10) * (UST / U10); }
+    else { cd = T.CDFAC * (R(8.058) + R(0.967) * U10 - R(0.016) * (U10 * U10)) * R(1E-4); UST = U10 * dsqrt(cd); }
+    Z0 = P_::XNLEV * dexp(-R(0.4) / dsqrt(cd));
+  }
+
+  __device__ R wsigstar(R ustar, R z0) const {
+    const R C1 = R(1.03E-3), C2 = R(0.04E-3), P1 = R(1.48), P2 = R(-0.21);
+    R u = ustar * (R(1.0) / P_::XKAPPA) * (dlog(R(10.0)) - dlog(z0));
+    u = dmax(u, R(1.0));
+    R um1 = R(1.0) / u, c2u = C2 * dpow(u, P1), up2 = dpow(u, P2);
+    R cdv = (C1 + c2u) * up2;
+    R dcd = (P2 * C1 + (P1 + P2) * c2u) * up2 * um1;
+    R sconv = R(1.0) + R(0.5) * u / cdv * dcd;
+    return dmin(R(0.1), sconv * um1 * dpow(R(0.5) * P_::XKAPPA * (WSTAR * WSTAR * WSTAR), R(1.0) / R(3.0)));
+  }
+
+  // SINPUT_ARD: writes SL, SP(=SPOS), FL, LL; sequential over frequency because
+  // of sheltering (XSTRESS/YSTRESS of lower frequencies feed the next one).
+  __device__ void sinput_ard(R USTAR, R Z0) const {
+    const int kl = KL(), ml = ML();
+    const R SWELLF = R(0.66), FU = R(0.022), FUD = R(-0.018), SWELLF4 = R(1.5E05), SWELLF5 = R(1.2), SWELLF7 = R(3.6E05);
+    const R rog = P_::ROWATER * P_::G;
+    const R const1 = T.BETAMAX / (P_::XKAPPA * P_::XKAPPA) / P_::ROWATER;
+    const R nu = P_::RNUAIR;
+    const R delabm1 = R(200) / (R(8.0) - R(0.3));
+    const R shelter = dabs(T.TAUWSHELTER);
+    R sig_n = wsigstar(USTAR, Z0);
+    R uo = 0, ao = 0;
+    for (int m = lane; m < ml; m += 32) {
+      R t = 0;
+      for (int k = 0; k < kl; ++k) t = t + w.F[k + kl * m];
+      R sig = P_::ZPI * S.FR[m];
+      uo = uo + S.DFIM[m] * (sig * sig) * t;
+      ao = ao + S.DFIM[m] * t;
+    }
+    R tiny = sizeof(R) == 4 ? R(FLT_MIN) : R(DBL_MIN);
+    R uorbt = R(2.0) * dsqrt(tiny + warp_sum(uo));
+    R aorb = R(2.0) * dsqrt(tiny + warp_sum(ao));
+    R re = (R(4.0) / nu) * uorbt * aorb;
+    R z0noz = dmax(P_::RNUAIRM / dmax(USTAR, R(0.0001)), R(0.04) * dmin(R(0.0005), Z0));
+    R xi = (dlog10(dmax(aorb / z0noz, R(3.0))) - R(0.3)) * delabm1;
+    int ind = min(199, max(1, (int)xi));  // xi >= 4.6 for finite input; clamp keeps NaN input in bounds
+    R deli1 = dmin(R(1.0), xi - R(ind));
+    R fww = S.SWELLFT[ind - 1] * (R(1.0) - deli1) + S.SWELLFT[ind] * deli1;
+    R temp2 = fww * uorbt;
+    R smooth = R(0.5) * dtanh((re - SWELLF4) / SWELLF7);
+    R pturb = R(0.5) + smooth, pvisc = R(0.5) - smooth;
+    R usg[2] = {(USTAR * (R(1.0) + sig_n)) * (USTAR * (R(1.0) + sig_n)), (USTAR * (R(1.0) - sig_n)) * (USTAR * (R(1.0) - sig_n))};
+    R su = dsin(UDIR), cu = dcos(UDIR);
+    R taux[2] = {usg[0] * su, usg[1] * su}, tauy[2] = {usg[0] * cu, usg[1] * cu};
+    R xst[2] = {0, 0}, yst[2] = {0, 0};
+    R rogoroair = rog / dmax(ROAIRN, R(1.0)), roairn_pvisc = ROAIRN * pvisc;
+    for (int m = 0; m < ml; ++m) {
+      R sig = P_::ZPI * S.FR[m], sig2 = sig * sig;
+      R xk, cm;
+      if (T.shallow) { xk = tfak(m); cm = xk * (R(1.0) / sig); }
+      else { cm = sig / P_::G; xk = sig2 / P_::G; }
+      R ustp[2], usdirp[2], ucn[2], ucnz[2];
+      for (int g = 0; g < 2; ++g) {
+        R tpx = taux[g] - shelter * xst[g], tpy = tauy[g] - shelter * yst[g];
+        ustp[g] = dpow(tpx * tpx + tpy * tpy, R(0.25));
+        usdirp[g] = datan2(tpx, tpy);
+        ucn[g] = ustp[g] * cm;
+        ucnz[g] = P_::XKAPPA / (ucn[g] + T.ZALP);
+      }
+      R constf = rogoroair * cm * S.DFIM[m];
+      R zcn = dlog(xk * Z0);
+      R cnsn = (sig * const1) * ROAIRN;
+      R coef = -(SWELLF * R(16.) * sig2 / (P_::G * P_::ROWATER));
+      R coef5 = -(SWELLF5 * R(2.) * dsqrt(R(2.) * nu * sig) / P_::ROWATER);
+      R dstab1 = coef5 * roairn_pvisc * xk, tmp1 = coef * ROAIRN;
+      R px[2] = {0, 0}, py[2] = {0, 0};
+      for (int k = lane; k < kl; k += 32) {
+        R f = w.F[k + kl * m];
+        R slp[2], flp[2];
+        uint8_t ll = 0;
+        for (int g = 0; g < 2; ++g) {
+          R c = dcos(S.TH[k] - usdirp[g]);
+          R ufac = 0;
+          if (c > R(0.01)) {
+            R x = c * ucn[g], zlog = zcn + ucnz[g] / c;
+            if (zlog < R(0.0)) { R z2x = zlog * zlog * x; ufac = dexp(zlog) * z2x * z2x; ll = 1; }
+          }
+          R dstab = dstab1 + pturb * (tmp1 * (temp2 + (FU + FUD * c) * ustp[g]));
+          slp[g] = cnsn * ufac;
+          flp[g] = slp[g] + dstab;
+          slp[g] = slp[g] * f;
+          px[g] = px[g] + slp[g] * (constf * S.SINTH[k]);
+          py[g] = py[g] + slp[g] * (constf * S.COSTH[k]);
+        }
+        int b = k + kl * m;
+        w.SP[b] = R(0.5) * (slp[0] + slp[1]);
+        R fl = R(0.5) * (flp[0] + flp[1]);
+        w.FL[b] = fl;
+        w.SL[b] = fl * f;
+        w.LL[b] = ll;
+      }
+      for (int g = 0; g < 2; ++g) { xst[g] = xst[g] + warp_sum(px[g]); yst[g] = yst[g] + warp_sum(py[g]); }
+    }
+    __syncwarp();
+  }
+
+  // STRESSO with TAU_PHI_HF: wave stress TAUW and energy flux PHIAW.
+  __device__ void tau_phi_hf(int mij, R ustar, R z0, R& tauhf, R& phihf) const {
+    const R gm1 = R(1.0) / P_::G;
+    R omegac = P_::ZPI * S.FR[mij - 1];
+    R tauw = ustar * ustar, ust = ustar;
+    R xloggz0 = dlog(P_::G * z0);
+    R omegacc = dmax(omegac, T.X0TAUHF * P_::G / ustar);
+    R sqrtz0og = dsqrt(z0 * gm1), sqrtgz0 = R(1.0) / sqrtz0og;
+    R zinf = dlog(omegacc * sqrtz0og);
+    R delz = dmax((R(0.0) - zinf) / R(18), R(0.0));
+    tauhf = 0; phihf = 0;
+    for (int j = 0; j < 19; ++j) {
+      R y = dexp(zinf + R(j) * delz);
+      R cm1 = y * sqrtgz0 * gm1;
+      R zlog = dmin(xloggz0 + R(2.0) * dlog(cm1) + P_::XKAPPA / (ust * cm1 + T.ZALP), R(0.0));
+      R z2 = zlog * zlog;
+      R fnc2 = dexp(zlog) * (z2 * z2) * tauw * S.WTAUHF[j] * delz;
+      ust = dsqrt(tauw);
+      tauhf = tauhf + fnc2;
+      phihf = phihf + fnc2 / y;
+    }
+    phihf = sqrtz0og * phihf;
+  }
+
+  __device__ void stresso(R USTAR, R Z0, int mij, R& TAUW, R& PHIAW) const {
+    const int kl = KL(), ml = ML();
+    const R gm1 = R(1.0) / P_::G;
+    const R cst = T.DELTH * ((P_::ZPI * P_::ZPI) * (P_::ZPI * P_::ZPI)) * gm1;
+    R pphi = 0, px = 0, py = 0;
+    const int nb = kl * mij;
+    for (int b = lane; b < nb; b += 32) {
+      int m = b / kl, k = b - m * kl;
+      R rw = S.RHOWG[m];
+      if (m == mij - 1 && mij != ml) rw = R(0.5) * rw;
+      R cm = T.shallow ? tfak(m) * (R(1.0) / (P_::ZPI * S.FR[m])) : (P_::ZPI * S.FR[m]) * gm1;
+      R sp = dmax(w.SP[b], R(0.));
+      pphi = pphi + sp * rw;
+      R cmr = cm * rw;
+      px = px + (sp * S.SINTH[k]) * cmr;
+      py = py + (sp * S.COSTH[k]) * cmr;
+    }
+    R t1 = 0, t2 = 0;
+    for (int k = lane; k < kl; k += 32) {
+      R cw = dmax(dcos(S.TH[k] - UDIR), R(0.));
+      R f = w.F[k + kl * (mij - 1)];
+      t2 = t2 + f * (cw * cw);
+      t1 = t1 + f * (cw * cw * cw);
+    }
+    pphi = warp_sum(pphi); px = warp_sum(px); py = warp_sum(py); t1 = warp_sum(t1); t2 = warp_sum(t2);
+    R tau1, phi1;
+    tau_phi_hf(mij, USTAR, Z0, tau1, phi1);
+    R tauhf = cst * S.FR5[mij - 1] * gm1 * t1 * tau1;
+    R phihf = P_::ROAIR * cst * S.FR5[mij - 1] * t2 * phi1;
+    PHIAW = pphi + phihf;
+    R xs = px / P_::ROAIR + tauhf * dsin(UDIR);
+    R ys = py / P_::ROAIR + tauhf * dcos(UDIR);
+    R tw = dsqrt(xs * xs + ys * ys);
+    tw = dmin(tw, USTAR * USTAR - R(0.00001));
+    TAUW = dmax(tw, R(0.));
+  }
+
+  __device__ int frcutindex(R fm, R fmws, R ustar) const {
+    R fpmh = R(2.5) / S.FR[0];
+    R fppm = R(3.0) * P_::G / (R(28.0) * P_::ZPI * S.FR[0]);
+    R fpm4 = dmax(dmax(fmws, fm) * fpmh, fppm / dmax(ustar, R(1.0E-6)));
+    int mij = (int)lround((double)(dlog10(fpm4) * T.INV_LOG_CO)) + 1;
+    return min(max(1, mij), ML());
+  }
+  __device__ int frcutindex_st6(R fmean, R ustar) const {
+    const int nk = ML();
+    R fxfm = R(6.) * P_::ZPI, fxpm = R(4.0) * P_::G / R(28.);
+    R signk = P_::ZPI * S.FR[nk - 1];
+    R facti1 = R(1.) / dlog(P_::CO), facti2 = R(1.) - dlog(P_::ZPI * S.FR[0]) * facti1;
+    R fhigh = dmax(fxfm * fmean, fxpm / ustar);
+    int nkh = min(nk, (int)(facti2 + facti1 * dlog(dmax(R(1.E-7), fhigh))));
+    int nkh1 = min(nk, nkh + 1);
+    fhigh = dmin(signk, fhigh);
+    return max(2, min(nkh1, (int)(facti2 + facti1 * dlog(dmax(R(1.E-7), fhigh)))));
+  }
+
+  // IMPHFTAIL: diagnostic tail above MIJ.
+  __device__ void imphftail(int mij) const {
+    const int kl = KL(), ml = ML();
+    R* t = w.t(7);
+    for (int m = mij - 1 + lane; m < ml; m += 32) {
+      if (T.shallow) { R akm1 = R(1.) / tfak(m); t[m] = (akm1 * akm1 * akm1) / tcgond(m); }
+      else t[m] = S.FRM5[m];
+    }
+    __syncwarp();
+    const R base = t[mij - 1];
+    const int nb = kl * (ml - mij);
+    for (int i = lane; i < nb; i += 32) {
+      int m = mij + i / kl, k = i - (m - mij) * kl;
+      w.F[k + kl * m] = (t[m] / base) * w.F[k + kl * (mij - 1)];
+    }
+    __syncwarp();
+  }
+
+  // SDISSIP_ARD: saturation-based whitecapping (SSDSC3 = SSDSC5 = 0).
+  __device__ void sdissip_ard() const {
+    const int kl = KL(), ml = ML(), nw = 2 * T.NSDSNTH + 1;
+    const R tmp03 = R(1.0) / R(9.0E-4), c6 = R(0.3), c6m1 = R(1.) - c6;
+    for (int m = 0; m < ml; ++m) {
+      R sig = P_::ZPI * S.FR[m], facsat;
+      if (T.shallow) { R xk = tfak(m); facsat = (xk * xk * xk) * (R(1.0) / P_::ZPI) * tcgond(m); }
+      else { R xk = sig * sig / P_::G; facsat = (xk * xk * xk) * (R(0.5) * (R(1.0) / P_::ZPI)) * P_::G / sig; }
+      R bth[2] = {0, 0}, bmax = 0;
+      for (int s = 0; s < 2; ++s) {
+        int k = lane + 32 * s;
+        if (k < kl) {
+          R acc = 0;
+          for (int j = 0; j < nw; ++j) acc = acc + S.SATW[k + kl * j] * w.F[(S.INDSAT[k + kl * j] - 1) + kl * m];
+          bth[s] = acc * facsat;
+          bmax = dmax(bmax, bth[s]);
+        }
+      }
+      bmax = warp_max(bmax);
+      R d0 = dmax(R(0.), bmax * tmp03 - R(1.0));
+      R temp1 = c6 * (d0 * d0);
+      R ssdsc2_sig = R(-2.2E-5) * sig;
+      for (int s = 0; s < 2; ++s) {
+        int k = lane + 32 * s;
+        if (k < kl) {
+          R dd = dmax(R(0.), bth[s] * tmp03 - R(1.0));
+          R d = ssdsc2_sig * (temp1 + c6m1 * (dd * dd));
+          int b = k + kl * m;
+          w.SL[b] = w.SL[b] + d * w.F[b];
+          w.FL[b] = w.FL[b] + d;
+        }
+      }
+    }
+    __syncwarp();
+  }
+
+  // SNONLIN (DIA) for ISNONLIN = 0 (depth scaling from AKMEAN) or the
+  // MAKE_SHALLOW_SNL table.
+  __device__ void snonlin(R AKMEAN) const {
+    const int kl = KL(), ml = ML();
+    R enhfr = R(1);
+    if (T.shallow && T.isnonlin == 0) {
+      enhfr = dmax(R(0.75) * DEPTH * AKMEAN, R(.5));
+      enhfr = R(1.) + (R(5.5) / enhfr) * (R(1.) - R(.833) * enhfr) * dexp(R(-1.25) * enhfr);
+    }
+    const int mfr1 = -T.MFRSTLW + 1, mfrl = ml - T.KFRH + mfr1;
+    R* SL = w.SL; R* FL = w.FL; const R* F = w.F;
+    for (int mc = 1; mc <= T.MLSTHG; ++mc) {
+      const int im = mc - T.MFRSTLW;
+      const int MP = S.IKP[im], MP1 = S.IKP1[im], MM = S.IKM[im], MM1 = S.IKM1[im];
+      const int* ic5 = S.INL + 5 * (mc - 1);
+      const int IC = ic5[0], IP = ic5[1], IP1 = ic5[2], IM = ic5[3], IM1 = ic5[4];
+      const R* rc = S.RNL + 25 * (mc - 1);
+      R ftemp = S.AF11[im];
+      if (T.shallow) ftemp = ftemp * (T.isnonlin == 0 ? enhfr : __ldg(&T.ENH[ij + (size_t)T.enh_ld * (mc - 1)]));
+      const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
+      const R ftail = (regime == 0) ? R(1) : rc[0];
+      for (int kh = 0; kh < 2; ++kh) {
+        R ad[2], delad[2], delap[2], delam[2];
+        int kk[2], k1[2], k2[2], k11[2], k21[2];
+        for (int s = 0; s < 2; ++s) {
+          int k = lane + 32 * s;
+          kk[s] = k;
+          if (k < kl) {
+            int sl = k + kl * kh;
+            k1[s] = S.K1W[sl] - 1; k2[s] = S.K2W[sl] - 1; k11[s] = S.K11W[sl] - 1; k21[s] = S.K21W[sl] - 1;
+            R sap = rc[1] * F[k1[s] + kl * (IP - 1)] + rc[2] * F[k11[s] + kl * (IP - 1)] + rc[3] * F[k1[s] + kl * (IP1 - 1)] +
+                    rc[4] * F[k11[s] + kl * (IP1 - 1)];
+            R sam = rc[13] * F[k2[s] + kl * (IM - 1)] + rc[14] * F[k21[s] + kl * (IM - 1)] + rc[15] * F[k2[s] + kl * (IM1 - 1)] +
+                    rc[16] * F[k21[s] + kl * (IM1 - 1)];
+            R fij = F[k + kl * (IC - 1)] * ftail;
+            R fad1 = fij * (sap + sam);
+            R fad2 = fad1 - R(2.) * sap * sam;
+            fad1 = fad1 + fad2;
+            R fcen = ftemp * fij;
+            ad[s] = fad2 * fcen;
+            delad[s] = fad1 * ftemp;
+            delap[s] = (fij - R(2.) * sam) * T.DAL1 * fcen;
+            delam[s] = (fij - R(2.) * sap) * T.DAL2 * fcen;
+          }
+        }
+        // one target per step: within a step lanes hit distinct bins
+#define DIA_UPD(KIDX, MROW, SLV, FLV)                                     \
+  {                                                                       \
+    for (int s = 0; s < 2; ++s)                                           \
+      if (kk[s] < kl) {                                                   \
+        int b = (KIDX) + kl * ((MROW) - 1);                               \
+        SL[b] = SL[b] + (SLV);                                            \
+        FL[b] = FL[b] + (FLV);                                            \
+      }                                                                   \
+    __syncwarp();                                                         \
+  }
+        if (regime == 0) {
+          DIA_UPD(kk[s], mc, -R(2.) * ad[s], -R(2.) * delad[s]);
+          DIA_UPD(k2[s], MM, ad[s] * rc[20], delam[s] * rc[23]);
+          DIA_UPD(k21[s], MM, ad[s] * rc[19], delam[s] * rc[24]);
+          DIA_UPD(k2[s], MM1, ad[s] * rc[17], delam[s] * rc[21]);
+          DIA_UPD(k21[s], MM1, ad[s] * rc[18], delam[s] * rc[22]);
+          DIA_UPD(k1[s], MP, ad[s] * rc[8], delap[s] * rc[11]);
+          DIA_UPD(k11[s], MP, ad[s] * rc[7], delap[s] * rc[12]);
+          DIA_UPD(k1[s], MP1, ad[s] * rc[5], delap[s] * rc[9]);
+          DIA_UPD(k11[s], MP1, ad[s] * rc[6], delap[s] * rc[10]);
+        } else if (regime == 1) {
+          DIA_UPD(k2[s], MM, ad[s] * rc[20], delam[s] * rc[23]);
+          DIA_UPD(k21[s], MM, ad[s] * rc[19], delam[s] * rc[24]);
+          if (MM1 <= ml) {
+            DIA_UPD(k2[s], MM1, ad[s] * rc[17], delam[s] * rc[21]);
+            DIA_UPD(k21[s], MM1, ad[s] * rc[18], delam[s] * rc[22]);
+            if (mc <= ml) {
+              DIA_UPD(kk[s], mc, -R(2.) * ad[s], -R(2.) * delad[s]);
+              if (MP <= ml) {
+                DIA_UPD(k1[s], MP, ad[s] * rc[8], delap[s] * rc[11]);
+                DIA_UPD(k11[s], MP, ad[s] * rc[7], delap[s] * rc[12]);
+                if (MP1 <= ml) {
+                  DIA_UPD(k1[s], MP1, ad[s] * rc[5], delap[s] * rc[9]);
+                  DIA_UPD(k11[s], MP1, ad[s] * rc[6], delap[s] * rc[10]);
+                }
+              }
+            }
+          }
+        } else {
+          if (MM1 >= 1) {
+            DIA_UPD(k2[s], MM1, ad[s] * rc[17], delam[s] * rc[21]);
+            DIA_UPD(k21[s], MM1, ad[s] * rc[18], delam[s] * rc[22]);
+          }
+          DIA_UPD(kk[s], mc, -R(2.) * ad[s], -R(2.) * delad[s]);
+          DIA_UPD(k1[s], MP, ad[s] * rc[8], delap[s] * rc[11]);
+          DIA_UPD(k11[s], MP, ad[s] * rc[7], delap[s] * rc[12]);
+          DIA_UPD(k1[s], MP1, ad[s] * rc[5], delap[s] * rc[9]);
+          DIA_UPD(k11[s], MP1, ad[s] * rc[6], delap[s] * rc[10]);
+        }
+#undef DIA_UPD
+      }
+    }
+  }
+
+  // ---- ST6 ----------------------------------------------------------------
+  // WAVNU2: wave number and group velocity per frequency -> scratch 0, 1
+  __device__ void wavnu2() const {
+    R* WN = w.t(0); R* CG = w.t(1);
+    const R H = DEPTH, eps = R(1E-7);
+    for (int m = lane; m < ML(); m += 32) {
+      R w0 = dabs(P_::ZPI * S.FR[m]);
+      R k = (w0 < dsqrt(P_::G / H)) ? w0 / dsqrt(P_::G * H) : w0 * w0 / P_::G;
+      R kold = 0;
+      for (int i = 0; i < 15; ++i) {
+        R dif = dabs(k - kold), rdif = (k != R(0)) ? dif / k : R(0);
+        if (dif < eps && rdif < eps) break;
+        kold = k;
+        R th = dtanh(kold * H);
+        R f1 = P_::G * kold * th - w0 * w0;
+        R fd = (kold * H > R(25)) ? P_::G * th : P_::G * th + P_::G * kold * H / (dcosh(kold * H) * dcosh(kold * H));
+        k = kold - f1 / fd;
+      }
+      R cg = (R(2) * k * H > R(25)) ? w0 / k * R(0.5) : w0 / k * R(0.5) * (R(1) + (R(2) * k * H / dsinh(R(2) * k * H)));
+      WN[m] = k; CG[m] = cg;
+    }
+    __syncwarp();
+  }
+
+  // positive ST6 input growth rate D (before the stress reduction) of bin (k,m)
+  __device__ R st6_d1(int k, int m, R uproxy, R cu, R su, R sqrtbn, R& a, R& w2) const {
+    const R* WN = w.t(0); const R* CG = w.t(1);
+    R sig = P_::ZPI * S.FR[m];
+    a = w.F[k + KL() * m] * CG[m] / (P_::ZPI * sig);
+    R proj = uproxy * (WN[m] / sig) * (S.COSTH[k] * cu + S.SINTH[k] * su) - R(1.);
+    R w1 = dmax(R(0.), proj); w1 = w1 * w1;
+    R ww = dmin(R(0.), proj); w2 = ww * ww;
+    return (ROAIRN / P_::ROWATER) * sig * (R(2.8) - (R(1.) + dtanh(R(10.) * sqrtbn * w1 - R(11.)))) * sqrtbn * w1;
+  }
+  __device__ R st6_d2(int m, R sqrtbn, R w2) const {
+    R sig = P_::ZPI * S.FR[m];
+    return (ROAIRN / P_::ROWATER) * sig * R(0.09) * (R(2.8) - (R(1.) + dtanh(R(10.) * sqrtbn * w2 - R(11.)))) * sqrtbn * w2;
+  }
+
+  // directional integrals of the (positive or |negative|) stress spectrum,
+  // extended to 10 Hz: x in scratch 4, y in scratch 5, returns TAUWINDS parts
+  __device__ void st6_extend(R* sdx, R* sdy, R* cinv10, R* dsii10) const {
+    const int nk = ML(), nk10 = T.NK10;
+    const R* WN = w.t(0);
+    const R sig1 = P_::ZPI * S.FR[0];
+    for (int i = lane; i < nk10; i += 32) {
+      R sig10 = (nk < nk10) ? sig1 * dpow(P_::CO, R(i + 1) - R(1.0)) : P_::ZPI * S.FR[i];
+      R ci = (i < nk) ? WN[i] / (P_::ZPI * S.FR[i]) : sig10 * R(0.101978);
+      R ds;
+      if (nk < nk10) {
+        ds = R(0.5) * sig10 * (P_::CO - R(1.0) / P_::CO);
+        if (i == 0) ds = R(0.5) * sig10 * (P_::CO - R(1.0));
+        if (i == nk10 - 1) ds = R(0.5) * sig10 * (P_::CO - R(1.0)) / P_::CO;
+      } else ds = P_::ZPI * S.DF[i];
+      cinv10[i] = ci; dsii10[i] = ds;
+    }
+    __syncwarp();
+    if (nk < nk10) {
+      R signk = sig1 * dpow(P_::CO, R(nk) - R(1.0));
+      for (int i = nk + lane; i < nk10; i += 32) {
+        R sig10 = sig1 * dpow(P_::CO, R(i + 1) - R(1.0));
+        R r = (signk / sig10) * (signk / sig10);
+        sdx[i] = sdx[nk - 1] * r; sdy[i] = sdy[nk - 1] * r;
+      }
+    }
+    __syncwarp();
+  }
+
+  // SINPUT_ST6 with LFACTOR and TAU_WAVE_ATMOS; writes SL, SP, FL; TAUW out.
+  __device__ void sinput_st6(R USTAR, R& TAUW) const {
+    const int kl = KL(), nk = ML(), nk10 = T.NK10;
+    const R* CG = w.t(1);
+    R* SQB = w.t(2); R* LF = w.t(3); R* SDX = w.t(4); R* SDY = w.t(5); R* CI10 = w.t(6); R* DS10 = w.t(7);
+    const R cu = dcos(UDIR), su = dsin(UDIR), uproxy = R(32.) * USTAR;
+    // narrowness and saturation per frequency
+    for (int m = lane; m < nk; m += 32) {
+      R sig = P_::ZPI * S.FR[m];
+      R s = 0, mx = 0;
+      for (int k = 0; k < kl; ++k) {
+        R a = w.F[k + kl * m] * CG[m] / (P_::ZPI * sig);
+        s = s + a;
+        mx = (k == 0) ? a : dmax(mx, a);
+      }
+      R s2 = 0;
+      for (int k = 0; k < kl; ++k) {
+        R a = w.F[k + kl * m] * CG[m] / (P_::ZPI * sig);
+        s2 = s2 + ((mx < R(1.0E-34)) ? R(1.) : a / mx);
+      }
+      R adensig = s * sig * T.DELTH, anar = R(1.0) / (s2 * T.DELTH);
+      R wn = w.t(0)[m];
+      SQB[m] = dsqrt(anar * adensig * (wn * wn * wn));
+    }
+    __syncwarp();
+    // positive stress spectrum sums per frequency
+    for (int m = lane; m < nk; m += 32) {
+      R sig = P_::ZPI * S.FR[m], bx = 0, by = 0;
+      for (int k = 0; k < kl; ++k) {
+        R a, w2;
+        R d = st6_d1(k, m, uproxy, cu, su, SQB[m], a, w2);
+        R sd = d * a * sig / CG[m];
+        bx = bx + dmax(R(0.), sd) * S.COSTH[k];
+        by = by + dmax(R(0.), sd) * S.SINTH[k];
+      }
+      SDX[m] = bx * T.DELTH; SDY[m] = by * T.DELTH;
+    }
+    __syncwarp();
+    st6_extend(SDX, SDY, CI10, DS10);
+    // LFACTOR: iterate the high-frequency reduction until the total stress matches u*^2
+    const R gro = P_::G * P_::ROWATER;
+    R tau_tot = USTAR * USTAR * ROAIRN;
+    R tau_vis = dmax(R(0.0), -(R(5.0E-5) * U10) + R(1.1E-3)) * (U10 * U10) * ROAIRN;
+    tau_vis = dmin(R(0.95) * tau_tot, tau_vis);
+    R tvx = tau_vis * dcos(UDIR), tvy = tau_vis * dsin(UDIR);
+    R px = 0, py = 0;
+    for (int i = lane; i < nk10; i += 32) { px = px + SDX[i] * CI10[i] * DS10[i]; py = py + SDY[i] * CI10[i] * DS10[i]; }
+    R tauwx = gro * warp_sum(px), tauwy = gro * warp_sum(py);
+    R tau = dsqrt((tvx + tauwx) * (tvx + tauwx) + (tvy + tauwy) * (tvy + tauwy));
+    R err = (tau - tau_tot) / tau_tot;
+    for (int i = lane; i < nk10; i += 32) LF[i] = R(1.0);
+    if (tau > tau_tot) {
+      bool over = false;
+      R rtau = err / R(90.), drtau = R(2.0);
+      int sgn = (err >= R(0)) ? 1 : -1;
+      for (int it = 0; it < 80; ++it) {
+        px = 0; py = 0;
+        for (int i = lane; i < nk10; i += 32) {
+          R lf = dmin(R(1.0), dexp((R(1.0) - uproxy * CI10[i]) * rtau));
+          LF[i] = lf;
+          px = px + (SDX[i] * lf) * CI10[i] * DS10[i];
+          py = py + (SDY[i] * lf) * CI10[i] * DS10[i];
+        }
+        tauwx = gro * warp_sum(px); tauwy = gro * warp_sum(py);
+        tau = dsqrt((tvx + tauwx) * (tvx + tauwx) + (tvy + tauwy) * (tvy + tauwy));
+        err = (tau - tau_tot) / tau_tot;
+        int sold = sgn;
+        sgn = (err >= R(0)) ? 1 : -1;
+        if (sgn != sold) over = true;
+        if (over) drtau = dmax(R(0.5) * (R(1.0) + drtau), R(1.00010));
+        rtau = (sgn > 0) ? rtau * drtau : rtau * (R(1) / drtau);
+        if (dabs(err) < R(1.54E-4)) break;
+      }
+    }
+    __syncwarp();
+    R sumlf = 0;
+    for (int m = lane; m < nk; m += 32) sumlf = sumlf + LF[m];
+    const bool reduce = warp_sum(sumlf) < R(nk);
+    // negative input part: |min(0,S)| directional sums
+    for (int m = lane; m < nk; m += 32) {
+      R sig = P_::ZPI * S.FR[m], bx = 0, by = 0;
+      for (int k = 0; k < kl; ++k) {
+        R a, w2;
+        R d = st6_d1(k, m, uproxy, cu, su, SQB[m], a, w2);
+        if (reduce) d = d * LF[m];
+        d = d - st6_d2(m, SQB[m], w2);
+        R sd = d * a * sig / CG[m];
+        bx = bx + dabs(dmin(R(0.), sd)) * S.COSTH[k];
+        by = by + dabs(dmin(R(0.), sd)) * S.SINTH[k];
+      }
+      SDX[m] = bx * T.DELTH; SDY[m] = by * T.DELTH;
+    }
+    __syncwarp();
+    // LF entries above nk are not needed any more; reuse the extension
+    st6_extend(SDX, SDY, CI10, DS10);
+    px = 0; py = 0;
+    for (int i = lane; i < nk10; i += 32) { px = px + SDX[i] * CI10[i] * DS10[i]; py = py + SDY[i] * CI10[i] * DS10[i]; }
+    R tnx = gro * warp_sum(px), tny = gro * warp_sum(py);
+    (void)tnx; (void)tny;  // TAUNW is a diagnostic the driver does not read back
+    TAUW = dsqrt(tauwx * tauwx + tauwy * tauwy);
+    for (int b = lane; b < kl * nk; b += 32) {
+      int m = b / kl, k = b - m * kl;
+      R a, w2;
+      R d = st6_d1(k, m, uproxy, cu, su, SQB[m], a, w2);
+      if (reduce) d = d * LF[m];
+      R dpos = d;
+      R dtot = d - st6_d2(m, SQB[m], w2);
+      R f = w.F[b];
+      w.SL[b] = dtot * f;
+      w.SP[b] = dpos * f;
+      w.FL[b] = dtot;
+      w.LL[b] = (dpos * f > R(0));
+    }
+    __syncwarp();
+  }
+
+  // SDISSIP_ST6 (T1 + T2 breaking) followed by W3SWL6 (swell dissipation)
+  __device__ void sdissip_st6() const {
+    const int kl = KL(), nk = ML();
+    const R* WN = w.t(0); const R* CG = w.t(1);
+    R* ADF = w.t(2); R* T12 = w.t(3);
+    const R bnt = R(0.035) * R(0.035);
+    for (int m = lane; m < nk; m += 32) {
+      R et = (P_::ZPI * bnt) / (CG[m] * (WN[m] * WN[m] * WN[m]));
+      R s = 0;
+      for (int k = 0; k < kl; ++k) s = s + w.F[k + kl * m];
+      R nex = dmax(R(0.0), s * T.DELTH - et) / et;
+      R nex4 = (nex * nex) * (nex * nex);
+      T12[m] = R(4.75E-6) * S.FR[m] * nex4;  // T1
+      R xfac = (R(1.0) - R(1.0) / P_::CO) / (P_::CO - R(1.0) / P_::CO);
+      R dfii = (m > 0 && m < nk - 1) ? S.DF[m] * xfac : S.DF[m];
+      ADF[m] = nex4 * dfii;
+    }
+    __syncwarp();
+    // T2 is a cumulative sum over frequency: inclusive warp scan in chunks of 32
+    R carry = 0;
+    for (int base = 0; base < nk; base += 32) {
+      int m = base + lane;
+      R v = (m < nk) ? ADF[m] : R(0);
+      for (int o = 1; o < 32; o <<= 1) { R u = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v = v + u; }
+      v = v + carry;
+      if (m < nk) T12[m] = R(-1.0) * (dmax(R(0.0), T12[m]) + dmax(R(0.0), R(7.00E-5) * v));
+      carry = __shfl_sync(0xffffffffu, v, 31);
+    }
+    __syncwarp();
+    for (int b = lane; b < kl * nk; b += 32) {
+      int m = b / kl;
+      w.SL[b] = w.SL[b] + T12[m] * w.F[b];
+      w.FL[b] = w.FL[b] + T12[m];
+    }
+    __syncwarp();
+    // W3SWL6
+    R* BN = w.t(4); R* AB = w.t(5);
+    R ps = 0, amax = -R(1), iw = 0;
+    int imax = 0;
+    for (int m = lane; m < nk; m += 32) {
+      R sig = P_::ZPI * S.FR[m];
+      R s = 0, mx = 0;
+      for (int k = 0; k < kl; ++k) { R a = w.F[k + kl * m] * CG[m] / (P_::ZPI * sig); s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
+      R s2 = 0;
+      for (int k = 0; k < kl; ++k) { R a = w.F[k + kl * m] * CG[m] / (P_::ZPI * sig); s2 = s2 + ((mx < R(1.0E-34)) ? R(1.) : a / mx); }
+      R anar = R(1.0) / (s2 * T.DELTH);
+      AB[m] = s;
+      BN[m] = anar * (s * sig * T.DELTH) * (WN[m] * WN[m] * WN[m]);
+      ps = ps + s * (P_::ZPI * S.DFIM[m] * sig) / CG[m];
+      if (s > amax) { amax = s; imax = m; }
+    }
+    (void)iw;
+    // first maximum over frequency (MAXLOC)
+    for (int o = 16; o > 0; o >>= 1) {
+      R oa = __shfl_xor_sync(0xffffffffu, amax, o);
+      int oi = __shfl_xor_sync(0xffffffffu, imax, o);
+      if (oa > amax || (oa == amax && oi < imax)) { amax = oa; imax = oi; }
+    }
+    R b1 = R(0.0041) * (R(2.) * dsqrt(warp_sum(ps)) * WN[imax]);
+    __syncwarp();
+    for (int m = lane; m < nk; m += 32) {
+      R sig = P_::ZPI * S.FR[m];
+      T12[m] = (AB[m] > R(1.E-30)) ? -(R(2.) / R(3.) * b1 * sig * dsqrt(BN[m])) : R(0);
+    }
+    __syncwarp();
+    for (int b = lane; b < kl * nk; b += 32) {
+      int m = b / kl;
+      w.SL[b] = w.SL[b] + T12[m] * w.F[b];
+      w.FL[b] = w.FL[b] + T12[m];
+    }
+    __syncwarp();
+  }
+
+  // ---- the whole IMPLSCH step for this point --------------------------------
+  __device__ void run(PointState<R>& ps) const {
+    const int kl = KL(), ml = ML(), ns = kl * ml;
+    R TAUW = ps.TAUW, USTAR, Z0;
+    R emean, fmean, akmean = 0, emeanws, fmeanws, phiaw = 0;
+    const int ju = min(300, max((int)lround((double)(U10 / T.DELU)), 1));
+    integrals(nullptr, emean, fmean, (T.shallow && T.isnonlin == 0) ? &akmean : nullptr);
+    if (T.iphys == 2) { wavnu2(); w3flx4(USTAR, Z0); }
+    else airsea(TAUW, USTAR, Z0);
+    if (T.iphys == 1) sinput_ard(USTAR, Z0);
+    else sinput_st6(USTAR, TAUW);
+    integrals(w.LL, emeanws, fmeanws, nullptr);
+    int mij = (T.iphys == 2) ? frcutindex_st6(fmean, USTAR) : frcutindex(fmean, fmeanws, USTAR);
+    R tdummy;
+    if (T.iphys == 2) { stresso(USTAR, Z0, mij, tdummy, phiaw); w3flx4(USTAR, Z0); }
+    else { stresso(USTAR, Z0, mij, TAUW, phiaw); airsea(TAUW, USTAR, Z0); }
+    imphftail(mij);
+    if (T.iphys == 1) sinput_ard(USTAR, Z0);
+    stresso(USTAR, Z0, mij, (T.iphys == 2) ? tdummy : TAUW, phiaw);
+    if (T.lcflx) {  // SMIN = SL - SPOS, kept in SP from here on
+      for (int b = lane; b < ns; b += 32) w.SP[b] = w.SL[b] - w.SP[b];
+      __syncwarp();
+    }
+    if (T.iphys == 1) sdissip_ard();
+    else sdissip_st6();
+    snonlin(akmean);
+    // SBOTTOM factor per frequency (scratch 6); SL_BOT = SBO*F is formed on the fly
+    R* SBO = w.t(6);
+    if (T.shallow) {
+      const R cst = R(-2.0) * R(0.038) / P_::G;
+      for (int m = lane; m < ml; m += 32) {
+        R wav = tfak(m);
+        SBO[m] = cst * wav / dsinh(dmin(R(2.) * DEPTH * wav, R(50.)));
+      }
+      __syncwarp();
+    }
+    if (T.lcflx) {  // WNFLUXES on SSOURCE = SL - SMIN and SL_BOT
+      const R rog = P_::ROWATER * P_::G, scdfm = R(0.5) * T.DELTH * (R(1.) - R(1.) / P_::CO);
+      R a[6] = {0, 0, 0, 0, 0, 0};
+      for (int b = lane; b < kl * mij; b += 32) {
+        int m = b / kl, k = b - m * kl;
+        R cfm = (m < mij - 1) ? rog * S.DFIM[m] : rog * scdfm * S.FR[m];
+        R cm = T.shallow ? tfak(m) / (P_::ZPI * S.FR[m]) : P_::ZPI * S.FR[m] / P_::G;
+        R src = w.SL[b] - w.SP[b];
+        a[0] = a[0] + src * cfm;
+        a[1] = a[1] + cm * src * cfm * S.SINTH[k];
+        a[2] = a[2] + cm * src * cfm * S.COSTH[k];
+        if (T.shallow) {
+          R bot = SBO[m] * w.F[b];
+          a[3] = a[3] + bot * cfm;
+          a[4] = a[4] + cm * bot * cfm * S.SINTH[k];
+          a[5] = a[5] + cm * bot * cfm * S.COSTH[k];
+        }
+      }
+      for (int i = 0; i < 6; ++i) a[i] = warp_sum(a[i]);
+      R tau = P_::ROAIR * USTAR * USTAR;
+      ps.flx[0] = phiaw - a[0];
+      ps.flx[1] = tau * dsin(UDIR) - a[1];
+      ps.flx[2] = tau * dcos(UDIR) - a[2];
+      ps.flx[3] = -a[3]; ps.flx[4] = -a[4]; ps.flx[5] = -a[5];
+      ps.flx[6] = phiaw;
+    }
+    // implicit integration with the growth limiter and the minimum-energy floor
+    const R delt = T.DELT, fmx = dmax(fmeanws, fmean);
+    for (int b = lane; b < ns; b += 32) {
+      int m = b / kl, k = b - m * kl;
+      R sl = w.SL[b];
+      if (T.shallow) sl = sl + SBO[m] * w.F[b];
+      R fl = w.FL[b];
+      if (T.shallow) fl = fl + SBO[m];
+      R t1 = delt * sl / dmax(R(1.), R(1.) - delt * fl);
+      R t3 = dmin(dabs(t1), USTAR * S.DELFL[m] * fmx);
+      R f = w.F[b] + ((t1 >= R(0)) ? t3 : -t3);
+      R c = dmax(R(0.), dcos(S.TH[k] - UDIR));
+      w.F[b] = dmax(f, __ldg(&T.FLMINFR[(ju - 1) + 300 * m]) * (c * c));
+    }
+    __syncwarp();
+    integrals(nullptr, emean, fmean, nullptr);
+    integrals(w.LL, emeanws, fmeanws, nullptr);
+    mij = (T.iphys == 2) ? frcutindex_st6(fmean, USTAR) : frcutindex(fmean, fmeanws, USTAR);
+    imphftail(mij);
+    ps.TAUW = TAUW; ps.USTAR = USTAR; ps.Z0 = Z0;
+  }
+};
+
+}  // namespace wamgpu

@@ -1,0 +1,34 @@
+// Launchers shared between the translation units of libwamgpu.
+#pragma once
+#include <cuda_runtime.h>
+#include <climits>
+#include <cstring>
+#include <algorithm>
+#include "wamgpu_config.hpp"
+
+namespace wamgpu {
+
+template <typename R> struct PropArgs;
+
+// CHECK_CFL coefficient classes, in the order the extrema kernel reports them
+enum CflClass { CFL_LAT11 = 0, CFL_LAT21, CFL_LAT12, CFL_LAT22, CFL_LON1, CFL_LON2, CFL_TH1, CFL_TH2, CFL_SG1, CFL_SG2, CFL_SUM, CFL_NCLASS };
+
+// Per-point inputs/outputs of one IMPLSCH launch (device pointers).
+template <typename R> struct ImplArgs {
+  int nsea, ld;
+  R* fl3;
+  const R* u10; const R* udir; const R* roairn; const R* wstar; const R* depth; const int* indep;
+  R* tauw; R* ustar; R* z0;
+  R* fluxes;   // 7 x nsea or null
+  int* status; // bit 0: non-finite output
+};
+
+template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const ImplArgs<R>& a, int points_per_cta, cudaStream_t s);
+template <typename R> size_t implsch_smem_bytes(const DevTables<R>& T, int points_per_cta);
+template <typename R> cudaError_t implsch_set_max_smem(int points_per_cta, size_t bytes);
+
+template <typename R> cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s);
+template <typename R> cudaError_t launch_cfl_extrema(const PropArgs<R>& A, long long* ext, int nsm, cudaStream_t s);
+double cfl_decode(long long v, int precision);
+
+}  // namespace wamgpu

@@ -1,0 +1,43 @@
+// Internal view of the C-ABI configuration plus the device-side table block.
+#pragma once
+#include "../../include/wamgpu.h"
+
+namespace wamgpu {
+
+using Config = wamgpu_config;
+
+// Upper bounds of the spectral grid handled by the kernels (shared-memory
+// sizing and per-lane register arrays).  wamgpu_create rejects larger grids.
+constexpr int MAX_KL = 64;
+constexpr int MAX_ML = 48;
+constexpr int MAX_NK10 = 96;   // ST6 frequency axis extended to 10 Hz (LFACTOR)
+constexpr int SCR = 96;        // per-warp per-frequency scratch length (>= MAX_ML, MAX_KL, MAX_NK10)
+
+// Offsets (in elements) of the small tables inside the packed blocks that
+// every IMPLSCH CTA stages into shared memory.
+struct SmallLayout {
+  // float block
+  int FR, DF, DFIM, DFIMOFR, FR5, FRM5, RHOWG_DFIM, TH, COSTH, SINTH, DELFL, AF11, RNLCOEF, SATW, WTAUHF, SWELLFT;
+  int nreal;
+  // int block
+  int K1W, K2W, K11W, K21W, INLCOEF, IKP, IKP1, IKM, IKM1, INDSAT;
+  int nint;
+};
+
+// Everything the kernels need besides the per-point fields; passed by value.
+template <typename R> struct DevTables {
+  int KL, ML, NS, NDEPTH, MFRSTLW, MLSTHG, KFRH, NSDSNTH, NK10;
+  int iphys, shallow, isnonlin, lcflx;
+  R DELTH, DELTR, INV_LOG_CO, MO_TAIL, MM1_TAIL, DELU, DAL1, DAL2, X0TAUHF;
+  R BETAMAX, ZALP, ALPHA, TAUWSHELTER, CDFAC, DELT;
+  SmallLayout lay;
+  const R* small;      // packed float tables (global copy)
+  const int* ismall;   // packed int tables (global copy)
+  const R* TFAK;       // [(jd) + NDEPTH*m], jd 0-based
+  const R* TCGOND;
+  const R* FLMINFR;    // [(ju) + 300*m], ju 0-based
+  const R* ENH;        // [ij + nsea*(mc-1)] when shallow && isnonlin != 0, else null
+  int enh_ld;
+};
+
+}  // namespace wamgpu

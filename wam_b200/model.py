@@ -1,0 +1,198 @@
+"""Host-side mirror of the reference module interface for the hot path.
+
+The reference's "operator API" is a set of Fortran module procedures
+(wam_source_module.f90 / wam_propagation_module.f90).  `WamModel` exposes the
+same procedures with the same argument meaning on top of libwamgpu's C ABI:
+
+    PREPARE_PROPAGATION          -> WamModel.prepare_propagation()
+    PREPARE_SOURCE(DEPTH)        -> WamModel.prepare_source()
+    IMPLSCH(FL3, U10, UDIR, TAUW, USTAR, Z0, ROAIRN, WSTAR, DEPTH, INDEP)
+                                 -> WamModel.implsch(...)        (host arrays)
+    PROPAGS(F3)                  -> WamModel.propags(F3)         (host array)
+
+plus device-resident forms (`implsch_dev`, `propags_dev`) that take torch CUDA
+tensors.  Errors raise WamgpuError where the reference calls ABORT1.
+Spectra use the reference layout FL3(IJ,K,M) (sea point fastest): as a numpy
+array that is shape (NSEA, KL, ML) in Fortran order, or equivalently a
+C-contiguous (ML, KL, NSEA) array.
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import WamgpuConfig, WamgpuError, load
+
+_PF = ctypes.POINTER(ctypes.c_float)
+_PI = ctypes.POINTER(ctypes.c_int)
+
+
+def effective_parameters(iphys, ml, betamax=1.20, cdfac=1.13):
+    """Module parameters after INITMDL (initmdl.f90:153-160, wam_general_module.f90:63-74)."""
+    if iphys == 1:
+        zalp, alpha, tauwshelter = 0.0080, 0.0062, 0.25
+    else:
+        zalp, alpha, tauwshelter = 0.0080, 0.0060, 0.0
+    if ml <= 30:
+        alpha = 0.0075
+    return dict(betamax=betamax, zalp=zalp, alpha=alpha, tauwshelter=tauwshelter, cdfac=cdfac)
+
+
+def make_config(kl, ml, fr1, iphys, idelt, idelpro, delphi, shallow_run=True, spherical_run=True,
+                refraction_d_run=False, refraction_c_run=False, reduced_grid=False, isnonlin=0, lcflx=False,
+                betamax=1.20, cdfac=1.13, iref=1, ndepth=69, deptha=1.0, depthd=1.1, precision=4, device=0):
+    """Configuration dict (field names of struct wamgpu_config)."""
+    cfg = dict(kl=kl, ml=ml, fr1=fr1, iref=iref, iphys=iphys, shallow_run=int(shallow_run),
+               spherical_run=int(spherical_run), refraction_d_run=int(refraction_d_run),
+               refraction_c_run=int(refraction_c_run), reduced_grid=int(reduced_grid), isnonlin=isnonlin,
+               lcflx=int(lcflx), idelt=idelt, idelpro=idelpro, ndepth=ndepth, deptha=deptha, depthd=depthd,
+               delphi=float(delphi), precision=precision, device=device)
+    cfg.update(effective_parameters(iphys, ml, betamax, cdfac))
+    return cfg
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _fp(a):
+    return a.ctypes.data_as(_PF)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_PI)
+
+
+class WamModel:
+    """One rank's slab of sea points on one GPU (one context, one stream)."""
+
+    def __init__(self, cfg: dict):
+        self.L = load()
+        fields = {f for f, _ in WamgpuConfig._fields_}
+        c = WamgpuConfig(**{k: v for k, v in cfg.items() if k in fields})
+        self.cfg = dict(cfg)
+        self.kl, self.ml = cfg["kl"], cfg["ml"]
+        self.dtype = np.float64 if cfg.get("precision", 4) == 8 else np.float32
+        h = ctypes.c_void_p()
+        rc = self.L.wamgpu_create(ctypes.byref(c), ctypes.byref(h))
+        self.h = h
+        if rc != 0:
+            msg = self.L.wamgpu_last_error(h).decode() if h else "wamgpu_create failed"
+            if h:
+                self.L.wamgpu_destroy(h)
+            self.h = None
+            raise WamgpuError(f"wamgpu_create: {msg} ({rc})")
+        self.nsea = 0
+        self.counter = 1
+        self.total_cfl = 0.0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.wamgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise WamgpuError(f"{what}: {self.L.wamgpu_last_error(self.h).decode()} ({rc})")
+
+    # ---- tables and grid -------------------------------------------------
+    def table(self, name):
+        n = self.L.wamgpu_get_table(self.h, name.encode(), None, None)
+        if n < 0:
+            raise KeyError(name)
+        f = np.zeros(n, np.float32)
+        i = np.zeros(n, np.int32)
+        self.L.wamgpu_get_table(self.h, name.encode(), _fp(f), _ip(i))
+        return i if name in ("IKP", "IKP1", "IKM", "IKM1", "K1W", "K2W", "K11W", "K21W", "INLCOEF", "INDICESSAT",
+                             "DIA_SCALARS", "INDEP") else f
+
+    def set_grid(self, g):
+        """Grid-module arrays (dict from wam_b200.grid.regular_grid or equivalent)."""
+        n = int(g["nsea"])
+        self._g = {k: np.ascontiguousarray(g[k], np.int32) for k in ("klat", "klon", "kfromij")}
+        self._g.update({k: _f32(g[k]) for k in ("wlat", "sinph", "cosph", "dellam")})
+        G = self._g
+        self._check(self.L.wamgpu_set_grid(self.h, n, _ip(G["klat"]), _ip(G["klon"]), _fp(G["wlat"]),
+                                           _ip(G["kfromij"]), len(G["sinph"]), _fp(G["sinph"]), _fp(G["cosph"]),
+                                           _fp(G["dellam"])), "set_grid")
+        self.nsea = n
+
+    def set_depth(self, depth):
+        self._check(self.L.wamgpu_set_depth(self.h, _fp(_f32(depth))), "set_depth")
+
+    def set_current(self, u=None, v=None):
+        uu = None if u is None else _f32(u)
+        vv = None if v is None else _f32(v)
+        self._check(self.L.wamgpu_set_current(self.h, _fp(uu) if uu is not None else None,
+                                              _fp(vv) if vv is not None else None), "set_current")
+
+    def prepare_propagation(self):
+        """PREPARE_PROPAGATION incl. CHECK_CFL; returns (total_cfl, COUNTER)."""
+        cfl = ctypes.c_float()
+        cnt = ctypes.c_int()
+        self._check(self.L.wamgpu_prepare_propagation(self.h, ctypes.byref(cfl), ctypes.byref(cnt)),
+                    "prepare_propagation")
+        self.total_cfl, self.counter = cfl.value, cnt.value
+        return self.total_cfl, self.counter
+
+    def prepare_source(self):
+        self._check(self.L.wamgpu_prepare_source(self.h), "prepare_source")
+
+    def indep(self):
+        out = np.zeros(self.nsea, np.int32)
+        self._check(self.L.wamgpu_get_indep(self.h, _ip(out)), "get_indep")
+        return out
+
+    # ---- reference-facing procedures on host arrays ------------------------
+    def implsch(self, fl3, u10, udir, tauw, ustar, z0, roairn, wstar, depth=None, indep=None):
+        """IMPLSCH in place on float32 host arrays (fl3 Fortran-ordered (NSEA,KL,ML))."""
+        for a in (fl3, tauw, ustar, z0):
+            if not (a.dtype == np.float32 and (a.flags.f_contiguous or a.ndim == 1)):
+                raise WamgpuError("IMPLSCH in/out arrays must be float32 and Fortran-contiguous")
+        args = [_fp(fl3), _fp(_keep(self, u10)), _fp(_keep(self, udir)), _fp(tauw), _fp(ustar), _fp(z0),
+                _fp(_keep(self, roairn)), _fp(_keep(self, wstar)),
+                _fp(_keep(self, depth)) if depth is not None else None,
+                _ip(np.ascontiguousarray(indep, np.int32)) if indep is not None else None]
+        self._check(self.L.wamgpu_implsch_host(self.h, *args), "implsch")
+        self._kept = []
+
+    def propags(self, f3):
+        if not (f3.dtype == np.float32 and f3.flags.f_contiguous):
+            raise WamgpuError("PROPAGS array must be float32 and Fortran-contiguous")
+        self._check(self.L.wamgpu_propags_host(self.h, _fp(f3)), "propags")
+
+    def fluxes(self):
+        out = np.zeros(7 * self.nsea, np.float32)
+        self._check(self.L.wamgpu_get_fluxes(self.h, _fp(out)), "get_fluxes")
+        return out.reshape(7, self.nsea)
+
+    # ---- device-resident forms (torch CUDA tensors) ------------------------
+    def implsch_dev(self, fl3, u10, udir, tauw, ustar, z0, roairn, wstar, ld=None, stream=None):
+        """fl3: tensor of shape (ML, KL, ld) (contiguous, sea point fastest)."""
+        ld = fl3.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        self._check(self.L.wamgpu_implsch_dev(self.h, fl3.data_ptr(), ld, u10.data_ptr(), udir.data_ptr(),
+                                              tauw.data_ptr(), ustar.data_ptr(), z0.data_ptr(), roairn.data_ptr(),
+                                              wstar.data_ptr(), s), "implsch_dev")
+
+    def propags_dev(self, f3, ld=None, scratch=None, stream=None):
+        ld = f3.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        sc = None if scratch is None else ctypes.c_void_p(scratch.data_ptr())
+        self._check(self.L.wamgpu_propags_dev(self.h, f3.data_ptr(), ld, sc, s), "propags_dev")
+
+    def sync(self):
+        self._check(self.L.wamgpu_sync(self.h), "sync")
+
+
+def _keep(model, a):
+    arr = _f32(a)
+    if not hasattr(model, "_kept"):
+        model._kept = []
+    model._kept.append(arr)
+    return arr
