@@ -1,0 +1,304 @@
+"""Benchmark of WAM Cycle 7's per-time-step hot path on B200.
+
+Metric: spectral-point updates per second (one bin = one (sea point,
+direction, frequency) advanced by one source step IDELT together with its
+IDELT/IDELPRO propagation steps), forward, FP32.
+
+Workload (default): the 0.1-degree regional configuration, 1200x900 grid
+(45S-45N, 60W-60E) with ~30% seeded blob land (~760k sea points), depth
+10-5000 m from a seeded Gaussian random field, KL=36 x ML=30 spectrum
+(FR1=0.0345 Hz), ST6 physics (IPHYS=2), spherical shallow-water propagation
+with depth refraction, IDELPRO=120 s, IDELT=600 s.  One step = 5 PROPAGS +
+1 IMPLSCH.  Inputs are seeded synthetic fields (no dataset exists for this
+path); the spectrum (3.3 GB) is far larger than L2, so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl wamgpu|reference]
+
+--impl reference times the CPU restatement of the reference (oracle/, the
+reference's Fortran cannot be compiled in this image) on a bounded sample of
+the same workload recipe with all host threads.  With N>1 (torchrun), every
+rank runs its own replica of the workload (weak scaling, no collective).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "spectral-pt updates/s fwd, adjoint, batched on 1 B200 at Hs rel err<=1e-4"
+UNIT = "spectral-point updates/s"
+FALLBACK_HBM = 6650.0  # GB/s, used only if MEASURED_PEAKS.json is absent
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="wamgpu", choices=["wamgpu", "reference"])
+    p.add_argument("--workload", default="c1")
+    p.add_argument("--scale", type=float, default=1.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference(args, wl_name, scale, budget_s, steps=None):
+    """The oracle (CPU restatement) on a bounded sample of the workload recipe."""
+    from oracle.oracle import Oracle
+    from wam_b200.synth import make_workload
+    w = make_workload(wl_name, scale=scale)
+    o = Oracle(w.cfg)
+    o.set_grid(w.grid)
+    o.set_fields(w.depth)
+    o.prepare_propagation()
+    o.prepare_source()
+    indep = o.indep()
+    f = w.spectrum_f().astype(float)
+    tw, us, zz = (a.astype(float) for a in (w.tauw, w.ustar, w.z0))
+    nthreads = os.cpu_count() or 1
+    n_done, t_tot = 0, 0.0
+    while (steps is None and t_tot < budget_s) or (steps is not None and n_done < steps):
+        t0 = time.perf_counter()
+        for _ in range(w.sub_steps):
+            f = o.propags(f)
+        f, tw, us, zz, _ = o.implsch(f, w.u10, w.udir, tw, us, zz, w.roairn, w.wstar, w.depth, indep,
+                                     nthreads=nthreads)
+        t_tot += time.perf_counter() - t0
+        n_done += 1
+    bins = w.nsea * w.cfg["kl"] * w.cfg["ml"]
+    return dict(value=bins * n_done / t_tot, nsea=w.nsea, steps=n_done, seconds=t_tot, cores=nthreads,
+                grid=f"{w.grid['nx']}x{w.grid['ny']}")
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    # sample: the workload recipe at 1/8 linear scale (~12k sea points), one step per timed step
+    per_step = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_reference(args, args.workload, 0.125, 0.0, steps=1)
+        if i >= args.warmup:
+            per_step.append(r)
+    secs = sum(r["seconds"] for r in per_step)
+    bins = per_step[0]["nsea"] * 36 * 30
+    val = bins * len(per_step) / secs
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(per_step),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": f"{args.workload} recipe at 1/8 linear scale ({per_step[0]['grid']}, "
+                                   f"{per_step[0]['nsea']} sea points): 5 PROPAGS + 1 IMPLSCH per step"},
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": per_step[0]["cores"], "kind": "port",
+                             "sample": f"{per_step[0]['nsea']} sea points x {len(per_step)} source steps"},
+            "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    from wam_b200 import WamModel
+    from wam_b200.synth import make_workload
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = torch.device("cuda", local)
+    w = make_workload(args.workload, scale=args.scale, device=local)
+    cfg = dict(w.cfg, device=local)
+    m = WamModel(cfg)
+    m.set_grid(w.grid)
+    m.set_depth(w.depth)
+    cfl, counter = m.prepare_propagation()
+    m.prepare_source()
+    n, KL, ML = w.nsea, cfg["kl"], cfg["ml"]
+    nprop = cfg["idelt"] // cfg["idelpro"]
+    ld = (n + 31) // 32 * 32
+    F = w.spectrum_device(torch, dev, ld=ld)
+    S = torch.empty_like(F)
+    t = lambda a: torch.tensor(np.asarray(a), dtype=torch.float32, device=dev)
+    u10, udir, roairn, wstar = t(w.u10), t(w.udir), t(w.roairn), t(w.wstar)
+    tauw, ustar, z0 = t(w.tauw), t(w.ustar), t(w.z0)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        m.step_dev(F, nprop, u10, udir, tauw, ustar, z0, roairn, wstar, scratch=S, ld=ld, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    m.timing()  # discard warm-up timings
+    m.set_timing(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    kt = m.timing()
+    m.set_timing(False)
+    m.sync()
+    ms_t = torch.tensor([ms], device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms = float(ms_t.item())
+    bins = n * KL * ML
+    value = world * bins * args.steps / (ms / 1e3)
+    # roofline of the dominant kernel (algorithmic bytes: FL3 read + write + 12 per-point words)
+    hbm, hbm_kind = peaks()
+    per_launch_bytes = n * (8 * KL * ML + 48)
+    kernels = {}
+    for name, (kms, cnt) in kt.items():
+        if cnt:
+            avg = kms / cnt
+            kernels[name] = {"launches": cnt, "avg_ms": avg, "share": kms / max(ms, 1e-9),
+                             "achieved_gbs": per_launch_bytes / (avg / 1e3) / 1e9}
+    dom = max(kernels, key=lambda k: kernels[k]["avg_ms"] * kernels[k]["launches"])
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof):
+        with open(prof) as f:
+            tr = json.load(f)
+        key = f"{dom}_{args.workload}"
+        if key in tr:
+            traffic = tr[key]["dram_bytes_per_point"] * n
+    roof = {"bound": "hbm", "achieved": kernels[dom]["achieved_gbs"], "peak": hbm, "unit": "GB/s",
+            "frac": kernels[dom]["achieved_gbs"] / hbm, "traffic": traffic, "kernel": dom,
+            "peak_kind": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)" if hbm_kind == "measured" else "fallback"}
+    # end to end through the C ABI with host buffers (pinned): FL3 and the point fields in, results back
+    e2e = None
+    if not args.no_e2e and rank == 0:
+        m2 = m
+        hf = torch.empty((ML, KL, n), dtype=torch.float32, pin_memory=True)
+        hf.copy_(F[:, :, :n])
+        pin = lambda a: torch.tensor(np.asarray(a), dtype=torch.float32).pin_memory()
+        hu, hd, hr, hw = pin(w.u10), pin(w.udir), pin(w.roairn), pin(w.wstar)
+        ht, hs, hz = tauw.cpu().pin_memory(), ustar.cpu().pin_memory(), z0.cpu().pin_memory()
+        fp = lambda x: x.numpy()
+        arr = hf.numpy()
+        fmt = np.lib.stride_tricks.as_strided(arr, shape=(n, KL, ML), strides=(4, 4 * n, 4 * n * KL))
+        m2.step(fmt, nprop, fp(hu), fp(hd), fp(ht), fp(hs), fp(hz), fp(hr), fp(hw))  # warm
+        ksteps = max(2, min(args.steps, 5))
+        t0 = time.perf_counter()
+        for _ in range(ksteps):
+            m2.step(fmt, nprop, fp(hu), fp(hd), fp(ht), fp(hs), fp(hz), fp(hr), fp(hw))
+        dt = time.perf_counter() - t0
+        h2d = 4 * (n * KL * ML + 7 * n)
+        d2h = 4 * (n * KL * ML + 3 * n)
+        e2e = {"value": bins * ksteps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "steps": ksteps, "ms_per_step": 1e3 * dt / ksteps,
+               "how": "wamgpu_step_host on pinned host FL3 + fields: H2D, 5 PROPAGS + IMPLSCH, D2H each step"}
+    cpu = None
+    if not args.no_cpu_baseline and rank == 0 and world == 1:
+        r = cpu_reference(args, args.workload, 0.125, 15.0)
+        cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port",
+               "sample": f"{args.workload} recipe at 1/8 scale ({r['grid']}, {r['nsea']} sea points), "
+                         f"{r['steps']} source steps (5 PROPAGS + IMPLSCH) in {r['seconds']:.1f} s"}
+    if rank == 0:
+        launches = sum(v["launches"] for v in kernels.values())
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fields; no dataset for this path)",
+                "config": {"workload": f"{args.workload}: 0.1 deg 1200x900 regional, ST6, KL=36 ML=30, "
+                                       f"IDELPRO=120 s IDELT=600 s (5 PROPAGS + 1 IMPLSCH per step)"
+                                       if args.workload == "c1" and args.scale == 1.0 else
+                                       f"{args.workload} at scale {args.scale}",
+                           "nsea": n, "bins_per_point": KL * ML, "counter": counter, "total_cfl": cfl,
+                           "l2": "spectrum 3.3 GB >> 126 MB L2, no flush needed",
+                           "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+                "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    m.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -131,9 +131,27 @@ WAMGPU_API int wamgpu_implsch_dev(wamgpu_ctx* ctx, void* fl3, int ld, const void
                        void* z0, const void* roairn, const void* wstar, void* stream);
 WAMGPU_API int wamgpu_propags_dev(wamgpu_ctx* ctx, void* f3, int ld, void* scratch, void* stream);
 
+/* One pass of the WAMODEL PROP/PHYSICS loop body (wamodel.f90:286-360):
+ * nprop PROPAGS calls (IDELT/IDELPRO of them per source step) followed by
+ * one IMPLSCH, with the spectrum resident on the device for the whole pass.
+ * The _host form copies FL3 and the per-point fields in once and back once
+ * (FP32 contexts); the _dev form works on caller-owned device buffers. */
+WAMGPU_API int wamgpu_step_dev(wamgpu_ctx* ctx, void* fl3, int ld, void* scratch, int nprop, const void* u10,
+                               const void* udir, void* tauw, void* ustar, void* z0, const void* roairn,
+                               const void* wstar, void* stream);
+WAMGPU_API int wamgpu_step_host(wamgpu_ctx* ctx, float* fl3, int nprop, const float* u10, const float* udir,
+                                float* tauw, float* ustar, float* z0, const float* roairn, const float* wstar);
+
 /* Flux-module arrays of the last LCFLX step, 7 blocks of NSEA in the order
  * PHIOC, TAUOC_X, TAUOC_Y, PHIBOT, TAUBOT_X, TAUBOT_Y, PHIAW (host copy). */
 WAMGPU_API int wamgpu_get_fluxes(wamgpu_ctx* ctx, float* out7);
+
+/* Kernel timing (tracing): while enabled, every PROPAGS and IMPLSCH launch is
+ * bracketed by CUDA events on its stream.  wamgpu_get_timing waits for them
+ * and returns the summed milliseconds and launch counts since the last call:
+ * ms[0]/count[0] for PROPAGS, ms[1]/count[1] for IMPLSCH. */
+WAMGPU_API int wamgpu_set_timing(wamgpu_ctx* ctx, int enable);
+WAMGPU_API int wamgpu_get_timing(wamgpu_ctx* ctx, float* ms, int* count);
 
 /* Synchronises the context stream; returns WAMGPU_E_NUMERIC if a kernel
  * reported non-finite output since the last call. */

@@ -39,8 +39,13 @@ SIGNATURES = {
     "wamgpu_implsch_dev": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                    c_void_p, c_void_p, c_void_p]),
     "wamgpu_propags_dev": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "wamgpu_step_dev": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wamgpu_step_host": (c_int, [c_void_p, PF, c_int, PF, PF, PF, PF, PF, PF, PF]),
     "wamgpu_get_fluxes": (c_int, [c_void_p, PF]),
     "wamgpu_sync": (c_int, [c_void_p]),
+    "wamgpu_set_timing": (c_int, [c_void_p, c_int]),
+    "wamgpu_get_timing": (c_int, [c_void_p, PF, PI]),
 }
 
 _lib = None

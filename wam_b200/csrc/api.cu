@@ -52,6 +52,10 @@ struct wamgpu_ctx {
   bool have_grid = false, prepared = false;
   int counter = 1; double total_cfl = 0, cfl_min = 0; int variant = 0;
   std::unique_ptr<ImplBase> impl;
+  // opt-in kernel timing: event pairs per kernel class (0 = PROPAGS, 1 = IMPLSCH)
+  bool timing = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev[2];
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pool;
   // precision-specific part
   virtual ~wamgpu_ctx() {}
 };
@@ -69,6 +73,25 @@ template <typename R> struct Impl : ImplBase {
   // model state used by the host-buffer entry points
   DevBuf fl3, scratch, u10, udir, tauw, ustar, z0, roairn, wstar, fluxes, status, cflext;
   std::vector<R> dco, dpsn;  // host
+};
+
+struct TimedLaunch {
+  wamgpu_ctx* ctx; int cls; cudaStream_t s; std::pair<cudaEvent_t, cudaEvent_t> e{nullptr, nullptr};
+  TimedLaunch(wamgpu_ctx* c, int k, cudaStream_t st) : ctx(c), cls(k), s(st) {
+    if (!ctx->timing) return;
+    if (ctx->ev_pool.empty()) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a); cudaEventCreate(&b);
+      ctx->ev_pool.push_back({a, b});
+    }
+    e = ctx->ev_pool.back(); ctx->ev_pool.pop_back();
+    cudaEventRecord(e.first, s);
+  }
+  ~TimedLaunch() {
+    if (!e.first) return;
+    cudaEventRecord(e.second, s);
+    ctx->ev[cls].push_back(e);
+  }
 };
 
 int fail(wamgpu_ctx* c, int code, const std::string& msg) {
@@ -374,7 +397,7 @@ template <typename R> int prepare_source_t(wamgpu_ctx* ctx, Impl<R>& I) {
 
 template <typename R>
 int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u10, const void* udir, void* tauw,
-                  void* ustar, void* z0, const void* roairn, const void* wstar, cudaStream_t s) {
+                  void* ustar, void* z0, const void* roairn, const void* wstar, cudaStream_t s, const void* fl3_in = nullptr) {
   if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first (INDEP)");
   if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
   if (ctx->cfg.shallow_run && ctx->cfg.isnonlin != 0 && !I.dt.ENH)
@@ -383,12 +406,12 @@ int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u1
   if (ctx->cfg.lcflx) CK(I.fluxes.ensure((size_t)7 * ctx->nsea * sizeof(R) + 16), "alloc");
   ImplArgs<R> a;
   a.nsea = ctx->nsea; a.ld = ld;
-  a.fl3 = (R*)fl3; a.u10 = (const R*)u10; a.udir = (const R*)udir; a.roairn = (const R*)roairn; a.wstar = (const R*)wstar;
+  a.fl3 = (R*)fl3; a.fl3_in = fl3_in ? (const R*)fl3_in : (const R*)fl3; a.u10 = (const R*)u10; a.udir = (const R*)udir; a.roairn = (const R*)roairn; a.wstar = (const R*)wstar;
   a.depth = I.d_depth.template as<R>(); a.indep = I.d_indep.template as<int>();
   a.tauw = (R*)tauw; a.ustar = (R*)ustar; a.z0 = (R*)z0;
   a.fluxes = ctx->cfg.lcflx ? I.fluxes.template as<R>() : nullptr;
   a.status = I.status.template as<int>();
-  CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch");
+  { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch"); }
   return WAMGPU_OK;
 }
 
@@ -404,10 +427,32 @@ template <typename R> int propags_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* f3v, 
   R* src = f3; R* dst = sc;
   if (cnt % 2 == 1) { CK(cudaMemcpyAsync(sc, f3, bytes, cudaMemcpyDeviceToDevice, s), "copy F1"); src = sc; dst = f3; }
   for (int it = 0; it < cnt; ++it) {
-    CK(launch_propags<R>(I.pa, src, ld, dst, ld, s), "propags launch");
+    { TimedLaunch tl(ctx, 0, s); CK(launch_propags<R>(I.pa, src, ld, dst, ld, s), "propags launch"); }
     std::swap(src, dst);
   }
   return WAMGPU_OK;
+}
+
+// One pass of WAMODEL's PROP/PHYSICS loop body (wamodel.f90:286-360): nprop
+// PROPAGS calls (each COUNTER sub-steps) followed by one IMPLSCH.  All
+// sub-steps ping-pong between f3 and scratch and IMPLSCH reads whichever
+// buffer the last one wrote, writing its result into f3: no device copies.
+template <typename R>
+int step_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* f3v, int ld, void* scratch, int nprop, const void* u10, const void* udir,
+               void* tauw, void* ustar, void* z0, const void* roairn, const void* wstar, cudaStream_t s) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  if (nprop < 0) return fail(ctx, WAMGPU_E_ARG, "nprop < 0");
+  R* f3 = (R*)f3v;
+  const size_t bytes = (size_t)ld * ctx->cfg.kl * ctx->cfg.ml * sizeof(R);
+  R* sc = (R*)scratch;
+  if (!sc) { CK(I.scratch.ensure(bytes), "alloc scratch"); sc = I.scratch.template as<R>(); }
+  R* src = f3; R* dst = sc;
+  for (int it = 0; it < nprop * ctx->counter; ++it) {
+    { TimedLaunch tl(ctx, 0, s); CK(launch_propags<R>(I.pa, src, ld, dst, ld, s), "propags launch"); }
+    std::swap(src, dst);
+  }
+  return implsch_dev_t<R>(ctx, I, f3, ld, u10, udir, tauw, ustar, z0, roairn, wstar, s, src);
 }
 
 template <typename R> std::vector<R> to_r(const float* p, size_t n) {
@@ -448,6 +493,30 @@ int implsch_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, const float* u10, co
     }
   }
   CK(cudaStreamSynchronize(s), "implsch sync");
+  return wamgpu_sync(ctx);
+}
+
+template <typename R>
+int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float* u10, const float* udir, float* tauw,
+                float* ustar, float* z0, const float* roairn, const float* wstar) {
+  static_assert(sizeof(R) == 4 || sizeof(R) == 8, "");
+  if (sizeof(R) != 4) return fail(ctx, WAMGPU_E_ARG, "wamgpu_step_host is FP32 only; use wamgpu_step_dev");
+  const int n = ctx->nsea;
+  const size_t nb = (size_t)n * ctx->cfg.kl * ctx->cfg.ml;
+  cudaStream_t s = ctx->stream;
+  CK(I.fl3.ensure(nb * sizeof(R)), "alloc");
+  for (DevBuf* b : {&I.u10, &I.udir, &I.tauw, &I.ustar, &I.z0, &I.roairn, &I.wstar}) CK(b->ensure((size_t)n * sizeof(R) + 16), "alloc");
+  struct Up { void* d; const float* h; size_t n; };
+  Up ups[] = {{I.fl3.p, fl3, nb}, {I.u10.p, u10, (size_t)n}, {I.udir.p, udir, (size_t)n}, {I.tauw.p, tauw, (size_t)n},
+              {I.ustar.p, ustar, (size_t)n}, {I.z0.p, z0, (size_t)n}, {I.roairn.p, roairn, (size_t)n}, {I.wstar.p, wstar, (size_t)n}};
+  for (auto& u : ups) CK(cudaMemcpyAsync(u.d, u.h, u.n * 4, cudaMemcpyHostToDevice, s), "H2D");
+  int rc = step_dev_t<R>(ctx, I, I.fl3.p, n, nullptr, nprop, I.u10.p, I.udir.p, I.tauw.p, I.ustar.p, I.z0.p, I.roairn.p,
+                         I.wstar.p, s);
+  if (rc) return rc;
+  struct Dn { float* h; void* d; size_t n; };
+  Dn dns[] = {{fl3, I.fl3.p, nb}, {tauw, I.tauw.p, (size_t)n}, {ustar, I.ustar.p, (size_t)n}, {z0, I.z0.p, (size_t)n}};
+  for (auto& d : dns) CK(cudaMemcpyAsync(d.h, d.d, d.n * 4, cudaMemcpyDeviceToHost, s), "D2H");
+  CK(cudaStreamSynchronize(s), "step sync");
   return wamgpu_sync(ctx);
 }
 
@@ -539,6 +608,8 @@ int wamgpu_destroy(wamgpu_ctx* ctx) {
   if (!ctx) return WAMGPU_OK;
   if (ctx->stream) { cudaSetDevice(ctx->cfg.device); cudaStreamSynchronize(ctx->stream); }
   ctx->impl.reset();
+  for (int c = 0; c < 2; ++c) for (auto& e : ctx->ev[c]) ctx->ev_pool.push_back(e);
+  for (auto& e : ctx->ev_pool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return WAMGPU_OK;
@@ -650,6 +721,22 @@ int wamgpu_propags_dev(wamgpu_ctx* ctx, void* f3, int ld, void* scratch, void* s
   return DISPATCH_CTX(ctx, propags_dev_t, f3, ld, scratch, s);
 }
 
+int wamgpu_step_dev(wamgpu_ctx* ctx, void* fl3, int ld, void* scratch, int nprop, const void* u10, const void* udir,
+                    void* tauw, void* ustar, void* z0, const void* roairn, const void* wstar, void* stream) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!fl3 || !u10 || !udir || !tauw || !ustar || !z0 || !roairn || !wstar) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, step_dev_t, fl3, ld, scratch, nprop, u10, udir, tauw, ustar, z0, roairn, wstar, s);
+}
+
+int wamgpu_step_host(wamgpu_ctx* ctx, float* fl3, int nprop, const float* u10, const float* udir, float* tauw,
+                     float* ustar, float* z0, const float* roairn, const float* wstar) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!fl3 || !u10 || !udir || !tauw || !ustar || !z0 || !roairn || !wstar) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  cudaSetDevice(ctx->cfg.device);
+  return DISPATCH_CTX(ctx, step_host_t, fl3, nprop, u10, udir, tauw, ustar, z0, roairn, wstar);
+}
+
 int wamgpu_get_fluxes(wamgpu_ctx* ctx, float* out7) {
   if (!ctx || !ctx->impl || !out7) return WAMGPU_E_ARG;
   if (!ctx->cfg.lcflx) return fail(ctx, WAMGPU_E_STATE, "LCFLX is off");
@@ -665,6 +752,29 @@ int wamgpu_get_fluxes(wamgpu_ctx* ctx, float* out7) {
     auto* I = static_cast<Impl<float>*>(ctx->impl.get());
     CK(cudaMemcpyAsync(out7, I->fluxes.p, n * 4, cudaMemcpyDeviceToHost, ctx->stream), "D2H");
     CK(cudaStreamSynchronize(ctx->stream), "sync");
+  }
+  return WAMGPU_OK;
+}
+
+int wamgpu_set_timing(wamgpu_ctx* ctx, int enable) {
+  if (!ctx) return WAMGPU_E_ARG;
+  ctx->timing = enable != 0;
+  return WAMGPU_OK;
+}
+
+int wamgpu_get_timing(wamgpu_ctx* ctx, float* ms, int* count) {
+  if (!ctx || !ms || !count) return WAMGPU_E_ARG;
+  cudaSetDevice(ctx->cfg.device);
+  for (int c = 0; c < 2; ++c) {
+    ms[c] = 0.f; count[c] = (int)ctx->ev[c].size();
+    for (auto& e : ctx->ev[c]) {
+      float t = 0.f;
+      CK(cudaEventSynchronize(e.second), "timing");
+      CK(cudaEventElapsedTime(&t, e.first, e.second), "timing");
+      ms[c] += t;
+      ctx->ev_pool.push_back(e);
+    }
+    ctx->ev[c].clear();
   }
   return WAMGPU_OK;
 }

@@ -25,7 +25,7 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
   // stage the P spectra: consecutive threads take consecutive points of one bin
   for (int idx = tid; idx < P * NS; idx += nthr) {
     int p = idx % P, b = idx / P, ij = ij0 + p;
-    if (ij < a.nsea) reinterpret_cast<R*>(ws0 + p * wsb)[b] = a.fl3[ij + (size_t)a.ld * b];
+    if (ij < a.nsea) reinterpret_cast<R*>(ws0 + p * wsb)[b] = a.fl3_in[ij + (size_t)a.ld * b];
   }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, ij = ij0 + warp;

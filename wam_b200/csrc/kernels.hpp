@@ -16,7 +16,8 @@ enum CflClass { CFL_LAT11 = 0, CFL_LAT21, CFL_LAT12, CFL_LAT22, CFL_LON1, CFL_LO
 // Per-point inputs/outputs of one IMPLSCH launch (device pointers).
 template <typename R> struct ImplArgs {
   int nsea, ld;
-  R* fl3;
+  const R* fl3_in;  // spectrum read (may equal fl3)
+  R* fl3;           // spectrum written
   const R* u10; const R* udir; const R* roairn; const R* wstar; const R* depth; const int* indep;
   R* tauw; R* ustar; R* z0;
   R* fluxes;   // 7 x nsea or null

@@ -186,6 +186,35 @@ class WamModel:
         sc = None if scratch is None else ctypes.c_void_p(scratch.data_ptr())
         self._check(self.L.wamgpu_propags_dev(self.h, f3.data_ptr(), ld, sc, s), "propags_dev")
 
+    def step(self, fl3, nprop, u10, udir, tauw, ustar, z0, roairn, wstar):
+        """nprop x PROPAGS then IMPLSCH on host arrays (one H2D and one D2H of FL3)."""
+        for a in (fl3, tauw, ustar, z0):
+            if a.dtype != np.float32:
+                raise WamgpuError("step arrays must be float32")
+        self._check(self.L.wamgpu_step_host(self.h, _fp(fl3), int(nprop), _fp(_keep(self, u10)), _fp(_keep(self, udir)),
+                                            _fp(tauw), _fp(ustar), _fp(z0), _fp(_keep(self, roairn)),
+                                            _fp(_keep(self, wstar))), "step")
+        self._kept = []
+
+    def step_dev(self, fl3, nprop, u10, udir, tauw, ustar, z0, roairn, wstar, scratch=None, ld=None, stream=None):
+        """nprop x PROPAGS then IMPLSCH on device tensors; fl3 shape (ML, KL, ld)."""
+        ld = fl3.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        sc = None if scratch is None else ctypes.c_void_p(scratch.data_ptr())
+        self._check(self.L.wamgpu_step_dev(self.h, fl3.data_ptr(), ld, sc, int(nprop), u10.data_ptr(), udir.data_ptr(),
+                                           tauw.data_ptr(), ustar.data_ptr(), z0.data_ptr(), roairn.data_ptr(),
+                                           wstar.data_ptr(), s), "step_dev")
+
+    def set_timing(self, enable=True):
+        self._check(self.L.wamgpu_set_timing(self.h, int(enable)), "set_timing")
+
+    def timing(self):
+        """{'propags': (ms, launches), 'implsch': (ms, launches)} since the last call."""
+        ms = np.zeros(2, np.float32)
+        cnt = np.zeros(2, np.int32)
+        self._check(self.L.wamgpu_get_timing(self.h, _fp(ms), _ip(cnt)), "get_timing")
+        return {"propags": (float(ms[0]), int(cnt[0])), "implsch": (float(ms[1]), int(cnt[1]))}
+
     def sync(self):
         self._check(self.L.wamgpu_sync(self.h), "sync")
 

@@ -46,8 +46,8 @@ def grf(rng, nx, ny, corr):
     return f
 
 
-def jonswap_spectrum(fr, th, fp, alpha, gamma, sa, sb, udir):
-    """Start spectrum F(IJ,K,M) [NSEA, KL, ML] float32: JONSWAP x cos^2 spreading."""
+def jonswap_factors(fr, th, fp, alpha, gamma, sa, sb, udir):
+    """Frequency part E(IJ,M) and directional part D(IJ,K) of the start spectrum."""
     fr = np.asarray(fr, np.float64)[None, :]
     fp = np.asarray(fp, np.float64)[:, None]
     alpha = np.broadcast_to(np.asarray(alpha, np.float64), (fp.shape[0],))[:, None]
@@ -57,7 +57,13 @@ def jonswap_spectrum(fr, th, fp, alpha, gamma, sa, sb, udir):
     a2 = 0.5 * ((fr / fp - 1.0) / sig) ** 2
     et = et * np.where(a2 < 99.0, np.exp(np.log(gamma) * np.exp(-np.minimum(a2, 99.0))), 1.0)
     spr = np.maximum(0.0, np.cos(np.asarray(th)[None, :] - np.asarray(udir)[:, None])) ** 2 * (2.0 / math.pi)
-    return (et[:, None, :] * spr[:, :, None]).astype(np.float32)
+    return et.astype(np.float32), spr.astype(np.float32)
+
+
+def jonswap_spectrum(fr, th, fp, alpha, gamma, sa, sb, udir):
+    """Start spectrum F(IJ,K,M) [NSEA, KL, ML] float32: JONSWAP x cos^2 spreading."""
+    et, spr = jonswap_factors(fr, th, fp, alpha, gamma, sa, sb, udir)
+    return et[:, None, :] * spr[:, :, None]
 
 
 def wind_from_uv(u, v):
@@ -70,9 +76,10 @@ def wind_from_uv(u, v):
 class Workload:
     """Grid, configuration, fields and start state of one configuration."""
 
-    def __init__(self, name, cfg, grid, depth, u10, udir, fl3, wind_fn=None, n_src_steps=1, sub_steps=1):
+    def __init__(self, name, cfg, grid, depth, u10, udir, e_fm, d_fk, wind_fn=None, n_src_steps=1, sub_steps=1):
         self.name, self.cfg, self.grid = name, cfg, grid
-        self.depth, self.u10, self.udir, self.fl3 = depth, u10, udir, fl3
+        self.depth, self.u10, self.udir = depth, u10, udir
+        self.e_fm, self.d_fk = e_fm, d_fk  # start spectrum = E(IJ,M) * D(IJ,K)
         self.wind_fn = wind_fn
         self.nsea = grid["nsea"]
         self.n_src_steps = n_src_steps
@@ -84,8 +91,18 @@ class Workload:
         self.wstar = np.zeros(self.nsea, np.float32)
 
     def spectrum_f(self):
-        """FL3 as a Fortran-ordered (NSEA, KL, ML) float32 array."""
-        return np.asfortranarray(self.fl3)
+        """Start FL3 as a Fortran-ordered (NSEA, KL, ML) float32 array."""
+        return np.asfortranarray(self.e_fm[:, None, :] * self.d_fk[:, :, None])
+
+    def spectrum_device(self, torch, device, ld=None, dtype=None):
+        """Start FL3 on the device as a (ML, KL, ld) tensor (sea point fastest)."""
+        ld = self.nsea if ld is None else ld
+        dtype = torch.float32 if dtype is None else dtype
+        e = torch.tensor(self.e_fm.T, device=device, dtype=dtype)   # (ML, NSEA)
+        d = torch.tensor(self.d_fk.T, device=device, dtype=dtype)   # (KL, NSEA)
+        f = torch.zeros((self.cfg["ml"], self.cfg["kl"], ld), device=device, dtype=dtype)
+        f[:, :, :self.nsea] = e[:, None, :] * d[None, :, :]
+        return f
 
 
 def _finish(name, cfg, g, depth_grid, u_grid, v_grid, rng, seed_fn=None, **kw):
@@ -97,8 +114,8 @@ def _finish(name, cfg, g, depth_grid, u_grid, v_grid, rng, seed_fn=None, **kw):
     u10, udir = wind_from_uv(u, v)
     fr = cfg["fr1"] * 1.1 ** np.arange(cfg["ml"])
     th = (np.arange(cfg["kl"]) + 0.5) * (2 * math.pi / cfg["kl"])
-    fl3 = jonswap_spectrum(fr, th, np.full(g["nsea"], 0.2), 0.018, 3.3, 0.07, 0.09, udir)
-    return Workload(name, cfg, g, depth, u10, udir, fl3, **kw)
+    e_fm, d_fk = jonswap_factors(fr, th, np.full(g["nsea"], 0.2), 0.018, 3.3, 0.07, 0.09, udir)
+    return Workload(name, cfg, g, depth, u10, udir, e_fm, d_fk, **kw)
 
 
 def make_workload(name, seed=1234, scale=1.0, precision=4, device=0):
