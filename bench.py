@@ -198,11 +198,13 @@ def main():
     t = lambda a: torch.tensor(np.asarray(a), dtype=torch.float32, device=dev)
     u10, udir, roairn, wstar = t(w.u10), t(w.udir), t(w.roairn), t(w.wstar)
     tauw, ustar, z0 = t(w.tauw), t(w.ustar), t(w.z0)
-    stream = torch.cuda.current_stream(dev)
+    torch.cuda.synchronize()
+    stream = torch.cuda.Stream(dev)  # a non-default stream: handle 0 would select the library's own stream
 
     def step():
         m.step_dev(F, nprop, u10, udir, tauw, ustar, z0, roairn, wstar, scratch=S, ld=ld, stream=stream.cuda_stream)
 
+    torch.cuda.set_stream(stream)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()

@@ -23,7 +23,7 @@ UNITS = {
     "propags.cu": ["-fmad=false"],
     "api.cu": [],
 }
-HEADERS = ["implsch.cuh", "propags.cuh", "devmath.cuh", "kernels.hpp", "spectral_tables.hpp", "wamgpu_config.hpp"]
+HEADERS = ["implsch.cuh", "propags.cuh", "propargs.hpp", "devmath.cuh", "kernels.hpp", "spectral_tables.hpp", "wamgpu_config.hpp"]
 
 
 def _nvcc():

@@ -9,7 +9,7 @@
 #include "../../include/wamgpu.h"
 #include "wamgpu_config.hpp"
 #include "spectral_tables.hpp"
-#include "propags.cuh"
+#include "propargs.hpp"
 #include "kernels.hpp"
 
 using namespace wamgpu;
@@ -315,7 +315,8 @@ template <typename R> int prepare_prop(wamgpu_ctx* ctx, Impl<R>& I, float* total
   A.dvphi = I.d_dvphi.template as<R>(); A.dvlam = I.d_dvlam.template as<R>();
   A.u = I.d_u.template as<R>(); A.v = I.d_v.template as<R>();
   A.TCGOND = I.tcgond.template as<R>(); A.TSIHKD = I.tsihkd.template as<R>(); A.TFAK = I.tfak.template as<R>();
-  A.GOM = I.gom.template as<R>(); A.FR = I.fr.template as<R>(); A.SINTH = I.sinth.template as<R>(); A.COSTH = I.costh.template as<R>();
+  A.GOM = I.gom.template as<R>(); A.FR = I.fr.template as<R>();
+  CK(set_direction_tables<R>(t.SINTH.data(), t.COSTH.data(), KL), "direction tables");
   // CHECK_CFL (:1917-2138) from the extrema of the recomputed coefficients
   CK(I.cflext.ensure(2 * CFL_NCLASS * sizeof(long long)), "alloc");
   CK(launch_cfl_extrema<R>(A, I.cflext.template as<long long>(), ctx->nsm, s), "cfl kernel");

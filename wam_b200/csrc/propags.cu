@@ -5,40 +5,40 @@
 
 namespace wamgpu {
 
-template <typename R>
+// One thread per (sea point, frequency) walking the directions.
+template <typename R, int VAR, bool RED, bool REFRD>
 __global__ void __launch_bounds__(128) propags_kernel(const PropArgs<R> A, const R* __restrict__ f1, int ld1,
                                                       R* __restrict__ f3, int ld3) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int m = blockIdx.y;
   if (i >= A.nsea) return;
-  const PropCore<R> P(A);
+  using S = Site<R, VAR, RED, REFRD>;
+  const S site(A, i, m);
   const int KL = A.KL, ML = A.ML;
-  const bool cur = A.variant == V_CART_DEEP_CUR || A.variant == V_CART_SHALLOW_CUR || A.variant == V_SPHER_DEEP_CURR ||
-                   A.variant == V_SPHER_SHALLOW_CURR;
   const size_t plane = (size_t)ld1 * KL;
-  auto F = [&](int p1, int k, int mm) -> R { return p1 == 0 ? R(0) : __ldg(&f1[(p1 - 1) + (size_t)ld1 * k + plane * mm]); };
-  const int s0 = P.klat(i, 0, 0), n0 = P.klat(i, 1, 0), w0 = P.klon(i, 0), e0 = P.klon(i, 1);
-  const int s1 = A.reduced ? P.klat(i, 0, 1) : 0, n1 = A.reduced ? P.klat(i, 1, 1) : 0;
-  const bool theta = A.refr_d || A.spherical;
-  const int mm = (m == 0) ? 0 : m - 1, mp = (m == ML - 1) ? ML - 1 : m + 1;
-  R fkm = F(i + 1, KL - 1, m), fk = F(i + 1, 0, m);
+  const R* fm = f1 + plane * m;
+  auto F = [&](int p1, int k) -> R { return p1 == 0 ? R(0) : __ldg(&fm[(p1 - 1) + (size_t)ld1 * k]); };
+  const bool theta = REFRD || S::SPH;
+  R fkm = F(i + 1, KL - 1), fk = F(i + 1, 0);
+  R* out = f3 + i + (size_t)ld3 * KL * m;
   for (int k = 0; k < KL; ++k) {
     const int kp = (k + 1 == KL) ? 0 : k + 1;
-    R fkp = F(i + 1, kp, m);
-    const Coefs<R> c = P.coef(i, k, m);
+    const R fkp = F(i + 1, kp);
+    const Coefs<R> c = site.coef(k);
     R v;
-    if (!cur) {
-      const R sn = __ldg(&A.SINTH[k]), cs = __ldg(&A.COSTH[k]);
-      const int lat = (cs >= R(0.)) ? s0 : n0, lon = (sn >= R(0.)) ? w0 : e0;
-      v = c.sum * fk + c.lat11 * F(lat, k, m) + c.lon1 * F(lon, k, m);
+    if (!S::CUR) {
+      const bool ic0 = ccos<R>(k) >= R(0.), is0 = csin<R>(k) >= R(0.);
+      v = c.sum * fk + c.lat11 * F(ic0 ? site.s0 : site.n0, k) + c.lon1 * F(is0 ? site.w0 : site.e0, k);
       if (theta) v = v + c.th1 * fkp + c.th2 * fkm;
-      if (A.reduced) v = v + c.lat12 * F((cs >= R(0.)) ? s1 : n1, k, m);
+      if (RED) v = v + c.lat12 * F(ic0 ? site.s1 : site.n1, k);
     } else {
-      v = c.sum * fk + c.lat21 * F(n0, k, m) + c.lat11 * F(s0, k, m) + c.lon2 * F(e0, k, m) + c.lon1 * F(w0, k, m) +
-          c.th1 * fkp + c.th2 * fkm + c.sg1 * F(i + 1, k, mp) + c.sg2 * F(i + 1, k, mm);
-      if (A.reduced) v = v + c.lat22 * F(n1, k, m) + c.lat12 * F(s1, k, m);
+      const int mm = (m == 0) ? 0 : m - 1, mp = (m == ML - 1) ? ML - 1 : m + 1;
+      const R fmp = __ldg(&f1[i + (size_t)ld1 * k + plane * mp]), fmm = __ldg(&f1[i + (size_t)ld1 * k + plane * mm]);
+      v = c.sum * fk + c.lat21 * F(site.n0, k) + c.lat11 * F(site.s0, k) + c.lon2 * F(site.e0, k) +
+          c.lon1 * F(site.w0, k) + c.th1 * fkp + c.th2 * fkm + c.sg1 * fmp + c.sg2 * fmm;
+      if (RED) v = v + c.lat22 * F(site.n1, k) + c.lat12 * F(site.s1, k);
     }
-    f3[i + (size_t)ld3 * (k + (size_t)KL * m)] = v;
+    out[(size_t)ld3 * k] = v;
     fkm = fk; fk = fkp;
   }
 }
@@ -47,20 +47,20 @@ __global__ void __launch_bounds__(128) propags_kernel(const PropArgs<R> A, const
 __device__ __forceinline__ int f2o(float f) { int i = __float_as_int(f); return i >= 0 ? i : i ^ 0x7fffffff; }
 __device__ __forceinline__ long long d2o(double d) { long long i = __double_as_longlong(d); return i >= 0 ? i : i ^ 0x7fffffffffffffffLL; }
 
-// ext[2*c] = max, ext[2*c+1] = min of coefficient class c (CFL_* below)
-template <typename R>
+// ext[2*c] = max, ext[2*c+1] = min of coefficient class c (CflClass)
+template <typename R, int VAR, bool RED, bool REFRD>
 __global__ void __launch_bounds__(256) cfl_extrema_kernel(const PropArgs<R> A, long long* ext) {
-  const PropCore<R> P(A);
-  const size_t n = (size_t)A.nsea * A.KL * A.ML;
+  const size_t n = (size_t)A.nsea * A.ML;
   R mx[CFL_NCLASS], mn[CFL_NCLASS];
   for (int c = 0; c < CFL_NCLASS; ++c) { mx[c] = R(-1e30); mn[c] = R(1e30); }
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
-    int i = (int)(t % A.nsea);
-    size_t km = t / A.nsea;
-    int k = (int)(km % A.KL), m = (int)(km / A.KL);
-    Coefs<R> c = P.coef(i, k, m);
-    R v[CFL_NCLASS] = {c.lat11, c.lat21, c.lat12, c.lat22, c.lon1, c.lon2, c.th1, c.th2, c.sg1, c.sg2, c.sum};
-    for (int q = 0; q < CFL_NCLASS; ++q) { mx[q] = dmax(mx[q], v[q]); mn[q] = dmin(mn[q], v[q]); }
+    const int i = (int)(t % A.nsea), m = (int)(t / A.nsea);
+    const Site<R, VAR, RED, REFRD> site(A, i, m);
+    for (int k = 0; k < A.KL; ++k) {
+      Coefs<R> c = site.coef(k);
+      R v[CFL_NCLASS] = {c.lat11, c.lat21, c.lat12, c.lat22, c.lon1, c.lon2, c.th1, c.th2, c.sg1, c.sg2, c.sum};
+      for (int q = 0; q < CFL_NCLASS; ++q) { mx[q] = dmax(mx[q], v[q]); mn[q] = dmin(mn[q], v[q]); }
+    }
   }
   for (int q = 0; q < CFL_NCLASS; ++q) {
     mx[q] = warp_max(mx[q]);
@@ -82,22 +82,62 @@ __global__ void cfl_init_kernel(long long* ext) {
   if (q < CFL_NCLASS) { ext[2 * q] = LLONG_MIN; ext[2 * q + 1] = LLONG_MAX; }
 }
 
+template <typename R> cudaError_t set_direction_tables(const R* sinth, const R* costh, int kl);
+template <> cudaError_t set_direction_tables<float>(const float* s, const float* c, int kl) {
+  cudaError_t e = cudaMemcpyToSymbol(c_sinth_f, s, kl * sizeof(float));
+  return e != cudaSuccess ? e : cudaMemcpyToSymbol(c_costh_f, c, kl * sizeof(float));
+}
+template <> cudaError_t set_direction_tables<double>(const double* s, const double* c, int kl) {
+  cudaError_t e = cudaMemcpyToSymbol(c_sinth_d, s, kl * sizeof(double));
+  return e != cudaSuccess ? e : cudaMemcpyToSymbol(c_costh_d, c, kl * sizeof(double));
+}
+
+// Compile-time dispatch over the ten reference variants (eight coefficient
+// families x reduced grid x depth refraction).
+template <typename R, template <typename, int, bool, bool> class K, typename... Args>
+cudaError_t dispatch(const PropArgs<R>& A, Args&&... args) {
+  const bool red = A.reduced != 0, rd = A.refr_d != 0;
+#define VCASE(V)                                                             \
+  case V:                                                                    \
+    if (red) { if (rd) return K<R, V, true, true>::run(A, args...); return K<R, V, true, false>::run(A, args...); } \
+    if (rd) return K<R, V, false, true>::run(A, args...);                    \
+    return K<R, V, false, false>::run(A, args...);
+  switch (A.variant) {
+    VCASE(V_CART_DEEP) VCASE(V_CART_SHALLOW) VCASE(V_CART_DEEP_CUR) VCASE(V_CART_SHALLOW_CUR)
+    VCASE(V_SPHER_DEEP) VCASE(V_SPHER_SHALLOW) VCASE(V_SPHER_DEEP_CURR) VCASE(V_SPHER_SHALLOW_CURR)
+  }
+#undef VCASE
+  return cudaErrorInvalidValue;
+}
+
+template <typename R, int V, bool RED, bool RD> struct PropLaunch {
+  static cudaError_t run(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s) {
+    dim3 grid((A.nsea + 127) / 128, A.ML);
+    propags_kernel<R, V, RED, RD><<<grid, 128, 0, s>>>(A, f1, ld1, f3, ld3);
+    return cudaGetLastError();
+  }
+};
+template <typename R, int V, bool RED, bool RD> struct CflLaunch {
+  static cudaError_t run(const PropArgs<R>& A, long long* ext, int blocks, cudaStream_t s) {
+    cfl_extrema_kernel<R, V, RED, RD><<<blocks, 256, 0, s>>>(A, ext);
+    return cudaGetLastError();
+  }
+};
+
 template <typename R>
 cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s) {
   if (A.nsea == 0) return cudaSuccess;
-  dim3 grid((A.nsea + 127) / 128, A.ML);
-  propags_kernel<R><<<grid, 128, 0, s>>>(A, f1, ld1, f3, ld3);
-  return cudaGetLastError();
+  return dispatch<R, PropLaunch>(A, f1, ld1, f3, ld3, s);
 }
 
 template <typename R>
 cudaError_t launch_cfl_extrema(const PropArgs<R>& A, long long* ext, int nsm, cudaStream_t s) {
   cfl_init_kernel<<<1, 32, 0, s>>>(ext);
-  size_t n = (size_t)A.nsea * A.KL * A.ML;
+  if (A.nsea == 0) return cudaGetLastError();
+  size_t n = (size_t)A.nsea * A.ML;
   int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)nsm * 8);
   if (blocks < 1) blocks = 1;
-  cfl_extrema_kernel<R><<<blocks, 256, 0, s>>>(A, ext);
-  return cudaGetLastError();
+  return dispatch<R, CflLaunch>(A, ext, blocks, s);
 }
 
 double cfl_decode(long long v, int precision) {
@@ -114,5 +154,7 @@ template cudaError_t launch_propags<float>(const PropArgs<float>&, const float*,
 template cudaError_t launch_propags<double>(const PropArgs<double>&, const double*, int, double*, int, cudaStream_t);
 template cudaError_t launch_cfl_extrema<float>(const PropArgs<float>&, long long*, int, cudaStream_t);
 template cudaError_t launch_cfl_extrema<double>(const PropArgs<double>&, long long*, int, cudaStream_t);
+template cudaError_t set_direction_tables<float>(const float*, const float*, int);
+template cudaError_t set_direction_tables<double>(const double*, const double*, int);
 
 }  // namespace wamgpu

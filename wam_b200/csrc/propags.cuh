@@ -22,246 +22,227 @@
 #include <cstdint>
 #include "wamgpu_config.hpp"
 #include "devmath.cuh"
+#include "propargs.hpp"
 
 namespace wamgpu {
-
-enum PropVariant : int {
-  V_CART_DEEP = 0, V_CART_SHALLOW = 1, V_CART_DEEP_CUR = 2, V_CART_SHALLOW_CUR = 3,
-  V_SPHER_DEEP = 4, V_SPHER_SHALLOW = 5, V_SPHER_DEEP_CURR = 6, V_SPHER_SHALLOW_CURR = 7
-};
-
-// Per-sea-point metadata (index i = 0-based local point; neighbour values are
-// 1-based local numbers, 0 = land).  Arrays are of length n_ext (local points
-// followed by halo points) unless noted.
-template <typename R> struct PropArgs {
-  int nsea, ld, KL, ML, variant, reduced, refr_d, spherical, counter, NDEPTH;
-  R DELPH0, DELTH0, DELTHR, DELFR0, rcounter;
-  const int* klat;    // [i + nsea*(ic + 2*j)]   (nsea entries per slot)
-  const int* klon;    // [i + nsea*dir]
-  const R* wlat;      // [i + nsea*ic]
-  const R* dpsn;      // [i + nsea*ic]
-  const R* della0;    // [i]   (variant-specific longitude metric factor)
-  const R* drgm;      // [i]   SINPH*DCO
-  const int* indep;   // [n_ext] depth-table index (1-based), CGOND of point and neighbours
-  const int* indep_g; // [i]   averaged depth index for refraction
-  const R* ddphi;     // [i]   depth gradients (DDLAM already times DCO on spherical grids)
-  const R* ddlam;
-  const R* duphi; const R* dulam; const R* dvphi; const R* dvlam;  // current gradients
-  const R* u; const R* v;    // [n_ext] currents (land slot reads as 0)
-  const R* TCGOND; const R* TSIHKD; const R* TFAK;  // depth tables [(jd-1) + NDEPTH*m]
-  const R* GOM; const R* FR; const R* SINTH; const R* COSTH;  // small tables (global)
-};
 
 template <typename R> struct Coefs {
   R sum, lat11, lat21, lat12, lat22, lon1, lon2, th1, th2, sg1, sg2;
 };
 
-template <typename R> struct PropCore {
+// Direction tables in constant memory: every lane of a warp reads the same
+// direction in the stencil loop, so these are broadcast reads.
+__constant__ float c_sinth_f[MAX_KL], c_costh_f[MAX_KL];
+__constant__ double c_sinth_d[MAX_KL], c_costh_d[MAX_KL];
+template <typename R> __device__ __forceinline__ R csin(int k);
+template <typename R> __device__ __forceinline__ R ccos(int k);
+template <> __device__ __forceinline__ float csin<float>(int k) { return c_sinth_f[k]; }
+template <> __device__ __forceinline__ float ccos<float>(int k) { return c_costh_f[k]; }
+template <> __device__ __forceinline__ double csin<double>(int k) { return c_sinth_d[k]; }
+template <> __device__ __forceinline__ double ccos<double>(int k) { return c_costh_d[k]; }
+
+constexpr bool var_shallow(int v) { return v == V_CART_SHALLOW || v == V_SPHER_SHALLOW || v == V_CART_SHALLOW_CUR || v == V_SPHER_SHALLOW_CURR; }
+constexpr bool var_current(int v) { return v == V_CART_DEEP_CUR || v == V_SPHER_DEEP_CURR || v == V_CART_SHALLOW_CUR || v == V_SPHER_SHALLOW_CURR; }
+constexpr bool var_spher(int v) { return v >= V_SPHER_DEEP; }
+
+// Everything about sea point i at frequency m that does not depend on the
+// direction, loaded once; coef(k) then evaluates the reference's coefficient
+// expressions for one direction.
+template <typename R, int VAR, bool RED, bool REFRD> struct Site {
+  static constexpr bool SH = var_shallow(VAR), CUR = var_current(VAR), SPH = var_spher(VAR);
   const PropArgs<R>& A;
-  __device__ explicit PropCore(const PropArgs<R>& a) : A(a) {}
-  __device__ int klat(int i, int ic, int j) const { return __ldg(&A.klat[i + A.nsea * (ic + 2 * j)]); }
-  __device__ int klon(int i, int d) const { return __ldg(&A.klon[i + A.nsea * d]); }
-  // CGOND of a 1-based local point (0 = land slot: deepest table entry)
-  __device__ R cgond(int p1, int m) const {
+  int i, m, s0, n0, w0, e0, s1, n1;
+  R gom, cg, cgS, cgN, cgW, cgE, cgS1, cgN1, d0, dr, ps, pn, wl1, wl2, tsi, ddphi, ddlam;
+  R duphi, dulam, dvphi, dvlam, u0, uW, uE, v0, vS, vN, vS1, vN1;
+  R dfp, dfm, cgP, cgM, tsiP, tsiM, tfk, tfkP, tfkM, tempc;
+  int mp, mm;
+
+  __device__ R cgond(int p1, int mm_) const {
     int jd = (p1 == 0) ? A.NDEPTH : __ldg(&A.indep[p1 - 1]);
-    return __ldg(&A.TCGOND[(jd - 1) + A.NDEPTH * m]);
+    return __ldg(&A.TCGOND[(jd - 1) + A.NDEPTH * mm_]);
   }
   __device__ R uv(const R* f, int p1) const { return p1 == 0 ? R(0) : __ldg(&f[p1 - 1]); }
 
-  // depth-refraction turning rate THDD(i,k,m) (PREPARE_PROPAGATION :482-492)
-  // plus the current part THDC (:521-536)
-  __device__ R thdd(int i, int k, int m, R tsihkd_g) const {
-    R t = 0;
-    if (A.variant == V_CART_SHALLOW || A.variant == V_SPHER_SHALLOW || A.variant == V_CART_SHALLOW_CUR ||
-        A.variant == V_SPHER_SHALLOW_CURR) {
-      R temp = __ldg(&A.SINTH[k]) * __ldg(&A.ddphi[i]) - __ldg(&A.COSTH[k]) * __ldg(&A.ddlam[i]);
-      t = temp * tsihkd_g;
+  __device__ Site(const PropArgs<R>& a, int i_, int m_) : A(a), i(i_), m(m_) {
+    const int ns = A.nsea;
+    s0 = __ldg(&A.klat[i]); n0 = __ldg(&A.klat[i + ns]);
+    w0 = __ldg(&A.klon[i]); e0 = __ldg(&A.klon[i + ns]);
+    s1 = RED ? __ldg(&A.klat[i + 2 * ns]) : 0; n1 = RED ? __ldg(&A.klat[i + 3 * ns]) : 0;
+    gom = __ldg(&A.GOM[m]);
+    d0 = __ldg(&A.della0[i]);
+    dr = SPH ? __ldg(&A.drgm[i]) : R(0);
+    ps = SPH ? __ldg(&A.dpsn[i]) : R(1); pn = SPH ? __ldg(&A.dpsn[i + ns]) : R(1);
+    wl1 = RED ? __ldg(&A.wlat[i]) : R(1); wl2 = RED ? __ldg(&A.wlat[i + ns]) : R(1);
+    if (SH) {
+      cg = cgond(i + 1, m); cgS = cgond(s0, m); cgN = cgond(n0, m); cgW = cgond(w0, m); cgE = cgond(e0, m);
+      cgS1 = RED ? cgond(s1, m) : R(0); cgN1 = RED ? cgond(n1, m) : R(0);
     }
-    if (A.variant == V_CART_DEEP_CUR || A.variant == V_SPHER_DEEP_CURR || A.variant == V_CART_SHALLOW_CUR ||
-        A.variant == V_SPHER_SHALLOW_CURR) {
-      R sn = __ldg(&A.SINTH[k]), cs = __ldg(&A.COSTH[k]);
+    if (SH && (REFRD || CUR)) {
+      int ig = __ldg(&A.indep_g[i]);
+      tsi = __ldg(&A.TSIHKD[(ig - 1) + A.NDEPTH * m]);
+      ddphi = __ldg(&A.ddphi[i]); ddlam = __ldg(&A.ddlam[i]);
+    }
+    if (CUR) {
+      duphi = __ldg(&A.duphi[i]); dulam = __ldg(&A.dulam[i]); dvphi = __ldg(&A.dvphi[i]); dvlam = __ldg(&A.dvlam[i]);
+      u0 = uv(A.u, i + 1); uW = uv(A.u, w0); uE = uv(A.u, e0);
+      v0 = uv(A.v, i + 1); vS = uv(A.v, s0); vN = uv(A.v, n0);
+      vS1 = RED ? uv(A.v, s1) : R(0); vN1 = RED ? uv(A.v, n1) : R(0);
+      if (SH) {
+        mm = (m == 0) ? 0 : m - 1; mp = (m == A.ML - 1) ? A.ML - 1 : m + 1;
+        dfp = A.DELFR0 / __ldg(&A.FR[m]); dfm = A.DELFR0 / __ldg(&A.FR[mm]);
+        int ig = __ldg(&A.indep_g[i]);
+        cgP = cgond(i + 1, mp); cgM = cgond(i + 1, mm);
+        tsiP = __ldg(&A.TSIHKD[(ig - 1) + A.NDEPTH * mp]); tsiM = __ldg(&A.TSIHKD[(ig - 1) + A.NDEPTH * mm]);
+        tfk = __ldg(&A.TFAK[(ig - 1) + A.NDEPTH * m]); tfkP = __ldg(&A.TFAK[(ig - 1) + A.NDEPTH * mp]);
+        tfkM = __ldg(&A.TFAK[(ig - 1) + A.NDEPTH * mm]);
+        tempc = __ldg(&A.v[i]) * ddphi + __ldg(&A.u[i]) * ddlam;
+      }
+    }
+  }
+
+  // THDD(i,k,m): depth part (PREPARE_PROPAGATION :482-492) plus current part (:521-536)
+  __device__ R thdd(int k) const {
+    R sn = csin<R>(k), cs = ccos<R>(k);
+    R t = R(0);
+    if (SH) t = (sn * ddphi - cs * ddlam) * tsi;
+    if (CUR) {
       R ss = sn * sn, sc = sn * cs, cc = cs * cs;
-      R thdc = ss * __ldg(&A.duphi[i]) + sc * __ldg(&A.dvphi[i]) - sc * __ldg(&A.dulam[i]) - cc * __ldg(&A.dvlam[i]);
-      t = (A.variant == V_CART_DEEP_CUR || A.variant == V_SPHER_DEEP_CURR) ? thdc : t + thdc;
+      R thdc = ss * duphi + sc * dvphi - sc * dulam - cc * dvlam;
+      t = SH ? t + thdc : thdc;
     }
     return t;
   }
-  // frequency shifting rate SIDC(i,k,m) (PREPARE_PROPAGATION :541-563)
-  __device__ R sidc(int i, int k, int m) const {
-    R sd = __ldg(&A.SINTH[k]), cd = __ldg(&A.COSTH[k]);
+  // SIDC(i,k,m') for m' = m, mp, mm (:541-563)
+  __device__ R sidc_base(int k) const {
+    R sd = csin<R>(k), cd = ccos<R>(k);
     R ss = sd * sd, sc = sd * cd, cc = cd * cd;
-    R base = -(sc * __ldg(&A.duphi[i])) - cc * __ldg(&A.dvphi[i]) - ss * __ldg(&A.dulam[i]) - sc * __ldg(&A.dvlam[i]);
-    if (A.variant == V_CART_DEEP_CUR || A.variant == V_SPHER_DEEP_CURR) return base;
-    int ig = __ldg(&A.indep_g[i]);
-    R tempc = __ldg(&A.v[i]) * __ldg(&A.ddphi[i]) + __ldg(&A.u[i]) * __ldg(&A.ddlam[i]);
-    return (base * cgond(i + 1, m) + tempc * __ldg(&A.TSIHKD[(ig - 1) + A.NDEPTH * m])) *
-           __ldg(&A.TFAK[(ig - 1) + A.NDEPTH * m]);
+    return -(sc * duphi) - cc * dvphi - ss * dulam - sc * dvlam;
   }
 
-  // Coefficients of point i (0-based), direction k, frequency m (0-based).
-  __device__ Coefs<R> coef(int i, int k, int m) const {
+  __device__ Coefs<R> coef(int k) const {
     Coefs<R> c = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    const int KL = A.KL, ML = A.ML;
+    const int KL = A.KL;
     const int kp = (k + 1 == KL) ? 0 : k + 1, km = (k == 0) ? KL - 1 : k - 1;
-    const R sn = __ldg(&A.SINTH[k]), cs = __ldg(&A.COSTH[k]);
-    const int IS = (sn >= R(0.)) ? 0 : 1, IT = 1 - IS, IC = (cs >= R(0.)) ? 0 : 1, ID = 1 - IC;
+    const R sn = csin<R>(k), cs = ccos<R>(k);
+    const bool IS0 = sn >= R(0.), IC0 = cs >= R(0.);
     const R z = R(0.);
-    R tsi = 0;
-    if (A.variant == V_CART_SHALLOW || A.variant == V_SPHER_SHALLOW || A.variant == V_CART_SHALLOW_CUR ||
-        A.variant == V_SPHER_SHALLOW_CURR) {
-      if (A.refr_d || A.variant == V_CART_SHALLOW_CUR || A.variant == V_SPHER_SHALLOW_CURR)
-        tsi = __ldg(&A.TSIHKD[(__ldg(&A.indep_g[i]) - 1) + A.NDEPTH * m]);
-    }
-    switch (A.variant) {
-      case V_CART_DEEP: {
-        R dpn = dabs(cs * A.DELPH0 * __ldg(&A.GOM[m]));
-        R sd = dabs(sn * __ldg(&A.GOM[m]));
-        R dle = sd * __ldg(&A.della0[i]);
-        c.sum = R(1.) - dle - dpn; c.lon1 = dle; c.lat11 = dpn;
-      } break;
-      case V_CART_SHALLOW: {
-        R sd = dabs(sn), cd = dabs(cs * A.DELPH0), cg = cgond(i + 1, m), d0 = __ldg(&A.della0[i]);
-        c.lon1 = sd * (cgond(klon(i, IS), m) + cg) * d0;
-        c.lat11 = cd * (cgond(klat(i, IC, 0), m) + cg);
-        c.sum = R(1.) - sd * (cgond(klon(i, IT), m) + cg) * d0 - cd * (cgond(klat(i, ID, 0), m) + cg);
-        if (A.refr_d) {
-          R t0 = thdd(i, k, m, tsi);
-          R dtp = (t0 + thdd(i, kp, m, tsi)) * A.DELTHR, dtm = (t0 + thdd(i, km, m, tsi)) * A.DELTHR;
-          c.sum = c.sum - dmax(z, dtp) + dmin(z, dtm);
-          c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
-        }
-      } break;
-      case V_CART_DEEP_CUR:
-      case V_SPHER_DEEP_CURR: {
-        const bool sph = A.variant == V_SPHER_DEEP_CURR;
-        R gom = __ldg(&A.GOM[m]);
-        R cgs = gom * sn, cgc = gom * cs, d0 = __ldg(&A.della0[i]);
-        auto wok1 = [&](int p) { return uv(A.u, p) + cgs; };
-        auto wok2 = [&](int p) { return (uv(A.v, p) + cgc) * A.DELPH0; };
-        R w1 = wok1(i + 1), w2 = wok2(i + 1);
-        R dlw = (w1 + wok1(klon(i, 0))) * d0, dle = (w1 + wok1(klon(i, 1))) * d0;
-        R dtc = R(1.) - dmax(z, dle) + dmin(z, dlw);
-        c.lon2 = -dmin(z, dle); c.lon1 = dmax(z, dlw);
-        if (!sph) {
-          R dps = w2 + wok2(klat(i, 0, 0)), dpn = w2 + wok2(klat(i, 1, 0));
-          dtc = dtc - dmax(z, dpn) + dmin(z, dps);
-          c.lat21 = -dmin(z, dpn); c.lat11 = dmax(z, dps);
-        } else if (A.reduced) {
-          R wl1 = __ldg(&A.wlat[i]), wl2 = __ldg(&A.wlat[i + A.nsea]);
-          R p1 = __ldg(&A.dpsn[i]), p2 = __ldg(&A.dpsn[i + A.nsea]);
-          R dps = (w2 + wok2(klat(i, 0, 0)) * p1) * wl1, dps2 = (w2 + wok2(klat(i, 0, 1)) * p1) * (R(1.) - wl1);
-          R dpn = (w2 + wok2(klat(i, 1, 0)) * p2) * wl2, dpn2 = (w2 + wok2(klat(i, 1, 1)) * p2) * (R(1.) - wl2);
-          dtc = dtc - dmax(z, dpn) - dmax(z, dpn2) + dmin(z, dps) + dmin(z, dps2);
-          c.lat21 = -dmin(z, dpn); c.lat22 = -dmin(z, dpn2); c.lat11 = dmax(z, dps); c.lat12 = dmax(z, dps2);
-        } else {
-          R dps = w2 + wok2(klat(i, 0, 0)) * __ldg(&A.dpsn[i]);
-          R dpn = w2 + wok2(klat(i, 1, 0)) * __ldg(&A.dpsn[i + A.nsea]);
-          dtc = dtc - dmax(z, dpn) + dmin(z, dps);
-          c.lat11 = dmax(z, dps); c.lat21 = -dmin(z, dpn);
-        }
-        R t0 = thdd(i, k, ML - 1, tsi), tp = thdd(i, kp, ML - 1, tsi), tm = thdd(i, km, ML - 1, tsi);
-        R dtp, dtm;
-        if (sph) {
-          R sp = A.DELTH0 * (sn + __ldg(&A.SINTH[kp])) * gom, sm = A.DELTH0 * (sn + __ldg(&A.SINTH[km])) * gom;
-          R dr = __ldg(&A.drgm[i]);
-          dtp = sp * dr + (t0 + tp) * A.DELTHR; dtm = sm * dr + (t0 + tm) * A.DELTHR;
-        } else {
-          dtp = (t0 + tp) * A.DELTHR; dtm = (t0 + tm) * A.DELTHR;
-        }
-        dtc = dtc - dmax(z, dtp) + dmin(z, dtm);
+    if (VAR == V_CART_DEEP) {
+      R dpn = dabs(cs * A.DELPH0 * gom);
+      R sd = dabs(sn * gom);
+      R dle = sd * d0;
+      c.sum = R(1.) - dle - dpn; c.lon1 = dle; c.lat11 = dpn;
+    } else if (VAR == V_CART_SHALLOW) {
+      R sd = dabs(sn), cd = dabs(cs * A.DELPH0);
+      c.lon1 = sd * ((IS0 ? cgW : cgE) + cg) * d0;
+      c.lat11 = cd * ((IC0 ? cgS : cgN) + cg);
+      c.sum = R(1.) - sd * ((IS0 ? cgE : cgW) + cg) * d0 - cd * ((IC0 ? cgN : cgS) + cg);
+      if (REFRD) {
+        R t0 = thdd(k);
+        R dtp = (t0 + thdd(kp)) * A.DELTHR, dtm = (t0 + thdd(km)) * A.DELTHR;
+        c.sum = c.sum - dmax(z, dtp) + dmin(z, dtm);
         c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
-        R dom = sidc(i, k, ML - 1) * A.DELFR0;
-        c.sum = dtc - dabs(dom);
-        c.sg1 = -dmin(z, dom) / R(1.1); c.sg2 = dmax(z, dom) * R(1.1);
-      } break;
-      case V_CART_SHALLOW_CUR:
-      case V_SPHER_SHALLOW_CURR: {
-        const bool sph = A.variant == V_SPHER_SHALLOW_CURR;
-        const int mm = (m == 0) ? 0 : m - 1, mp = (m == ML - 1) ? ML - 1 : m + 1;
-        R dfp = A.DELFR0 / __ldg(&A.FR[m]), dfm = A.DELFR0 / __ldg(&A.FR[mm]);
-        R d0 = __ldg(&A.della0[i]);
-        auto wok1 = [&](int p) { return uv(A.u, p) + sn * cgond(p, m); };
-        auto wok2 = [&](int p) { return (uv(A.v, p) + cs * cgond(p, m)) * A.DELPH0; };
-        R w1 = wok1(i + 1), w2 = wok2(i + 1);
-        R dlw = (w1 + wok1(klon(i, 0))) * d0, dle = (w1 + wok1(klon(i, 1))) * d0;
-        R dtc = R(1.) - dmax(z, dle) + dmin(z, dlw);
-        c.lon1 = dmax(z, dlw); c.lon2 = -dmin(z, dle);
-        if (!sph) {
-          R dps = w2 + wok2(klat(i, 0, 0)), dpn = w2 + wok2(klat(i, 1, 0));
-          dtc = dtc - dmax(z, dpn) + dmin(z, dps);
-          c.lat11 = dmax(z, dps); c.lat21 = -dmin(z, dpn);
-        } else if (A.reduced) {
-          R wl1 = __ldg(&A.wlat[i]), wl2 = __ldg(&A.wlat[i + A.nsea]);
-          R dps = w2 + __ldg(&A.dpsn[i]) * (wl1 * wok2(klat(i, 0, 0)) + (R(1.) - wl1) * wok2(klat(i, 0, 1)));
-          R dps2 = dps * (R(1.) - wl1); dps = dps * wl1;
-          R dpn = w2 + __ldg(&A.dpsn[i + A.nsea]) * (wl2 * wok2(klat(i, 1, 0)) + (R(1.) - wl2) * wok2(klat(i, 1, 1)));
-          R dpn2 = dpn * (R(1.) - wl2); dpn = dpn * wl2;
-          dtc = dtc - dmax(z, dpn) - dmax(z, dpn2) + dmin(z, dps) + dmin(z, dps2);
-          c.lat11 = dmax(z, dps); c.lat12 = dmax(z, dps2); c.lat21 = -dmin(z, dpn); c.lat22 = -dmin(z, dpn2);
-        } else {
-          R dps = w2 + __ldg(&A.dpsn[i]) * wok2(klat(i, 0, 0));
-          R dpn = w2 + __ldg(&A.dpsn[i + A.nsea]) * wok2(klat(i, 1, 0));
-          dtc = dtc - dmax(z, dpn) + dmin(z, dps);
-          c.lat11 = dmax(z, dps); c.lat21 = -dmin(z, dpn);
-        }
-        R t0 = thdd(i, k, m, tsi), tp = thdd(i, kp, m, tsi), tm = thdd(i, km, m, tsi);
-        R dtp, dtm;
-        if (sph) {
-          R sp = A.DELTH0 * (sn + __ldg(&A.SINTH[kp])), sm = A.DELTH0 * (sn + __ldg(&A.SINTH[km]));
-          R dr = __ldg(&A.drgm[i]), cg = cgond(i + 1, m);
-          dtp = sp * dr * cg + (t0 + tp) * A.DELTHR; dtm = sm * dr * cg + (t0 + tm) * A.DELTHR;
-        } else {
-          dtp = (t0 + tp) * A.DELTHR; dtm = (t0 + tm) * A.DELTHR;
-        }
-        dtc = dtc - dmax(z, dtp) + dmin(z, dtm);
-        c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
-        R s0 = sidc(i, k, m);
-        R dop = (s0 + sidc(i, k, mp)) * dfp, dom = (s0 + sidc(i, k, mm)) * dfm;
-        c.sg1 = -dmin(z, dop) / R(1.1); c.sg2 = dmax(z, dom) * R(1.1);
-        c.sum = sph ? (dtc - dmax(z, dop) + dmin(z, dom)) : (dtc - dmax(z, dop) + dmin(z, dom));
-      } break;
-      case V_SPHER_DEEP: {
-        R sda = dabs(sn), cda = dabs(cs * A.DELPH0);
-        R sp = A.DELTH0 * (sn + __ldg(&A.SINTH[kp])), sm = A.DELTH0 * (sn + __ldg(&A.SINTH[km]));
-        R gom = __ldg(&A.GOM[m]);
-        R dpn = cda * (__ldg(&A.dpsn[i + A.nsea * IC]) + R(1.));
-        R dle = sda * __ldg(&A.della0[i]);
-        R dtc = cda * (__ldg(&A.dpsn[i + A.nsea * ID]) + R(1.)) + dle;
-        R dr = __ldg(&A.drgm[i]);
-        R dtp = dr * sp, dtm = dr * sm;
-        dtc = dtc + dmax(z, dtp) - dmin(z, dtm);
-        c.lat11 = gom * dpn; c.lon1 = gom * dle;
-        c.th1 = -(gom * dmin(z, dtp)); c.th2 = gom * dmax(z, dtm);
-        c.sum = R(1.) - gom * dtc;
-        if (A.reduced) { R wl = __ldg(&A.wlat[i + A.nsea * IC]); c.lat12 = c.lat11 * (R(1.) - wl); c.lat11 = c.lat11 * wl; }
-      } break;
-      case V_SPHER_SHALLOW: {
-        R sda = dabs(sn), cda = dabs(cs * A.DELPH0);
-        R sp = A.DELTH0 * (sn + __ldg(&A.SINTH[kp])), sm = A.DELTH0 * (sn + __ldg(&A.SINTH[km]));
-        R cg = cgond(i + 1, m), d0 = __ldg(&A.della0[i]);
-        auto cgklat = [&](int ic) {
-          R p = __ldg(&A.dpsn[i + A.nsea * ic]);
-          if (A.reduced) {
-            R wl = __ldg(&A.wlat[i + A.nsea * ic]);
-            return cg + p * (wl * cgond(klat(i, ic, 0), m) + (R(1.) - wl) * cgond(klat(i, ic, 1), m));
-          }
-          return cg + p * cgond(klat(i, ic, 0), m);
-        };
-        R dtc = R(1.) - cda * cgklat(ID);
-        c.lat11 = cda * cgklat(IC);
-        dtc = dtc - sda * (cgond(klon(i, IT), m) + cg) * d0;
-        c.lon1 = sda * (cgond(klon(i, IS), m) + cg) * d0;
-        R dtp = __ldg(&A.drgm[i]) * cg, dtm;
-        if (A.refr_d) {
-          R t0 = thdd(i, k, m, tsi);
-          dtm = dtp * sm + (t0 + thdd(i, km, m, tsi)) * A.DELTHR;
-          dtp = dtp * sp + (t0 + thdd(i, kp, m, tsi)) * A.DELTHR;
-        } else { dtm = dtp * sm; dtp = dtp * sp; }
-        dtc = dtc - dmax(z, dtp) + dmin(z, dtm);
-        c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
-        c.sum = dtc;
-        if (A.reduced) { R wl = __ldg(&A.wlat[i + A.nsea * IC]); c.lat12 = c.lat11 * (R(1.) - wl); c.lat11 = c.lat11 * wl; }
-      } break;
+      }
+    } else if (VAR == V_SPHER_DEEP) {
+      R sda = dabs(sn), cda = dabs(cs * A.DELPH0);
+      R sp = A.DELTH0 * (sn + csin<R>(kp)), sm = A.DELTH0 * (sn + csin<R>(km));
+      R dpn = cda * ((IC0 ? ps : pn) + R(1.));
+      R dle = sda * d0;
+      R dtc = cda * ((IC0 ? pn : ps) + R(1.)) + dle;
+      R dtp = dr * sp, dtm = dr * sm;
+      dtc = dtc + dmax(z, dtp) - dmin(z, dtm);
+      c.lat11 = gom * dpn; c.lon1 = gom * dle;
+      c.th1 = -(gom * dmin(z, dtp)); c.th2 = gom * dmax(z, dtm);
+      c.sum = R(1.) - gom * dtc;
+      if (RED) { R wl = IC0 ? wl1 : wl2; c.lat12 = c.lat11 * (R(1.) - wl); c.lat11 = c.lat11 * wl; }
+    } else if (VAR == V_SPHER_SHALLOW) {
+      R sda = dabs(sn), cda = dabs(cs * A.DELPH0);
+      R sp = A.DELTH0 * (sn + csin<R>(kp)), sm = A.DELTH0 * (sn + csin<R>(km));
+      R cgk1, cgk2;  // CGKLAT(IJ,M,1) south and (IJ,M,2) north
+      if (RED) {
+        cgk1 = cg + ps * (wl1 * cgS + (R(1.) - wl1) * cgS1);
+        cgk2 = cg + pn * (wl2 * cgN + (R(1.) - wl2) * cgN1);
+      } else { cgk1 = cg + ps * cgS; cgk2 = cg + pn * cgN; }
+      R dtc = R(1.) - cda * (IC0 ? cgk2 : cgk1);
+      c.lat11 = cda * (IC0 ? cgk1 : cgk2);
+      dtc = dtc - sda * ((IS0 ? cgE : cgW) + cg) * d0;
+      c.lon1 = sda * ((IS0 ? cgW : cgE) + cg) * d0;
+      R dtp = dr * cg, dtm;
+      if (REFRD) {
+        R t0 = thdd(k);
+        dtm = dtp * sm + (t0 + thdd(km)) * A.DELTHR;
+        dtp = dtp * sp + (t0 + thdd(kp)) * A.DELTHR;
+      } else { dtm = dtp * sm; dtp = dtp * sp; }
+      dtc = dtc - dmax(z, dtp) + dmin(z, dtm);
+      c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
+      c.sum = dtc;
+      if (RED) { R wl = IC0 ? wl1 : wl2; c.lat12 = c.lat11 * (R(1.) - wl); c.lat11 = c.lat11 * wl; }
+    } else if (VAR == V_CART_DEEP_CUR || VAR == V_SPHER_DEEP_CURR) {
+      R cgs = gom * sn, cgc = gom * cs;
+      R w1 = u0 + cgs, w2 = (v0 + cgc) * A.DELPH0;
+      R dlw = (w1 + (uW + cgs)) * d0, dle = (w1 + (uE + cgs)) * d0;
+      R dtc = R(1.) - dmax(z, dle) + dmin(z, dlw);
+      c.lon2 = -dmin(z, dle); c.lon1 = dmax(z, dlw);
+      auto wok2 = [&](R vv) { return (vv + cgc) * A.DELPH0; };
+      if (!SPH) {
+        R dps = w2 + wok2(vS), dpn = w2 + wok2(vN);
+        dtc = dtc - dmax(z, dpn) + dmin(z, dps);
+        c.lat21 = -dmin(z, dpn); c.lat11 = dmax(z, dps);
+      } else if (RED) {
+        R dps = (w2 + wok2(vS) * ps) * wl1, dps2 = (w2 + wok2(vS1) * ps) * (R(1.) - wl1);
+        R dpn = (w2 + wok2(vN) * pn) * wl2, dpn2 = (w2 + wok2(vN1) * pn) * (R(1.) - wl2);
+        dtc = dtc - dmax(z, dpn) - dmax(z, dpn2) + dmin(z, dps) + dmin(z, dps2);
+        c.lat21 = -dmin(z, dpn); c.lat22 = -dmin(z, dpn2); c.lat11 = dmax(z, dps); c.lat12 = dmax(z, dps2);
+      } else {
+        R dps = w2 + wok2(vS) * ps, dpn = w2 + wok2(vN) * pn;
+        dtc = dtc - dmax(z, dpn) + dmin(z, dps);
+        c.lat11 = dmax(z, dps); c.lat21 = -dmin(z, dpn);
+      }
+      R t0 = thdd(k), tp = thdd(kp), tm = thdd(km);
+      R dtp, dtm;
+      if (SPH) {
+        R sp = A.DELTH0 * (sn + csin<R>(kp)) * gom, sm = A.DELTH0 * (sn + csin<R>(km)) * gom;
+        dtp = sp * dr + (t0 + tp) * A.DELTHR; dtm = sm * dr + (t0 + tm) * A.DELTHR;
+      } else { dtp = (t0 + tp) * A.DELTHR; dtm = (t0 + tm) * A.DELTHR; }
+      dtc = dtc - dmax(z, dtp) + dmin(z, dtm);
+      c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
+      R dom = sidc_base(k) * A.DELFR0;
+      c.sum = dtc - dabs(dom);
+      c.sg1 = -dmin(z, dom) / R(1.1); c.sg2 = dmax(z, dom) * R(1.1);
+    } else {  // V_CART_SHALLOW_CUR, V_SPHER_SHALLOW_CURR
+      R w1 = u0 + sn * cg, w2 = (v0 + cs * cg) * A.DELPH0;
+      R dlw = (w1 + (uW + sn * cgW)) * d0, dle = (w1 + (uE + sn * cgE)) * d0;
+      R dtc = R(1.) - dmax(z, dle) + dmin(z, dlw);
+      c.lon1 = dmax(z, dlw); c.lon2 = -dmin(z, dle);
+      auto wok2 = [&](R vv, R cgv) { return (vv + cs * cgv) * A.DELPH0; };
+      if (!SPH) {
+        R dps = w2 + wok2(vS, cgS), dpn = w2 + wok2(vN, cgN);
+        dtc = dtc - dmax(z, dpn) + dmin(z, dps);
+        c.lat11 = dmax(z, dps); c.lat21 = -dmin(z, dpn);
+      } else if (RED) {
+        R dps = w2 + ps * (wl1 * wok2(vS, cgS) + (R(1.) - wl1) * wok2(vS1, cgS1));
+        R dps2 = dps * (R(1.) - wl1); dps = dps * wl1;
+        R dpn = w2 + pn * (wl2 * wok2(vN, cgN) + (R(1.) - wl2) * wok2(vN1, cgN1));
+        R dpn2 = dpn * (R(1.) - wl2); dpn = dpn * wl2;
+        dtc = dtc - dmax(z, dpn) - dmax(z, dpn2) + dmin(z, dps) + dmin(z, dps2);
+        c.lat11 = dmax(z, dps); c.lat12 = dmax(z, dps2); c.lat21 = -dmin(z, dpn); c.lat22 = -dmin(z, dpn2);
+      } else {
+        R dps = w2 + ps * wok2(vS, cgS), dpn = w2 + pn * wok2(vN, cgN);
+        dtc = dtc - dmax(z, dpn) + dmin(z, dps);
+        c.lat11 = dmax(z, dps); c.lat21 = -dmin(z, dpn);
+      }
+      R t0 = thdd(k), tp = thdd(kp), tm = thdd(km);
+      R dtp, dtm;
+      if (SPH) {
+        R sp = A.DELTH0 * (sn + csin<R>(kp)), sm = A.DELTH0 * (sn + csin<R>(km));
+        dtp = sp * dr * cg + (t0 + tp) * A.DELTHR; dtm = sm * dr * cg + (t0 + tm) * A.DELTHR;
+      } else { dtp = (t0 + tp) * A.DELTHR; dtm = (t0 + tm) * A.DELTHR; }
+      dtc = dtc - dmax(z, dtp) + dmin(z, dtm);
+      c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
+      R b = sidc_base(k);
+      R s0v = (b * cg + tempc * tsi) * tfk, sPv = (b * cgP + tempc * tsiP) * tfkP, sMv = (b * cgM + tempc * tsiM) * tfkM;
+      R dop = (s0v + sPv) * dfp, dom = (s0v + sMv) * dfm;
+      c.sg1 = -dmin(z, dop) / R(1.1); c.sg2 = dmax(z, dom) * R(1.1);
+      c.sum = dtc - dmax(z, dop) + dmin(z, dom);
     }
     if (A.counter != 1) {  // CHECK_CFL sub-stepping rescale :2126-2134
       const R rc = A.rcounter;
