@@ -124,10 +124,30 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
   auto putr = [&](int& off, const std::vector<R>& v) { off = (int)sr.size(); sr.insert(sr.end(), v.begin(), v.end()); };
   std::vector<R> delfl(t.ML);
   for (int m = 0; m < t.ML; ++m) delfl[m] = R(5.0E-07) * Phys<R>::G / powi(t.FR[m], 4) * R(c.idelt);
+  // ST6 frequency axis extended to 10 Hz and its bandwidths (LFACTOR :4554-4599)
+  int nk10;
+  {
+    const R sig1 = Phys<R>::ZPI * t.FR[0];
+    nk10 = (int)std::ceil(std::log(R(10.) / (sig1 / Phys<R>::ZPI)) / std::log(Phys<R>::CO)) + 1;
+    nk10 = std::max(t.ML, nk10);
+  }
+  std::vector<R> sig10(nk10), dsii10(nk10);
+  {
+    const R co = Phys<R>::CO, sig1 = Phys<R>::ZPI * t.FR[0];
+    if (t.ML < nk10) {
+      for (int i = 0; i < nk10; ++i) sig10[i] = sig1 * std::pow(co, R(i + 1) - R(1.0));
+      for (int i = 0; i < nk10; ++i) dsii10[i] = R(0.5) * sig10[i] * (co - R(1.0) / co);
+      dsii10[0] = R(0.5) * sig10[0] * (co - R(1.0));
+      dsii10[nk10 - 1] = R(0.5) * sig10[nk10 - 1] * (co - R(1.0)) / co;
+    } else {
+      for (int i = 0; i < nk10; ++i) { sig10[i] = Phys<R>::ZPI * t.FR[i]; dsii10[i] = Phys<R>::ZPI * t.DF[i]; }
+    }
+  }
   putr(L.FR, t.FR); putr(L.DF, t.DF); putr(L.DFIM, t.DFIM); putr(L.DFIMOFR, t.DFIMOFR); putr(L.FR5, t.FR5);
   putr(L.FRM5, t.FRM5); putr(L.RHOWG_DFIM, t.RHOWG_DFIM); putr(L.TH, t.TH); putr(L.COSTH, t.COSTH);
   putr(L.SINTH, t.SINTH); putr(L.DELFL, delfl); putr(L.AF11, t.AF11); putr(L.RNLCOEF, t.RNLCOEF);
   putr(L.SATW, t.SATWEIGHTS); putr(L.WTAUHF, t.WTAUHF); putr(L.SWELLFT, t.SWELLFT);
+  putr(L.SIG10, sig10); putr(L.DSII10, dsii10);
   L.nreal = (int)sr.size();
   std::vector<int> si;
   auto puti = [&](int& off, const std::vector<int>& v) { off = (int)si.size(); si.insert(si.end(), v.begin(), v.end()); };
@@ -148,11 +168,10 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
   DevTables<R>& d = I.dt;
   d.KL = t.KL; d.ML = t.ML; d.NS = t.KL * t.ML; d.NDEPTH = t.NDEPTH; d.MFRSTLW = t.MFRSTLW; d.MLSTHG = t.MLSTHG;
   d.KFRH = t.KFRH; d.NSDSNTH = t.NSDSNTH;
-  {
-    const R sig1 = Phys<R>::ZPI * t.FR[0];
-    int nk10 = (int)std::ceil(std::log(R(10.) / (sig1 / Phys<R>::ZPI)) / std::log(Phys<R>::CO)) + 1;
-    d.NK10 = std::max(t.ML, nk10);
-  }
+  d.NK10 = nk10;
+  d.ld = t.KL | 1;
+  d.scr = (std::max(std::max(t.ML, t.KL), nk10) + 31) / 32 * 32;
+  d.need_sp = c.lcflx ? 1 : 0;
   d.iphys = c.iphys; d.shallow = c.shallow_run; d.isnonlin = c.isnonlin; d.lcflx = c.lcflx;
   d.DELTH = t.DELTH; d.DELTR = t.DELTR; d.INV_LOG_CO = t.INV_LOG_CO; d.MO_TAIL = t.MO_TAIL; d.MM1_TAIL = t.MM1_TAIL;
   d.DELU = t.DELU; d.DAL1 = t.DAL1; d.DAL2 = t.DAL2; d.X0TAUHF = t.X0TAUHF;
@@ -180,20 +199,35 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
       else if (mc >= mfrl) ok = in(MM) && (MM1 > ML || (in(MM1) && (mc > ML || (in(mc) && (MP > ML || (in(MP) && (MP1 > ML || in(MP1))))))));
       else ok = (MM1 < 1 || in(MM1)) && in(mc) && in(MP) && in(MP1);
       if (!ok) return fail(ctx, WAMGPU_E_ARG, "DIA scatter target outside the spectrum");
+      // the kernel updates the rows MC, MM, MM1, MP, MP1 of one phase without
+      // ordering between them: they must be distinct
+      int rows[5] = {mc, MM, MM1, MP, MP1};
+      for (int x = 0; x < 5; ++x)
+        for (int y = x + 1; y < 5; ++y)
+          if (rows[x] == rows[y] && in(rows[x]) && in(rows[y]))
+            return fail(ctx, WAMGPU_E_ARG, "DIA target rows coincide; unsupported frequency ratio");
     }
   }
-  // CTA shape: the largest of 8/4/2 points whose workspace fits the opt-in shared memory
+  // CTA shape: the number of sea points per CTA that keeps the most warps
+  // resident per SM under the shared-memory budget (ties go to larger CTAs,
+  // whose spectrum loads use longer contiguous runs)
   int dev = c.device;
-  int maxsm = 0;
+  int maxsm = 0, smpersm = 0;
   CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev), "device attribute");
-  int choices[3] = {8, 4, 2};
+  CK(cudaDeviceGetAttribute(&smpersm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev), "device attribute");
+  const int choices_f[3] = {8, 6, 4}, choices_d[2] = {4, 2};
+  const int* choices = sizeof(R) == 4 ? choices_f : choices_d;
+  const int nchoice = sizeof(R) == 4 ? 3 : 2;
   ctx->P = 0;
-  for (int P : choices) {
-    if (sizeof(R) == 8 && P == 8) continue;
-    if (sizeof(R) == 4 && P == 2) continue;
+  int best_warps = 0;
+  for (int q = 0; q < nchoice; ++q) {
+    int P = choices[q];
     size_t need = implsch_smem_bytes(d, P);
-    if ((int)need <= maxsm) { ctx->P = P; CK(implsch_set_max_smem<R>(P, need), "smem attribute"); break; }
+    if ((int)need > maxsm) continue;
+    int ctas = std::min(32 / P, (int)(smpersm / (need + 1024)));
+    if (P * ctas > best_warps) { best_warps = P * ctas; ctx->P = P; }
   }
+  if (ctx->P) CK(implsch_set_max_smem<R>(ctx->P, implsch_smem_bytes(d, ctx->P)), "smem attribute");
   if (!ctx->P) return fail(ctx, WAMGPU_E_ARG, "spectrum too large for the shared-memory workspace");
   CK(cudaStreamSynchronize(s), "table upload");
   return WAMGPU_OK;

@@ -18,14 +18,15 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
   const int tid = threadIdx.x, nthr = blockDim.x;
   for (int i = tid; i < T.lay.nreal; i += nthr) sR[i] = T.small[i];
   for (int i = tid; i < T.lay.nint; i += nthr) sI[i] = T.ismall[i];
-  const int NS = T.NS;
-  const size_t wsb = warp_ws_bytes<R>(NS);
+  const int NS = T.NS, KL = T.KL, LD = T.ld;
+  const size_t wsb = warp_ws_bytes<R>(LD, T.ML, T.need_sp, T.scr);
   unsigned char* ws0 = smem + tables_bytes<R>(T.lay);
   const int ij0 = blockIdx.x * P;
   // stage the P spectra: consecutive threads take consecutive points of one bin
   for (int idx = tid; idx < P * NS; idx += nthr) {
     int p = idx % P, b = idx / P, ij = ij0 + p;
-    if (ij < a.nsea) reinterpret_cast<R*>(ws0 + p * wsb)[b] = a.fl3_in[ij + (size_t)a.ld * b];
+    int m = b / KL, k = b - m * KL;
+    if (ij < a.nsea) reinterpret_cast<R*>(ws0 + p * wsb)[k + LD * m] = a.fl3_in[ij + (size_t)a.ld * b];
   }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, ij = ij0 + warp;
@@ -34,9 +35,13 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
     S.bind(sR, sI, T.lay);
     WarpWS<R> w;
     unsigned char* base = ws0 + warp * wsb;
+    const int nrow = LD * T.ML;
+    w.ld = LD; w.scr = T.scr;
     w.F = reinterpret_cast<R*>(base);
-    w.SL = w.F + NS; w.FL = w.SL + NS; w.SP = w.FL + NS; w.T = w.SP + NS;
-    w.LL = reinterpret_cast<uint8_t*>(w.T + 8 * SCR);
+    w.SL = w.F + nrow; w.FL = w.SL + nrow;
+    w.SP = T.need_sp ? w.FL + nrow : nullptr;
+    w.T = w.FL + nrow * (T.need_sp ? 2 : 1);
+    w.LL = reinterpret_cast<uint8_t*>(w.T + 8 * T.scr);
     Src<R> src(T, S, w, lane, ij, a.indep[ij], a.u10[ij], a.udir[ij], a.roairn[ij], a.wstar[ij], a.depth[ij]);
     PointState<R> ps;
     ps.TAUW = a.tauw[ij];
@@ -51,8 +56,9 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
   __syncthreads();
   for (int idx = tid; idx < P * NS; idx += nthr) {
     int p = idx % P, b = idx / P, ijs = ij0 + p;
+    int m = b / KL, k = b - m * KL;
     if (ijs < a.nsea) {
-      R v = reinterpret_cast<R*>(ws0 + p * wsb)[b];
+      R v = reinterpret_cast<R*>(ws0 + p * wsb)[k + LD * m];
       a.fl3[ijs + (size_t)a.ld * b] = v;
       if (!isfinite(v)) atomicOr(a.status, 1);
     }
@@ -60,28 +66,42 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
 }
 
 template <typename R> size_t implsch_smem_bytes(const DevTables<R>& T, int P) {
-  return tables_bytes<R>(T.lay) + (size_t)P * warp_ws_bytes<R>(T.NS);
+  return tables_bytes<R>(T.lay) + (size_t)P * warp_ws_bytes<R>(T.ld, T.ML, T.need_sp, T.scr);
 }
 
-// CTA shapes compiled: FP32 with 4 or 8 points per CTA, FP64 with 2 or 4.
-template <typename R> constexpr int p_small() { return sizeof(R) == 4 ? 4 : 2; }
-template <typename R> constexpr int p_large() { return sizeof(R) == 4 ? 8 : 4; }
+// CTA shapes compiled: FP32 with 4, 6 or 8 sea points per CTA, FP64 with 2 or 4.
+template <typename R, int P> cudaError_t set_smem_one(size_t bytes) {
+  return cudaFuncSetAttribute(implsch_kernel<R, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+template <typename R, int P> void launch_one(const DevTables<R>& T, const ImplArgs<R>& a, size_t smem, cudaStream_t s) {
+  implsch_kernel<R, P><<<(a.nsea + P - 1) / P, P * 32, smem, s>>>(T, a);
+}
 
 template <typename R> cudaError_t implsch_set_max_smem(int P, size_t bytes) {
-  if (P == p_small<R>())
-    return cudaFuncSetAttribute(implsch_kernel<R, p_small<R>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (P == p_large<R>())
-    return cudaFuncSetAttribute(implsch_kernel<R, p_large<R>()>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (sizeof(R) == 4) {
+    if (P == 4) return set_smem_one<R, 4>(bytes);
+    if (P == 6) return set_smem_one<R, 6>(bytes);
+    if (P == 8) return set_smem_one<R, 8>(bytes);
+  } else {
+    if (P == 2) return set_smem_one<R, 2>(bytes);
+    if (P == 4) return set_smem_one<R, 4>(bytes);
+  }
   return cudaErrorInvalidValue;
 }
 
 template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const ImplArgs<R>& a, int P, cudaStream_t s) {
   if (a.nsea == 0) return cudaSuccess;
   size_t smem = implsch_smem_bytes(T, P);
-  int grid = (a.nsea + P - 1) / P;
-  if (P == p_small<R>()) implsch_kernel<R, p_small<R>()><<<grid, p_small<R>() * 32, smem, s>>>(T, a);
-  else if (P == p_large<R>()) implsch_kernel<R, p_large<R>()><<<grid, p_large<R>() * 32, smem, s>>>(T, a);
-  else return cudaErrorInvalidValue;
+  if (sizeof(R) == 4) {
+    if (P == 4) launch_one<R, 4>(T, a, smem, s);
+    else if (P == 6) launch_one<R, 6>(T, a, smem, s);
+    else if (P == 8) launch_one<R, 8>(T, a, smem, s);
+    else return cudaErrorInvalidValue;
+  } else {
+    if (P == 2) launch_one<R, 2>(T, a, smem, s);
+    else if (P == 4) launch_one<R, 4>(T, a, smem, s);
+    else return cudaErrorInvalidValue;
+  }
   return cudaGetLastError();
 }
 

@@ -3,24 +3,31 @@
 // layout) into shared memory together with the static tables, and each warp
 // then runs the reference's per-point statement sequence with its 32 lanes
 // spread over directions, frequencies or spectral bins; spectral integrals
-// and stresses are warp-shuffle reductions.  The DIA runs quadruplet by
-// quadruplet with lanes over directions: for fixed (MC,KH) the nine target
-// bins of different lanes are distinct (K1W..K21W are rotations), so each
-// target update is one conflict-free shared-memory step followed by
-// __syncwarp.
+// and stresses are warp-shuffle reductions.
+//
+// Shared-memory rows of a point's spectrum use an odd stride ld >= KL, so
+// lanes walking different frequencies of the same direction hit distinct
+// banks.  The DIA runs quadruplet by quadruplet with lanes over directions:
+// for fixed (MC,KH) the targets of different lanes within one target family
+// are distinct (K1W..K21W are rotations) and the five frequency rows of a
+// phase are distinct, so each of the two update phases is conflict-free and
+// only the phases are separated by __syncwarp.
 //
 // Routine map (myWAveModel/WAM wam_source_module.f90 unless noted):
-//   IMPLSCH :374-700        implsch_point
+//   IMPLSCH :374-700        Src::run
 //   SINPUT_ARD :2312-2738   sinput_ard        SINPUT_ST6 :4704-4925   sinput_st6
-//   LFACTOR :4465-4700      st6_lfactor       TAU_WAVE_ATMOS :5258    st6_taunw
+//   LFACTOR :4465-4700      sinput_st6        TAUWINDS :5555-5587     sinput_st6
 //   SDISSIP_ARD :1704-1962  sdissip_ard       SDISSIP_ST6 :4929-5102  sdissip_st6
-//   W3SWL6 :5106-5252       w3swl6            SNONLIN :2742-3047      snonlin
-//   STRESSO :3164-3356      stresso           TAU_PHI_HF :3853-3966   tau_phi_hf
+//   W3SWL6 :5106-5252       sdissip_st6       SNONLIN :2742-3047      snonlin
+//   STRESSO :3164-3356      stresso_*         TAU_PHI_HF :3853-3966   tau_phi_hf
 //   AIRSEA :868-971         airsea            W3FLX4 :5372-5443       w3flx4
 //   WSIGSTAR :4250-4339     wsigstar          WAVNU2 :4343-4461       wavnu2
 //   FRCUTINDEX :3569, FRCUTINDEX_ST6 :5447    IMPHFTAIL :3651-3731
-//   SBOTTOM :1527-1589      WNFLUXES :3970-4054
+//   SBOTTOM :1527-1589      WNFLUXES :3970-4054  (both in Src::run)
 //   TOTAL_ENERGY/FEMEAN/WM1 wam_interface_module.f90:1342,207,1591
+// Two reference computations whose results IMPLSCH never reads are not
+// evaluated: TAU_WAVE_ATMOS (TAUNW of SINPUT_ST6) and, for ST6 without
+// LCFLX, STRESSO (its TAUW is a dummy and PHIAW only feeds the flux module).
 #pragma once
 #include <cstdint>
 #include <cfloat>
@@ -32,27 +39,31 @@ namespace wamgpu {
 
 // Shared-memory view of the small tables.
 template <typename R> struct STabs {
-  const R *FR, *DF, *DFIM, *DFIMOFR, *FR5, *FRM5, *RHOWG, *TH, *COSTH, *SINTH, *DELFL, *AF11, *RNL, *SATW, *WTAUHF, *SWELLFT;
+  const R *FR, *DF, *DFIM, *DFIMOFR, *FR5, *FRM5, *RHOWG, *TH, *COSTH, *SINTH, *DELFL, *AF11, *RNL, *SATW, *WTAUHF,
+      *SWELLFT, *SIG10, *DSII10;
   const int *K1W, *K2W, *K11W, *K21W, *INL, *IKP, *IKP1, *IKM, *IKM1, *INDSAT;
   __device__ void bind(const R* r, const int* i, const SmallLayout& L) {
     FR = r + L.FR; DF = r + L.DF; DFIM = r + L.DFIM; DFIMOFR = r + L.DFIMOFR; FR5 = r + L.FR5; FRM5 = r + L.FRM5;
     RHOWG = r + L.RHOWG_DFIM; TH = r + L.TH; COSTH = r + L.COSTH; SINTH = r + L.SINTH; DELFL = r + L.DELFL;
     AF11 = r + L.AF11; RNL = r + L.RNLCOEF; SATW = r + L.SATW; WTAUHF = r + L.WTAUHF; SWELLFT = r + L.SWELLFT;
+    SIG10 = r + L.SIG10; DSII10 = r + L.DSII10;
     K1W = i + L.K1W; K2W = i + L.K2W; K11W = i + L.K11W; K21W = i + L.K21W; INL = i + L.INLCOEF;
     IKP = i + L.IKP; IKP1 = i + L.IKP1; IKM = i + L.IKM; IKM1 = i + L.IKM1; INDSAT = i + L.INDSAT;
   }
 };
 
-// Per-warp (per sea point) shared-memory workspace.
+// Per-warp (per sea point) shared-memory workspace: bin (k,m) at k + ld*m.
 template <typename R> struct WarpWS {
-  R *F, *SL, *FL, *SP;  // spectrum, source, diagonal derivative, positive input (later SMIN)
-  R* T;                 // 8 x SCR per-frequency / per-direction scratch
+  R *F, *SL, *FL, *SP;  // spectrum, source, diagonal derivative, positive input (SMIN when LCFLX)
+  R* T;                 // 8 scratch rows of length scr (per frequency / direction)
   uint8_t* LL;          // LLWS mask
-  __device__ R* t(int i) const { return T + i * SCR; }
+  int ld, scr;
+  __device__ R* t(int i) const { return T + i * scr; }
 };
 
-template <typename R> __host__ __device__ inline size_t warp_ws_bytes(int NS) {
-  size_t b = (size_t)(4 * NS + 8 * SCR) * sizeof(R) + (size_t)NS;
+template <typename R> __host__ __device__ inline size_t warp_ws_bytes(int ld, int ML, int need_sp, int scr) {
+  size_t n = (size_t)ld * ML;
+  size_t b = ((3 + (need_sp ? 1 : 0)) * n + 8 * (size_t)scr) * sizeof(R) + n;
   return (b + 15) & ~size_t(15);
 }
 
@@ -80,13 +91,13 @@ template <typename R> struct Src {
 
   // TOTAL_ENERGY + FEMEAN (+ WM1 for AKMEAN); masked when mask != null.
   __device__ void integrals(const uint8_t* mask, R& emean, R& fmean, R* akmean) const {
-    const int kl = KL(), ml = ML();
+    const int kl = KL(), ml = ML(), ld = w.ld;
     R pe = 0, pf = 0, pa = 0, tail = 0;
     const R DEL2 = dsqrt(P_::G) / P_::ZPI;
     for (int m = lane; m < ml; m += 32) {
       R t = 0;
-      const R* f = w.F + kl * m;
-      if (mask) { const uint8_t* mk = mask + kl * m; for (int k = 0; k < kl; ++k) if (mk[k]) t = t + f[k]; }
+      const R* f = w.F + ld * m;
+      if (mask) { const uint8_t* mk = mask + ld * m; for (int k = 0; k < kl; ++k) if (mk[k]) t = t + f[k]; }
       else for (int k = 0; k < kl; ++k) t = t + f[k];
       pe = pe + t * S.DFIM[m];
       pf = pf + t * S.DFIMOFR[m];
@@ -149,21 +160,23 @@ template <typename R> struct Src {
     return dmin(R(0.1), sconv * um1 * dpow(R(0.5) * P_::XKAPPA * (WSTAR * WSTAR * WSTAR), R(1.0) / R(3.0)));
   }
 
-  // SINPUT_ARD: writes SL, SP(=SPOS), FL, LL; sequential over frequency because
-  // of sheltering (XSTRESS/YSTRESS of lower frequencies feed the next one).
+  // SINPUT_ARD: writes SL, FL, LL (and SP when kept) plus the per-frequency
+  // sums of SPOS, SPOS*SIN, SPOS*COS that STRESSO integrates (scratch 0..2).
+  // Sequential over frequency because of sheltering.
   __device__ void sinput_ard(R USTAR, R Z0) const {
-    const int kl = KL(), ml = ML();
+    const int kl = KL(), ml = ML(), ld = w.ld;
     const R SWELLF = R(0.66), FU = R(0.022), FUD = R(-0.018), SWELLF4 = R(1.5E05), SWELLF5 = R(1.2), SWELLF7 = R(3.6E05);
     const R rog = P_::ROWATER * P_::G;
     const R const1 = T.BETAMAX / (P_::XKAPPA * P_::XKAPPA) / P_::ROWATER;
     const R nu = P_::RNUAIR;
     const R delabm1 = R(200) / (R(8.0) - R(0.3));
     const R shelter = dabs(T.TAUWSHELTER);
+    R* ST = w.t(0); R* SX = w.t(1); R* SY = w.t(2);
     R sig_n = wsigstar(USTAR, Z0);
     R uo = 0, ao = 0;
     for (int m = lane; m < ml; m += 32) {
       R t = 0;
-      for (int k = 0; k < kl; ++k) t = t + w.F[k + kl * m];
+      for (int k = 0; k < kl; ++k) t = t + w.F[k + ld * m];
       R sig = P_::ZPI * S.FR[m];
       uo = uo + S.DFIM[m] * (sig * sig) * t;
       ao = ao + S.DFIM[m] * t;
@@ -204,9 +217,9 @@ template <typename R> struct Src {
       R coef = -(SWELLF * R(16.) * sig2 / (P_::G * P_::ROWATER));
       R coef5 = -(SWELLF5 * R(2.) * dsqrt(R(2.) * nu * sig) / P_::ROWATER);
       R dstab1 = coef5 * roairn_pvisc * xk, tmp1 = coef * ROAIRN;
-      R px[2] = {0, 0}, py[2] = {0, 0};
+      R px[2] = {0, 0}, py[2] = {0, 0}, st = 0, sx = 0, sy = 0;
       for (int k = lane; k < kl; k += 32) {
-        R f = w.F[k + kl * m];
+        R f = w.F[k + ld * m];
         R slp[2], flp[2];
         uint8_t ll = 0;
         for (int g = 0; g < 2; ++g) {
@@ -223,19 +236,22 @@ template <typename R> struct Src {
           px[g] = px[g] + slp[g] * (constf * S.SINTH[k]);
           py[g] = py[g] + slp[g] * (constf * S.COSTH[k]);
         }
-        int b = k + kl * m;
-        w.SP[b] = R(0.5) * (slp[0] + slp[1]);
+        int b = k + ld * m;
+        R spos = R(0.5) * (slp[0] + slp[1]);  // >= 0
+        if (w.SP) w.SP[b] = spos;
+        st = st + spos; sx = sx + spos * S.SINTH[k]; sy = sy + spos * S.COSTH[k];
         R fl = R(0.5) * (flp[0] + flp[1]);
         w.FL[b] = fl;
         w.SL[b] = fl * f;
         w.LL[b] = ll;
       }
       for (int g = 0; g < 2; ++g) { xst[g] = xst[g] + warp_sum(px[g]); yst[g] = yst[g] + warp_sum(py[g]); }
+      st = warp_sum(st); sx = warp_sum(sx); sy = warp_sum(sy);
+      if (lane == 0) { ST[m] = st; SX[m] = sx; SY[m] = sy; }
     }
     __syncwarp();
   }
 
-  // STRESSO with TAU_PHI_HF: wave stress TAUW and energy flux PHIAW.
   __device__ void tau_phi_hf(int mij, R ustar, R z0, R& tauhf, R& phihf) const {
     const R gm1 = R(1.0) / P_::G;
     R omegac = P_::ZPI * S.FR[mij - 1];
@@ -259,27 +275,16 @@ template <typename R> struct Src {
     phihf = sqrtz0og * phihf;
   }
 
-  __device__ void stresso(R USTAR, R Z0, int mij, R& TAUW, R& PHIAW) const {
-    const int kl = KL(), ml = ML();
+  // STRESSO from per-lane partial sums of the resolved part plus the
+  // high-frequency tail.
+  __device__ void stresso_finish(R USTAR, R Z0, int mij, R pphi, R px, R py, R& TAUW, R& PHIAW) const {
+    const int kl = KL(), ld = w.ld;
     const R gm1 = R(1.0) / P_::G;
     const R cst = T.DELTH * ((P_::ZPI * P_::ZPI) * (P_::ZPI * P_::ZPI)) * gm1;
-    R pphi = 0, px = 0, py = 0;
-    const int nb = kl * mij;
-    for (int b = lane; b < nb; b += 32) {
-      int m = b / kl, k = b - m * kl;
-      R rw = S.RHOWG[m];
-      if (m == mij - 1 && mij != ml) rw = R(0.5) * rw;
-      R cm = T.shallow ? tfak(m) * (R(1.0) / (P_::ZPI * S.FR[m])) : (P_::ZPI * S.FR[m]) * gm1;
-      R sp = dmax(w.SP[b], R(0.));
-      pphi = pphi + sp * rw;
-      R cmr = cm * rw;
-      px = px + (sp * S.SINTH[k]) * cmr;
-      py = py + (sp * S.COSTH[k]) * cmr;
-    }
     R t1 = 0, t2 = 0;
     for (int k = lane; k < kl; k += 32) {
       R cw = dmax(dcos(S.TH[k] - UDIR), R(0.));
-      R f = w.F[k + kl * (mij - 1)];
+      R f = w.F[k + ld * (mij - 1)];
       t2 = t2 + f * (cw * cw);
       t1 = t1 + f * (cw * cw * cw);
     }
@@ -294,6 +299,37 @@ template <typename R> struct Src {
     R tw = dsqrt(xs * xs + ys * ys);
     tw = dmin(tw, USTAR * USTAR - R(0.00001));
     TAUW = dmax(tw, R(0.));
+  }
+  __device__ R rhowgdfth(int m, int mij) const {
+    R rw = S.RHOWG[m];
+    return (m == mij - 1 && mij != ML()) ? R(0.5) * rw : rw;
+  }
+  __device__ R cmw(int m) const {
+    return T.shallow ? tfak(m) * (R(1.0) / (P_::ZPI * S.FR[m])) : (P_::ZPI * S.FR[m]) * (R(1.0) / P_::G);
+  }
+  // ST4: the per-frequency sums were formed by SINPUT_ARD (scratch 0..2)
+  __device__ void stresso_sums(R USTAR, R Z0, int mij, R& TAUW, R& PHIAW) const {
+    const R* ST = w.t(0); const R* SX = w.t(1); const R* SY = w.t(2);
+    R pphi = 0, px = 0, py = 0;
+    for (int m = lane; m < mij; m += 32) {
+      R rw = rhowgdfth(m, mij), cmr = cmw(m) * rw;
+      pphi = pphi + ST[m] * rw; px = px + SX[m] * cmr; py = py + SY[m] * cmr;
+    }
+    stresso_finish(USTAR, Z0, mij, pphi, px, py, TAUW, PHIAW);
+  }
+  // ST6 with LCFLX: sums over the stored positive input
+  __device__ void stresso_sp(R USTAR, R Z0, int mij, R& TAUW, R& PHIAW) const {
+    const int kl = KL(), ld = w.ld;
+    R pphi = 0, px = 0, py = 0;
+    for (int b = lane; b < kl * mij; b += 32) {
+      int m = b / kl, k = b - m * kl;
+      R rw = rhowgdfth(m, mij), cmr = cmw(m) * rw;
+      R sp = dmax(w.SP[k + ld * m], R(0.));
+      pphi = pphi + sp * rw;
+      px = px + (sp * S.SINTH[k]) * cmr;
+      py = py + (sp * S.COSTH[k]) * cmr;
+    }
+    stresso_finish(USTAR, Z0, mij, pphi, px, py, TAUW, PHIAW);
   }
 
   __device__ int frcutindex(R fm, R fmws, R ustar) const {
@@ -317,7 +353,7 @@ template <typename R> struct Src {
 
   // IMPHFTAIL: diagnostic tail above MIJ.
   __device__ void imphftail(int mij) const {
-    const int kl = KL(), ml = ML();
+    const int kl = KL(), ml = ML(), ld = w.ld;
     R* t = w.t(7);
     for (int m = mij - 1 + lane; m < ml; m += 32) {
       if (T.shallow) { R akm1 = R(1.) / tfak(m); t[m] = (akm1 * akm1 * akm1) / tcgond(m); }
@@ -327,26 +363,27 @@ template <typename R> struct Src {
     const R base = t[mij - 1];
     const int nb = kl * (ml - mij);
     for (int i = lane; i < nb; i += 32) {
-      int m = mij + i / kl, k = i - (m - mij) * kl;
-      w.F[k + kl * m] = (t[m] / base) * w.F[k + kl * (mij - 1)];
+      int dm = i / kl, k = i - dm * kl, m = mij + dm;
+      w.F[k + ld * m] = (t[m] / base) * w.F[k + ld * (mij - 1)];
     }
     __syncwarp();
   }
 
   // SDISSIP_ARD: saturation-based whitecapping (SSDSC3 = SSDSC5 = 0).
   __device__ void sdissip_ard() const {
-    const int kl = KL(), ml = ML(), nw = 2 * T.NSDSNTH + 1;
+    const int kl = KL(), ml = ML(), nw = 2 * T.NSDSNTH + 1, ld = w.ld;
     const R tmp03 = R(1.0) / R(9.0E-4), c6 = R(0.3), c6m1 = R(1.) - c6;
     for (int m = 0; m < ml; ++m) {
       R sig = P_::ZPI * S.FR[m], facsat;
       if (T.shallow) { R xk = tfak(m); facsat = (xk * xk * xk) * (R(1.0) / P_::ZPI) * tcgond(m); }
       else { R xk = sig * sig / P_::G; facsat = (xk * xk * xk) * (R(0.5) * (R(1.0) / P_::ZPI)) * P_::G / sig; }
+      const R* fm = w.F + ld * m;
       R bth[2] = {0, 0}, bmax = 0;
       for (int s = 0; s < 2; ++s) {
         int k = lane + 32 * s;
         if (k < kl) {
           R acc = 0;
-          for (int j = 0; j < nw; ++j) acc = acc + S.SATW[k + kl * j] * w.F[(S.INDSAT[k + kl * j] - 1) + kl * m];
+          for (int j = 0; j < nw; ++j) acc = acc + S.SATW[k + kl * j] * fm[S.INDSAT[k + kl * j] - 1];
           bth[s] = acc * facsat;
           bmax = dmax(bmax, bth[s]);
         }
@@ -360,7 +397,7 @@ template <typename R> struct Src {
         if (k < kl) {
           R dd = dmax(R(0.), bth[s] * tmp03 - R(1.0));
           R d = ssdsc2_sig * (temp1 + c6m1 * (dd * dd));
-          int b = k + kl * m;
+          int b = k + ld * m;
           w.SL[b] = w.SL[b] + d * w.F[b];
           w.FL[b] = w.FL[b] + d;
         }
@@ -372,7 +409,7 @@ template <typename R> struct Src {
   // SNONLIN (DIA) for ISNONLIN = 0 (depth scaling from AKMEAN) or the
   // MAKE_SHALLOW_SNL table.
   __device__ void snonlin(R AKMEAN) const {
-    const int kl = KL(), ml = ML();
+    const int kl = KL(), ml = ML(), ld = w.ld;
     R enhfr = R(1);
     if (T.shallow && T.isnonlin == 0) {
       enhfr = dmax(R(0.75) * DEPTH * AKMEAN, R(.5));
@@ -380,30 +417,42 @@ template <typename R> struct Src {
     }
     const int mfr1 = -T.MFRSTLW + 1, mfrl = ml - T.KFRH + mfr1;
     R* SL = w.SL; R* FL = w.FL; const R* F = w.F;
+    // angular partners of this lane's directions, per KH and sub-pass (0-based)
+    int k1[2][2], k2[2][2], k11[2][2], k21[2][2];
+    for (int kh = 0; kh < 2; ++kh)
+      for (int s = 0; s < 2; ++s) {
+        int k = min(lane + 32 * s, kl - 1), sl = k + kl * kh;
+        k1[kh][s] = S.K1W[sl] - 1; k2[kh][s] = S.K2W[sl] - 1; k11[kh][s] = S.K11W[sl] - 1; k21[kh][s] = S.K21W[sl] - 1;
+      }
+    const int nsub = kl > 32 ? 2 : 1;
     for (int mc = 1; mc <= T.MLSTHG; ++mc) {
       const int im = mc - T.MFRSTLW;
       const int MP = S.IKP[im], MP1 = S.IKP1[im], MM = S.IKM[im], MM1 = S.IKM1[im];
       const int* ic5 = S.INL + 5 * (mc - 1);
-      const int IC = ic5[0], IP = ic5[1], IP1 = ic5[2], IM = ic5[3], IM1 = ic5[4];
+      const int rIC = ld * (ic5[0] - 1), rIP = ld * (ic5[1] - 1), rIP1 = ld * (ic5[2] - 1), rIM = ld * (ic5[3] - 1),
+                rIM1 = ld * (ic5[4] - 1);
       const R* rc = S.RNL + 25 * (mc - 1);
       R ftemp = S.AF11[im];
       if (T.shallow) ftemp = ftemp * (T.isnonlin == 0 ? enhfr : __ldg(&T.ENH[ij + (size_t)T.enh_ld * (mc - 1)]));
       const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
       const R ftail = (regime == 0) ? R(1) : rc[0];
+      // which targets this frequency writes (uniform over the warp)
+      const bool wMM = regime != 2, wMM1 = regime == 0 || (regime == 1 && MM1 <= ml) || (regime == 2 && MM1 >= 1);
+      const bool wMC = regime != 1 || (MM1 <= ml && mc <= ml);
+      const bool wMP = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml);
+      const bool wMP1 = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml && MP1 <= ml);
+      const int rMC = ld * (mc - 1), rMM = ld * (MM - 1), rMM1 = ld * (MM1 - 1), rMP = ld * (MP - 1), rMP1 = ld * (MP1 - 1);
+      const R g1 = rc[1], g2 = rc[2], g3 = rc[3], g4 = rc[4], g5 = rc[13], g6 = rc[14], g7 = rc[15], g8 = rc[16];
       for (int kh = 0; kh < 2; ++kh) {
         R ad[2], delad[2], delap[2], delam[2];
-        int kk[2], k1[2], k2[2], k11[2], k21[2];
         for (int s = 0; s < 2; ++s) {
           int k = lane + 32 * s;
-          kk[s] = k;
-          if (k < kl) {
-            int sl = k + kl * kh;
-            k1[s] = S.K1W[sl] - 1; k2[s] = S.K2W[sl] - 1; k11[s] = S.K11W[sl] - 1; k21[s] = S.K21W[sl] - 1;
-            R sap = rc[1] * F[k1[s] + kl * (IP - 1)] + rc[2] * F[k11[s] + kl * (IP - 1)] + rc[3] * F[k1[s] + kl * (IP1 - 1)] +
-                    rc[4] * F[k11[s] + kl * (IP1 - 1)];
-            R sam = rc[13] * F[k2[s] + kl * (IM - 1)] + rc[14] * F[k21[s] + kl * (IM - 1)] + rc[15] * F[k2[s] + kl * (IM1 - 1)] +
-                    rc[16] * F[k21[s] + kl * (IM1 - 1)];
-            R fij = F[k + kl * (IC - 1)] * ftail;
+          ad[s] = delad[s] = delap[s] = delam[s] = R(0);
+          if (s < nsub && k < kl) {
+            const int a1 = k1[kh][s], a11 = k11[kh][s], a2 = k2[kh][s], a21 = k21[kh][s];
+            R sap = g1 * F[a1 + rIP] + g2 * F[a11 + rIP] + g3 * F[a1 + rIP1] + g4 * F[a11 + rIP1];
+            R sam = g5 * F[a2 + rIM] + g6 * F[a21 + rIM] + g7 * F[a2 + rIM1] + g8 * F[a21 + rIM1];
+            R fij = F[k + rIC] * ftail;
             R fad1 = fij * (sap + sam);
             R fad2 = fad1 - R(2.) * sap * sam;
             fad1 = fad1 + fad2;
@@ -414,57 +463,27 @@ template <typename R> struct Src {
             delam[s] = (fij - R(2.) * sap) * T.DAL2 * fcen;
           }
         }
-        // one target per step: within a step lanes hit distinct bins
-#define DIA_UPD(KIDX, MROW, SLV, FLV)                                     \
-  {                                                                       \
-    for (int s = 0; s < 2; ++s)                                           \
-      if (kk[s] < kl) {                                                   \
-        int b = (KIDX) + kl * ((MROW) - 1);                               \
-        SL[b] = SL[b] + (SLV);                                            \
-        FL[b] = FL[b] + (FLV);                                            \
-      }                                                                   \
-    __syncwarp();                                                         \
-  }
-        if (regime == 0) {
-          DIA_UPD(kk[s], mc, -R(2.) * ad[s], -R(2.) * delad[s]);
-          DIA_UPD(k2[s], MM, ad[s] * rc[20], delam[s] * rc[23]);
-          DIA_UPD(k21[s], MM, ad[s] * rc[19], delam[s] * rc[24]);
-          DIA_UPD(k2[s], MM1, ad[s] * rc[17], delam[s] * rc[21]);
-          DIA_UPD(k21[s], MM1, ad[s] * rc[18], delam[s] * rc[22]);
-          DIA_UPD(k1[s], MP, ad[s] * rc[8], delap[s] * rc[11]);
-          DIA_UPD(k11[s], MP, ad[s] * rc[7], delap[s] * rc[12]);
-          DIA_UPD(k1[s], MP1, ad[s] * rc[5], delap[s] * rc[9]);
-          DIA_UPD(k11[s], MP1, ad[s] * rc[6], delap[s] * rc[10]);
-        } else if (regime == 1) {
-          DIA_UPD(k2[s], MM, ad[s] * rc[20], delam[s] * rc[23]);
-          DIA_UPD(k21[s], MM, ad[s] * rc[19], delam[s] * rc[24]);
-          if (MM1 <= ml) {
-            DIA_UPD(k2[s], MM1, ad[s] * rc[17], delam[s] * rc[21]);
-            DIA_UPD(k21[s], MM1, ad[s] * rc[18], delam[s] * rc[22]);
-            if (mc <= ml) {
-              DIA_UPD(kk[s], mc, -R(2.) * ad[s], -R(2.) * delad[s]);
-              if (MP <= ml) {
-                DIA_UPD(k1[s], MP, ad[s] * rc[8], delap[s] * rc[11]);
-                DIA_UPD(k11[s], MP, ad[s] * rc[7], delap[s] * rc[12]);
-                if (MP1 <= ml) {
-                  DIA_UPD(k1[s], MP1, ad[s] * rc[5], delap[s] * rc[9]);
-                  DIA_UPD(k11[s], MP1, ad[s] * rc[6], delap[s] * rc[10]);
-                }
-              }
-            }
-          }
-        } else {
-          if (MM1 >= 1) {
-            DIA_UPD(k2[s], MM1, ad[s] * rc[17], delam[s] * rc[21]);
-            DIA_UPD(k21[s], MM1, ad[s] * rc[18], delam[s] * rc[22]);
-          }
-          DIA_UPD(kk[s], mc, -R(2.) * ad[s], -R(2.) * delad[s]);
-          DIA_UPD(k1[s], MP, ad[s] * rc[8], delap[s] * rc[11]);
-          DIA_UPD(k11[s], MP, ad[s] * rc[7], delap[s] * rc[12]);
-          DIA_UPD(k1[s], MP1, ad[s] * rc[5], delap[s] * rc[9]);
-          DIA_UPD(k11[s], MP1, ad[s] * rc[6], delap[s] * rc[10]);
+        // phase A: the centre, the K2 and the K1 family (five distinct rows)
+        for (int s = 0; s < nsub; ++s) {
+          const int k = lane + 32 * s;
+          if (k >= kl) continue;
+          if (wMC) { int b = k + rMC; SL[b] = SL[b] - R(2.) * ad[s]; FL[b] = FL[b] - R(2.) * delad[s]; }
+          if (wMM) { int b = k2[kh][s] + rMM; SL[b] = SL[b] + ad[s] * rc[20]; FL[b] = FL[b] + delam[s] * rc[23]; }
+          if (wMM1) { int b = k2[kh][s] + rMM1; SL[b] = SL[b] + ad[s] * rc[17]; FL[b] = FL[b] + delam[s] * rc[21]; }
+          if (wMP) { int b = k1[kh][s] + rMP; SL[b] = SL[b] + ad[s] * rc[8]; FL[b] = FL[b] + delap[s] * rc[11]; }
+          if (wMP1) { int b = k1[kh][s] + rMP1; SL[b] = SL[b] + ad[s] * rc[5]; FL[b] = FL[b] + delap[s] * rc[9]; }
         }
-#undef DIA_UPD
+        __syncwarp();
+        // phase B: the K21 and K11 families
+        for (int s = 0; s < nsub; ++s) {
+          const int k = lane + 32 * s;
+          if (k >= kl) continue;
+          if (wMM) { int b = k21[kh][s] + rMM; SL[b] = SL[b] + ad[s] * rc[19]; FL[b] = FL[b] + delam[s] * rc[24]; }
+          if (wMM1) { int b = k21[kh][s] + rMM1; SL[b] = SL[b] + ad[s] * rc[18]; FL[b] = FL[b] + delam[s] * rc[22]; }
+          if (wMP) { int b = k11[kh][s] + rMP; SL[b] = SL[b] + ad[s] * rc[7]; FL[b] = FL[b] + delap[s] * rc[12]; }
+          if (wMP1) { int b = k11[kh][s] + rMP1; SL[b] = SL[b] + ad[s] * rc[6]; FL[b] = FL[b] + delap[s] * rc[10]; }
+        }
+        __syncwarp();
       }
     }
   }
@@ -493,90 +512,66 @@ template <typename R> struct Src {
     __syncwarp();
   }
 
-  // positive ST6 input growth rate D (before the stress reduction) of bin (k,m)
-  __device__ R st6_d1(int k, int m, R uproxy, R cu, R su, R sqrtbn, R& a, R& w2) const {
-    const R* WN = w.t(0); const R* CG = w.t(1);
-    R sig = P_::ZPI * S.FR[m];
-    a = w.F[k + KL() * m] * CG[m] / (P_::ZPI * sig);
-    R proj = uproxy * (WN[m] / sig) * (S.COSTH[k] * cu + S.SINTH[k] * su) - R(1.);
-    R w1 = dmax(R(0.), proj); w1 = w1 * w1;
-    R ww = dmin(R(0.), proj); w2 = ww * ww;
-    return (ROAIRN / P_::ROWATER) * sig * (R(2.8) - (R(1.) + dtanh(R(10.) * sqrtbn * w1 - R(11.)))) * sqrtbn * w1;
-  }
-  __device__ R st6_d2(int m, R sqrtbn, R w2) const {
-    R sig = P_::ZPI * S.FR[m];
-    return (ROAIRN / P_::ROWATER) * sig * R(0.09) * (R(2.8) - (R(1.) + dtanh(R(10.) * sqrtbn * w2 - R(11.)))) * sqrtbn * w2;
-  }
-
-  // directional integrals of the (positive or |negative|) stress spectrum,
-  // extended to 10 Hz: x in scratch 4, y in scratch 5, returns TAUWINDS parts
-  __device__ void st6_extend(R* sdx, R* sdy, R* cinv10, R* dsii10) const {
-    const int nk = ML(), nk10 = T.NK10;
-    const R* WN = w.t(0);
-    const R sig1 = P_::ZPI * S.FR[0];
-    for (int i = lane; i < nk10; i += 32) {
-      R sig10 = (nk < nk10) ? sig1 * dpow(P_::CO, R(i + 1) - R(1.0)) : P_::ZPI * S.FR[i];
-      R ci = (i < nk) ? WN[i] / (P_::ZPI * S.FR[i]) : sig10 * R(0.101978);
-      R ds;
-      if (nk < nk10) {
-        ds = R(0.5) * sig10 * (P_::CO - R(1.0) / P_::CO);
-        if (i == 0) ds = R(0.5) * sig10 * (P_::CO - R(1.0));
-        if (i == nk10 - 1) ds = R(0.5) * sig10 * (P_::CO - R(1.0)) / P_::CO;
-      } else ds = P_::ZPI * S.DF[i];
-      cinv10[i] = ci; dsii10[i] = ds;
-    }
-    __syncwarp();
-    if (nk < nk10) {
-      R signk = sig1 * dpow(P_::CO, R(nk) - R(1.0));
-      for (int i = nk + lane; i < nk10; i += 32) {
-        R sig10 = sig1 * dpow(P_::CO, R(i + 1) - R(1.0));
-        R r = (signk / sig10) * (signk / sig10);
-        sdx[i] = sdx[nk - 1] * r; sdy[i] = sdy[nk - 1] * r;
-      }
-    }
-    __syncwarp();
-  }
-
-  // SINPUT_ST6 with LFACTOR and TAU_WAVE_ATMOS; writes SL, SP, FL; TAUW out.
+  // SINPUT_ST6 with LFACTOR: writes SL, FL, LL (and SP when kept); TAUW out.
+  // The positive growth rate D1 and the negative-input term D2 of every bin
+  // are formed once (kept in SL and FL until the final pass).
   __device__ void sinput_st6(R USTAR, R& TAUW) const {
-    const int kl = KL(), nk = ML(), nk10 = T.NK10;
-    const R* CG = w.t(1);
-    R* SQB = w.t(2); R* LF = w.t(3); R* SDX = w.t(4); R* SDY = w.t(5); R* CI10 = w.t(6); R* DS10 = w.t(7);
+    const int kl = KL(), nk = ML(), nk10 = T.NK10, ld = w.ld;
+    const R* WN = w.t(0); const R* CG = w.t(1);
+    R* SQB = w.t(2); R* LF = w.t(3); R* SDX = w.t(4); R* SDY = w.t(5); R* CI10 = w.t(6);
     const R cu = dcos(UDIR), su = dsin(UDIR), uproxy = R(32.) * USTAR;
-    // narrowness and saturation per frequency
+    const R raw = ROAIRN / P_::ROWATER;
+    // directional narrowness and saturation per frequency
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m];
+      const R* fm = w.F + ld * m;
       R s = 0, mx = 0;
-      for (int k = 0; k < kl; ++k) {
-        R a = w.F[k + kl * m] * CG[m] / (P_::ZPI * sig);
-        s = s + a;
-        mx = (k == 0) ? a : dmax(mx, a);
-      }
+      for (int k = 0; k < kl; ++k) { R a = fm[k] * CG[m] / (P_::ZPI * sig); s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
       R s2 = 0;
-      for (int k = 0; k < kl; ++k) {
-        R a = w.F[k + kl * m] * CG[m] / (P_::ZPI * sig);
-        s2 = s2 + ((mx < R(1.0E-34)) ? R(1.) : a / mx);
-      }
+      for (int k = 0; k < kl; ++k) { R a = fm[k] * CG[m] / (P_::ZPI * sig); s2 = s2 + ((mx < R(1.0E-34)) ? R(1.) : a / mx); }
       R adensig = s * sig * T.DELTH, anar = R(1.0) / (s2 * T.DELTH);
-      R wn = w.t(0)[m];
-      SQB[m] = dsqrt(anar * adensig * (wn * wn * wn));
+      SQB[m] = dsqrt(anar * adensig * (WN[m] * WN[m] * WN[m]));
     }
     __syncwarp();
-    // positive stress spectrum sums per frequency
+    // growth rates per bin
+    for (int b = lane; b < kl * nk; b += 32) {
+      int m = b / kl, k = b - m * kl;
+      R sig = P_::ZPI * S.FR[m], sqb = SQB[m];
+      R proj = uproxy * (WN[m] / sig) * (S.COSTH[k] * cu + S.SINTH[k] * su) - R(1.);
+      R w1 = dmax(R(0.), proj); w1 = w1 * w1;
+      R w2 = dmin(R(0.), proj); w2 = w2 * w2;
+      R d1 = raw * sig * (R(2.8) - (R(1.) + dtanh(R(10.) * sqb * w1 - R(11.)))) * sqb * w1;
+      R d2 = raw * sig * R(0.09) * (R(2.8) - (R(1.) + dtanh(R(10.) * sqb * w2 - R(11.)))) * sqb * w2;
+      w.SL[k + ld * m] = d1;
+      w.FL[k + ld * m] = d2;
+    }
+    __syncwarp();
+    // directional sums of the positive stress spectrum (LFACTOR :4580-4595)
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m], bx = 0, by = 0;
+      const R* fm = w.F + ld * m; const R* d1 = w.SL + ld * m;
       for (int k = 0; k < kl; ++k) {
-        R a, w2;
-        R d = st6_d1(k, m, uproxy, cu, su, SQB[m], a, w2);
-        R sd = d * a * sig / CG[m];
+        R a = fm[k] * CG[m] / (P_::ZPI * sig);
+        R sd = d1[k] * a * sig / CG[m];
         bx = bx + dmax(R(0.), sd) * S.COSTH[k];
         by = by + dmax(R(0.), sd) * S.SINTH[k];
       }
       SDX[m] = bx * T.DELTH; SDY[m] = by * T.DELTH;
+      CI10[m] = WN[m] / sig;
     }
     __syncwarp();
-    st6_extend(SDX, SDY, CI10, DS10);
-    // LFACTOR: iterate the high-frequency reduction until the total stress matches u*^2
+    // extension to 10 Hz with an f^-2 tail (point-independent axis in S.SIG10/S.DSII10)
+    if (nk < nk10) {
+      const R signk = S.SIG10[nk - 1];
+      for (int i = nk + lane; i < nk10; i += 32) {
+        R r = (signk / S.SIG10[i]) * (signk / S.SIG10[i]);
+        SDX[i] = SDX[nk - 1] * r; SDY[i] = SDY[nk - 1] * r;
+        CI10[i] = S.SIG10[i] * R(0.101978);
+      }
+    }
+    __syncwarp();
+    const R* DS10 = S.DSII10;
+    // LFACTOR: shrink the high-frequency input until the total stress matches u*^2
     const R gro = P_::G * P_::ROWATER;
     R tau_tot = USTAR * USTAR * ROAIRN;
     R tau_vis = dmax(R(0.0), -(R(5.0E-5) * U10) + R(1.1E-3)) * (U10 * U10) * ROAIRN;
@@ -587,7 +582,7 @@ template <typename R> struct Src {
     R tauwx = gro * warp_sum(px), tauwy = gro * warp_sum(py);
     R tau = dsqrt((tvx + tauwx) * (tvx + tauwx) + (tvy + tauwy) * (tvy + tauwy));
     R err = (tau - tau_tot) / tau_tot;
-    for (int i = lane; i < nk10; i += 32) LF[i] = R(1.0);
+    for (int i = lane; i < nk; i += 32) LF[i] = R(1.0);
     if (tau > tau_tot) {
       bool over = false;
       R rtau = err / R(90.), drtau = R(2.0);
@@ -596,7 +591,7 @@ template <typename R> struct Src {
         px = 0; py = 0;
         for (int i = lane; i < nk10; i += 32) {
           R lf = dmin(R(1.0), dexp((R(1.0) - uproxy * CI10[i]) * rtau));
-          LF[i] = lf;
+          if (i < nk) LF[i] = lf;
           px = px + (SDX[i] * lf) * CI10[i] * DS10[i];
           py = py + (SDY[i] * lf) * CI10[i] * DS10[i];
         }
@@ -615,58 +610,36 @@ template <typename R> struct Src {
     R sumlf = 0;
     for (int m = lane; m < nk; m += 32) sumlf = sumlf + LF[m];
     const bool reduce = warp_sum(sumlf) < R(nk);
-    // negative input part: |min(0,S)| directional sums
-    for (int m = lane; m < nk; m += 32) {
-      R sig = P_::ZPI * S.FR[m], bx = 0, by = 0;
-      for (int k = 0; k < kl; ++k) {
-        R a, w2;
-        R d = st6_d1(k, m, uproxy, cu, su, SQB[m], a, w2);
-        if (reduce) d = d * LF[m];
-        d = d - st6_d2(m, SQB[m], w2);
-        R sd = d * a * sig / CG[m];
-        bx = bx + dabs(dmin(R(0.), sd)) * S.COSTH[k];
-        by = by + dabs(dmin(R(0.), sd)) * S.SINTH[k];
-      }
-      SDX[m] = bx * T.DELTH; SDY[m] = by * T.DELTH;
-    }
-    __syncwarp();
-    // LF entries above nk are not needed any more; reuse the extension
-    st6_extend(SDX, SDY, CI10, DS10);
-    px = 0; py = 0;
-    for (int i = lane; i < nk10; i += 32) { px = px + SDX[i] * CI10[i] * DS10[i]; py = py + SDY[i] * CI10[i] * DS10[i]; }
-    R tnx = gro * warp_sum(px), tny = gro * warp_sum(py);
-    (void)tnx; (void)tny;  // TAUNW is a diagnostic the driver does not read back
     TAUW = dsqrt(tauwx * tauwx + tauwy * tauwy);
     for (int b = lane; b < kl * nk; b += 32) {
-      int m = b / kl, k = b - m * kl;
-      R a, w2;
-      R d = st6_d1(k, m, uproxy, cu, su, SQB[m], a, w2);
+      int m = b / kl, k = b - m * kl, p = k + ld * m;
+      R d = w.SL[p];
       if (reduce) d = d * LF[m];
-      R dpos = d;
-      R dtot = d - st6_d2(m, SQB[m], w2);
-      R f = w.F[b];
-      w.SL[b] = dtot * f;
-      w.SP[b] = dpos * f;
-      w.FL[b] = dtot;
-      w.LL[b] = (dpos * f > R(0));
+      R dtot = d - w.FL[p];
+      R f = w.F[p];
+      w.SL[p] = dtot * f;
+      w.FL[p] = dtot;
+      if (w.SP) w.SP[p] = d * f;
+      w.LL[p] = (d * f > R(0));
     }
     __syncwarp();
   }
 
   // SDISSIP_ST6 (T1 + T2 breaking) followed by W3SWL6 (swell dissipation)
   __device__ void sdissip_st6() const {
-    const int kl = KL(), nk = ML();
+    const int kl = KL(), nk = ML(), ld = w.ld;
     const R* WN = w.t(0); const R* CG = w.t(1);
     R* ADF = w.t(2); R* T12 = w.t(3);
     const R bnt = R(0.035) * R(0.035);
+    const R xfac = (R(1.0) - R(1.0) / P_::CO) / (P_::CO - R(1.0) / P_::CO);
     for (int m = lane; m < nk; m += 32) {
       R et = (P_::ZPI * bnt) / (CG[m] * (WN[m] * WN[m] * WN[m]));
       R s = 0;
-      for (int k = 0; k < kl; ++k) s = s + w.F[k + kl * m];
+      const R* fm = w.F + ld * m;
+      for (int k = 0; k < kl; ++k) s = s + fm[k];
       R nex = dmax(R(0.0), s * T.DELTH - et) / et;
       R nex4 = (nex * nex) * (nex * nex);
       T12[m] = R(4.75E-6) * S.FR[m] * nex4;  // T1
-      R xfac = (R(1.0) - R(1.0) / P_::CO) / (P_::CO - R(1.0) / P_::CO);
       R dfii = (m > 0 && m < nk - 1) ? S.DF[m] * xfac : S.DF[m];
       ADF[m] = nex4 * dfii;
     }
@@ -682,29 +655,23 @@ template <typename R> struct Src {
       carry = __shfl_sync(0xffffffffu, v, 31);
     }
     __syncwarp();
-    for (int b = lane; b < kl * nk; b += 32) {
-      int m = b / kl;
-      w.SL[b] = w.SL[b] + T12[m] * w.F[b];
-      w.FL[b] = w.FL[b] + T12[m];
-    }
-    __syncwarp();
-    // W3SWL6
+    // W3SWL6 per-frequency quantities
     R* BN = w.t(4); R* AB = w.t(5);
-    R ps = 0, amax = -R(1), iw = 0;
+    R ps = 0, amax = -R(1);
     int imax = 0;
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m];
+      const R* fm = w.F + ld * m;
       R s = 0, mx = 0;
-      for (int k = 0; k < kl; ++k) { R a = w.F[k + kl * m] * CG[m] / (P_::ZPI * sig); s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
+      for (int k = 0; k < kl; ++k) { R a = fm[k] * CG[m] / (P_::ZPI * sig); s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
       R s2 = 0;
-      for (int k = 0; k < kl; ++k) { R a = w.F[k + kl * m] * CG[m] / (P_::ZPI * sig); s2 = s2 + ((mx < R(1.0E-34)) ? R(1.) : a / mx); }
+      for (int k = 0; k < kl; ++k) { R a = fm[k] * CG[m] / (P_::ZPI * sig); s2 = s2 + ((mx < R(1.0E-34)) ? R(1.) : a / mx); }
       R anar = R(1.0) / (s2 * T.DELTH);
       AB[m] = s;
       BN[m] = anar * (s * sig * T.DELTH) * (WN[m] * WN[m] * WN[m]);
       ps = ps + s * (P_::ZPI * S.DFIM[m] * sig) / CG[m];
       if (s > amax) { amax = s; imax = m; }
     }
-    (void)iw;
     // first maximum over frequency (MAXLOC)
     for (int o = 16; o > 0; o >>= 1) {
       R oa = __shfl_xor_sync(0xffffffffu, amax, o);
@@ -715,20 +682,21 @@ template <typename R> struct Src {
     __syncwarp();
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m];
-      T12[m] = (AB[m] > R(1.E-30)) ? -(R(2.) / R(3.) * b1 * sig * dsqrt(BN[m])) : R(0);
+      AB[m] = (AB[m] > R(1.E-30)) ? -(R(2.) / R(3.) * b1 * sig * dsqrt(BN[m])) : R(0);
     }
     __syncwarp();
     for (int b = lane; b < kl * nk; b += 32) {
-      int m = b / kl;
-      w.SL[b] = w.SL[b] + T12[m] * w.F[b];
-      w.FL[b] = w.FL[b] + T12[m];
+      int m = b / kl, k = b - m * kl, p = k + ld * m;
+      R f = w.F[p];
+      w.SL[p] = (w.SL[p] + T12[m] * f) + AB[m] * f;
+      w.FL[p] = (w.FL[p] + T12[m]) + AB[m];
     }
     __syncwarp();
   }
 
   // ---- the whole IMPLSCH step for this point --------------------------------
   __device__ void run(PointState<R>& ps) const {
-    const int kl = KL(), ml = ML(), ns = kl * ml;
+    const int kl = KL(), ml = ML(), ld = w.ld;
     R TAUW = ps.TAUW, USTAR, Z0;
     R emean, fmean, akmean = 0, emeanws, fmeanws, phiaw = 0;
     const int ju = min(300, max((int)lround((double)(U10 / T.DELU)), 1));
@@ -739,14 +707,14 @@ template <typename R> struct Src {
     else sinput_st6(USTAR, TAUW);
     integrals(w.LL, emeanws, fmeanws, nullptr);
     int mij = (T.iphys == 2) ? frcutindex_st6(fmean, USTAR) : frcutindex(fmean, fmeanws, USTAR);
-    R tdummy;
-    if (T.iphys == 2) { stresso(USTAR, Z0, mij, tdummy, phiaw); w3flx4(USTAR, Z0); }
-    else { stresso(USTAR, Z0, mij, TAUW, phiaw); airsea(TAUW, USTAR, Z0); }
+    if (T.iphys == 2) { w3flx4(USTAR, Z0); }
+    else { stresso_sums(USTAR, Z0, mij, TAUW, phiaw); airsea(TAUW, USTAR, Z0); }
     imphftail(mij);
     if (T.iphys == 1) sinput_ard(USTAR, Z0);
-    stresso(USTAR, Z0, mij, (T.iphys == 2) ? tdummy : TAUW, phiaw);
+    if (T.iphys == 1) stresso_sums(USTAR, Z0, mij, TAUW, phiaw);
+    else if (T.lcflx) { R td; stresso_sp(USTAR, Z0, mij, td, phiaw); }
     if (T.lcflx) {  // SMIN = SL - SPOS, kept in SP from here on
-      for (int b = lane; b < ns; b += 32) w.SP[b] = w.SL[b] - w.SP[b];
+      for (int b = lane; b < kl * ml; b += 32) { int m = b / kl, p = b - m * kl + ld * m; w.SP[p] = w.SL[p] - w.SP[p]; }
       __syncwarp();
     }
     if (T.iphys == 1) sdissip_ard();
@@ -766,15 +734,15 @@ template <typename R> struct Src {
       const R rog = P_::ROWATER * P_::G, scdfm = R(0.5) * T.DELTH * (R(1.) - R(1.) / P_::CO);
       R a[6] = {0, 0, 0, 0, 0, 0};
       for (int b = lane; b < kl * mij; b += 32) {
-        int m = b / kl, k = b - m * kl;
+        int m = b / kl, k = b - m * kl, p = k + ld * m;
         R cfm = (m < mij - 1) ? rog * S.DFIM[m] : rog * scdfm * S.FR[m];
         R cm = T.shallow ? tfak(m) / (P_::ZPI * S.FR[m]) : P_::ZPI * S.FR[m] / P_::G;
-        R src = w.SL[b] - w.SP[b];
+        R src = w.SL[p] - w.SP[p];
         a[0] = a[0] + src * cfm;
         a[1] = a[1] + cm * src * cfm * S.SINTH[k];
         a[2] = a[2] + cm * src * cfm * S.COSTH[k];
         if (T.shallow) {
-          R bot = SBO[m] * w.F[b];
+          R bot = SBO[m] * w.F[p];
           a[3] = a[3] + bot * cfm;
           a[4] = a[4] + cm * bot * cfm * S.SINTH[k];
           a[5] = a[5] + cm * bot * cfm * S.COSTH[k];
@@ -790,17 +758,16 @@ template <typename R> struct Src {
     }
     // implicit integration with the growth limiter and the minimum-energy floor
     const R delt = T.DELT, fmx = dmax(fmeanws, fmean);
-    for (int b = lane; b < ns; b += 32) {
-      int m = b / kl, k = b - m * kl;
-      R sl = w.SL[b];
-      if (T.shallow) sl = sl + SBO[m] * w.F[b];
-      R fl = w.FL[b];
-      if (T.shallow) fl = fl + SBO[m];
+    for (int b = lane; b < kl * ml; b += 32) {
+      int m = b / kl, k = b - m * kl, p = k + ld * m;
+      R f0 = w.F[p];
+      R sl = w.SL[p], fl = w.FL[p];
+      if (T.shallow) { sl = sl + SBO[m] * f0; fl = fl + SBO[m]; }
       R t1 = delt * sl / dmax(R(1.), R(1.) - delt * fl);
       R t3 = dmin(dabs(t1), USTAR * S.DELFL[m] * fmx);
-      R f = w.F[b] + ((t1 >= R(0)) ? t3 : -t3);
+      R f = f0 + ((t1 >= R(0)) ? t3 : -t3);
       R c = dmax(R(0.), dcos(S.TH[k] - UDIR));
-      w.F[b] = dmax(f, __ldg(&T.FLMINFR[(ju - 1) + 300 * m]) * (c * c));
+      w.F[p] = dmax(f, __ldg(&T.FLMINFR[(ju - 1) + 300 * m]) * (c * c));
     }
     __syncwarp();
     integrals(nullptr, emean, fmean, nullptr);

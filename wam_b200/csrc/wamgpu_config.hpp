@@ -17,7 +17,8 @@ constexpr int SCR = 96;        // per-warp per-frequency scratch length (>= MAX_
 // every IMPLSCH CTA stages into shared memory.
 struct SmallLayout {
   // float block
-  int FR, DF, DFIM, DFIMOFR, FR5, FRM5, RHOWG_DFIM, TH, COSTH, SINTH, DELFL, AF11, RNLCOEF, SATW, WTAUHF, SWELLFT;
+  int FR, DF, DFIM, DFIMOFR, FR5, FRM5, RHOWG_DFIM, TH, COSTH, SINTH, DELFL, AF11, RNLCOEF, SATW, WTAUHF, SWELLFT,
+      SIG10, DSII10;
   int nreal;
   // int block
   int K1W, K2W, K11W, K21W, INLCOEF, IKP, IKP1, IKM, IKM1, INDSAT;
@@ -27,6 +28,7 @@ struct SmallLayout {
 // Everything the kernels need besides the per-point fields; passed by value.
 template <typename R> struct DevTables {
   int KL, ML, NS, NDEPTH, MFRSTLW, MLSTHG, KFRH, NSDSNTH, NK10;
+  int ld, scr, need_sp;  // shared-memory row stride (odd, >= KL), scratch row length, SPOS array kept
   int iphys, shallow, isnonlin, lcflx;
   R DELTH, DELTR, INV_LOG_CO, MO_TAIL, MM1_TAIL, DELU, DAL1, DAL2, X0TAUHF;
   R BETAMAX, ZALP, ALPHA, TAUWSHELTER, CDFAC, DELT;
