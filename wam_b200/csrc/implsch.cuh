@@ -97,7 +97,7 @@ template <typename R> struct Src {
     for (int m = lane; m < ml; m += 32) {
       R t = 0;
       const R* f = w.F + ld * m;
-      if (mask) { const uint8_t* mk = mask + ld * m; for (int k = 0; k < kl; ++k) if (mk[k]) t = t + f[k]; }
+      if (mask) { const uint8_t* mk = mask + ld * m; for (int k = 0; k < kl; ++k) t = t + (mk[k] ? f[k] : R(0)); }
       else for (int k = 0; k < kl; ++k) t = t + f[k];
       pe = pe + t * S.DFIM[m];
       pf = pf + t * S.DFIMOFR[m];
@@ -441,13 +441,17 @@ template <typename R> struct Src {
       const bool wMC = regime != 1 || (MM1 <= ml && mc <= ml);
       const bool wMP = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml);
       const bool wMP1 = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml && MP1 <= ml);
-      const int rMC = ld * (mc - 1), rMM = ld * (MM - 1), rMM1 = ld * (MM1 - 1), rMP = ld * (MP - 1), rMP1 = ld * (MP1 - 1);
+      // row offsets of targets this frequency does not write are clamped to row 0,
+      // so the batched loads below never leave the spectrum
+      const int rMC = wMC ? ld * (mc - 1) : 0, rMM = wMM ? ld * (MM - 1) : 0, rMM1 = wMM1 ? ld * (MM1 - 1) : 0,
+                rMP = wMP ? ld * (MP - 1) : 0, rMP1 = wMP1 ? ld * (MP1 - 1) : 0;
       const R g1 = rc[1], g2 = rc[2], g3 = rc[3], g4 = rc[4], g5 = rc[13], g6 = rc[14], g7 = rc[15], g8 = rc[16];
-      for (int kh = 0; kh < 2; ++kh) {
-        R ad[2], delad[2], delap[2], delam[2];
+      // all (KH, sub-pass) interactions of this frequency first: independent gathers
+      R ad[2][2], delad[2][2], delap[2][2], delam[2][2];
+      for (int kh = 0; kh < 2; ++kh)
         for (int s = 0; s < 2; ++s) {
-          int k = lane + 32 * s;
-          ad[s] = delad[s] = delap[s] = delam[s] = R(0);
+          const int k = lane + 32 * s;
+          ad[kh][s] = delad[kh][s] = delap[kh][s] = delam[kh][s] = R(0);
           if (s < nsub && k < kl) {
             const int a1 = k1[kh][s], a11 = k11[kh][s], a2 = k2[kh][s], a21 = k21[kh][s];
             R sap = g1 * F[a1 + rIP] + g2 * F[a11 + rIP] + g3 * F[a1 + rIP1] + g4 * F[a11 + rIP1];
@@ -457,31 +461,42 @@ template <typename R> struct Src {
             R fad2 = fad1 - R(2.) * sap * sam;
             fad1 = fad1 + fad2;
             R fcen = ftemp * fij;
-            ad[s] = fad2 * fcen;
-            delad[s] = fad1 * ftemp;
-            delap[s] = (fij - R(2.) * sam) * T.DAL1 * fcen;
-            delam[s] = (fij - R(2.) * sap) * T.DAL2 * fcen;
+            ad[kh][s] = fad2 * fcen;
+            delad[kh][s] = fad1 * ftemp;
+            delap[kh][s] = (fij - R(2.) * sam) * T.DAL1 * fcen;
+            delam[kh][s] = (fij - R(2.) * sap) * T.DAL2 * fcen;
           }
         }
-        // phase A: the centre, the K2 and the K1 family (five distinct rows)
+      // Scatter in two phases per KH.  Within a phase the rows are distinct
+      // (checked on the host) and each target family is a rotation, so every
+      // lane's targets differ from every other lane's: all loads of a phase
+      // are issued before its stores.
+      for (int kh = 0; kh < 2; ++kh) {
         for (int s = 0; s < nsub; ++s) {
           const int k = lane + 32 * s;
-          if (k >= kl) continue;
-          if (wMC) { int b = k + rMC; SL[b] = SL[b] - R(2.) * ad[s]; FL[b] = FL[b] - R(2.) * delad[s]; }
-          if (wMM) { int b = k2[kh][s] + rMM; SL[b] = SL[b] + ad[s] * rc[20]; FL[b] = FL[b] + delam[s] * rc[23]; }
-          if (wMM1) { int b = k2[kh][s] + rMM1; SL[b] = SL[b] + ad[s] * rc[17]; FL[b] = FL[b] + delam[s] * rc[21]; }
-          if (wMP) { int b = k1[kh][s] + rMP; SL[b] = SL[b] + ad[s] * rc[8]; FL[b] = FL[b] + delap[s] * rc[11]; }
-          if (wMP1) { int b = k1[kh][s] + rMP1; SL[b] = SL[b] + ad[s] * rc[5]; FL[b] = FL[b] + delap[s] * rc[9]; }
+          if (k >= kl) break;
+          const int bC = k + rMC, b2 = k2[kh][s] + rMM, b21 = k2[kh][s] + rMM1, b1 = k1[kh][s] + rMP,
+                    b11 = k1[kh][s] + rMP1;
+          R sC = SL[bC], fC = FL[bC], s2 = SL[b2], f2 = FL[b2], s21 = SL[b21], f21 = FL[b21];
+          R s1 = SL[b1], f1 = FL[b1], s11 = SL[b11], f11 = FL[b11];
+          const R A = ad[kh][s], DM = delam[kh][s], DP = delap[kh][s];
+          if (wMC) { SL[bC] = sC - R(2.) * A; FL[bC] = fC - R(2.) * delad[kh][s]; }
+          if (wMM) { SL[b2] = s2 + A * rc[20]; FL[b2] = f2 + DM * rc[23]; }
+          if (wMM1) { SL[b21] = s21 + A * rc[17]; FL[b21] = f21 + DM * rc[21]; }
+          if (wMP) { SL[b1] = s1 + A * rc[8]; FL[b1] = f1 + DP * rc[11]; }
+          if (wMP1) { SL[b11] = s11 + A * rc[5]; FL[b11] = f11 + DP * rc[9]; }
         }
         __syncwarp();
-        // phase B: the K21 and K11 families
         for (int s = 0; s < nsub; ++s) {
           const int k = lane + 32 * s;
-          if (k >= kl) continue;
-          if (wMM) { int b = k21[kh][s] + rMM; SL[b] = SL[b] + ad[s] * rc[19]; FL[b] = FL[b] + delam[s] * rc[24]; }
-          if (wMM1) { int b = k21[kh][s] + rMM1; SL[b] = SL[b] + ad[s] * rc[18]; FL[b] = FL[b] + delam[s] * rc[22]; }
-          if (wMP) { int b = k11[kh][s] + rMP; SL[b] = SL[b] + ad[s] * rc[7]; FL[b] = FL[b] + delap[s] * rc[12]; }
-          if (wMP1) { int b = k11[kh][s] + rMP1; SL[b] = SL[b] + ad[s] * rc[6]; FL[b] = FL[b] + delap[s] * rc[10]; }
+          if (k >= kl) break;
+          const int b2 = k21[kh][s] + rMM, b21 = k21[kh][s] + rMM1, b1 = k11[kh][s] + rMP, b11 = k11[kh][s] + rMP1;
+          R s2 = SL[b2], f2 = FL[b2], s21 = SL[b21], f21 = FL[b21], s1 = SL[b1], f1 = FL[b1], s11 = SL[b11], f11 = FL[b11];
+          const R A = ad[kh][s], DM = delam[kh][s], DP = delap[kh][s];
+          if (wMM) { SL[b2] = s2 + A * rc[19]; FL[b2] = f2 + DM * rc[24]; }
+          if (wMM1) { SL[b21] = s21 + A * rc[18]; FL[b21] = f21 + DM * rc[22]; }
+          if (wMP) { SL[b1] = s1 + A * rc[7]; FL[b1] = f1 + DP * rc[12]; }
+          if (wMP1) { SL[b11] = s11 + A * rc[6]; FL[b11] = f11 + DP * rc[10]; }
         }
         __syncwarp();
       }
