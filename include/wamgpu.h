@@ -131,6 +131,29 @@ WAMGPU_API int wamgpu_implsch_dev(wamgpu_ctx* ctx, void* fl3, int ld, const void
                        void* z0, const void* roairn, const void* wstar, void* stream);
 WAMGPU_API int wamgpu_propags_dev(wamgpu_ctx* ctx, void* f3, int ld, void* scratch, void* stream);
 
+/* Fixed-scratch form of wamgpu_propags_dev.  NO COUNTERPART IN THE REFERENCE
+ * (its PROPAGS, wam_propagation_module.f90:635-829, sub-steps through a
+ * local array of the model).  It serves callers that can neither hand in a
+ * scratch spectrum nor let the library cudaMalloc one: hosts whose free
+ * device memory is held by another allocator (the allocation would fail)
+ * and pipelines that must not pass through the device-wide synchronisation
+ * of the cudaFree that replacing a grown buffer implies.
+ *  - The F1 ping-pong buffer of the COUNTER sub-steps is one file-scope
+ *    device array of WAMGPU_STATIC_SCRATCH_BYTES per device.  A spectrum of
+ *    more than that (ld*KL*ML*element size) is rejected with WAMGPU_E_ARG
+ *    before any work is queued.
+ *  - The first call on a device looks the array's address up
+ *    (cudaGetSymbolAddress, which may load the module) and keeps it for the
+ *    process; make that first call before any stream capture.
+ *  - Nothing is allocated, freed or cleared: every scratch element a call
+ *    reads it wrote earlier in the same call.
+ *  - There is ONE array per device: calls whose GPU work overlaps (other
+ *    streams, other contexts on the same device) race on it; order them on
+ *    one stream.
+ *  - Kernel timing (wamgpu_set_timing) does not cover this entry point. */
+#define WAMGPU_STATIC_SCRATCH_BYTES 33554432
+WAMGPU_API int wamgpu_propags_dev_static(wamgpu_ctx* ctx, void* f3, int ld, void* stream);
+
 /* One pass of the WAMODEL PROP/PHYSICS loop body (wamodel.f90:286-360):
  * nprop PROPAGS calls (IDELT/IDELPRO of them per source step) followed by
  * one IMPLSCH, with the spectrum resident on the device for the whole pass.

@@ -39,6 +39,7 @@ SIGNATURES = {
     "wamgpu_implsch_dev": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                    c_void_p, c_void_p, c_void_p]),
     "wamgpu_propags_dev": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "wamgpu_propags_dev_static": (c_int, [c_void_p, c_void_p, c_int, c_void_p]),
     "wamgpu_step_dev": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                                 c_void_p, c_void_p, c_void_p, c_void_p]),
     "wamgpu_step_host": (c_int, [c_void_p, PF, c_int, PF, PF, PF, PF, PF, PF, PF]),

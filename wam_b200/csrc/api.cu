@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 #include "../../include/wamgpu.h"
@@ -468,6 +469,58 @@ template <typename R> int propags_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* f3v, 
   return WAMGPU_OK;
 }
 
+// Address of the fixed PROPAGS scratch on the context's device, looked up
+// once per device with that device current (first call) and kept for the
+// process.
+constexpr int kMaxStaticDevices = 64;
+std::mutex g_static_mu;
+void* g_static_addr[kMaxStaticDevices] = {};
+
+int static_scratch(wamgpu_ctx* ctx, void** out) {
+  const int dev = ctx->cfg.device;
+  if (dev < 0 || dev >= kMaxStaticDevices) return fail(ctx, WAMGPU_E_ARG, "device ordinal beyond the static scratch table");
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (!g_static_addr[dev]) {
+    int prev = -1;
+    CK(cudaGetDevice(&prev), "cudaGetDevice");
+    if (prev != dev) CK(cudaSetDevice(dev), "cudaSetDevice");
+    void* p = nullptr;
+    const cudaError_t e = static_scratch_address(&p);
+    if (prev != dev) cudaSetDevice(prev);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress (static PROPAGS scratch)");
+    if (!p) return fail(ctx, WAMGPU_E_CUDA, "static PROPAGS scratch has no device address");
+    g_static_addr[dev] = p;
+  }
+  *out = g_static_addr[dev];
+  return WAMGPU_OK;
+}
+
+// PROPAGS with the F1 ping-pong spectrum in the fixed device array: no
+// allocation, no clearing (each scratch element read was written earlier in
+// the call), sizes above the array rejected before anything is queued.
+template <typename R> int propags_dev_static_t(wamgpu_ctx* ctx, Impl<R>& I, void* f3v, int ld, cudaStream_t s) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  const size_t bytes = (size_t)ld * ctx->cfg.kl * ctx->cfg.ml * sizeof(R);
+  if (bytes > (size_t)WAMGPU_STATIC_SCRATCH_BYTES)
+    return fail(ctx, WAMGPU_E_ARG, "spectrum of " + std::to_string(bytes) + " bytes exceeds the static PROPAGS scratch of " +
+                                       std::to_string((size_t)WAMGPU_STATIC_SCRATCH_BYTES) +
+                                       " bytes; use wamgpu_propags_dev with a scratch spectrum");
+  void* base = nullptr;
+  const int rc = static_scratch(ctx, &base);
+  if (rc) return rc;
+  R* f3 = (R*)f3v;
+  R* sc = (R*)base;
+  const int cnt = ctx->counter;
+  R* src = f3; R* dst = sc;
+  if (cnt % 2 == 1) { CK(cudaMemcpyAsync(sc, f3, bytes, cudaMemcpyDeviceToDevice, s), "copy F1"); src = sc; dst = f3; }
+  for (int it = 0; it < cnt; ++it) {
+    CK(launch_propags<R>(I.pa, src, ld, dst, ld, s), "propags launch");
+    std::swap(src, dst);
+  }
+  return WAMGPU_OK;
+}
+
 // One pass of WAMODEL's PROP/PHYSICS loop body (wamodel.f90:286-360): nprop
 // PROPAGS calls (each COUNTER sub-steps) followed by one IMPLSCH.  All
 // sub-steps ping-pong between f3 and scratch and IMPLSCH reads whichever
@@ -754,6 +807,12 @@ int wamgpu_propags_dev(wamgpu_ctx* ctx, void* f3, int ld, void* scratch, void* s
   if (!ctx || !ctx->impl || !f3) return WAMGPU_E_ARG;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   return DISPATCH_CTX(ctx, propags_dev_t, f3, ld, scratch, s);
+}
+
+int wamgpu_propags_dev_static(wamgpu_ctx* ctx, void* f3, int ld, void* stream) {
+  if (!ctx || !ctx->impl || !f3) return WAMGPU_E_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, propags_dev_static_t, f3, ld, s);
 }
 
 int wamgpu_step_dev(wamgpu_ctx* ctx, void* fl3, int ld, void* scratch, int nprop, const void* u10, const void* udir,

@@ -31,6 +31,7 @@ template <typename R> cudaError_t implsch_set_max_smem(int points_per_cta, size_
 template <typename R> cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s);
 template <typename R> cudaError_t launch_cfl_extrema(const PropArgs<R>& A, long long* ext, int nsm, cudaStream_t s);
 double cfl_decode(long long v, int precision);
+cudaError_t static_scratch_address(void** p);
 // direction cosines for the propagation kernels (constant memory of the
 // current device)
 template <typename R> cudaError_t set_direction_tables(const R* sinth, const R* costh, int kl);

@@ -140,6 +140,13 @@ cudaError_t launch_cfl_extrema(const PropArgs<R>& A, long long* ext, int nsm, cu
   return dispatch<R, CflLaunch>(A, ext, blocks, s);
 }
 
+// Fixed F1 ping-pong spectrum of wamgpu_propags_dev_static: one per device,
+// reserved when the module loads, never allocated or freed by the library.
+static __device__ __align__(256) unsigned char g_static_prop_scratch[WAMGPU_STATIC_SCRATCH_BYTES];
+
+// Device address of g_static_prop_scratch on the current device.
+cudaError_t static_scratch_address(void** p) { return cudaGetSymbolAddress(p, g_static_prop_scratch); }
+
 double cfl_decode(long long v, int precision) {
   if (precision == 4) {
     int i = (int)v;

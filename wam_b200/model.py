@@ -186,6 +186,14 @@ class WamModel:
         sc = None if scratch is None else ctypes.c_void_p(scratch.data_ptr())
         self._check(self.L.wamgpu_propags_dev(self.h, f3.data_ptr(), ld, sc, s), "propags_dev")
 
+    def propags_dev_static(self, f3, ld=None, stream=None):
+        """PROPAGS through the fixed per-device scratch (no allocation; calls
+        overlapping on one device race, spectra above WAMGPU_STATIC_SCRATCH_BYTES
+        are rejected)."""
+        ld = f3.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        self._check(self.L.wamgpu_propags_dev_static(self.h, f3.data_ptr(), ld, s), "propags_dev_static")
+
     def step(self, fl3, nprop, u10, udir, tauw, ustar, z0, roairn, wstar):
         """nprop x PROPAGS then IMPLSCH on host arrays (one H2D and one D2H of FL3)."""
         for a in (fl3, tauw, ustar, z0):
