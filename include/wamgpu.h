@@ -5,7 +5,7 @@
  * spectral propagation PROPAGS with depth and current refraction.
  *
  * The Fortran driver binds these entry points through ISO_C_BINDING behind
- * the reference's own module procedure names (see INTEGRATION.md).  Every
+ * the reference's own module procedure names.  Every
  * entry point that replaces a reference procedure cites it; references are
  * myWAveModel/WAM file:line.
  *
@@ -158,7 +158,12 @@ WAMGPU_API int wamgpu_propags_dev_static(wamgpu_ctx* ctx, void* f3, int ld, void
  * nprop PROPAGS calls (IDELT/IDELPRO of them per source step) followed by
  * one IMPLSCH, with the spectrum resident on the device for the whole pass.
  * The _host form copies FL3 and the per-point fields in once and back once
- * (FP32 contexts); the _dev form works on caller-owned device buffers. */
+ * (FP32 contexts), overlapping the copies with the kernels on a second
+ * stream: without current refraction the spectrum goes up in groups of
+ * frequency planes, each propagated as soon as it has arrived, and the
+ * result comes down by sea-point ranges as IMPLSCH finishes them.  Host
+ * buffers should be pinned for the copies to overlap.  The _dev form works
+ * on caller-owned device buffers. */
 WAMGPU_API int wamgpu_step_dev(wamgpu_ctx* ctx, void* fl3, int ld, void* scratch, int nprop, const void* u10,
                                const void* udir, void* tauw, void* ustar, void* z0, const void* roairn,
                                const void* wstar, void* stream);

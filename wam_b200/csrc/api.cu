@@ -42,6 +42,8 @@ struct wamgpu_ctx {
   Config cfg{};
   std::string err;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // host<->device copies overlapped with the kernels of a host-buffer step
+  std::vector<cudaEvent_t> xfer_ev;     // ordering events between the two streams
   int nsm = 148;
   int P = 8;  // sea points per IMPLSCH CTA
   // grid (reference convention, host)
@@ -446,6 +448,7 @@ int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u1
   a.depth = I.d_depth.template as<R>(); a.indep = I.d_indep.template as<int>();
   a.tauw = (R*)tauw; a.ustar = (R*)ustar; a.z0 = (R*)z0;
   a.fluxes = ctx->cfg.lcflx ? I.fluxes.template as<R>() : nullptr;
+  a.flx_ld = ctx->nsea;
   a.status = I.status.template as<int>();
   { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch"); }
   return WAMGPU_OK;
@@ -584,26 +587,96 @@ int implsch_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, const float* u10, co
   return wamgpu_sync(ctx);
 }
 
+// Host-buffer form of one WAMODEL pass, with the copies overlapped:
+//  - without current refraction a PROPAGS sub-step of frequency plane m reads
+//    only plane m, so the spectrum goes up in groups of planes on the copy
+//    stream and each group is propagated (all nprop*COUNTER sub-steps) as
+//    soon as it has arrived;
+//  - IMPLSCH then runs over ranges of sea points, and each range's spectrum
+//    and TAUW/USTAR/Z0 go down on the copy stream while the next range is
+//    integrated.
+// Results are identical to the unsplit sequence: every kernel sees the same
+// inputs and writes the same elements.
 template <typename R>
 int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float* u10, const float* udir, float* tauw,
                 float* ustar, float* z0, const float* roairn, const float* wstar) {
   static_assert(sizeof(R) == 4 || sizeof(R) == 8, "");
   if (sizeof(R) != 4) return fail(ctx, WAMGPU_E_ARG, "wamgpu_step_host is FP32 only; use wamgpu_step_dev");
-  const int n = ctx->nsea;
-  const size_t nb = (size_t)n * ctx->cfg.kl * ctx->cfg.ml;
-  cudaStream_t s = ctx->stream;
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
+  if (nprop < 0) return fail(ctx, WAMGPU_E_ARG, "nprop < 0");
+  if (ctx->cfg.shallow_run && ctx->cfg.isnonlin != 0 && !I.dt.ENH)
+    return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_source first (ISNONLIN table)");
+  const int n = ctx->nsea, KL = ctx->cfg.kl, ML = ctx->cfg.ml;
+  const size_t plane = (size_t)n * KL, nb = plane * ML;
+  cudaStream_t s = ctx->stream, c = ctx->copy_stream;
   CK(I.fl3.ensure(nb * sizeof(R)), "alloc");
+  CK(I.scratch.ensure(nb * sizeof(R)), "alloc scratch");
   for (DevBuf* b : {&I.u10, &I.udir, &I.tauw, &I.ustar, &I.z0, &I.roairn, &I.wstar}) CK(b->ensure((size_t)n * sizeof(R) + 16), "alloc");
-  struct Up { void* d; const float* h; size_t n; };
-  Up ups[] = {{I.fl3.p, fl3, nb}, {I.u10.p, u10, (size_t)n}, {I.udir.p, udir, (size_t)n}, {I.tauw.p, tauw, (size_t)n},
-              {I.ustar.p, ustar, (size_t)n}, {I.z0.p, z0, (size_t)n}, {I.roairn.p, roairn, (size_t)n}, {I.wstar.p, wstar, (size_t)n}};
-  for (auto& u : ups) CK(cudaMemcpyAsync(u.d, u.h, u.n * 4, cudaMemcpyHostToDevice, s), "H2D");
-  int rc = step_dev_t<R>(ctx, I, I.fl3.p, n, nullptr, nprop, I.u10.p, I.udir.p, I.tauw.p, I.ustar.p, I.z0.p, I.roairn.p,
-                         I.wstar.p, s);
-  if (rc) return rc;
-  struct Dn { float* h; void* d; size_t n; };
-  Dn dns[] = {{fl3, I.fl3.p, nb}, {tauw, I.tauw.p, (size_t)n}, {ustar, I.ustar.p, (size_t)n}, {z0, I.z0.p, (size_t)n}};
-  for (auto& d : dns) CK(cudaMemcpyAsync(d.h, d.d, d.n * 4, cudaMemcpyDeviceToHost, s), "D2H");
+  if (!I.status.p) { CK(I.status.ensure(16), "alloc"); CK(cudaMemsetAsync(I.status.p, 0, 16, s), "memset"); }
+  if (ctx->cfg.lcflx) CK(I.fluxes.ensure((size_t)7 * n * sizeof(R) + 16), "alloc");
+  struct Up { void* d; const float* h; };
+  Up ups[] = {{I.u10.p, u10}, {I.udir.p, udir}, {I.tauw.p, tauw}, {I.ustar.p, ustar}, {I.z0.p, z0}, {I.roairn.p, roairn},
+              {I.wstar.p, wstar}};
+  for (auto& u : ups) CK(cudaMemcpyAsync(u.d, u.h, (size_t)n * 4, cudaMemcpyHostToDevice, s), "H2D");
+  R* f3 = I.fl3.template as<R>();
+  R* sc = I.scratch.template as<R>();
+  const int nsub = nprop * ctx->counter;
+  const bool split = n > 0 && nsub > 0 && propags_planes_independent(I.pa.variant);
+  const int ngrp = split ? std::min(ML, 6) : 1;
+  const int npart = n > 0 ? std::min(8, (n + 1023) / 1024) : 1;
+  if ((int)ctx->xfer_ev.size() < ngrp + npart)
+    for (int i = (int)ctx->xfer_ev.size(); i < ngrp + npart; ++i) {
+      cudaEvent_t e;
+      CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+      ctx->xfer_ev.push_back(e);
+    }
+  // upload and propagate, plane group by plane group
+  R* fin = f3;
+  for (int g = 0; g < ngrp; ++g) {
+    const int m0 = (int)((long long)ML * g / ngrp), m1 = (int)((long long)ML * (g + 1) / ngrp);
+    if (split) {
+      CK(cudaMemcpyAsync(f3 + plane * m0, fl3 + plane * m0, plane * (m1 - m0) * 4, cudaMemcpyHostToDevice, c), "H2D");
+      CK(cudaEventRecord(ctx->xfer_ev[g], c), "event");
+      CK(cudaStreamWaitEvent(s, ctx->xfer_ev[g], 0), "wait");
+    } else {
+      CK(cudaMemcpyAsync(f3, fl3, nb * 4, cudaMemcpyHostToDevice, s), "H2D");
+    }
+    R* src = f3; R* dst = sc;
+    for (int it = 0; it < nsub; ++it) {
+      { TimedLaunch tl(ctx, 0, s); CK(launch_propags<R>(I.pa, src, n, dst, n, s, split ? m0 : 0, split ? m1 - m0 : -1), "propags launch"); }
+      std::swap(src, dst);
+    }
+    fin = src;
+  }
+  // integrate and download, sea-point range by range
+  for (int q = 0; q < npart; ++q) {
+    const int p0 = (int)((long long)n * q / npart), p1 = (int)((long long)n * (q + 1) / npart);
+    if (p1 > p0) {
+      ImplArgs<R> a;
+      a.nsea = p1 - p0; a.ld = n;
+      a.fl3_in = fin + p0; a.fl3 = f3 + p0;
+      a.u10 = I.u10.template as<R>() + p0; a.udir = I.udir.template as<R>() + p0;
+      a.roairn = I.roairn.template as<R>() + p0; a.wstar = I.wstar.template as<R>() + p0;
+      a.depth = I.d_depth.template as<R>() + p0; a.indep = I.d_indep.template as<int>() + p0;
+      a.tauw = I.tauw.template as<R>() + p0; a.ustar = I.ustar.template as<R>() + p0; a.z0 = I.z0.template as<R>() + p0;
+      a.fluxes = ctx->cfg.lcflx ? I.fluxes.template as<R>() + p0 : nullptr;
+      a.flx_ld = n;
+      a.status = I.status.template as<int>();
+      DevTables<R> dt = I.dt;
+      if (dt.ENH) dt.ENH += p0;
+      { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(dt, a, ctx->P, s), "implsch launch"); }
+    }
+    CK(cudaEventRecord(ctx->xfer_ev[ngrp + q], s), "event");
+    CK(cudaStreamWaitEvent(c, ctx->xfer_ev[ngrp + q], 0), "wait");
+    if (p1 > p0) {
+      const size_t w = (size_t)(p1 - p0) * 4;
+      CK(cudaMemcpy2DAsync(fl3 + p0, (size_t)n * 4, f3 + p0, (size_t)n * 4, w, (size_t)KL * ML, cudaMemcpyDeviceToHost, c), "D2H");
+      CK(cudaMemcpyAsync(tauw + p0, I.tauw.template as<R>() + p0, w, cudaMemcpyDeviceToHost, c), "D2H");
+      CK(cudaMemcpyAsync(ustar + p0, I.ustar.template as<R>() + p0, w, cudaMemcpyDeviceToHost, c), "D2H");
+      CK(cudaMemcpyAsync(z0 + p0, I.z0.template as<R>() + p0, w, cudaMemcpyDeviceToHost, c), "D2H");
+    }
+  }
+  CK(cudaStreamSynchronize(c), "step copies");
   CK(cudaStreamSynchronize(s), "step sync");
   return wamgpu_sync(ctx);
 }
@@ -683,6 +756,7 @@ int wamgpu_create(const wamgpu_config* cfg, wamgpu_ctx** out) {
   if (c.device < 0 || c.device >= ndev) return bail(fail(ctx, WAMGPU_E_ARG, "device ordinal out of range"));
   if ((e = cudaSetDevice(c.device)) != cudaSuccess) return bail(cuda_fail(ctx, e, "cudaSetDevice"));
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(cuda_fail(ctx, e, "stream"));
+  if ((e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(cuda_fail(ctx, e, "stream"));
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, c.device);
   int rc;
   if (c.precision == 8) { auto* I = new Impl<double>(); ctx->impl.reset(I); rc = build_tables<double>(ctx, *I); }
@@ -695,9 +769,12 @@ int wamgpu_create(const wamgpu_config* cfg, wamgpu_ctx** out) {
 int wamgpu_destroy(wamgpu_ctx* ctx) {
   if (!ctx) return WAMGPU_OK;
   if (ctx->stream) { cudaSetDevice(ctx->cfg.device); cudaStreamSynchronize(ctx->stream); }
+  if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
   ctx->impl.reset();
   for (int c = 0; c < 2; ++c) for (auto& e : ctx->ev[c]) ctx->ev_pool.push_back(e);
   for (auto& e : ctx->ev_pool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
+  for (auto e : ctx->xfer_ev) cudaEventDestroy(e);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return WAMGPU_OK;

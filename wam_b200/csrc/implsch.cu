@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
     if (lane == 0) {
       a.tauw[ij] = ps.TAUW; a.ustar[ij] = ps.USTAR; a.z0[ij] = ps.Z0;
       if (T.lcflx && a.fluxes)
-        for (int q = 0; q < 7; ++q) a.fluxes[ij + (size_t)a.nsea * q] = ps.flx[q];
+        for (int q = 0; q < 7; ++q) a.fluxes[ij + (size_t)a.flx_ld * q] = ps.flx[q];
       if (!isfinite(ps.TAUW) || !isfinite(ps.USTAR) || !isfinite(ps.Z0)) atomicOr(a.status, 1);
     }
   }

@@ -20,7 +20,8 @@ template <typename R> struct ImplArgs {
   R* fl3;           // spectrum written
   const R* u10; const R* udir; const R* roairn; const R* wstar; const R* depth; const int* indep;
   R* tauw; R* ustar; R* z0;
-  R* fluxes;   // 7 x nsea or null
+  R* fluxes;   // 7 x flx_ld or null
+  int flx_ld;  // leading dimension of fluxes (the full NSEA when a launch covers a range of points)
   int* status; // bit 0: non-finite output
 };
 
@@ -28,7 +29,12 @@ template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const Im
 template <typename R> size_t implsch_smem_bytes(const DevTables<R>& T, int points_per_cta);
 template <typename R> cudaError_t implsch_set_max_smem(int points_per_cta, size_t bytes);
 
-template <typename R> cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s);
+// PROPAGS over the frequency planes m0 .. m0+mcount-1 (mcount < 0: to ML).
+template <typename R>
+cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s, int m0 = 0,
+                           int mcount = -1);
+// True when a sub-step of plane m reads only plane m (no current refraction).
+bool propags_planes_independent(int variant);
 template <typename R> cudaError_t launch_cfl_extrema(const PropArgs<R>& A, long long* ext, int nsm, cudaStream_t s);
 double cfl_decode(long long v, int precision);
 cudaError_t static_scratch_address(void** p);

@@ -8,9 +8,9 @@ namespace wamgpu {
 // One thread per (sea point, frequency) walking the directions.
 template <typename R, int VAR, bool RED, bool REFRD>
 __global__ void __launch_bounds__(128) propags_kernel(const PropArgs<R> A, const R* __restrict__ f1, int ld1,
-                                                      R* __restrict__ f3, int ld3) {
+                                                      R* __restrict__ f3, int ld3, int m0) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int m = blockIdx.y;
+  const int m = m0 + blockIdx.y;
   if (i >= A.nsea) return;
   using S = Site<R, VAR, RED, REFRD>;
   const S site(A, i, m);
@@ -111,9 +111,9 @@ cudaError_t dispatch(const PropArgs<R>& A, Args&&... args) {
 }
 
 template <typename R, int V, bool RED, bool RD> struct PropLaunch {
-  static cudaError_t run(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s) {
-    dim3 grid((A.nsea + 127) / 128, A.ML);
-    propags_kernel<R, V, RED, RD><<<grid, 128, 0, s>>>(A, f1, ld1, f3, ld3);
+  static cudaError_t run(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, int m0, int mcount, cudaStream_t s) {
+    dim3 grid((A.nsea + 127) / 128, mcount);
+    propags_kernel<R, V, RED, RD><<<grid, 128, 0, s>>>(A, f1, ld1, f3, ld3, m0);
     return cudaGetLastError();
   }
 };
@@ -125,9 +125,16 @@ template <typename R, int V, bool RED, bool RD> struct CflLaunch {
 };
 
 template <typename R>
-cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s) {
-  if (A.nsea == 0) return cudaSuccess;
-  return dispatch<R, PropLaunch>(A, f1, ld1, f3, ld3, s);
+cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s, int m0, int mcount) {
+  if (mcount < 0) mcount = A.ML - m0;
+  if (m0 < 0 || mcount < 0 || m0 + mcount > A.ML) return cudaErrorInvalidValue;
+  if (A.nsea == 0 || mcount == 0) return cudaSuccess;
+  return dispatch<R, PropLaunch>(A, f1, ld1, f3, ld3, m0, mcount, s);
+}
+
+bool propags_planes_independent(int variant) {
+  return variant != V_CART_DEEP_CUR && variant != V_CART_SHALLOW_CUR && variant != V_SPHER_DEEP_CURR &&
+         variant != V_SPHER_SHALLOW_CURR;
 }
 
 template <typename R>
@@ -157,8 +164,8 @@ double cfl_decode(long long v, int precision) {
   double d; memcpy(&d, &i, 8); return d;
 }
 
-template cudaError_t launch_propags<float>(const PropArgs<float>&, const float*, int, float*, int, cudaStream_t);
-template cudaError_t launch_propags<double>(const PropArgs<double>&, const double*, int, double*, int, cudaStream_t);
+template cudaError_t launch_propags<float>(const PropArgs<float>&, const float*, int, float*, int, cudaStream_t, int, int);
+template cudaError_t launch_propags<double>(const PropArgs<double>&, const double*, int, double*, int, cudaStream_t, int, int);
 template cudaError_t launch_cfl_extrema<float>(const PropArgs<float>&, long long*, int, cudaStream_t);
 template cudaError_t launch_cfl_extrema<double>(const PropArgs<double>&, long long*, int, cudaStream_t);
 template cudaError_t set_direction_tables<float>(const float*, const float*, int);
