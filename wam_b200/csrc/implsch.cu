@@ -21,12 +21,13 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
   const int NS = T.NS, KL = T.KL, LD = T.ld;
   const size_t wsb = warp_ws_bytes<R>(LD, T.ML, T.need_sp, T.scr);
   unsigned char* ws0 = smem + tables_bytes<R>(T.lay);
+  const size_t foff = ws_f_offset<R>(LD, T.ML);  // F follows the interleaved {SL, FL} block
   const int ij0 = blockIdx.x * P;
   // stage the P spectra: consecutive threads take consecutive points of one bin
   for (int idx = tid; idx < P * NS; idx += nthr) {
     int p = idx % P, b = idx / P, ij = ij0 + p;
     int m = b / KL, k = b - m * KL;
-    if (ij < a.nsea) reinterpret_cast<R*>(ws0 + p * wsb)[k + LD * m] = a.fl3_in[ij + (size_t)a.ld * b];
+    if (ij < a.nsea) reinterpret_cast<R*>(ws0 + p * wsb + foff)[k + LD * m] = a.fl3_in[ij + (size_t)a.ld * b];
   }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, ij = ij0 + warp;
@@ -37,10 +38,10 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
     unsigned char* base = ws0 + warp * wsb;
     const int nrow = LD * T.ML;
     w.ld = LD; w.scr = T.scr;
-    w.F = reinterpret_cast<R*>(base);
-    w.SL = w.F + nrow; w.FL = w.SL + nrow;
-    w.SP = T.need_sp ? w.FL + nrow : nullptr;
-    w.T = w.FL + nrow * (T.need_sp ? 2 : 1);
+    w.SF = reinterpret_cast<typename WarpWS<R>::R2*>(base);
+    w.F = reinterpret_cast<R*>(base + foff);
+    w.SP = T.need_sp ? w.F + nrow : nullptr;
+    w.T = w.F + nrow * (T.need_sp ? 2 : 1);
     w.LL = reinterpret_cast<uint8_t*>(w.T + 8 * T.scr);
     Src<R> src(T, S, w, lane, ij, a.indep[ij], a.u10[ij], a.udir[ij], a.roairn[ij], a.wstar[ij], a.depth[ij]);
     PointState<R> ps;
@@ -58,7 +59,7 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
     int p = idx % P, b = idx / P, ijs = ij0 + p;
     int m = b / KL, k = b - m * KL;
     if (ijs < a.nsea) {
-      R v = reinterpret_cast<R*>(ws0 + p * wsb)[k + LD * m];
+      R v = reinterpret_cast<R*>(ws0 + p * wsb + foff)[k + LD * m];
       a.fl3[ijs + (size_t)a.ld * b] = v;
       if (!isfinite(v)) atomicOr(a.status, 1);
     }

@@ -52,14 +52,26 @@ template <typename R> struct STabs {
   }
 };
 
+template <typename R> struct Vec2;
+template <> struct Vec2<float> { using type = float2; };
+template <> struct Vec2<double> { using type = double2; };
+
 // Per-warp (per sea point) shared-memory workspace: bin (k,m) at k + ld*m.
+// The source term SL and its diagonal derivative FL are always touched
+// together, so they are interleaved (SF[b] = {SL, FL}): one 2-wide access per
+// bin, which halves the load/store count of the DIA scatter.
 template <typename R> struct WarpWS {
-  R *F, *SL, *FL, *SP;  // spectrum, source, diagonal derivative, positive input (SMIN when LCFLX)
+  using R2 = typename Vec2<R>::type;
+  R2* SF;               // {SL, FL} per bin (first: 2*sizeof(R)-aligned)
+  R *F, *SP;            // spectrum, positive input (SMIN when LCFLX)
   R* T;                 // 8 scratch rows of length scr (per frequency / direction)
   uint8_t* LL;          // LLWS mask
   int ld, scr;
   __device__ R* t(int i) const { return T + i * scr; }
 };
+
+// Byte offset of the spectrum F inside a warp's workspace (after SF).
+template <typename R> __host__ __device__ inline size_t ws_f_offset(int ld, int ML) { return 2 * (size_t)ld * ML * sizeof(R); }
 
 template <typename R> __host__ __device__ inline size_t warp_ws_bytes(int ld, int ML, int need_sp, int scr) {
   size_t n = (size_t)ld * ML;
@@ -88,6 +100,21 @@ template <typename R> struct Src {
   __device__ int ML() const { return T.ML; }
   __device__ R tfak(int m) const { return __ldg(&T.TFAK[(INDEP - 1) + T.NDEPTH * m]); }
   __device__ R tcgond(int m) const { return __ldg(&T.TCGOND[(INDEP - 1) + T.NDEPTH * m]); }
+  using R2 = typename Vec2<R>::type;
+  __device__ static R2 r2(R a, R b) { R2 v; v.x = a; v.y = b; return v; }
+
+  // Lane-strided walk over the bins of frequencies [0, nm): bin b = lane + 32 i
+  // is direction k = b mod KL of frequency m = b div KL; (m, k) advance by
+  // (32 div KL, 32 mod KL) with one carry instead of a division per bin.
+  template <class Fn> __device__ __forceinline__ void for_bins(int nm, Fn&& fn) const {
+    const int kl = KL(), n = kl * nm, q = 32 / kl, r = 32 - q * kl;
+    int m = lane / kl, k = lane - m * kl;
+    for (int b = lane; b < n; b += 32) {
+      fn(m, k);
+      k += r; m += q;
+      if (k >= kl) { k -= kl; ++m; }
+    }
+  }
 
   // TOTAL_ENERGY + FEMEAN (+ WM1 for AKMEAN); masked when mask != null.
   __device__ void integrals(const uint8_t* mask, R& emean, R& fmean, R* akmean) const {
@@ -241,8 +268,7 @@ template <typename R> struct Src {
         if (w.SP) w.SP[b] = spos;
         st = st + spos; sx = sx + spos * S.SINTH[k]; sy = sy + spos * S.COSTH[k];
         R fl = R(0.5) * (flp[0] + flp[1]);
-        w.FL[b] = fl;
-        w.SL[b] = fl * f;
+        w.SF[b] = r2(fl * f, fl);
         w.LL[b] = ll;
       }
       for (int g = 0; g < 2; ++g) { xst[g] = xst[g] + warp_sum(px[g]); yst[g] = yst[g] + warp_sum(py[g]); }
@@ -321,14 +347,13 @@ template <typename R> struct Src {
   __device__ void stresso_sp(R USTAR, R Z0, int mij, R& TAUW, R& PHIAW) const {
     const int kl = KL(), ld = w.ld;
     R pphi = 0, px = 0, py = 0;
-    for (int b = lane; b < kl * mij; b += 32) {
-      int m = b / kl, k = b - m * kl;
+    for_bins(mij, [&](int m, int k) {
       R rw = rhowgdfth(m, mij), cmr = cmw(m) * rw;
       R sp = dmax(w.SP[k + ld * m], R(0.));
       pphi = pphi + sp * rw;
       px = px + (sp * S.SINTH[k]) * cmr;
       py = py + (sp * S.COSTH[k]) * cmr;
-    }
+    });
     stresso_finish(USTAR, Z0, mij, pphi, px, py, TAUW, PHIAW);
   }
 
@@ -361,11 +386,10 @@ template <typename R> struct Src {
     }
     __syncwarp();
     const R base = t[mij - 1];
-    const int nb = kl * (ml - mij);
-    for (int i = lane; i < nb; i += 32) {
-      int dm = i / kl, k = i - dm * kl, m = mij + dm;
+    for_bins(ml - mij, [&](int dm, int k) {
+      const int m = mij + dm;
       w.F[k + ld * m] = (t[m] / base) * w.F[k + ld * (mij - 1)];
-    }
+    });
     __syncwarp();
   }
 
@@ -398,8 +422,10 @@ template <typename R> struct Src {
           R dd = dmax(R(0.), bth[s] * tmp03 - R(1.0));
           R d = ssdsc2_sig * (temp1 + c6m1 * (dd * dd));
           int b = k + ld * m;
-          w.SL[b] = w.SL[b] + d * w.F[b];
-          w.FL[b] = w.FL[b] + d;
+          R2 v = w.SF[b];
+          v.x = v.x + d * w.F[b];
+          v.y = v.y + d;
+          w.SF[b] = v;
         }
       }
     }
@@ -416,7 +442,7 @@ template <typename R> struct Src {
       enhfr = R(1.) + (R(5.5) / enhfr) * (R(1.) - R(.833) * enhfr) * dexp(R(-1.25) * enhfr);
     }
     const int mfr1 = -T.MFRSTLW + 1, mfrl = ml - T.KFRH + mfr1;
-    R* SL = w.SL; R* FL = w.FL; const R* F = w.F;
+    R2* SF = w.SF; const R* F = w.F;
     // angular partners of this lane's directions, per KH and sub-pass (0-based)
     int k1[2][2], k2[2][2], k11[2][2], k21[2][2];
     for (int kh = 0; kh < 2; ++kh)
@@ -477,26 +503,25 @@ template <typename R> struct Src {
           if (k >= kl) break;
           const int bC = k + rMC, b2 = k2[kh][s] + rMM, b21 = k2[kh][s] + rMM1, b1 = k1[kh][s] + rMP,
                     b11 = k1[kh][s] + rMP1;
-          R sC = SL[bC], fC = FL[bC], s2 = SL[b2], f2 = FL[b2], s21 = SL[b21], f21 = FL[b21];
-          R s1 = SL[b1], f1 = FL[b1], s11 = SL[b11], f11 = FL[b11];
+          R2 vC = SF[bC], v2 = SF[b2], v21 = SF[b21], v1 = SF[b1], v11 = SF[b11];
           const R A = ad[kh][s], DM = delam[kh][s], DP = delap[kh][s];
-          if (wMC) { SL[bC] = sC - R(2.) * A; FL[bC] = fC - R(2.) * delad[kh][s]; }
-          if (wMM) { SL[b2] = s2 + A * rc[20]; FL[b2] = f2 + DM * rc[23]; }
-          if (wMM1) { SL[b21] = s21 + A * rc[17]; FL[b21] = f21 + DM * rc[21]; }
-          if (wMP) { SL[b1] = s1 + A * rc[8]; FL[b1] = f1 + DP * rc[11]; }
-          if (wMP1) { SL[b11] = s11 + A * rc[5]; FL[b11] = f11 + DP * rc[9]; }
+          if (wMC) { vC.x = vC.x - R(2.) * A; vC.y = vC.y - R(2.) * delad[kh][s]; SF[bC] = vC; }
+          if (wMM) { v2.x = v2.x + A * rc[20]; v2.y = v2.y + DM * rc[23]; SF[b2] = v2; }
+          if (wMM1) { v21.x = v21.x + A * rc[17]; v21.y = v21.y + DM * rc[21]; SF[b21] = v21; }
+          if (wMP) { v1.x = v1.x + A * rc[8]; v1.y = v1.y + DP * rc[11]; SF[b1] = v1; }
+          if (wMP1) { v11.x = v11.x + A * rc[5]; v11.y = v11.y + DP * rc[9]; SF[b11] = v11; }
         }
         __syncwarp();
         for (int s = 0; s < nsub; ++s) {
           const int k = lane + 32 * s;
           if (k >= kl) break;
           const int b2 = k21[kh][s] + rMM, b21 = k21[kh][s] + rMM1, b1 = k11[kh][s] + rMP, b11 = k11[kh][s] + rMP1;
-          R s2 = SL[b2], f2 = FL[b2], s21 = SL[b21], f21 = FL[b21], s1 = SL[b1], f1 = FL[b1], s11 = SL[b11], f11 = FL[b11];
+          R2 v2 = SF[b2], v21 = SF[b21], v1 = SF[b1], v11 = SF[b11];
           const R A = ad[kh][s], DM = delam[kh][s], DP = delap[kh][s];
-          if (wMM) { SL[b2] = s2 + A * rc[19]; FL[b2] = f2 + DM * rc[24]; }
-          if (wMM1) { SL[b21] = s21 + A * rc[18]; FL[b21] = f21 + DM * rc[22]; }
-          if (wMP) { SL[b1] = s1 + A * rc[7]; FL[b1] = f1 + DP * rc[12]; }
-          if (wMP1) { SL[b11] = s11 + A * rc[6]; FL[b11] = f11 + DP * rc[10]; }
+          if (wMM) { v2.x = v2.x + A * rc[19]; v2.y = v2.y + DM * rc[24]; SF[b2] = v2; }
+          if (wMM1) { v21.x = v21.x + A * rc[18]; v21.y = v21.y + DM * rc[22]; SF[b21] = v21; }
+          if (wMP) { v1.x = v1.x + A * rc[7]; v1.y = v1.y + DP * rc[12]; SF[b1] = v1; }
+          if (wMP1) { v11.x = v11.x + A * rc[6]; v11.y = v11.y + DP * rc[10]; SF[b11] = v11; }
         }
         __syncwarp();
       }
@@ -536,43 +561,45 @@ template <typename R> struct Src {
     R* SQB = w.t(2); R* LF = w.t(3); R* SDX = w.t(4); R* SDY = w.t(5); R* CI10 = w.t(6);
     const R cu = dcos(UDIR), su = dsin(UDIR), uproxy = R(32.) * USTAR;
     const R raw = ROAIRN / P_::ROWATER;
-    // directional narrowness and saturation per frequency
+    // directional narrowness and saturation per frequency; CI10 = k/sigma
+    // (the per-frequency factors of the direction loops are formed once)
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m];
       const R* fm = w.F + ld * m;
+      const R cgs = CG[m] / (P_::ZPI * sig);
       R s = 0, mx = 0;
-      for (int k = 0; k < kl; ++k) { R a = fm[k] * CG[m] / (P_::ZPI * sig); s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
+      for (int k = 0; k < kl; ++k) { R a = fm[k] * cgs; s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
       R s2 = 0;
-      for (int k = 0; k < kl; ++k) { R a = fm[k] * CG[m] / (P_::ZPI * sig); s2 = s2 + ((mx < R(1.0E-34)) ? R(1.) : a / mx); }
+      if (mx < R(1.0E-34)) s2 = R(kl);
+      else { const R rmx = R(1.) / mx; for (int k = 0; k < kl; ++k) s2 = s2 + (fm[k] * cgs) * rmx; }
       R adensig = s * sig * T.DELTH, anar = R(1.0) / (s2 * T.DELTH);
       SQB[m] = dsqrt(anar * adensig * (WN[m] * WN[m] * WN[m]));
+      CI10[m] = WN[m] / sig;
     }
     __syncwarp();
-    // growth rates per bin
-    for (int b = lane; b < kl * nk; b += 32) {
-      int m = b / kl, k = b - m * kl;
+    // growth rates per bin: D1 in SF.x, D2 in SF.y
+    for_bins(nk, [&](int m, int k) {
       R sig = P_::ZPI * S.FR[m], sqb = SQB[m];
-      R proj = uproxy * (WN[m] / sig) * (S.COSTH[k] * cu + S.SINTH[k] * su) - R(1.);
+      R proj = uproxy * CI10[m] * (S.COSTH[k] * cu + S.SINTH[k] * su) - R(1.);
       R w1 = dmax(R(0.), proj); w1 = w1 * w1;
       R w2 = dmin(R(0.), proj); w2 = w2 * w2;
       R d1 = raw * sig * (R(2.8) - (R(1.) + dtanh(R(10.) * sqb * w1 - R(11.)))) * sqb * w1;
       R d2 = raw * sig * R(0.09) * (R(2.8) - (R(1.) + dtanh(R(10.) * sqb * w2 - R(11.)))) * sqb * w2;
-      w.SL[k + ld * m] = d1;
-      w.FL[k + ld * m] = d2;
-    }
+      w.SF[k + ld * m] = r2(d1, d2);
+    });
     __syncwarp();
     // directional sums of the positive stress spectrum (LFACTOR :4580-4595)
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m], bx = 0, by = 0;
-      const R* fm = w.F + ld * m; const R* d1 = w.SL + ld * m;
+      const R* fm = w.F + ld * m; const R2* d1 = w.SF + ld * m;
+      const R cgs = CG[m] / (P_::ZPI * sig), scg = sig / CG[m];
       for (int k = 0; k < kl; ++k) {
-        R a = fm[k] * CG[m] / (P_::ZPI * sig);
-        R sd = d1[k] * a * sig / CG[m];
+        R a = fm[k] * cgs;
+        R sd = d1[k].x * a * scg;
         bx = bx + dmax(R(0.), sd) * S.COSTH[k];
         by = by + dmax(R(0.), sd) * S.SINTH[k];
       }
       SDX[m] = bx * T.DELTH; SDY[m] = by * T.DELTH;
-      CI10[m] = WN[m] / sig;
     }
     __syncwarp();
     // extension to 10 Hz with an f^-2 tail (point-independent axis in S.SIG10/S.DSII10)
@@ -626,17 +653,17 @@ template <typename R> struct Src {
     for (int m = lane; m < nk; m += 32) sumlf = sumlf + LF[m];
     const bool reduce = warp_sum(sumlf) < R(nk);
     TAUW = dsqrt(tauwx * tauwx + tauwy * tauwy);
-    for (int b = lane; b < kl * nk; b += 32) {
-      int m = b / kl, k = b - m * kl, p = k + ld * m;
-      R d = w.SL[p];
+    for_bins(nk, [&](int m, int k) {
+      const int p = k + ld * m;
+      const R2 v = w.SF[p];
+      R d = v.x;
       if (reduce) d = d * LF[m];
-      R dtot = d - w.FL[p];
+      R dtot = d - v.y;
       R f = w.F[p];
-      w.SL[p] = dtot * f;
-      w.FL[p] = dtot;
+      w.SF[p] = r2(dtot * f, dtot);
       if (w.SP) w.SP[p] = d * f;
       w.LL[p] = (d * f > R(0));
-    }
+    });
     __syncwarp();
   }
 
@@ -677,10 +704,12 @@ template <typename R> struct Src {
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m];
       const R* fm = w.F + ld * m;
+      const R cgs = CG[m] / (P_::ZPI * sig);
       R s = 0, mx = 0;
-      for (int k = 0; k < kl; ++k) { R a = fm[k] * CG[m] / (P_::ZPI * sig); s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
+      for (int k = 0; k < kl; ++k) { R a = fm[k] * cgs; s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
       R s2 = 0;
-      for (int k = 0; k < kl; ++k) { R a = fm[k] * CG[m] / (P_::ZPI * sig); s2 = s2 + ((mx < R(1.0E-34)) ? R(1.) : a / mx); }
+      if (mx < R(1.0E-34)) s2 = R(kl);
+      else { const R rmx = R(1.) / mx; for (int k = 0; k < kl; ++k) s2 = s2 + (fm[k] * cgs) * rmx; }
       R anar = R(1.0) / (s2 * T.DELTH);
       AB[m] = s;
       BN[m] = anar * (s * sig * T.DELTH) * (WN[m] * WN[m] * WN[m]);
@@ -700,12 +729,14 @@ template <typename R> struct Src {
       AB[m] = (AB[m] > R(1.E-30)) ? -(R(2.) / R(3.) * b1 * sig * dsqrt(BN[m])) : R(0);
     }
     __syncwarp();
-    for (int b = lane; b < kl * nk; b += 32) {
-      int m = b / kl, k = b - m * kl, p = k + ld * m;
-      R f = w.F[p];
-      w.SL[p] = (w.SL[p] + T12[m] * f) + AB[m] * f;
-      w.FL[p] = (w.FL[p] + T12[m]) + AB[m];
-    }
+    for_bins(nk, [&](int m, int k) {
+      const int p = k + ld * m;
+      const R f = w.F[p];
+      R2 v = w.SF[p];
+      v.x = (v.x + T12[m] * f) + AB[m] * f;
+      v.y = (v.y + T12[m]) + AB[m];
+      w.SF[p] = v;
+    });
     __syncwarp();
   }
 
@@ -729,7 +760,7 @@ template <typename R> struct Src {
     if (T.iphys == 1) stresso_sums(USTAR, Z0, mij, TAUW, phiaw);
     else if (T.lcflx) { R td; stresso_sp(USTAR, Z0, mij, td, phiaw); }
     if (T.lcflx) {  // SMIN = SL - SPOS, kept in SP from here on
-      for (int b = lane; b < kl * ml; b += 32) { int m = b / kl, p = b - m * kl + ld * m; w.SP[p] = w.SL[p] - w.SP[p]; }
+      for_bins(ml, [&](int m, int k) { const int p = k + ld * m; w.SP[p] = w.SF[p].x - w.SP[p]; });
       __syncwarp();
     }
     if (T.iphys == 1) sdissip_ard();
@@ -748,11 +779,11 @@ template <typename R> struct Src {
     if (T.lcflx) {  // WNFLUXES on SSOURCE = SL - SMIN and SL_BOT
       const R rog = P_::ROWATER * P_::G, scdfm = R(0.5) * T.DELTH * (R(1.) - R(1.) / P_::CO);
       R a[6] = {0, 0, 0, 0, 0, 0};
-      for (int b = lane; b < kl * mij; b += 32) {
-        int m = b / kl, k = b - m * kl, p = k + ld * m;
+      for_bins(mij, [&](int m, int k) {
+        const int p = k + ld * m;
         R cfm = (m < mij - 1) ? rog * S.DFIM[m] : rog * scdfm * S.FR[m];
         R cm = T.shallow ? tfak(m) / (P_::ZPI * S.FR[m]) : P_::ZPI * S.FR[m] / P_::G;
-        R src = w.SL[p] - w.SP[p];
+        R src = w.SF[p].x - w.SP[p];
         a[0] = a[0] + src * cfm;
         a[1] = a[1] + cm * src * cfm * S.SINTH[k];
         a[2] = a[2] + cm * src * cfm * S.COSTH[k];
@@ -762,7 +793,7 @@ template <typename R> struct Src {
           a[4] = a[4] + cm * bot * cfm * S.SINTH[k];
           a[5] = a[5] + cm * bot * cfm * S.COSTH[k];
         }
-      }
+      });
       for (int i = 0; i < 6; ++i) a[i] = warp_sum(a[i]);
       R tau = P_::ROAIR * USTAR * USTAR;
       ps.flx[0] = phiaw - a[0];
@@ -773,17 +804,24 @@ template <typename R> struct Src {
     }
     // implicit integration with the growth limiter and the minimum-energy floor
     const R delt = T.DELT, fmx = dmax(fmeanws, fmean);
-    for (int b = lane; b < kl * ml; b += 32) {
-      int m = b / kl, k = b - m * kl, p = k + ld * m;
+    R* C2 = w.t(2); R* LIM = w.t(3); R* FMIN = w.t(4);  // cos^2 spreading, limiter, floor
+    for (int k = lane; k < kl; k += 32) { R c = dmax(R(0.), dcos(S.TH[k] - UDIR)); C2[k] = c * c; }
+    for (int m = lane; m < ml; m += 32) {
+      LIM[m] = USTAR * S.DELFL[m] * fmx;
+      FMIN[m] = __ldg(&T.FLMINFR[(ju - 1) + 300 * m]);
+    }
+    __syncwarp();
+    for_bins(ml, [&](int m, int k) {
+      const int p = k + ld * m;
       R f0 = w.F[p];
-      R sl = w.SL[p], fl = w.FL[p];
+      const R2 v = w.SF[p];
+      R sl = v.x, fl = v.y;
       if (T.shallow) { sl = sl + SBO[m] * f0; fl = fl + SBO[m]; }
       R t1 = delt * sl / dmax(R(1.), R(1.) - delt * fl);
-      R t3 = dmin(dabs(t1), USTAR * S.DELFL[m] * fmx);
+      R t3 = dmin(dabs(t1), LIM[m]);
       R f = f0 + ((t1 >= R(0)) ? t3 : -t3);
-      R c = dmax(R(0.), dcos(S.TH[k] - UDIR));
-      w.F[p] = dmax(f, __ldg(&T.FLMINFR[(ju - 1) + 300 * m]) * (c * c));
-    }
+      w.F[p] = dmax(f, FMIN[m] * C2[k]);
+    });
     __syncwarp();
     integrals(nullptr, emean, fmean, nullptr);
     integrals(w.LL, emeanws, fmeanws, nullptr);
