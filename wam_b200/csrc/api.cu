@@ -192,6 +192,15 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
     for (int v : t.K2W) if (v < 1 || v > KL) return fail(ctx, WAMGPU_E_ARG, "DIA angular index out of range");
     for (int v : t.K11W) if (v < 1 || v > KL) return fail(ctx, WAMGPU_E_ARG, "DIA angular index out of range");
     for (int v : t.K21W) if (v < 1 || v > KL) return fail(ctx, WAMGPU_E_ARG, "DIA angular index out of range");
+    // the kernel forms partner and source directions as rotations of k by a
+    // constant per table and KH: each table must be one
+    for (const std::vector<int>* tb : {&t.K1W, &t.K2W, &t.K11W, &t.K21W})
+      for (int kh = 0; kh < 2; ++kh) {
+        const int off = ((*tb)[KL * kh] - 1) % KL;
+        for (int k = 0; k < KL; ++k)
+          if ((*tb)[k + KL * kh] - 1 != (k + off) % KL)
+            return fail(ctx, WAMGPU_E_ARG, "DIA angular partner table is not a rotation of the directions");
+      }
     for (int v : t.INLCOEF) if (v < 1 || v > ML) return fail(ctx, WAMGPU_E_ARG, "DIA frequency index out of range");
     for (int v : t.INDICESSAT) if (v < 1 || v > KL) return fail(ctx, WAMGPU_E_ARG, "saturation index out of range");
     auto in = [&](int m) { return m >= 1 && m <= ML; };

@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
     w.SF = reinterpret_cast<typename WarpWS<R>::R2*>(base);
     w.F = reinterpret_cast<R*>(base + foff);
     w.SP = T.need_sp ? w.F + nrow : nullptr;
-    w.T = w.F + nrow * (T.need_sp ? 2 : 1);
+    w.T = reinterpret_cast<R*>(base + ws_t_offset<R>(LD, T.ML, T.need_sp));
     w.LL = reinterpret_cast<uint8_t*>(w.T + 8 * T.scr);
     Src<R> src(T, S, w, lane, ij, a.indep[ij], a.u10[ij], a.udir[ij], a.roairn[ij], a.wstar[ij], a.depth[ij]);
     PointState<R> ps;

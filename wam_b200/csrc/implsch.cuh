@@ -64,7 +64,7 @@ template <typename R> struct WarpWS {
   using R2 = typename Vec2<R>::type;
   R2* SF;               // {SL, FL} per bin (first: 2*sizeof(R)-aligned)
   R *F, *SP;            // spectrum, positive input (SMIN when LCFLX)
-  R* T;                 // 8 scratch rows of length scr (per frequency / direction)
+  R* T;                 // 8 scratch rows of length scr (per frequency / direction; the DIA's buffer)
   uint8_t* LL;          // LLWS mask
   int ld, scr;
   __device__ R* t(int i) const { return T + i * scr; }
@@ -75,7 +75,14 @@ template <typename R> __host__ __device__ inline size_t ws_f_offset(int ld, int 
 
 template <typename R> __host__ __device__ inline size_t warp_ws_bytes(int ld, int ML, int need_sp, int scr) {
   size_t n = (size_t)ld * ML;
-  size_t b = ((3 + (need_sp ? 1 : 0)) * n + 8 * (size_t)scr) * sizeof(R) + n;
+  size_t b = ((3 + (need_sp ? 1 : 0)) * n + 8 * (size_t)scr) * sizeof(R) + n + 16;  // + alignment of T
+  return (b + 15) & ~size_t(15);
+}
+
+// Byte offset of the scratch rows T (16-byte aligned: the DIA keeps 2-wide
+// values there).
+template <typename R> __host__ __device__ inline size_t ws_t_offset(int ld, int ML, int need_sp) {
+  size_t b = ws_f_offset<R>(ld, ML) + (size_t)ld * ML * sizeof(R) * (need_sp ? 2 : 1);
   return (b + 15) & ~size_t(15);
 }
 
@@ -434,6 +441,17 @@ template <typename R> struct Src {
 
   // SNONLIN (DIA) for ISNONLIN = 0 (depth scaling from AKMEAN) or the
   // MAKE_SHALLOW_SNL table.
+  //
+  // Gather form of the reference's scatter.  For each MC the lanes first
+  // compute the interactions of their directions for both KH and leave
+  // {AD, DELAM} and {AD, DELAP} in a per-warp buffer; then every lane updates
+  // only its own direction column of the five target rows (MC, MM, MM1, MP,
+  // MP1), collecting the contributions whose partner tables point at it.  The
+  // partner tables K1W, K2W, K11W and K21W are rotations of the directions by
+  // a constant (checked on the host), so each source index is the column
+  // rotated back.  The target rows of one MC are distinct (checked on the
+  // host), and no two lanes write the same column, so the only ordering
+  // needed is around the buffer.
   __device__ void snonlin(R AKMEAN) const {
     const int kl = KL(), ml = ML(), ld = w.ld;
     R enhfr = R(1);
@@ -443,13 +461,15 @@ template <typename R> struct Src {
     }
     const int mfr1 = -T.MFRSTLW + 1, mfrl = ml - T.KFRH + mfr1;
     R2* SF = w.SF; const R* F = w.F;
-    // angular partners of this lane's directions, per KH and sub-pass (0-based)
-    int k1[2][2], k2[2][2], k11[2][2], k21[2][2];
-    for (int kh = 0; kh < 2; ++kh)
-      for (int s = 0; s < 2; ++s) {
-        int k = min(lane + 32 * s, kl - 1), sl = k + kl * kh;
-        k1[kh][s] = S.K1W[sl] - 1; k2[kh][s] = S.K2W[sl] - 1; k11[kh][s] = S.K11W[sl] - 1; k21[kh][s] = S.K21W[sl] - 1;
-      }
+    R2* XM = reinterpret_cast<R2*>(w.T);  // [kh*kl + k] = {AD, DELAM}
+    R2* XP = XM + 2 * kl;                 // [kh*kl + k] = {AD, DELAP}
+    // rotation offsets of the partner tables, per KH (warp-uniform)
+    int o1[2], o2[2], o11[2], o21[2];
+    for (int kh = 0; kh < 2; ++kh) {
+      o1[kh] = S.K1W[kl * kh] - 1; o2[kh] = S.K2W[kl * kh] - 1;
+      o11[kh] = S.K11W[kl * kh] - 1; o21[kh] = S.K21W[kl * kh] - 1;
+    }
+    auto rot = [kl](int k, int o) { const int t = k + o; return t >= kl ? t - kl : t; };
     const int nsub = kl > 32 ? 2 : 1;
     for (int mc = 1; mc <= T.MLSTHG; ++mc) {
       const int im = mc - T.MFRSTLW;
@@ -468,63 +488,50 @@ template <typename R> struct Src {
       const bool wMP = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml);
       const bool wMP1 = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml && MP1 <= ml);
       // row offsets of targets this frequency does not write are clamped to row 0,
-      // so the batched loads below never leave the spectrum
+      // so the loads below never leave the spectrum
       const int rMC = wMC ? ld * (mc - 1) : 0, rMM = wMM ? ld * (MM - 1) : 0, rMM1 = wMM1 ? ld * (MM1 - 1) : 0,
                 rMP = wMP ? ld * (MP - 1) : 0, rMP1 = wMP1 ? ld * (MP1 - 1) : 0;
       const R g1 = rc[1], g2 = rc[2], g3 = rc[3], g4 = rc[4], g5 = rc[13], g6 = rc[14], g7 = rc[15], g8 = rc[16];
-      // all (KH, sub-pass) interactions of this frequency first: independent gathers
-      R ad[2][2], delad[2][2], delap[2][2], delam[2][2];
-      for (int kh = 0; kh < 2; ++kh)
-        for (int s = 0; s < 2; ++s) {
-          const int k = lane + 32 * s;
-          ad[kh][s] = delad[kh][s] = delap[kh][s] = delam[kh][s] = R(0);
-          if (s < nsub && k < kl) {
-            const int a1 = k1[kh][s], a11 = k11[kh][s], a2 = k2[kh][s], a21 = k21[kh][s];
-            R sap = g1 * F[a1 + rIP] + g2 * F[a11 + rIP] + g3 * F[a1 + rIP1] + g4 * F[a11 + rIP1];
-            R sam = g5 * F[a2 + rIM] + g6 * F[a21 + rIM] + g7 * F[a2 + rIM1] + g8 * F[a21 + rIM1];
-            R fij = F[k + rIC] * ftail;
-            R fad1 = fij * (sap + sam);
-            R fad2 = fad1 - R(2.) * sap * sam;
-            fad1 = fad1 + fad2;
-            R fcen = ftemp * fij;
-            ad[kh][s] = fad2 * fcen;
-            delad[kh][s] = fad1 * ftemp;
-            delap[kh][s] = (fij - R(2.) * sam) * T.DAL1 * fcen;
-            delam[kh][s] = (fij - R(2.) * sap) * T.DAL2 * fcen;
-          }
+      // 1. interactions (both KH) of this lane's directions
+      R adc[2] = {R(0), R(0)}, delc[2] = {R(0), R(0)};  // centre: AD and DELAD summed over KH
+      for (int s = 0; s < nsub; ++s) {
+        const int k = lane + 32 * s;
+        if (k >= kl) break;
+        const R fij = F[k + rIC] * ftail;
+        for (int kh = 0; kh < 2; ++kh) {
+          const int a1 = rot(k, o1[kh]), a11 = rot(k, o11[kh]), a2 = rot(k, o2[kh]), a21 = rot(k, o21[kh]);
+          R sap = g1 * F[a1 + rIP] + g2 * F[a11 + rIP] + g3 * F[a1 + rIP1] + g4 * F[a11 + rIP1];
+          R sam = g5 * F[a2 + rIM] + g6 * F[a21 + rIM] + g7 * F[a2 + rIM1] + g8 * F[a21 + rIM1];
+          R fad1 = fij * (sap + sam);
+          R fad2 = fad1 - R(2.) * sap * sam;
+          fad1 = fad1 + fad2;
+          R fcen = ftemp * fij;
+          const R ad = fad2 * fcen;
+          adc[s] = adc[s] + ad;
+          delc[s] = delc[s] + fad1 * ftemp;
+          XM[kl * kh + k] = r2(ad, (fij - R(2.) * sap) * T.DAL2 * fcen);
+          XP[kl * kh + k] = r2(ad, (fij - R(2.) * sam) * T.DAL1 * fcen);
         }
-      // Scatter in two phases per KH.  Within a phase the rows are distinct
-      // (checked on the host) and each target family is a rotation, so every
-      // lane's targets differ from every other lane's: all loads of a phase
-      // are issued before its stores.
-      for (int kh = 0; kh < 2; ++kh) {
-        for (int s = 0; s < nsub; ++s) {
-          const int k = lane + 32 * s;
-          if (k >= kl) break;
-          const int bC = k + rMC, b2 = k2[kh][s] + rMM, b21 = k2[kh][s] + rMM1, b1 = k1[kh][s] + rMP,
-                    b11 = k1[kh][s] + rMP1;
-          R2 vC = SF[bC], v2 = SF[b2], v21 = SF[b21], v1 = SF[b1], v11 = SF[b11];
-          const R A = ad[kh][s], DM = delam[kh][s], DP = delap[kh][s];
-          if (wMC) { vC.x = vC.x - R(2.) * A; vC.y = vC.y - R(2.) * delad[kh][s]; SF[bC] = vC; }
-          if (wMM) { v2.x = v2.x + A * rc[20]; v2.y = v2.y + DM * rc[23]; SF[b2] = v2; }
-          if (wMM1) { v21.x = v21.x + A * rc[17]; v21.y = v21.y + DM * rc[21]; SF[b21] = v21; }
-          if (wMP) { v1.x = v1.x + A * rc[8]; v1.y = v1.y + DP * rc[11]; SF[b1] = v1; }
-          if (wMP1) { v11.x = v11.x + A * rc[5]; v11.y = v11.y + DP * rc[9]; SF[b11] = v11; }
-        }
-        __syncwarp();
-        for (int s = 0; s < nsub; ++s) {
-          const int k = lane + 32 * s;
-          if (k >= kl) break;
-          const int b2 = k21[kh][s] + rMM, b21 = k21[kh][s] + rMM1, b1 = k11[kh][s] + rMP, b11 = k11[kh][s] + rMP1;
-          R2 v2 = SF[b2], v21 = SF[b21], v1 = SF[b1], v11 = SF[b11];
-          const R A = ad[kh][s], DM = delam[kh][s], DP = delap[kh][s];
-          if (wMM) { v2.x = v2.x + A * rc[19]; v2.y = v2.y + DM * rc[24]; SF[b2] = v2; }
-          if (wMM1) { v21.x = v21.x + A * rc[18]; v21.y = v21.y + DM * rc[22]; SF[b21] = v21; }
-          if (wMP) { v1.x = v1.x + A * rc[7]; v1.y = v1.y + DP * rc[12]; SF[b1] = v1; }
-          if (wMP1) { v11.x = v11.x + A * rc[6]; v11.y = v11.y + DP * rc[10]; SF[b11] = v11; }
-        }
-        __syncwarp();
       }
+      __syncwarp();
+      // 2. this lane's column j of the five target rows
+      for (int s = 0; s < nsub; ++s) {
+        const int j = lane + 32 * s;
+        if (j >= kl) break;
+        const R2 m2a = XM[rot(j, kl - o2[0])], m2b = XM[kl + rot(j, kl - o2[1])];
+        const R2 m21a = XM[rot(j, kl - o21[0])], m21b = XM[kl + rot(j, kl - o21[1])];
+        const R2 p1a = XP[rot(j, kl - o1[0])], p1b = XP[kl + rot(j, kl - o1[1])];
+        const R2 p11a = XP[rot(j, kl - o11[0])], p11b = XP[kl + rot(j, kl - o11[1])];
+        R2 vC = SF[j + rMC], vM = SF[j + rMM], vM1 = SF[j + rMM1], vP = SF[j + rMP], vP1 = SF[j + rMP1];
+        const R a2 = m2a.x + m2b.x, d2 = m2a.y + m2b.y, a21 = m21a.x + m21b.x, d21 = m21a.y + m21b.y;
+        const R a1 = p1a.x + p1b.x, d1 = p1a.y + p1b.y, a11 = p11a.x + p11b.x, d11 = p11a.y + p11b.y;
+        if (wMC) { vC.x = vC.x - R(2.) * adc[s]; vC.y = vC.y - R(2.) * delc[s]; SF[j + rMC] = vC; }
+        if (wMM) { vM.x = vM.x + (a2 * rc[20] + a21 * rc[19]); vM.y = vM.y + (d2 * rc[23] + d21 * rc[24]); SF[j + rMM] = vM; }
+        if (wMM1) { vM1.x = vM1.x + (a2 * rc[17] + a21 * rc[18]); vM1.y = vM1.y + (d2 * rc[21] + d21 * rc[22]); SF[j + rMM1] = vM1; }
+        if (wMP) { vP.x = vP.x + (a1 * rc[8] + a11 * rc[7]); vP.y = vP.y + (d1 * rc[11] + d11 * rc[12]); SF[j + rMP] = vP; }
+        if (wMP1) { vP1.x = vP1.x + (a1 * rc[5] + a11 * rc[6]); vP1.y = vP1.y + (d1 * rc[9] + d11 * rc[10]); SF[j + rMP1] = vP1; }
+      }
+      __syncwarp();  // the next frequency overwrites XM / XP
     }
   }
 
