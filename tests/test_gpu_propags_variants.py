@@ -81,3 +81,29 @@ def test_counter_substeps(oracle_mod):
     got = f.copy(order="F")
     m.propags(got)
     assert np.array_equal(got, ref)
+
+
+def test_grids_with_different_directions_side_by_side(oracle_mod):
+    """Two live contexts with KL=24 and KL=36, the second prepared last, each
+    propagate with their own direction tables."""
+    from wam_b200 import WamModel
+    from wam_b200.synth import make_workload
+    models = []
+    for w in (make_workload("c0", scale=0.2), make_workload("c1", scale=0.02)):
+        m = WamModel(w.cfg)
+        m.set_grid(w.grid)
+        m.set_depth(w.depth)
+        m.prepare_propagation()
+        models.append((w, m))
+    for w, m in models:
+        o = oracle_mod.Oracle(w.cfg)
+        o.set_grid(w.grid)
+        o.set_fields(w.depth)
+        o.prepare_propagation()
+        f = w.spectrum_f()
+        ref = o.propags(f.astype(float)).astype(np.float32)
+        got = f.copy(order="F")
+        m.propags(got)
+        assert np.array_equal(got, ref), w.name
+    for _, m in models:
+        m.close()

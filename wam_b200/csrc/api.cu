@@ -362,7 +362,7 @@ template <typename R> int prepare_prop(wamgpu_ctx* ctx, Impl<R>& I, float* total
   A.u = I.d_u.template as<R>(); A.v = I.d_v.template as<R>();
   A.TCGOND = I.tcgond.template as<R>(); A.TSIHKD = I.tsihkd.template as<R>(); A.TFAK = I.tfak.template as<R>();
   A.GOM = I.gom.template as<R>(); A.FR = I.fr.template as<R>();
-  CK(set_direction_tables<R>(t.SINTH.data(), t.COSTH.data(), KL), "direction tables");
+  for (int k = 0; k < KL; ++k) { A.sinth[k] = t.SINTH[k]; A.costh[k] = t.COSTH[k]; }
   // CHECK_CFL (:1917-2138) from the extrema of the recomputed coefficients
   CK(I.cflext.ensure(2 * CFL_NCLASS * sizeof(long long)), "alloc");
   CK(launch_cfl_extrema<R>(A, I.cflext.template as<long long>(), ctx->nsm, s), "cfl kernel");

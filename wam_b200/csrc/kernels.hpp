@@ -38,8 +38,5 @@ bool propags_planes_independent(int variant);
 template <typename R> cudaError_t launch_cfl_extrema(const PropArgs<R>& A, long long* ext, int nsm, cudaStream_t s);
 double cfl_decode(long long v, int precision);
 cudaError_t static_scratch_address(void** p);
-// direction cosines for the propagation kernels (constant memory of the
-// current device)
-template <typename R> cudaError_t set_direction_tables(const R* sinth, const R* costh, int kl);
 
 }  // namespace wamgpu

@@ -7,7 +7,7 @@ namespace wamgpu {
 
 // One thread per (sea point, frequency) walking the directions.
 template <typename R, int VAR, bool RED, bool REFRD>
-__global__ void __launch_bounds__(128) propags_kernel(const PropArgs<R> A, const R* __restrict__ f1, int ld1,
+__global__ void __launch_bounds__(128) propags_kernel(const __grid_constant__ PropArgs<R> A, const R* __restrict__ f1, int ld1,
                                                       R* __restrict__ f3, int ld3, int m0) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int m = m0 + blockIdx.y;
@@ -21,13 +21,14 @@ __global__ void __launch_bounds__(128) propags_kernel(const PropArgs<R> A, const
   const bool theta = REFRD || S::SPH;
   R fkm = F(i + 1, KL - 1), fk = F(i + 1, 0);
   R* out = f3 + i + (size_t)ld3 * KL * m;
+  typename S::Win W = site.window(0);
   for (int k = 0; k < KL; ++k) {
     const int kp = (k + 1 == KL) ? 0 : k + 1;
     const R fkp = F(i + 1, kp);
-    const Coefs<R> c = site.coef(k);
+    const Coefs<R> c = site.coef_w(W);
     R v;
     if (!S::CUR) {
-      const bool ic0 = ccos<R>(k) >= R(0.), is0 = csin<R>(k) >= R(0.);
+      const bool ic0 = W.cs >= R(0.), is0 = W.sn >= R(0.);
       v = c.sum * fk + c.lat11 * F(ic0 ? site.s0 : site.n0, k) + c.lon1 * F(is0 ? site.w0 : site.e0, k);
       if (theta) v = v + c.th1 * fkp + c.th2 * fkm;
       if (RED) v = v + c.lat12 * F(ic0 ? site.s1 : site.n1, k);
@@ -40,6 +41,7 @@ __global__ void __launch_bounds__(128) propags_kernel(const PropArgs<R> A, const
     }
     out[(size_t)ld3 * k] = v;
     fkm = fk; fk = fkp;
+    site.advance(W, k);
   }
 }
 
@@ -49,7 +51,7 @@ __device__ __forceinline__ long long d2o(double d) { long long i = __double_as_l
 
 // ext[2*c] = max, ext[2*c+1] = min of coefficient class c (CflClass)
 template <typename R, int VAR, bool RED, bool REFRD>
-__global__ void __launch_bounds__(256) cfl_extrema_kernel(const PropArgs<R> A, long long* ext) {
+__global__ void __launch_bounds__(256) cfl_extrema_kernel(const __grid_constant__ PropArgs<R> A, long long* ext) {
   const size_t n = (size_t)A.nsea * A.ML;
   R mx[CFL_NCLASS], mn[CFL_NCLASS];
   for (int c = 0; c < CFL_NCLASS; ++c) { mx[c] = R(-1e30); mn[c] = R(1e30); }
@@ -80,16 +82,6 @@ __global__ void __launch_bounds__(256) cfl_extrema_kernel(const PropArgs<R> A, l
 __global__ void cfl_init_kernel(long long* ext) {
   int q = threadIdx.x;
   if (q < CFL_NCLASS) { ext[2 * q] = LLONG_MIN; ext[2 * q + 1] = LLONG_MAX; }
-}
-
-template <typename R> cudaError_t set_direction_tables(const R* sinth, const R* costh, int kl);
-template <> cudaError_t set_direction_tables<float>(const float* s, const float* c, int kl) {
-  cudaError_t e = cudaMemcpyToSymbol(c_sinth_f, s, kl * sizeof(float));
-  return e != cudaSuccess ? e : cudaMemcpyToSymbol(c_costh_f, c, kl * sizeof(float));
-}
-template <> cudaError_t set_direction_tables<double>(const double* s, const double* c, int kl) {
-  cudaError_t e = cudaMemcpyToSymbol(c_sinth_d, s, kl * sizeof(double));
-  return e != cudaSuccess ? e : cudaMemcpyToSymbol(c_costh_d, c, kl * sizeof(double));
 }
 
 // Compile-time dispatch over the ten reference variants (eight coefficient
@@ -168,7 +160,5 @@ template cudaError_t launch_propags<float>(const PropArgs<float>&, const float*,
 template cudaError_t launch_propags<double>(const PropArgs<double>&, const double*, int, double*, int, cudaStream_t, int, int);
 template cudaError_t launch_cfl_extrema<float>(const PropArgs<float>&, long long*, int, cudaStream_t);
 template cudaError_t launch_cfl_extrema<double>(const PropArgs<double>&, long long*, int, cudaStream_t);
-template cudaError_t set_direction_tables<float>(const float*, const float*, int);
-template cudaError_t set_direction_tables<double>(const double*, const double*, int);
 
 }  // namespace wamgpu

@@ -11,6 +11,10 @@
 // points, so every access to FL3(IJ,K,M) is coalesced; the north/south
 // neighbours of a latitude row are re-read from L2.
 //
+// Direction sines and cosines travel in the metadata block itself (a
+// __grid_constant__ kernel parameter), so grids with different KL can live
+// side by side in one process.
+//
 // The coefficient formulas keep the reference's operation order and are
 // compiled without FMA contraction, so they reproduce the reference's REAL
 // coefficients.  Routine map: PREP_CART_DEEP :928, PREP_CART_SHALLOW :974,
@@ -29,17 +33,6 @@ namespace wamgpu {
 template <typename R> struct Coefs {
   R sum, lat11, lat21, lat12, lat22, lon1, lon2, th1, th2, sg1, sg2;
 };
-
-// Direction tables in constant memory: every lane of a warp reads the same
-// direction in the stencil loop, so these are broadcast reads.
-__constant__ float c_sinth_f[MAX_KL], c_costh_f[MAX_KL];
-__constant__ double c_sinth_d[MAX_KL], c_costh_d[MAX_KL];
-template <typename R> __device__ __forceinline__ R csin(int k);
-template <typename R> __device__ __forceinline__ R ccos(int k);
-template <> __device__ __forceinline__ float csin<float>(int k) { return c_sinth_f[k]; }
-template <> __device__ __forceinline__ float ccos<float>(int k) { return c_costh_f[k]; }
-template <> __device__ __forceinline__ double csin<double>(int k) { return c_sinth_d[k]; }
-template <> __device__ __forceinline__ double ccos<double>(int k) { return c_costh_d[k]; }
 
 constexpr bool var_shallow(int v) { return v == V_CART_SHALLOW || v == V_SPHER_SHALLOW || v == V_CART_SHALLOW_CUR || v == V_SPHER_SHALLOW_CURR; }
 constexpr bool var_current(int v) { return v == V_CART_DEEP_CUR || v == V_SPHER_DEEP_CURR || v == V_CART_SHALLOW_CUR || v == V_SPHER_SHALLOW_CURR; }
@@ -62,6 +55,9 @@ template <typename R, int VAR, bool RED, bool REFRD> struct Site {
     return __ldg(&A.TCGOND[(jd - 1) + A.NDEPTH * mm_]);
   }
   __device__ R uv(const R* f, int p1) const { return p1 == 0 ? R(0) : __ldg(&f[p1 - 1]); }
+
+  __device__ R dir_sin(int k) const { return A.sinth[k]; }
+  __device__ R dir_cos(int k) const { return A.costh[k]; }
 
   __device__ Site(const PropArgs<R>& a, int i_, int m_) : A(a), i(i_), m(m_) {
     const int ns = A.nsea;
@@ -101,8 +97,8 @@ template <typename R, int VAR, bool RED, bool REFRD> struct Site {
   }
 
   // THDD(i,k,m): depth part (PREPARE_PROPAGATION :482-492) plus current part (:521-536)
-  __device__ R thdd(int k) const {
-    R sn = csin<R>(k), cs = ccos<R>(k);
+  __device__ R thdd(int k) const { return thdd_sc(dir_sin(k), dir_cos(k)); }
+  __device__ R thdd_sc(R sn, R cs) const {
     R t = R(0);
     if (SH) t = (sn * ddphi - cs * ddlam) * tsi;
     if (CUR) {
@@ -113,17 +109,40 @@ template <typename R, int VAR, bool RED, bool REFRD> struct Site {
     return t;
   }
   // SIDC(i,k,m') for m' = m, mp, mm (:541-563)
-  __device__ R sidc_base(int k) const {
-    R sd = csin<R>(k), cd = ccos<R>(k);
+  __device__ R sidc_base_sc(R sd, R cd) const {
     R ss = sd * sd, sc = sd * cd, cc = cd * cd;
     return -(sc * duphi) - cc * dvphi - ss * dulam - sc * dvlam;
   }
 
-  __device__ Coefs<R> coef(int k) const {
-    Coefs<R> c = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  // Direction-dependent inputs of the coefficients of direction k: sines and
+  // cosines of k and its neighbours and THDD of k-1, k, k+1.  The stencil loop
+  // slides this window along the directions instead of re-reading them.
+  struct Win { R sn, cs, snp, csp, snm, th0, thp, thm; };
+  static constexpr bool NEED_TH = (SH && REFRD) || CUR;
+  __device__ Win window(int k) const {
     const int KL = A.KL;
     const int kp = (k + 1 == KL) ? 0 : k + 1, km = (k == 0) ? KL - 1 : k - 1;
-    const R sn = csin<R>(k), cs = ccos<R>(k);
+    Win w;
+    w.sn = dir_sin(k); w.cs = dir_cos(k);
+    w.snp = dir_sin(kp); w.csp = dir_cos(kp);
+    w.snm = dir_sin(km);
+    if (NEED_TH) { w.th0 = thdd_sc(w.sn, w.cs); w.thp = thdd_sc(w.snp, w.csp); w.thm = thdd(km); }
+    else { w.th0 = w.thp = w.thm = R(0); }
+    return w;
+  }
+  // the window of direction k+1 from that of k
+  __device__ void advance(Win& w, int k) const {
+    const int KL = A.KL;
+    const int kpp = (k + 2 >= KL) ? k + 2 - KL : k + 2;
+    w.snm = w.sn; w.sn = w.snp; w.cs = w.csp;
+    w.snp = dir_sin(kpp); w.csp = dir_cos(kpp);
+    if (NEED_TH) { w.thm = w.th0; w.th0 = w.thp; w.thp = thdd_sc(w.snp, w.csp); }
+  }
+  __device__ Coefs<R> coef(int k) const { return coef_w(window(k)); }
+
+  __device__ Coefs<R> coef_w(const Win& W) const {
+    Coefs<R> c = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const R sn = W.sn, cs = W.cs;
     const bool IS0 = sn >= R(0.), IC0 = cs >= R(0.);
     const R z = R(0.);
     if (VAR == V_CART_DEEP) {
@@ -137,14 +156,14 @@ template <typename R, int VAR, bool RED, bool REFRD> struct Site {
       c.lat11 = cd * ((IC0 ? cgS : cgN) + cg);
       c.sum = R(1.) - sd * ((IS0 ? cgE : cgW) + cg) * d0 - cd * ((IC0 ? cgN : cgS) + cg);
       if (REFRD) {
-        R t0 = thdd(k);
-        R dtp = (t0 + thdd(kp)) * A.DELTHR, dtm = (t0 + thdd(km)) * A.DELTHR;
+        R t0 = W.th0;
+        R dtp = (t0 + W.thp) * A.DELTHR, dtm = (t0 + W.thm) * A.DELTHR;
         c.sum = c.sum - dmax(z, dtp) + dmin(z, dtm);
         c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
       }
     } else if (VAR == V_SPHER_DEEP) {
       R sda = dabs(sn), cda = dabs(cs * A.DELPH0);
-      R sp = A.DELTH0 * (sn + csin<R>(kp)), sm = A.DELTH0 * (sn + csin<R>(km));
+      R sp = A.DELTH0 * (sn + W.snp), sm = A.DELTH0 * (sn + W.snm);
       R dpn = cda * ((IC0 ? ps : pn) + R(1.));
       R dle = sda * d0;
       R dtc = cda * ((IC0 ? pn : ps) + R(1.)) + dle;
@@ -156,7 +175,7 @@ template <typename R, int VAR, bool RED, bool REFRD> struct Site {
       if (RED) { R wl = IC0 ? wl1 : wl2; c.lat12 = c.lat11 * (R(1.) - wl); c.lat11 = c.lat11 * wl; }
     } else if (VAR == V_SPHER_SHALLOW) {
       R sda = dabs(sn), cda = dabs(cs * A.DELPH0);
-      R sp = A.DELTH0 * (sn + csin<R>(kp)), sm = A.DELTH0 * (sn + csin<R>(km));
+      R sp = A.DELTH0 * (sn + W.snp), sm = A.DELTH0 * (sn + W.snm);
       R cgk1, cgk2;  // CGKLAT(IJ,M,1) south and (IJ,M,2) north
       if (RED) {
         cgk1 = cg + ps * (wl1 * cgS + (R(1.) - wl1) * cgS1);
@@ -168,9 +187,9 @@ template <typename R, int VAR, bool RED, bool REFRD> struct Site {
       c.lon1 = sda * ((IS0 ? cgW : cgE) + cg) * d0;
       R dtp = dr * cg, dtm;
       if (REFRD) {
-        R t0 = thdd(k);
-        dtm = dtp * sm + (t0 + thdd(km)) * A.DELTHR;
-        dtp = dtp * sp + (t0 + thdd(kp)) * A.DELTHR;
+        R t0 = W.th0;
+        dtm = dtp * sm + (t0 + W.thm) * A.DELTHR;
+        dtp = dtp * sp + (t0 + W.thp) * A.DELTHR;
       } else { dtm = dtp * sm; dtp = dtp * sp; }
       dtc = dtc - dmax(z, dtp) + dmin(z, dtm);
       c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
@@ -197,15 +216,15 @@ template <typename R, int VAR, bool RED, bool REFRD> struct Site {
         dtc = dtc - dmax(z, dpn) + dmin(z, dps);
         c.lat11 = dmax(z, dps); c.lat21 = -dmin(z, dpn);
       }
-      R t0 = thdd(k), tp = thdd(kp), tm = thdd(km);
+      R t0 = W.th0, tp = W.thp, tm = W.thm;
       R dtp, dtm;
       if (SPH) {
-        R sp = A.DELTH0 * (sn + csin<R>(kp)) * gom, sm = A.DELTH0 * (sn + csin<R>(km)) * gom;
+        R sp = A.DELTH0 * (sn + W.snp) * gom, sm = A.DELTH0 * (sn + W.snm) * gom;
         dtp = sp * dr + (t0 + tp) * A.DELTHR; dtm = sm * dr + (t0 + tm) * A.DELTHR;
       } else { dtp = (t0 + tp) * A.DELTHR; dtm = (t0 + tm) * A.DELTHR; }
       dtc = dtc - dmax(z, dtp) + dmin(z, dtm);
       c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
-      R dom = sidc_base(k) * A.DELFR0;
+      R dom = sidc_base_sc(sn, cs) * A.DELFR0;
       c.sum = dtc - dabs(dom);
       c.sg1 = -dmin(z, dom) / R(1.1); c.sg2 = dmax(z, dom) * R(1.1);
     } else {  // V_CART_SHALLOW_CUR, V_SPHER_SHALLOW_CURR
@@ -230,15 +249,15 @@ template <typename R, int VAR, bool RED, bool REFRD> struct Site {
         dtc = dtc - dmax(z, dpn) + dmin(z, dps);
         c.lat11 = dmax(z, dps); c.lat21 = -dmin(z, dpn);
       }
-      R t0 = thdd(k), tp = thdd(kp), tm = thdd(km);
+      R t0 = W.th0, tp = W.thp, tm = W.thm;
       R dtp, dtm;
       if (SPH) {
-        R sp = A.DELTH0 * (sn + csin<R>(kp)), sm = A.DELTH0 * (sn + csin<R>(km));
+        R sp = A.DELTH0 * (sn + W.snp), sm = A.DELTH0 * (sn + W.snm);
         dtp = sp * dr * cg + (t0 + tp) * A.DELTHR; dtm = sm * dr * cg + (t0 + tm) * A.DELTHR;
       } else { dtp = (t0 + tp) * A.DELTHR; dtm = (t0 + tm) * A.DELTHR; }
       dtc = dtc - dmax(z, dtp) + dmin(z, dtm);
       c.th1 = -dmin(z, dtp); c.th2 = dmax(z, dtm);
-      R b = sidc_base(k);
+      R b = sidc_base_sc(sn, cs);
       R s0v = (b * cg + tempc * tsi) * tfk, sPv = (b * cgP + tempc * tsiP) * tfkP, sMv = (b * cgM + tempc * tsiM) * tfkM;
       R dop = (s0v + sPv) * dfp, dom = (s0v + sMv) * dfm;
       c.sg1 = -dmin(z, dop) / R(1.1); c.sg2 = dmax(z, dom) * R(1.1);

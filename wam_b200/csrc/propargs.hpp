@@ -29,7 +29,11 @@ template <typename R> struct PropArgs {
   const R* duphi; const R* dulam; const R* dvphi; const R* dvlam;  // current gradients
   const R* u; const R* v;    // [n_ext] currents (land slot reads as 0)
   const R* TCGOND; const R* TSIHKD; const R* TFAK;  // depth tables [(jd-1) + NDEPTH*m]
-  const R* GOM; const R* FR;  // small tables (global); SINTH/COSTH live in constant memory
+  const R* GOM; const R* FR;  // small tables (global)
+  // SINTH/COSTH of this grid.  The struct is passed as a __grid_constant__
+  // kernel parameter, so these are constant-bank reads (broadcast: every lane
+  // of a warp reads the same direction), and every grid carries its own.
+  R sinth[MAX_KL], costh[MAX_KL];
 };
 
 }  // namespace wamgpu
