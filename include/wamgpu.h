@@ -181,6 +181,37 @@ WAMGPU_API int wamgpu_get_fluxes(wamgpu_ctx* ctx, float* out7);
 WAMGPU_API int wamgpu_set_timing(wamgpu_ctx* ctx, int enable);
 WAMGPU_API int wamgpu_get_timing(wamgpu_ctx* ctx, float* ms, int* count);
 
+/* Batched ensembles.  No single counterpart in the reference, where each
+ * member is a separate WAMODEL run calling PROPAGS (propagation:635-829) and
+ * IMPLSCH (source:374-700).  A batch advances many prepared member contexts
+ * of one precision on one device, each with its own grid size, KL/ML and
+ * physics: one pass runs every member's IDELT/IDELPRO x COUNTER PROPAGS
+ * sub-steps and then its IMPLSCH, with one launch per sub-step and
+ * coefficient family and one IMPLSCH launch for all members.  Results are
+ * bit-identical to wamgpu_step_dev of each member.
+ *  - wamgpu_batch_set_member gives member g's device state, as for
+ *    wamgpu_step_dev (scratch is required).
+ *  - wamgpu_batch_tune times the compiled CTA shapes (sea points per IMPLSCH
+ *    CTA, points per PROPAGS CTA) on the members' state, writing only
+ *    scratch, keeps the fastest and returns them.
+ *  - wamgpu_batch_step runs one pass on `stream` (NULL = the first member's
+ *    stream); after wamgpu_batch_capture it replays the captured CUDA graph.
+ *    wamgpu_batch_capture records one pass as a CUDA graph; setting a
+ *    member's state again discards it.
+ *  - wamgpu_batch_sync waits for the stream and checks every member's
+ *    non-finite flag. */
+typedef struct wamgpu_batch wamgpu_batch;
+WAMGPU_API int wamgpu_batch_create(wamgpu_ctx* const* members, int n, wamgpu_batch** out);
+WAMGPU_API int wamgpu_batch_destroy(wamgpu_batch* b);
+WAMGPU_API const char* wamgpu_batch_last_error(const wamgpu_batch* b);
+WAMGPU_API int wamgpu_batch_set_member(wamgpu_batch* b, int g, void* fl3, int ld, void* scratch, const void* u10,
+                                       const void* udir, void* tauw, void* ustar, void* z0, const void* roairn,
+                                       const void* wstar);
+WAMGPU_API int wamgpu_batch_tune(wamgpu_batch* b, void* stream, int* points_per_cta, int* propags_block);
+WAMGPU_API int wamgpu_batch_step(wamgpu_batch* b, void* stream);
+WAMGPU_API int wamgpu_batch_capture(wamgpu_batch* b, void* stream);
+WAMGPU_API int wamgpu_batch_sync(wamgpu_batch* b);
+
 /* Synchronises the context stream; returns WAMGPU_E_NUMERIC if a kernel
  * reported non-finite output since the last call. */
 WAMGPU_API int wamgpu_sync(wamgpu_ctx* ctx);

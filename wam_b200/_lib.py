@@ -47,6 +47,15 @@ SIGNATURES = {
     "wamgpu_sync": (c_int, [c_void_p]),
     "wamgpu_set_timing": (c_int, [c_void_p, c_int]),
     "wamgpu_get_timing": (c_int, [c_void_p, PF, PI]),
+    "wamgpu_batch_create": (c_int, [ctypes.POINTER(c_void_p), c_int, ctypes.POINTER(c_void_p)]),
+    "wamgpu_batch_destroy": (c_int, [c_void_p]),
+    "wamgpu_batch_last_error": (c_char_p, [c_void_p]),
+    "wamgpu_batch_set_member": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                                        c_void_p, c_void_p, c_void_p, c_void_p]),
+    "wamgpu_batch_tune": (c_int, [c_void_p, c_void_p, PI, PI]),
+    "wamgpu_batch_step": (c_int, [c_void_p, c_void_p]),
+    "wamgpu_batch_capture": (c_int, [c_void_p, c_void_p]),
+    "wamgpu_batch_sync": (c_int, [c_void_p]),
 }
 
 _lib = None

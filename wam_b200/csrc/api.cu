@@ -1,5 +1,6 @@
 // C ABI of libwamgpu (declarations and reference citations in include/wamgpu.h).
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -20,6 +21,14 @@ namespace {
 struct DevBuf {
   void* p = nullptr;
   size_t n = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) { o.p = nullptr; o.n = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) { if (p) cudaFree(p); p = o.p; n = o.n; o.p = nullptr; o.n = 0; }
+    return *this;
+  }
   ~DevBuf() { if (p) cudaFree(p); }
   cudaError_t ensure(size_t bytes) {
     if (bytes <= n && p) return cudaSuccess;
@@ -736,6 +745,274 @@ template <typename R> int get_table_t(const wamgpu_ctx* ctx, const Impl<R>& I, c
   return WAMGPU_E_ARG;
 }
 
+// ---- batched ensembles -------------------------------------------------------
+// Many member contexts (uneven NSEA, mixed KL/ML/IPHYS, one precision, one
+// device) advance together: each PROPAGS sub-step is one launch per
+// coefficient family over all members that still have that sub-step, and
+// IMPLSCH is one launch over all members.  The launch lists live on the
+// device, so a pass is a fixed sequence of launches that can be captured
+// once as a CUDA graph and replayed.
+struct BatchState {
+  void* fl3 = nullptr; void* scratch = nullptr; int ld = 0;
+  const void *u10 = nullptr, *udir = nullptr, *roairn = nullptr, *wstar = nullptr;
+  void *tauw = nullptr, *ustar = nullptr, *z0 = nullptr;
+};
+struct BatchList { int family = 0; int nmem = 0, nblocks = 0; DevBuf mem, first; };
+
+}  // namespace
+
+struct wamgpu_batch {
+  std::string err;
+  std::vector<wamgpu_ctx*> members;
+  int precision = 4, device = 0;
+  std::vector<BatchState> st;
+  int P = 0, bs = 128;  // IMPLSCH sea points per CTA, PROPAGS points per CTA
+  bool built = false;
+  std::vector<std::vector<BatchList>> sub;  // [sub-step][family group]
+  BatchList imp;
+  size_t imp_smem = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t stream = nullptr;
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr; graph = nullptr;
+  }
+};
+
+namespace {
+
+int bfail(wamgpu_batch* b, int code, const std::string& msg) {
+  if (b) b->err = msg;
+  return code;
+}
+#define BCK(call, where)                                                                    \
+  do {                                                                                      \
+    cudaError_t e_ = (call);                                                                \
+    if (e_ != cudaSuccess) return bfail(b, WAMGPU_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+template <typename T> cudaError_t upload_vec(DevBuf& d, const std::vector<T>& h, cudaStream_t s) {
+  cudaError_t e = d.ensure(h.size() * sizeof(T) + 16);
+  if (e != cudaSuccess || h.empty()) return e;
+  return cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+template <typename R> Impl<R>& impl_of(wamgpu_ctx* c) { return *static_cast<Impl<R>*>(c->impl.get()); }
+
+// sub-steps of a member in one pass: IDELT/IDELPRO propagation calls of COUNTER sub-steps each
+int member_nsub(const wamgpu_ctx* c) { return (c->cfg.idelt / c->cfg.idelpro) * c->counter; }
+
+template <typename R> size_t batch_smem(wamgpu_batch* b, int P) {
+  size_t mx = 0;
+  for (auto* c : b->members) mx = std::max(mx, implsch_smem_bytes(impl_of<R>(c).dt, P));
+  return mx;
+}
+constexpr size_t kMaxSmemPerCta = 232448;  // 227 KB opt-in limit of sm_100
+
+// IMPLSCH member list.  For tuning (out != null) each member reads its
+// current spectrum and writes `out`, TAUW/USTAR/Z0 go to `tmp3` and the
+// status flag to `tmp_status`: the members' state is left untouched.
+template <typename R>
+int batch_impl_list(wamgpu_batch* b, int P, BatchList& L, size_t& smem, const std::vector<R*>* out,
+                    const std::vector<R*>* tmp3, int* tmp_status, cudaStream_t s) {
+  const int n = (int)b->members.size();
+  std::vector<ImplMember<R>> mem(n);
+  std::vector<int> first(n + 1, 0);
+  for (int g = 0; g < n; ++g) {
+    wamgpu_ctx* c = b->members[g];
+    Impl<R>& I = impl_of<R>(c);
+    const BatchState& x = b->st[g];
+    if (!I.status.p) { BCK(I.status.ensure(16), "alloc"); BCK(cudaMemsetAsync(I.status.p, 0, 16, s), "memset"); }
+    if (c->cfg.lcflx) BCK(I.fluxes.ensure((size_t)7 * c->nsea * sizeof(R) + 16), "alloc");
+    ImplMember<R>& M = mem[g];
+    M.T = I.dt;
+    ImplArgs<R>& a = M.a;
+    a.nsea = c->nsea; a.ld = x.ld;
+    R* fin = (member_nsub(c) % 2 == 0) ? (R*)x.fl3 : (R*)x.scratch;  // buffer the last sub-step wrote
+    a.fl3_in = out ? (const R*)x.fl3 : fin;
+    a.fl3 = out ? (*out)[g] : (R*)x.fl3;
+    a.u10 = (const R*)x.u10; a.udir = (const R*)x.udir; a.roairn = (const R*)x.roairn; a.wstar = (const R*)x.wstar;
+    a.depth = I.d_depth.template as<R>(); a.indep = I.d_indep.template as<int>();
+    if (tmp3) { a.tauw = (*tmp3)[3 * g]; a.ustar = (*tmp3)[3 * g + 1]; a.z0 = (*tmp3)[3 * g + 2]; }
+    else { a.tauw = (R*)x.tauw; a.ustar = (R*)x.ustar; a.z0 = (R*)x.z0; }
+    a.fluxes = (c->cfg.lcflx && !tmp3) ? I.fluxes.template as<R>() : nullptr;
+    a.flx_ld = c->nsea;
+    a.status = tmp_status ? tmp_status : I.status.template as<int>();
+    first[g + 1] = first[g] + (c->nsea + P - 1) / P;
+  }
+  smem = batch_smem<R>(b, P);
+  if (smem + sizeof(ImplMember<R>) + 64 > kMaxSmemPerCta) return bfail(b, WAMGPU_E_ARG, "points per CTA too large for a member");
+  BCK(implsch_set_max_smem<R>(P, smem), "smem attribute");
+  BCK(upload_vec(L.mem, mem, s), "upload batch");
+  BCK(upload_vec(L.first, first, s), "upload batch");
+  L.nmem = n; L.nblocks = first[n];
+  return WAMGPU_OK;
+}
+
+template <typename R> int batch_build(wamgpu_batch* b, cudaStream_t s) {
+  const int n = (int)b->members.size();
+  for (int g = 0; g < n; ++g)
+    if (!b->st[g].fl3) return bfail(b, WAMGPU_E_STATE, "member " + std::to_string(g) + " has no state (wamgpu_batch_set_member)");
+  if (b->P == 0) b->P = sizeof(R) == 4 ? 6 : 2;
+  int maxsub = 0;
+  for (auto* c : b->members) maxsub = std::max(maxsub, member_nsub(c));
+  b->sub.clear();
+  b->sub.resize(maxsub);
+  auto key_of = [](const PropArgs<R>& A) { return A.variant * 4 + (A.reduced ? 2 : 0) + (A.refr_d ? 1 : 0); };
+  for (int it = 0; it < maxsub; ++it) {
+    std::vector<int> fam;  // coefficient families in order of first appearance
+    for (int g = 0; g < n; ++g) {
+      wamgpu_ctx* c = b->members[g];
+      if (member_nsub(c) <= it || c->nsea == 0) continue;
+      const int key = key_of(impl_of<R>(c).pa);
+      if (std::find(fam.begin(), fam.end(), key) == fam.end()) fam.push_back(key);
+    }
+    b->sub[it].resize(fam.size());
+    for (size_t f = 0; f < fam.size(); ++f) {
+      std::vector<PropMember<R>> mem;
+      std::vector<int> first(1, 0);
+      int rep = -1;
+      for (int g = 0; g < n; ++g) {
+        wamgpu_ctx* c = b->members[g];
+        if (member_nsub(c) <= it || c->nsea == 0) continue;
+        const PropArgs<R>& A = impl_of<R>(c).pa;
+        if (key_of(A) != fam[f]) continue;
+        if (rep < 0) rep = g;
+        PropMember<R> M;
+        M.A = A;
+        R* f3 = (R*)b->st[g].fl3; R* sc = (R*)b->st[g].scratch;
+        M.src = (it % 2 == 0) ? f3 : sc;
+        M.dst = (it % 2 == 0) ? sc : f3;
+        M.ld = b->st[g].ld;
+        M.nbi = (c->nsea + b->bs - 1) / b->bs;
+        mem.push_back(M);
+        first.push_back(first.back() + c->cfg.ml * M.nbi);
+      }
+      BatchList& L = b->sub[it][f];
+      L.family = rep;
+      L.nmem = (int)mem.size(); L.nblocks = first.back();
+      BCK(upload_vec(L.mem, mem, s), "upload batch");
+      BCK(upload_vec(L.first, first, s), "upload batch");
+    }
+  }
+  int rc = batch_impl_list<R>(b, b->P, b->imp, b->imp_smem, nullptr, nullptr, nullptr, s);
+  if (rc) return rc;
+  BCK(cudaStreamSynchronize(s), "batch upload");
+  b->built = true;
+  return WAMGPU_OK;
+}
+
+template <typename R> int batch_launch(wamgpu_batch* b, cudaStream_t s) {
+  for (auto& step : b->sub)
+    for (auto& L : step) {
+      const PropArgs<R>& fam = impl_of<R>(b->members[L.family]).pa;
+      BCK(launch_propags_batch<R>(fam, L.mem.template as<PropMember<R>>(), L.first.template as<int>(), L.nmem, L.nblocks,
+                                  b->bs, s), "batched PROPAGS");
+    }
+  BCK(launch_implsch_batch<R>(b->imp.mem.template as<ImplMember<R>>(), b->imp.first.template as<int>(), b->imp.nmem,
+                              b->imp.nblocks, b->P, b->imp_smem, s), "batched IMPLSCH");
+  return WAMGPU_OK;
+}
+
+// Autotuner: times the first batched PROPAGS sub-step with 128- and 256-point
+// CTAs (it reads FL3 and writes scratch only) and the batched IMPLSCH for
+// every compiled CTA shape out of place (spectra into scratch, TAUW/USTAR/Z0
+// and the status flag into temporaries), and keeps the fastest of each.
+template <typename R> int batch_tune(wamgpu_batch* b, cudaStream_t s, int* P_out, int* bs_out) {
+  const int n = (int)b->members.size();
+  b->drop_graph();
+  b->built = false;
+  int rc = batch_build<R>(b, s);
+  if (rc) return rc;
+  cudaEvent_t e0, e1;
+  BCK(cudaEventCreate(&e0), "event");
+  BCK(cudaEventCreate(&e1), "event");
+  auto timed = [&](auto&& launch, float& best) -> int {
+    best = 1e30f;
+    for (int r = 0; r < 4; ++r) {
+      BCK(cudaEventRecord(e0, s), "event");
+      int rc2 = launch();
+      if (rc2) return rc2;
+      BCK(cudaEventRecord(e1, s), "event");
+      BCK(cudaEventSynchronize(e1), "event");
+      float ms = 0;
+      BCK(cudaEventElapsedTime(&ms, e0, e1), "event");
+      if (r > 0) best = std::min(best, ms);
+    }
+    return WAMGPU_OK;
+  };
+  int best_bs = b->bs;
+  float best_t = 1e30f;
+  for (int cand : {128, 256}) {
+    b->bs = cand; b->built = false;
+    if ((rc = batch_build<R>(b, s))) break;
+    if (b->sub.empty()) { best_bs = cand; break; }
+    float t = 0;
+    rc = timed([&]() -> int {
+      for (auto& L : b->sub[0]) {
+        const PropArgs<R>& fam = impl_of<R>(b->members[L.family]).pa;
+        BCK(launch_propags_batch<R>(fam, L.mem.template as<PropMember<R>>(), L.first.template as<int>(), L.nmem, L.nblocks,
+                                    b->bs, s), "batched PROPAGS");
+      }
+      return WAMGPU_OK;
+    }, t);
+    if (rc) break;
+    if (t < best_t) { best_t = t; best_bs = cand; }
+  }
+  b->bs = best_bs;
+  DevBuf tmp, tstatus;
+  size_t tot = 0;
+  for (auto* c : b->members) tot += (size_t)c->nsea + 4;
+  if (!rc && tmp.ensure(3 * tot * sizeof(R) + 64) != cudaSuccess) rc = bfail(b, WAMGPU_E_NOMEM, "tuning buffers");
+  if (!rc && tstatus.ensure(16) != cudaSuccess) rc = bfail(b, WAMGPU_E_NOMEM, "tuning buffers");
+  std::vector<R*> out(n), t3(3 * n);
+  if (!rc) {
+    size_t off = 0;
+    for (int g = 0; g < n && !rc; ++g) {
+      const size_t ng = (size_t)b->members[g]->nsea;
+      out[g] = (R*)b->st[g].scratch;
+      for (int q = 0; q < 3; ++q) {
+        t3[3 * g + q] = tmp.template as<R>() + off;
+        const void* srcp = q == 0 ? b->st[g].tauw : (q == 1 ? b->st[g].ustar : b->st[g].z0);
+        if (ng && cudaMemcpyAsync(t3[3 * g + q], srcp, ng * sizeof(R), cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+          rc = bfail(b, WAMGPU_E_CUDA, "tuning copy");
+          break;
+        }
+        off += ng + 4;
+      }
+    }
+  }
+  int best_P = b->P;
+  best_t = 1e30f;
+  const std::vector<int> cands = sizeof(R) == 4 ? std::vector<int>{4, 6, 8} : std::vector<int>{2, 4};
+  for (int P : cands) {
+    if (rc) break;
+    if (batch_smem<R>(b, P) + sizeof(ImplMember<R>) + 64 > kMaxSmemPerCta) continue;
+    BatchList L;
+    size_t smem = 0;
+    if ((rc = batch_impl_list<R>(b, P, L, smem, &out, &t3, tstatus.template as<int>(), s))) break;
+    float t = 0;
+    rc = timed([&]() -> int {
+      BCK(launch_implsch_batch<R>(L.mem.template as<ImplMember<R>>(), L.first.template as<int>(), L.nmem, L.nblocks, P,
+                                  smem, s), "batched IMPLSCH");
+      return WAMGPU_OK;
+    }, t);
+    BCK(cudaStreamSynchronize(s), "tune");
+    if (!rc && t < best_t) { best_t = t; best_P = P; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  b->P = best_P;
+  b->built = false;
+  if ((rc = batch_build<R>(b, s))) return rc;
+  if (P_out) *P_out = b->P;
+  if (bs_out) *bs_out = b->bs;
+  return WAMGPU_OK;
+}
+
 #define DISPATCH_CTX(ctx, FN, ...)                                                              \
   ((ctx)->cfg.precision == 8 ? FN<double>((ctx), *static_cast<Impl<double>*>((ctx)->impl.get()), ##__VA_ARGS__) \
                              : FN<float>((ctx), *static_cast<Impl<float>*>((ctx)->impl.get()), ##__VA_ARGS__))
@@ -972,6 +1249,107 @@ int wamgpu_sync(wamgpu_ctx* ctx) {
       CK(cudaMemset(st->p, 0, sizeof(int)), "status");
       return fail(ctx, WAMGPU_E_NUMERIC, "non-finite values in IMPLSCH output");
     }
+  }
+  return WAMGPU_OK;
+}
+
+// ---- batched ensembles ---------------------------------------------------------
+
+int wamgpu_batch_create(wamgpu_ctx* const* members, int n, wamgpu_batch** out) {
+  if (!out) return WAMGPU_E_ARG;
+  *out = nullptr;
+  auto* b = new wamgpu_batch();
+  *out = b;
+  if (!members || n <= 0) return bfail(b, WAMGPU_E_ARG, "empty batch");
+  for (int g = 0; g < n; ++g) {
+    wamgpu_ctx* c = members[g];
+    if (!c || !c->impl) return bfail(b, WAMGPU_E_ARG, "null member context");
+    if (!c->prepared) return bfail(b, WAMGPU_E_STATE, "member " + std::to_string(g) + " not prepared (wamgpu_prepare_propagation)");
+    if (g > 0 && (c->cfg.precision != members[0]->cfg.precision || c->cfg.device != members[0]->cfg.device))
+      return bfail(b, WAMGPU_E_ARG, "members must share precision and device");
+    const bool enh = c->cfg.precision == 8 ? impl_of<double>(c).dt.ENH != nullptr : impl_of<float>(c).dt.ENH != nullptr;
+    if (c->cfg.shallow_run && c->cfg.isnonlin != 0 && !enh)
+      return bfail(b, WAMGPU_E_STATE, "member " + std::to_string(g) + " needs wamgpu_prepare_source");
+    b->members.push_back(c);
+  }
+  b->precision = members[0]->cfg.precision;
+  b->device = members[0]->cfg.device;
+  b->stream = members[0]->stream;
+  b->st.resize(n);
+  return WAMGPU_OK;
+}
+
+int wamgpu_batch_destroy(wamgpu_batch* b) {
+  if (!b) return WAMGPU_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  b->drop_graph();
+  delete b;
+  return WAMGPU_OK;
+}
+
+const char* wamgpu_batch_last_error(const wamgpu_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int wamgpu_batch_set_member(wamgpu_batch* b, int g, void* fl3, int ld, void* scratch, const void* u10, const void* udir,
+                            void* tauw, void* ustar, void* z0, const void* roairn, const void* wstar) {
+  if (!b) return WAMGPU_E_ARG;
+  if (g < 0 || g >= (int)b->members.size()) return bfail(b, WAMGPU_E_ARG, "member index out of range");
+  if (!fl3 || !scratch || !u10 || !udir || !tauw || !ustar || !z0 || !roairn || !wstar) return bfail(b, WAMGPU_E_ARG, "null argument");
+  if (ld < b->members[g]->nsea) return bfail(b, WAMGPU_E_ARG, "ld < nsea");
+  BatchState& x = b->st[g];
+  x.fl3 = fl3; x.ld = ld; x.scratch = scratch; x.u10 = u10; x.udir = udir; x.tauw = tauw; x.ustar = ustar; x.z0 = z0;
+  x.roairn = roairn; x.wstar = wstar;
+  b->built = false;
+  b->drop_graph();
+  return WAMGPU_OK;
+}
+
+int wamgpu_batch_tune(wamgpu_batch* b, void* stream, int* points_per_cta, int* propags_block) {
+  if (!b) return WAMGPU_E_ARG;
+  cudaSetDevice(b->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
+  return b->precision == 8 ? batch_tune<double>(b, s, points_per_cta, propags_block)
+                           : batch_tune<float>(b, s, points_per_cta, propags_block);
+}
+
+int wamgpu_batch_step(wamgpu_batch* b, void* stream) {
+  if (!b) return WAMGPU_E_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
+  if (b->exec) { BCK(cudaGraphLaunch(b->exec, s), "graph launch"); return WAMGPU_OK; }
+  if (!b->built) {
+    int rc = b->precision == 8 ? batch_build<double>(b, s) : batch_build<float>(b, s);
+    if (rc) return rc;
+  }
+  return b->precision == 8 ? batch_launch<double>(b, s) : batch_launch<float>(b, s);
+}
+
+int wamgpu_batch_capture(wamgpu_batch* b, void* stream) {
+  if (!b) return WAMGPU_E_ARG;
+  cudaSetDevice(b->device);
+  cudaStream_t s = stream ? (cudaStream_t)stream : b->stream;
+  b->drop_graph();
+  if (!b->built) {
+    int rc = b->precision == 8 ? batch_build<double>(b, s) : batch_build<float>(b, s);
+    if (rc) return rc;
+  }
+  BCK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "begin capture");
+  int rc = b->precision == 8 ? batch_launch<double>(b, s) : batch_launch<float>(b, s);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e != cudaSuccess) return bfail(b, WAMGPU_E_CUDA, std::string("end capture: ") + cudaGetErrorString(e));
+  b->graph = g;
+  BCK(cudaGraphInstantiate(&b->exec, b->graph, 0), "graph instantiate");
+  return WAMGPU_OK;
+}
+
+int wamgpu_batch_sync(wamgpu_batch* b) {
+  if (!b) return WAMGPU_E_ARG;
+  cudaSetDevice(b->device);
+  BCK(cudaStreamSynchronize(b->stream), "sync");
+  for (size_t g = 0; g < b->members.size(); ++g) {
+    int rc = wamgpu_sync(b->members[g]);
+    if (rc) return bfail(b, rc, "member " + std::to_string(g) + ": " + b->members[g]->err);
   }
   return WAMGPU_OK;
 }

@@ -1,6 +1,7 @@
 // IMPLSCH kernel entry: CTA of P warps = P consecutive sea points.
 #include "implsch.cuh"
 #include "kernels.hpp"
+#include <mutex>
 
 namespace wamgpu {
 
@@ -10,9 +11,9 @@ __host__ __device__ inline size_t tables_bytes(const SmallLayout& L) {
   return (b + 15) & ~size_t(15);
 }
 
+// One CTA: sea points blk*P .. blk*P+P-1 of the launch's arguments.
 template <typename R, int P>
-__global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, const ImplArgs<R> a) {
-  extern __shared__ __align__(16) unsigned char smem[];
+__device__ __forceinline__ void implsch_cta(const DevTables<R>& T, const ImplArgs<R>& a, int blk, unsigned char* smem) {
   R* sR = reinterpret_cast<R*>(smem);
   int* sI = reinterpret_cast<int*>(sR + T.lay.nreal);
   const int tid = threadIdx.x, nthr = blockDim.x;
@@ -22,7 +23,7 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
   const size_t wsb = warp_ws_bytes<R>(LD, T.ML, T.need_sp, T.scr);
   unsigned char* ws0 = smem + tables_bytes<R>(T.lay);
   const size_t foff = ws_f_offset<R>(LD, T.ML);  // F follows the interleaved {SL, FL} block
-  const int ij0 = blockIdx.x * P;
+  const int ij0 = blk * P;
   // stage the P spectra: consecutive threads take consecutive points of one bin
   for (int idx = tid; idx < P * NS; idx += nthr) {
     int p = idx % P, b = idx / P, ij = ij0 + p;
@@ -66,28 +67,81 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const DevTables<R> T, c
   }
 }
 
+template <typename R, int P>
+__global__ void __launch_bounds__(P * 32) implsch_kernel(const __grid_constant__ DevTables<R> T, const ImplArgs<R> a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  implsch_cta<R, P>(T, a, blockIdx.x, smem);
+}
+
+// Batched form: the CTAs of all members of an ensemble in one launch.  CTA b
+// belongs to member g with first[g] <= b < first[g + 1]; the member's tables
+// and arguments are copied into shared memory first.
+template <typename R, int P>
+__global__ void __launch_bounds__(P * 32) implsch_batch_kernel(const ImplMember<R>* __restrict__ mem,
+                                                              const int* __restrict__ first, int nmem) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ __align__(16) ImplMember<R> sm;
+  __shared__ int sg;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = nmem - 1;  // last g with first[g] <= blockIdx.x
+    while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (first[mid] <= (int)blockIdx.x) lo = mid; else hi = mid - 1; }
+    sg = lo;
+  }
+  __syncthreads();
+  const int g = sg;
+  {
+    const int nw = (int)(sizeof(ImplMember<R>) / sizeof(int));
+    const int* src = reinterpret_cast<const int*>(mem + g);
+    int* dst = reinterpret_cast<int*>(&sm);
+    for (int q = threadIdx.x; q < nw; q += blockDim.x) dst[q] = src[q];
+  }
+  __syncthreads();
+  implsch_cta<R, P>(sm.T, sm.a, (int)blockIdx.x - first[g], smem);
+}
+
 template <typename R> size_t implsch_smem_bytes(const DevTables<R>& T, int P) {
   return tables_bytes<R>(T.lay) + (size_t)P * warp_ws_bytes<R>(T.ld, T.ML, T.need_sp, T.scr);
 }
 
 // CTA shapes compiled: FP32 with 4, 6 or 8 sea points per CTA, FP64 with 2 or 4.
 template <typename R, int P> cudaError_t set_smem_one(size_t bytes) {
-  return cudaFuncSetAttribute(implsch_kernel<R, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaError_t e = cudaFuncSetAttribute(implsch_kernel<R, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(implsch_batch_kernel<R, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+template <typename R, int P>
+void launch_batch_one(const ImplMember<R>* mem, const int* first, int nmem, int nblocks, size_t smem, cudaStream_t s) {
+  implsch_batch_kernel<R, P><<<nblocks, P * 32, smem, s>>>(mem, first, nmem);
 }
 template <typename R, int P> void launch_one(const DevTables<R>& T, const ImplArgs<R>& a, size_t smem, cudaStream_t s) {
   implsch_kernel<R, P><<<(a.nsea + P - 1) / P, P * 32, smem, s>>>(T, a);
 }
 
+// The opt-in shared-memory limit of a kernel instance is process state of
+// the device: it is only ever raised, so a batch or a context with a small
+// spectrum never lowers it under another live context's need.
 template <typename R> cudaError_t implsch_set_max_smem(int P, size_t bytes) {
+  static std::mutex mu;
+  static size_t cur[2][64][9] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64 || P < 0 || P > 8) return cudaErrorInvalidValue;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& c = cur[sizeof(R) == 4 ? 0 : 1][dev][P];
+  if (bytes <= c) return cudaSuccess;
   if (sizeof(R) == 4) {
-    if (P == 4) return set_smem_one<R, 4>(bytes);
-    if (P == 6) return set_smem_one<R, 6>(bytes);
-    if (P == 8) return set_smem_one<R, 8>(bytes);
+    if (P == 4) e = set_smem_one<R, 4>(bytes);
+    else if (P == 6) e = set_smem_one<R, 6>(bytes);
+    else if (P == 8) e = set_smem_one<R, 8>(bytes);
+    else return cudaErrorInvalidValue;
   } else {
-    if (P == 2) return set_smem_one<R, 2>(bytes);
-    if (P == 4) return set_smem_one<R, 4>(bytes);
+    if (P == 2) e = set_smem_one<R, 2>(bytes);
+    else if (P == 4) e = set_smem_one<R, 4>(bytes);
+    else return cudaErrorInvalidValue;
   }
-  return cudaErrorInvalidValue;
+  if (e == cudaSuccess) c = bytes;
+  return e;
 }
 
 template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const ImplArgs<R>& a, int P, cudaStream_t s) {
@@ -106,6 +160,25 @@ template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const Im
   return cudaGetLastError();
 }
 
+template <typename R>
+cudaError_t launch_implsch_batch(const ImplMember<R>* mem, const int* first, int nmem, int nblocks, int P, size_t smem,
+                                 cudaStream_t s) {
+  if (nblocks == 0) return cudaSuccess;
+  if (sizeof(R) == 4) {
+    if (P == 4) launch_batch_one<R, 4>(mem, first, nmem, nblocks, smem, s);
+    else if (P == 6) launch_batch_one<R, 6>(mem, first, nmem, nblocks, smem, s);
+    else if (P == 8) launch_batch_one<R, 8>(mem, first, nmem, nblocks, smem, s);
+    else return cudaErrorInvalidValue;
+  } else {
+    if (P == 2) launch_batch_one<R, 2>(mem, first, nmem, nblocks, smem, s);
+    else if (P == 4) launch_batch_one<R, 4>(mem, first, nmem, nblocks, smem, s);
+    else return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template cudaError_t launch_implsch_batch<float>(const ImplMember<float>*, const int*, int, int, int, size_t, cudaStream_t);
+template cudaError_t launch_implsch_batch<double>(const ImplMember<double>*, const int*, int, int, int, size_t, cudaStream_t);
 template cudaError_t launch_implsch<float>(const DevTables<float>&, const ImplArgs<float>&, int, cudaStream_t);
 template cudaError_t launch_implsch<double>(const DevTables<double>&, const ImplArgs<double>&, int, cudaStream_t);
 template size_t implsch_smem_bytes<float>(const DevTables<float>&, int);

@@ -26,6 +26,17 @@ template <typename R> struct ImplArgs {
 };
 
 template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const ImplArgs<R>& a, int points_per_cta, cudaStream_t s);
+// One member of a batched IMPLSCH launch.
+template <typename R> struct ImplMember {
+  DevTables<R> T;
+  ImplArgs<R> a;
+};
+// CTA b of a batched launch works for member g with first[g] <= b < first[g+1]
+// (first[g] = sum of ceil(NSEA/P) over the members before g); smem is the
+// largest member's dynamic shared memory.
+template <typename R>
+cudaError_t launch_implsch_batch(const ImplMember<R>* mem, const int* first, int nmem, int nblocks, int points_per_cta,
+                                 size_t smem, cudaStream_t s);
 template <typename R> size_t implsch_smem_bytes(const DevTables<R>& T, int points_per_cta);
 template <typename R> cudaError_t implsch_set_max_smem(int points_per_cta, size_t bytes);
 
@@ -35,6 +46,21 @@ cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, in
                            int mcount = -1);
 // True when a sub-step of plane m reads only plane m (no current refraction).
 bool propags_planes_independent(int variant);
+// One member of a batched PROPAGS sub-step: its metadata, the buffers of
+// this sub-step and the number of point blocks per frequency.
+template <typename R> struct PropMember {
+  PropArgs<R> A;
+  const R* src;
+  R* dst;
+  int ld, nbi;
+};
+// All members of one coefficient family (variant, reduced grid, depth
+// refraction taken from `family`) in one launch of bs-point CTAs (128 or 256);
+// CTA b works for member g with first[g] <= b < first[g+1] (first[g] = sum of
+// ML*nbi over the members before g).
+template <typename R>
+cudaError_t launch_propags_batch(const PropArgs<R>& family, const PropMember<R>* mem, const int* first, int nmem,
+                                 int nblocks, int bs, cudaStream_t s);
 template <typename R> cudaError_t launch_cfl_extrema(const PropArgs<R>& A, long long* ext, int nsm, cudaStream_t s);
 double cfl_decode(long long v, int precision);
 cudaError_t static_scratch_address(void** p);

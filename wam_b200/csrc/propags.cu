@@ -5,13 +5,10 @@
 
 namespace wamgpu {
 
-// One thread per (sea point, frequency) walking the directions.
+// One thread per (sea point i, frequency m) walking the directions.
 template <typename R, int VAR, bool RED, bool REFRD>
-__global__ void __launch_bounds__(128) propags_kernel(const __grid_constant__ PropArgs<R> A, const R* __restrict__ f1, int ld1,
-                                                      R* __restrict__ f3, int ld3, int m0) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int m = m0 + blockIdx.y;
-  if (i >= A.nsea) return;
+__device__ __forceinline__ void propags_point(const PropArgs<R>& A, const R* __restrict__ f1, int ld1,
+                                              R* __restrict__ f3, int ld3, int i, int m) {
   using S = Site<R, VAR, RED, REFRD>;
   const S site(A, i, m);
   const int KL = A.KL, ML = A.ML;
@@ -43,6 +40,44 @@ __global__ void __launch_bounds__(128) propags_kernel(const __grid_constant__ Pr
     fkm = fk; fk = fkp;
     site.advance(W, k);
   }
+}
+
+template <typename R, int VAR, bool RED, bool REFRD>
+__global__ void __launch_bounds__(128) propags_kernel(const __grid_constant__ PropArgs<R> A, const R* __restrict__ f1,
+                                                      int ld1, R* __restrict__ f3, int ld3, int m0) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.nsea) return;
+  propags_point<R, VAR, RED, REFRD>(A, f1, ld1, f3, ld3, i, m0 + blockIdx.y);
+}
+
+// Batched form: every member of an ensemble (one coefficient family) in one
+// launch of BS-point CTAs.  CTA b belongs to member g with first[g] <= b <
+// first[g + 1] and covers frequency m and points ib*BS .. of that member; the
+// member's metadata block (direction tables included) is copied into shared
+// memory first.
+template <typename R, int VAR, bool RED, bool REFRD, int BS>
+__global__ void __launch_bounds__(BS) propags_batch_kernel(const PropMember<R>* __restrict__ mem,
+                                                           const int* __restrict__ first, int nmem) {
+  __shared__ __align__(16) PropMember<R> sm;
+  __shared__ int sg;
+  if (threadIdx.x == 0) {
+    int lo = 0, hi = nmem - 1;
+    while (lo < hi) { int mid = (lo + hi + 1) >> 1; if (first[mid] <= (int)blockIdx.x) lo = mid; else hi = mid - 1; }
+    sg = lo;
+  }
+  __syncthreads();
+  const int g = sg;
+  {
+    const int nw = (int)(sizeof(PropMember<R>) / sizeof(int));
+    const int* src = reinterpret_cast<const int*>(mem + g);
+    int* dst = reinterpret_cast<int*>(&sm);
+    for (int q = threadIdx.x; q < nw; q += BS) dst[q] = src[q];
+  }
+  __syncthreads();
+  const int lb = (int)blockIdx.x - first[g], m = lb / sm.nbi, ib = lb - m * sm.nbi;
+  const int i = ib * BS + threadIdx.x;
+  if (i >= sm.A.nsea) return;
+  propags_point<R, VAR, RED, REFRD>(sm.A, sm.src, sm.ld, sm.dst, sm.ld, i, m);
 }
 
 // Order-preserving float <-> int mapping for atomic max/min of extrema.
@@ -116,6 +151,23 @@ template <typename R, int V, bool RED, bool RD> struct CflLaunch {
   }
 };
 
+template <typename R, int V, bool RED, bool RD> struct PropBatchLaunch {
+  static cudaError_t run(const PropArgs<R>&, const PropMember<R>* mem, const int* first, int nmem, int nblocks, int bs,
+                         cudaStream_t s) {
+    if (bs == 128) propags_batch_kernel<R, V, RED, RD, 128><<<nblocks, 128, 0, s>>>(mem, first, nmem);
+    else if (bs == 256) propags_batch_kernel<R, V, RED, RD, 256><<<nblocks, 256, 0, s>>>(mem, first, nmem);
+    else return cudaErrorInvalidValue;
+    return cudaGetLastError();
+  }
+};
+
+template <typename R>
+cudaError_t launch_propags_batch(const PropArgs<R>& family, const PropMember<R>* mem, const int* first, int nmem,
+                                 int nblocks, int bs, cudaStream_t s) {
+  if (nblocks == 0) return cudaSuccess;
+  return dispatch<R, PropBatchLaunch>(family, mem, first, nmem, nblocks, bs, s);
+}
+
 template <typename R>
 cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s, int m0, int mcount) {
   if (mcount < 0) mcount = A.ML - m0;
@@ -158,6 +210,10 @@ double cfl_decode(long long v, int precision) {
 
 template cudaError_t launch_propags<float>(const PropArgs<float>&, const float*, int, float*, int, cudaStream_t, int, int);
 template cudaError_t launch_propags<double>(const PropArgs<double>&, const double*, int, double*, int, cudaStream_t, int, int);
+template cudaError_t launch_propags_batch<float>(const PropArgs<float>&, const PropMember<float>*, const int*, int, int,
+                                                 int, cudaStream_t);
+template cudaError_t launch_propags_batch<double>(const PropArgs<double>&, const PropMember<double>*, const int*, int,
+                                                  int, int, cudaStream_t);
 template cudaError_t launch_cfl_extrema<float>(const PropArgs<float>&, long long*, int, cudaStream_t);
 template cudaError_t launch_cfl_extrema<double>(const PropArgs<double>&, long long*, int, cudaStream_t);
 

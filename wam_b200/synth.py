@@ -15,6 +15,10 @@ Workloads (names used by bench.py and the tests):
   c2  c1 recipe at 400x300 (0.3 deg), ST4, 24 x 600 s (adjoint window)
   c4  0.25 deg 1440x680 (85S-85N), ~35% land, 10-6000 m, KL=36 ML=35 ST4,
       zonal wind profile + eddies, 300 s / 900 s
+  c3  ensemble of 32 members (make_ensemble): regional 0.25-1 deg grids of
+      2k-150k sea points (log-uniform), KL x ML 24x25 or 36x30, ST4 and ST6
+      alternating, each with its own c0-recipe wind (own seed, speed scaled by
+      a factor in 0.85-1.15), 4000 m, 900 s / 900 s
 Grids can be scaled down (`scale`) for parity tests.
 """
 import math
@@ -165,6 +169,37 @@ def make_workload(name, seed=1234, scale=1.0, precision=4, device=0):
         g["_mask"] = sea
         return _finish(name, cfg, g, depth, u, v, rng, n_src_steps=96, sub_steps=3)
     raise KeyError(name)
+
+
+def make_ensemble(n_members=32, seed=777, size_range=(2000, 150000), precision=4, device=0):
+    """Members of the batched-ensemble configuration (list of Workload)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for g in range(n_members):
+        target = float(np.exp(rng.uniform(math.log(size_range[0]), math.log(size_range[1]))))
+        if rng.random() < 0.5:
+            kl, ml, fr1 = 24, 25, 0.04177
+        else:
+            kl, ml, fr1 = 36, 30, 0.0345
+        iphys = 1 if g % 2 == 0 else 2
+        ncell = target / 0.9
+        nx = max(8, int(math.sqrt(1.5 * ncell)))
+        ny = max(6, int(ncell / nx))
+        res = min(float(rng.uniform(0.25, 1.0)), 100.0 / ny)
+        south = -0.5 * ny * res
+        west = float(rng.uniform(-180.0, 180.0 - nx * res))
+        sea = blob_mask(rng, nx, ny, 0.10, 3)
+        grid = regular_grid(sea, south, west, res, res)
+        cfg = make_config(kl, ml, fr1, iphys, 900, 900, grid["delphi"], shallow_run=False, spherical_run=True,
+                          betamax=1.42 if iphys == 1 else 1.20, precision=precision, device=device)
+        depth = np.full((nx, ny), 4000.0)
+        fac = float(rng.uniform(0.85, 1.15))
+        spd = fac * (5 + 15 * _unit(_smooth(rng.random((nx, ny)), 3)))
+        drc = 2 * math.pi * _unit(_smooth(rng.random((nx, ny)), 3))
+        u, v = spd * np.sin(drc), spd * np.cos(drc)
+        grid["_mask"] = sea
+        out.append(_finish(f"c3/{g}", cfg, grid, depth, u, v, rng, n_src_steps=96, sub_steps=1))
+    return out
 
 
 def _unit(x):
