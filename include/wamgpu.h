@@ -191,9 +191,13 @@ WAMGPU_API int wamgpu_get_timing(wamgpu_ctx* ctx, float* ms, int* count);
  * bit-identical to wamgpu_step_dev of each member.
  *  - wamgpu_batch_set_member gives member g's device state, as for
  *    wamgpu_step_dev (scratch is required).
- *  - wamgpu_batch_tune times the compiled CTA shapes (sea points per IMPLSCH
- *    CTA, points per PROPAGS CTA) on the members' state, writing only
- *    scratch, keeps the fastest and returns them.
+ *  - IMPLSCH runs one launch per class of members that share their source
+ *    tables (spectral grid and physics configuration), so each launch keeps
+ *    the occupancy of its own workspace size.
+ *  - wamgpu_batch_tune times the compiled CTA shapes on the members' state,
+ *    writing only scratch: points per PROPAGS CTA, and sea points per IMPLSCH
+ *    CTA for each class.  It keeps the fastest and returns the PROPAGS value
+ *    and the IMPLSCH value of the class with the most sea points.
  *  - wamgpu_batch_step runs one pass on `stream` (NULL = the first member's
  *    stream); after wamgpu_batch_capture it replays the captured CUDA graph.
  *    wamgpu_batch_capture records one pass as a CUDA graph; setting a

@@ -180,3 +180,21 @@ def test_hs_tm_after_simulated_hours(oracle_mod, name, scale, hours):
     err_tm = np.abs(tm_g - tm_o) / tm_o
     assert np.quantile(err_hs, 0.99) <= 1e-4 and err_hs.max() <= 1e-3, (err_hs.max(), np.quantile(err_hs, 0.99))
     assert np.quantile(err_tm, 0.99) <= 1e-4 and err_tm.max() <= 1e-3, (err_tm.max(), np.quantile(err_tm, 0.99))
+
+
+@pytest.mark.parametrize("iphys", [1, 2])
+def test_implsch_isnonlin_table(oracle_mod, iphys):
+    """SNONLIN with the MAKE_SHALLOW_SNL depth factors (ISNONLIN = 1,
+    wam_source_module.f90:975-1048) instead of the AKMEAN scaling: the shallow
+    regional grid, one FP32 step against the oracle."""
+    from wam_b200.synth import make_workload
+    w = make_workload("c2" if iphys == 1 else "c1", scale=0.02)
+    w.cfg = dict(w.cfg, isnonlin=1)
+    o, m = _setup(oracle_mod, w)
+    f, tw, us, zz, indep = _spinup(o, w)
+    fo, two, uso, zo, _ = o.implsch(f.astype(float), w.u10, w.udir, tw, us, zz, w.roairn, w.wstar, w.depth, indep)
+    fg = np.asfortranarray(f.copy())
+    tg, ug, zg = tw.copy(), us.copy(), zz.copy()
+    m.implsch(fg, w.u10, w.udir, tg, ug, zg, w.roairn, w.wstar)
+    _check_points(_point_rel(fg, fo), 2e-6 if iphys == 1 else 1e-4, "ISNONLIN=1 FL3")
+    assert np.max(np.abs(ug - uso) / uso) <= 1e-5

@@ -1,6 +1,7 @@
 // C ABI of libwamgpu (declarations and reference citations in include/wamgpu.h).
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -78,6 +79,7 @@ template <typename R> struct Impl : ImplBase {
   TableSet<R> tab;
   DevTables<R> dt{};
   PropArgs<R> pa{};
+  bool has_enh = false;  // MAKE_SHALLOW_SNL factors uploaded to `enh` ([ij + nsea*(mc-1)])
   DevBuf small, ismall, tfak, tcgond, tsihkd, flminfr, enh, gom, fr, sinth, costh;
   // per-point metadata
   DevBuf d_klat, d_klon, d_wlat, d_dpsn, d_della0, d_drgm, d_indep, d_indep_g, d_ddphi, d_ddlam, d_duphi, d_dulam,
@@ -192,7 +194,6 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
   d.lay = L;
   d.small = I.small.template as<R>(); d.ismall = I.ismall.template as<int>();
   d.TFAK = I.tfak.template as<R>(); d.TCGOND = I.tcgond.template as<R>(); d.FLMINFR = I.flminfr.template as<R>();
-  d.ENH = nullptr; d.enh_ld = 0;
   if (d.NK10 > MAX_NK10) return fail(ctx, WAMGPU_E_ARG, "frequency grid too low: 10 Hz extension exceeds kernel bound");
   // every DIA gather row and scatter target the kernel can touch lies inside the spectrum
   {
@@ -412,7 +413,7 @@ template <typename R> int prepare_prop(wamgpu_ctx* ctx, Impl<R>& I, float* total
   if (total_cfl) *total_cfl = (float)tc;
   if (counter) *counter = cnt;
   // per-point source inputs for the host entry points
-  I.dt.ENH = nullptr;
+  I.has_enh = false;
   ctx->prepared = true;
   return WAMGPU_OK;
 }
@@ -434,7 +435,7 @@ template <typename R> int set_grid_t(wamgpu_ctx* ctx, Impl<R>& I) {
 // MAKE_SHALLOW_SNL (:975-1048)
 template <typename R> int prepare_source_t(wamgpu_ctx* ctx, Impl<R>& I) {
   const Config& c = ctx->cfg;
-  I.dt.ENH = nullptr; I.dt.enh_ld = 0;
+  I.has_enh = false;
   if (!(c.shallow_run && c.isnonlin != 0)) return WAMGPU_OK;
   const TableSet<R>& t = I.tab;
   const int n = ctx->nsea, mlsthg = t.MLSTHG;
@@ -446,7 +447,7 @@ template <typename R> int prepare_source_t(wamgpu_ctx* ctx, Impl<R>& I) {
       enh[i + (size_t)n * (m - 1)] = std::min(R(10.), transf(aki(om, d), d));
     }
   CK(upload(I.enh, enh, ctx->stream), "upload ENH");
-  I.dt.ENH = I.enh.template as<R>(); I.dt.enh_ld = n;
+  I.has_enh = true;
   CK(cudaStreamSynchronize(ctx->stream), "ENH");
   return WAMGPU_OK;
 }
@@ -456,7 +457,7 @@ int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u1
                   void* ustar, void* z0, const void* roairn, const void* wstar, cudaStream_t s, const void* fl3_in = nullptr) {
   if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first (INDEP)");
   if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
-  if (ctx->cfg.shallow_run && ctx->cfg.isnonlin != 0 && !I.dt.ENH)
+  if (ctx->cfg.shallow_run && ctx->cfg.isnonlin != 0 && !I.has_enh)
     return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_source first (ISNONLIN table)");
   if (!I.status.p) { CK(I.status.ensure(16), "alloc"); CK(cudaMemsetAsync(I.status.p, 0, 16, s), "memset"); }
   if (ctx->cfg.lcflx) CK(I.fluxes.ensure((size_t)7 * ctx->nsea * sizeof(R) + 16), "alloc");
@@ -467,6 +468,7 @@ int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u1
   a.tauw = (R*)tauw; a.ustar = (R*)ustar; a.z0 = (R*)z0;
   a.fluxes = ctx->cfg.lcflx ? I.fluxes.template as<R>() : nullptr;
   a.flx_ld = ctx->nsea;
+  a.enh = I.has_enh ? I.enh.template as<R>() : nullptr; a.enh_ld = ctx->nsea;
   a.status = I.status.template as<int>();
   { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch"); }
   return WAMGPU_OK;
@@ -622,7 +624,7 @@ int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float*
   if (sizeof(R) != 4) return fail(ctx, WAMGPU_E_ARG, "wamgpu_step_host is FP32 only; use wamgpu_step_dev");
   if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
   if (nprop < 0) return fail(ctx, WAMGPU_E_ARG, "nprop < 0");
-  if (ctx->cfg.shallow_run && ctx->cfg.isnonlin != 0 && !I.dt.ENH)
+  if (ctx->cfg.shallow_run && ctx->cfg.isnonlin != 0 && !I.has_enh)
     return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_source first (ISNONLIN table)");
   const int n = ctx->nsea, KL = ctx->cfg.kl, ML = ctx->cfg.ml;
   const size_t plane = (size_t)n * KL, nb = plane * ML;
@@ -680,9 +682,8 @@ int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float*
       a.fluxes = ctx->cfg.lcflx ? I.fluxes.template as<R>() + p0 : nullptr;
       a.flx_ld = n;
       a.status = I.status.template as<int>();
-      DevTables<R> dt = I.dt;
-      if (dt.ENH) dt.ENH += p0;
-      { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(dt, a, ctx->P, s), "implsch launch"); }
+      a.enh = I.has_enh ? I.enh.template as<R>() + p0 : nullptr; a.enh_ld = n;
+      { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch"); }
     }
     CK(cudaEventRecord(ctx->xfer_ev[ngrp + q], s), "event");
     CK(cudaStreamWaitEvent(c, ctx->xfer_ev[ngrp + q], 0), "wait");
@@ -757,7 +758,7 @@ struct BatchState {
   const void *u10 = nullptr, *udir = nullptr, *roairn = nullptr, *wstar = nullptr;
   void *tauw = nullptr, *ustar = nullptr, *z0 = nullptr;
 };
-struct BatchList { int family = 0; int nmem = 0, nblocks = 0; DevBuf mem, first; };
+struct BatchList { int family = 0; int nmem = 0, nblocks = 0, P = 0; size_t smem = 0; DevBuf mem, first; };
 
 }  // namespace
 
@@ -766,11 +767,11 @@ struct wamgpu_batch {
   std::vector<wamgpu_ctx*> members;
   int precision = 4, device = 0;
   std::vector<BatchState> st;
-  int P = 0, bs = 128;  // IMPLSCH sea points per CTA, PROPAGS points per CTA
+  std::vector<int> Pc;  // IMPLSCH sea points per CTA of each source-table class (empty: the contexts' own choice)
+  int bs = 128;         // PROPAGS points per CTA
   bool built = false;
   std::vector<std::vector<BatchList>> sub;  // [sub-step][family group]
-  BatchList imp;
-  size_t imp_smem = 0;
+  std::vector<BatchList> imp;               // IMPLSCH, one list per shared-memory class
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   cudaStream_t stream = nullptr;
@@ -804,50 +805,83 @@ template <typename R> Impl<R>& impl_of(wamgpu_ctx* c) { return *static_cast<Impl
 // sub-steps of a member in one pass: IDELT/IDELPRO propagation calls of COUNTER sub-steps each
 int member_nsub(const wamgpu_ctx* c) { return (c->cfg.idelt / c->cfg.idelpro) * c->counter; }
 
-template <typename R> size_t batch_smem(wamgpu_batch* b, int P) {
-  size_t mx = 0;
-  for (auto* c : b->members) mx = std::max(mx, implsch_smem_bytes(impl_of<R>(c).dt, P));
-  return mx;
-}
 constexpr size_t kMaxSmemPerCta = 232448;  // 227 KB opt-in limit of sm_100
 
-// IMPLSCH member list.  For tuning (out != null) each member reads its
+// The configuration fields that determine a context's source tables
+// (DevTables): members that agree on them can share one batched IMPLSCH
+// launch with one member's tables as the kernel parameter.
+std::vector<double> source_key(const Config& c) {
+  return {double(c.kl), double(c.ml), c.fr1, double(c.iref), double(c.iphys), double(c.shallow_run),
+          double(c.isnonlin), double(c.lcflx), double(c.idelt), c.betamax, c.zalp, c.alpha, c.tauwshelter, c.cdfac,
+          double(c.ndepth), c.deptha, c.depthd, double(c.precision)};
+}
+
+// IMPLSCH member lists, one per source-table class, largest members first
+// (their CTAs start first).  For tuning (out != null) each member reads its
 // current spectrum and writes `out`, TAUW/USTAR/Z0 go to `tmp3` and the
 // status flag to `tmp_status`: the members' state is left untouched.
 template <typename R>
-int batch_impl_list(wamgpu_batch* b, int P, BatchList& L, size_t& smem, const std::vector<R*>* out,
-                    const std::vector<R*>* tmp3, int* tmp_status, cudaStream_t s) {
+int batch_impl_lists(wamgpu_batch* b, const std::vector<int>& Pin, std::vector<BatchList>& Ls, const std::vector<R*>* out,
+                     const std::vector<R*>* tmp3, int* tmp_status, cudaStream_t s) {
   const int n = (int)b->members.size();
-  std::vector<ImplMember<R>> mem(n);
-  std::vector<int> first(n + 1, 0);
+  std::vector<std::vector<double>> keys;
+  std::vector<int> cls(n);
   for (int g = 0; g < n; ++g) {
-    wamgpu_ctx* c = b->members[g];
-    Impl<R>& I = impl_of<R>(c);
-    const BatchState& x = b->st[g];
-    if (!I.status.p) { BCK(I.status.ensure(16), "alloc"); BCK(cudaMemsetAsync(I.status.p, 0, 16, s), "memset"); }
-    if (c->cfg.lcflx) BCK(I.fluxes.ensure((size_t)7 * c->nsea * sizeof(R) + 16), "alloc");
-    ImplMember<R>& M = mem[g];
-    M.T = I.dt;
-    ImplArgs<R>& a = M.a;
-    a.nsea = c->nsea; a.ld = x.ld;
-    R* fin = (member_nsub(c) % 2 == 0) ? (R*)x.fl3 : (R*)x.scratch;  // buffer the last sub-step wrote
-    a.fl3_in = out ? (const R*)x.fl3 : fin;
-    a.fl3 = out ? (*out)[g] : (R*)x.fl3;
-    a.u10 = (const R*)x.u10; a.udir = (const R*)x.udir; a.roairn = (const R*)x.roairn; a.wstar = (const R*)x.wstar;
-    a.depth = I.d_depth.template as<R>(); a.indep = I.d_indep.template as<int>();
-    if (tmp3) { a.tauw = (*tmp3)[3 * g]; a.ustar = (*tmp3)[3 * g + 1]; a.z0 = (*tmp3)[3 * g + 2]; }
-    else { a.tauw = (R*)x.tauw; a.ustar = (R*)x.ustar; a.z0 = (R*)x.z0; }
-    a.fluxes = (c->cfg.lcflx && !tmp3) ? I.fluxes.template as<R>() : nullptr;
-    a.flx_ld = c->nsea;
-    a.status = tmp_status ? tmp_status : I.status.template as<int>();
-    first[g + 1] = first[g] + (c->nsea + P - 1) / P;
+    std::vector<double> k = source_key(b->members[g]->cfg);
+    auto it = std::find(keys.begin(), keys.end(), k);
+    cls[g] = (int)(it - keys.begin());
+    if (it == keys.end()) keys.push_back(k);
   }
-  smem = batch_smem<R>(b, P);
-  if (smem + sizeof(ImplMember<R>) + 64 > kMaxSmemPerCta) return bfail(b, WAMGPU_E_ARG, "points per CTA too large for a member");
-  BCK(implsch_set_max_smem<R>(P, smem), "smem attribute");
-  BCK(upload_vec(L.mem, mem, s), "upload batch");
-  BCK(upload_vec(L.first, first, s), "upload batch");
-  L.nmem = n; L.nblocks = first[n];
+  Ls.clear();
+  Ls.resize(keys.size());
+  for (size_t ci = 0; ci < keys.size(); ++ci) {
+    std::vector<int> order;
+    for (int g = 0; g < n; ++g) if (cls[g] == (int)ci) order.push_back(g);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->members[x]->nsea > b->members[y]->nsea; });
+    // sea points per CTA: the tuned value of this class, else the contexts' own occupancy choice
+    const int P = (ci < Pin.size() && Pin[ci] > 0) ? Pin[ci] : b->members[order[0]]->P;
+    if (implsch_smem_bytes(impl_of<R>(b->members[order[0]]).dt, P) + sizeof(ImplArgs<R>) + 64 > kMaxSmemPerCta)
+      return bfail(b, WAMGPU_E_ARG, "points per CTA too large for a member");
+    std::vector<ImplArgs<R>> mem(order.size());
+    std::vector<int> first(order.size() + 1, 0);
+    for (size_t q = 0; q < order.size(); ++q) {
+      const int g = order[q];
+      wamgpu_ctx* c = b->members[g];
+      Impl<R>& I = impl_of<R>(c);
+      const BatchState& x = b->st[g];
+      if (!I.status.p) { BCK(I.status.ensure(16), "alloc"); BCK(cudaMemsetAsync(I.status.p, 0, 16, s), "memset"); }
+      if (c->cfg.lcflx) BCK(I.fluxes.ensure((size_t)7 * c->nsea * sizeof(R) + 16), "alloc");
+      ImplArgs<R>& a = mem[q];
+      a.nsea = c->nsea; a.ld = x.ld;
+      R* fin = (member_nsub(c) % 2 == 0) ? (R*)x.fl3 : (R*)x.scratch;  // buffer the last sub-step wrote
+      a.fl3_in = out ? (const R*)x.fl3 : fin;
+      a.fl3 = out ? (*out)[g] : (R*)x.fl3;
+      a.u10 = (const R*)x.u10; a.udir = (const R*)x.udir; a.roairn = (const R*)x.roairn; a.wstar = (const R*)x.wstar;
+      a.depth = I.d_depth.template as<R>(); a.indep = I.d_indep.template as<int>();
+      if (tmp3) { a.tauw = (*tmp3)[3 * g]; a.ustar = (*tmp3)[3 * g + 1]; a.z0 = (*tmp3)[3 * g + 2]; }
+      else { a.tauw = (R*)x.tauw; a.ustar = (R*)x.ustar; a.z0 = (R*)x.z0; }
+      a.fluxes = (c->cfg.lcflx && !tmp3) ? I.fluxes.template as<R>() : nullptr;
+      a.flx_ld = c->nsea;
+      a.enh = I.has_enh ? I.enh.template as<R>() : nullptr; a.enh_ld = c->nsea;
+      a.status = tmp_status ? tmp_status : I.status.template as<int>();
+      first[q + 1] = first[q] + (c->nsea + P - 1) / P;
+    }
+    BatchList& L = Ls[ci];
+    L.family = order[0];  // whose source tables the launch passes
+    L.P = P;
+    L.smem = implsch_smem_bytes(impl_of<R>(b->members[order[0]]).dt, P);
+    BCK(implsch_set_max_smem<R>(P, L.smem), "smem attribute");
+    BCK(upload_vec(L.mem, mem, s), "upload batch");
+    BCK(upload_vec(L.first, first, s), "upload batch");
+    L.nmem = (int)order.size(); L.nblocks = first.back();
+  }
+  return WAMGPU_OK;
+}
+
+template <typename R> int launch_impl_lists(wamgpu_batch* b, const std::vector<BatchList>& Ls, cudaStream_t s) {
+  for (const BatchList& L : Ls)
+    BCK(launch_implsch_batch<R>(impl_of<R>(b->members[L.family]).dt, L.mem.template as<ImplArgs<R>>(),
+                                L.first.template as<int>(), L.nmem, L.nblocks, L.P, L.smem, s), "batched IMPLSCH");
   return WAMGPU_OK;
 }
 
@@ -855,7 +889,6 @@ template <typename R> int batch_build(wamgpu_batch* b, cudaStream_t s) {
   const int n = (int)b->members.size();
   for (int g = 0; g < n; ++g)
     if (!b->st[g].fl3) return bfail(b, WAMGPU_E_STATE, "member " + std::to_string(g) + " has no state (wamgpu_batch_set_member)");
-  if (b->P == 0) b->P = sizeof(R) == 4 ? 6 : 2;
   int maxsub = 0;
   for (auto* c : b->members) maxsub = std::max(maxsub, member_nsub(c));
   b->sub.clear();
@@ -897,8 +930,9 @@ template <typename R> int batch_build(wamgpu_batch* b, cudaStream_t s) {
       BCK(upload_vec(L.first, first, s), "upload batch");
     }
   }
-  int rc = batch_impl_list<R>(b, b->P, b->imp, b->imp_smem, nullptr, nullptr, nullptr, s);
+  int rc = batch_impl_lists<R>(b, b->Pc, b->imp, nullptr, nullptr, nullptr, s);
   if (rc) return rc;
+
   BCK(cudaStreamSynchronize(s), "batch upload");
   b->built = true;
   return WAMGPU_OK;
@@ -911,9 +945,7 @@ template <typename R> int batch_launch(wamgpu_batch* b, cudaStream_t s) {
       BCK(launch_propags_batch<R>(fam, L.mem.template as<PropMember<R>>(), L.first.template as<int>(), L.nmem, L.nblocks,
                                   b->bs, s), "batched PROPAGS");
     }
-  BCK(launch_implsch_batch<R>(b->imp.mem.template as<ImplMember<R>>(), b->imp.first.template as<int>(), b->imp.nmem,
-                              b->imp.nblocks, b->P, b->imp_smem, s), "batched IMPLSCH");
-  return WAMGPU_OK;
+  return launch_impl_lists<R>(b, b->imp, s);
 }
 
 // Autotuner: times the first batched PROPAGS sub-step with 128- and 256-point
@@ -984,31 +1016,47 @@ template <typename R> int batch_tune(wamgpu_batch* b, cudaStream_t s, int* P_out
       }
     }
   }
-  int best_P = b->P;
-  best_t = 1e30f;
+  // IMPLSCH: each source-table class keeps its fastest CTA shape
+  const size_t ncls = b->imp.size();
+  std::vector<int> bestP(ncls, 0);
+  std::vector<float> bestT(ncls, 1e30f);
   const std::vector<int> cands = sizeof(R) == 4 ? std::vector<int>{4, 6, 8} : std::vector<int>{2, 4};
   for (int P : cands) {
     if (rc) break;
-    if (batch_smem<R>(b, P) + sizeof(ImplMember<R>) + 64 > kMaxSmemPerCta) continue;
-    BatchList L;
-    size_t smem = 0;
-    if ((rc = batch_impl_list<R>(b, P, L, smem, &out, &t3, tstatus.template as<int>(), s))) break;
-    float t = 0;
-    rc = timed([&]() -> int {
-      BCK(launch_implsch_batch<R>(L.mem.template as<ImplMember<R>>(), L.first.template as<int>(), L.nmem, L.nblocks, P,
-                                  smem, s), "batched IMPLSCH");
-      return WAMGPU_OK;
-    }, t);
+    std::vector<int> Pin(ncls, P);
+    for (size_t ci = 0; ci < ncls; ++ci)  // classes this shape does not fit keep their default
+      if (implsch_smem_bytes(impl_of<R>(b->members[b->imp[ci].family]).dt, P) + sizeof(ImplArgs<R>) + 64 > kMaxSmemPerCta)
+        Pin[ci] = 0;
+    std::vector<BatchList> Ls;
+    if ((rc = batch_impl_lists<R>(b, Pin, Ls, &out, &t3, tstatus.template as<int>(), s))) break;
+    for (size_t ci = 0; ci < ncls && !rc; ++ci) {
+      if (Pin[ci] == 0) continue;
+      float t = 0;
+      std::vector<BatchList> one(1);
+      one[0].family = Ls[ci].family; one[0].nmem = Ls[ci].nmem; one[0].nblocks = Ls[ci].nblocks; one[0].P = Ls[ci].P;
+      one[0].smem = Ls[ci].smem;
+      one[0].mem = std::move(Ls[ci].mem); one[0].first = std::move(Ls[ci].first);
+      rc = timed([&]() -> int { return launch_impl_lists<R>(b, one, s); }, t);
+      if (!rc && t < bestT[ci]) { bestT[ci] = t; bestP[ci] = P; }
+    }
     BCK(cudaStreamSynchronize(s), "tune");
-    if (!rc && t < best_t) { best_t = t; best_P = P; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (rc) return rc;
-  b->P = best_P;
+  b->Pc = bestP;
   b->built = false;
   if ((rc = batch_build<R>(b, s))) return rc;
-  if (P_out) *P_out = b->P;
+  if (P_out) {  // the shape of the class with the most sea points
+    size_t best = 0; int pc = b->imp.empty() ? 0 : b->imp[0].P;
+    for (size_t ci = 0; ci < b->imp.size(); ++ci) {
+      size_t pts = 0;
+      for (size_t g = 0; g < b->members.size(); ++g)
+        if (source_key(b->members[g]->cfg) == source_key(b->members[b->imp[ci].family]->cfg)) pts += b->members[g]->nsea;
+      if (pts > best) { best = pts; pc = b->imp[ci].P; }
+    }
+    *P_out = pc;
+  }
   if (bs_out) *bs_out = b->bs;
   return WAMGPU_OK;
 }
@@ -1267,7 +1315,7 @@ int wamgpu_batch_create(wamgpu_ctx* const* members, int n, wamgpu_batch** out) {
     if (!c->prepared) return bfail(b, WAMGPU_E_STATE, "member " + std::to_string(g) + " not prepared (wamgpu_prepare_propagation)");
     if (g > 0 && (c->cfg.precision != members[0]->cfg.precision || c->cfg.device != members[0]->cfg.device))
       return bfail(b, WAMGPU_E_ARG, "members must share precision and device");
-    const bool enh = c->cfg.precision == 8 ? impl_of<double>(c).dt.ENH != nullptr : impl_of<float>(c).dt.ENH != nullptr;
+    const bool enh = c->cfg.precision == 8 ? impl_of<double>(c).has_enh : impl_of<float>(c).has_enh;
     if (c->cfg.shallow_run && c->cfg.isnonlin != 0 && !enh)
       return bfail(b, WAMGPU_E_STATE, "member " + std::to_string(g) + " needs wamgpu_prepare_source");
     b->members.push_back(c);

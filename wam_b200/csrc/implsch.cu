@@ -44,7 +44,8 @@ __device__ __forceinline__ void implsch_cta(const DevTables<R>& T, const ImplArg
     w.SP = T.need_sp ? w.F + nrow : nullptr;
     w.T = reinterpret_cast<R*>(base + ws_t_offset<R>(LD, T.ML, T.need_sp));
     w.LL = reinterpret_cast<uint8_t*>(w.T + 8 * T.scr);
-    Src<R> src(T, S, w, lane, ij, a.indep[ij], a.u10[ij], a.udir[ij], a.roairn[ij], a.wstar[ij], a.depth[ij]);
+    Src<R> src(T, S, w, lane, ij, a.indep[ij], a.u10[ij], a.udir[ij], a.roairn[ij], a.wstar[ij], a.depth[ij], a.enh,
+               a.enh_ld);
     PointState<R> ps;
     ps.TAUW = a.tauw[ij];
     src.run(ps);
@@ -73,14 +74,16 @@ __global__ void __launch_bounds__(P * 32) implsch_kernel(const __grid_constant__
   implsch_cta<R, P>(T, a, blockIdx.x, smem);
 }
 
-// Batched form: the CTAs of all members of an ensemble in one launch.  CTA b
-// belongs to member g with first[g] <= b < first[g + 1]; the member's tables
-// and arguments are copied into shared memory first.
+// Batched form: the CTAs of all members that share the source tables T (one
+// spectral grid and physics configuration) in one launch.  CTA b belongs to
+// member g with first[g] <= b < first[g + 1]; the member's per-point argument
+// block is copied into shared memory first, T stays a kernel parameter.
 template <typename R, int P>
-__global__ void __launch_bounds__(P * 32) implsch_batch_kernel(const ImplMember<R>* __restrict__ mem,
+__global__ void __launch_bounds__(P * 32) implsch_batch_kernel(const __grid_constant__ DevTables<R> T,
+                                                              const ImplArgs<R>* __restrict__ mem,
                                                               const int* __restrict__ first, int nmem) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ __align__(16) ImplMember<R> sm;
+  __shared__ __align__(16) ImplArgs<R> sa;
   __shared__ int sg;
   if (threadIdx.x == 0) {
     int lo = 0, hi = nmem - 1;  // last g with first[g] <= blockIdx.x
@@ -90,13 +93,13 @@ __global__ void __launch_bounds__(P * 32) implsch_batch_kernel(const ImplMember<
   __syncthreads();
   const int g = sg;
   {
-    const int nw = (int)(sizeof(ImplMember<R>) / sizeof(int));
+    const int nw = (int)(sizeof(ImplArgs<R>) / sizeof(int));
     const int* src = reinterpret_cast<const int*>(mem + g);
-    int* dst = reinterpret_cast<int*>(&sm);
+    int* dst = reinterpret_cast<int*>(&sa);
     for (int q = threadIdx.x; q < nw; q += blockDim.x) dst[q] = src[q];
   }
   __syncthreads();
-  implsch_cta<R, P>(sm.T, sm.a, (int)blockIdx.x - first[g], smem);
+  implsch_cta<R, P>(T, sa, (int)blockIdx.x - first[g], smem);
 }
 
 template <typename R> size_t implsch_smem_bytes(const DevTables<R>& T, int P) {
@@ -110,8 +113,9 @@ template <typename R, int P> cudaError_t set_smem_one(size_t bytes) {
   return cudaFuncSetAttribute(implsch_batch_kernel<R, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 template <typename R, int P>
-void launch_batch_one(const ImplMember<R>* mem, const int* first, int nmem, int nblocks, size_t smem, cudaStream_t s) {
-  implsch_batch_kernel<R, P><<<nblocks, P * 32, smem, s>>>(mem, first, nmem);
+void launch_batch_one(const DevTables<R>& T, const ImplArgs<R>* mem, const int* first, int nmem, int nblocks, size_t smem,
+                      cudaStream_t s) {
+  implsch_batch_kernel<R, P><<<nblocks, P * 32, smem, s>>>(T, mem, first, nmem);
 }
 template <typename R, int P> void launch_one(const DevTables<R>& T, const ImplArgs<R>& a, size_t smem, cudaStream_t s) {
   implsch_kernel<R, P><<<(a.nsea + P - 1) / P, P * 32, smem, s>>>(T, a);
@@ -161,24 +165,26 @@ template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const Im
 }
 
 template <typename R>
-cudaError_t launch_implsch_batch(const ImplMember<R>* mem, const int* first, int nmem, int nblocks, int P, size_t smem,
-                                 cudaStream_t s) {
+cudaError_t launch_implsch_batch(const DevTables<R>& T, const ImplArgs<R>* mem, const int* first, int nmem, int nblocks,
+                                 int P, size_t smem, cudaStream_t s) {
   if (nblocks == 0) return cudaSuccess;
   if (sizeof(R) == 4) {
-    if (P == 4) launch_batch_one<R, 4>(mem, first, nmem, nblocks, smem, s);
-    else if (P == 6) launch_batch_one<R, 6>(mem, first, nmem, nblocks, smem, s);
-    else if (P == 8) launch_batch_one<R, 8>(mem, first, nmem, nblocks, smem, s);
+    if (P == 4) launch_batch_one<R, 4>(T, mem, first, nmem, nblocks, smem, s);
+    else if (P == 6) launch_batch_one<R, 6>(T, mem, first, nmem, nblocks, smem, s);
+    else if (P == 8) launch_batch_one<R, 8>(T, mem, first, nmem, nblocks, smem, s);
     else return cudaErrorInvalidValue;
   } else {
-    if (P == 2) launch_batch_one<R, 2>(mem, first, nmem, nblocks, smem, s);
-    else if (P == 4) launch_batch_one<R, 4>(mem, first, nmem, nblocks, smem, s);
+    if (P == 2) launch_batch_one<R, 2>(T, mem, first, nmem, nblocks, smem, s);
+    else if (P == 4) launch_batch_one<R, 4>(T, mem, first, nmem, nblocks, smem, s);
     else return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
 
-template cudaError_t launch_implsch_batch<float>(const ImplMember<float>*, const int*, int, int, int, size_t, cudaStream_t);
-template cudaError_t launch_implsch_batch<double>(const ImplMember<double>*, const int*, int, int, int, size_t, cudaStream_t);
+template cudaError_t launch_implsch_batch<float>(const DevTables<float>&, const ImplArgs<float>*, const int*, int, int, int,
+                                                 size_t, cudaStream_t);
+template cudaError_t launch_implsch_batch<double>(const DevTables<double>&, const ImplArgs<double>*, const int*, int, int,
+                                                  int, size_t, cudaStream_t);
 template cudaError_t launch_implsch<float>(const DevTables<float>&, const ImplArgs<float>&, int, cudaStream_t);
 template cudaError_t launch_implsch<double>(const DevTables<double>&, const ImplArgs<double>&, int, cudaStream_t);
 template size_t implsch_smem_bytes<float>(const DevTables<float>&, int);

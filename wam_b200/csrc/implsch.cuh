@@ -99,9 +99,12 @@ template <typename R> struct Src {
   WarpWS<R>& w;
   const int lane, ij, INDEP;
   const R U10, UDIR, ROAIRN, WSTAR, DEPTH;
+  const R* ENH;  // MAKE_SHALLOW_SNL factors of the launch's points (ISNONLIN != 0), else null
+  const int enh_ld;
   __device__ Src(const DevTables<R>& t, const STabs<R>& s, WarpWS<R>& ws, int l, int ij_, int indep, R u10, R udir,
-                 R roairn, R wstar, R depth)
-      : T(t), S(s), w(ws), lane(l), ij(ij_), INDEP(indep), U10(u10), UDIR(udir), ROAIRN(roairn), WSTAR(wstar), DEPTH(depth) {}
+                 R roairn, R wstar, R depth, const R* enh, int enh_ld_)
+      : T(t), S(s), w(ws), lane(l), ij(ij_), INDEP(indep), U10(u10), UDIR(udir), ROAIRN(roairn), WSTAR(wstar), DEPTH(depth),
+        ENH(enh), enh_ld(enh_ld_) {}
 
   __device__ int KL() const { return T.KL; }
   __device__ int ML() const { return T.ML; }
@@ -479,7 +482,7 @@ template <typename R> struct Src {
                 rIM1 = ld * (ic5[4] - 1);
       const R* rc = S.RNL + 25 * (mc - 1);
       R ftemp = S.AF11[im];
-      if (T.shallow) ftemp = ftemp * (T.isnonlin == 0 ? enhfr : __ldg(&T.ENH[ij + (size_t)T.enh_ld * (mc - 1)]));
+      if (T.shallow) ftemp = ftemp * (T.isnonlin == 0 ? enhfr : __ldg(&ENH[ij + (size_t)enh_ld * (mc - 1)]));
       const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
       const R ftail = (regime == 0) ? R(1) : rc[0];
       // which targets this frequency writes (uniform over the warp)

@@ -22,21 +22,19 @@ template <typename R> struct ImplArgs {
   R* tauw; R* ustar; R* z0;
   R* fluxes;   // 7 x flx_ld or null
   int flx_ld;  // leading dimension of fluxes (the full NSEA when a launch covers a range of points)
+  const R* enh;  // MAKE_SHALLOW_SNL factors [ij + enh_ld*(mc-1)] when shallow && isnonlin != 0, else null
+  int enh_ld;
   int* status; // bit 0: non-finite output
 };
 
 template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const ImplArgs<R>& a, int points_per_cta, cudaStream_t s);
-// One member of a batched IMPLSCH launch.
-template <typename R> struct ImplMember {
-  DevTables<R> T;
-  ImplArgs<R> a;
-};
-// CTA b of a batched launch works for member g with first[g] <= b < first[g+1]
-// (first[g] = sum of ceil(NSEA/P) over the members before g); smem is the
-// largest member's dynamic shared memory.
+// Batched IMPLSCH over members that share their source tables T (one
+// spectral grid and physics configuration): CTA b works for member g with
+// first[g] <= b < first[g+1] (first[g] = sum of ceil(NSEA/P) over the members
+// before g), whose per-point arguments are mem[g].
 template <typename R>
-cudaError_t launch_implsch_batch(const ImplMember<R>* mem, const int* first, int nmem, int nblocks, int points_per_cta,
-                                 size_t smem, cudaStream_t s);
+cudaError_t launch_implsch_batch(const DevTables<R>& T, const ImplArgs<R>* mem, const int* first, int nmem, int nblocks,
+                                 int points_per_cta, size_t smem, cudaStream_t s);
 template <typename R> size_t implsch_smem_bytes(const DevTables<R>& T, int points_per_cta);
 template <typename R> cudaError_t implsch_set_max_smem(int points_per_cta, size_t bytes);
 

@@ -38,8 +38,6 @@ template <typename R> struct DevTables {
   const R* TFAK;       // [(jd) + NDEPTH*m], jd 0-based
   const R* TCGOND;
   const R* FLMINFR;    // [(ju) + 300*m], ju 0-based
-  const R* ENH;        // [ij + nsea*(mc-1)] when shallow && isnonlin != 0, else null
-  int enh_ld;
 };
 
 }  // namespace wamgpu
