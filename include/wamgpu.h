@@ -181,6 +181,30 @@ WAMGPU_API int wamgpu_get_fluxes(wamgpu_ctx* ctx, float* out7);
 WAMGPU_API int wamgpu_set_timing(wamgpu_ctx* ctx, int enable);
 WAMGPU_API int wamgpu_get_timing(wamgpu_ctx* ctx, float* ms, int* count);
 
+/* One grid over several ranks, in latitude bands as in the reference's MPI
+ * decomposition: each rank owns a contiguous range NIJS..NIJL of the
+ * south-to-north ordered sea points and reads its neighbours' spectra from a
+ * halo (wam_mpi_comp_module.f90:1063-1095).  The reference packs exactly the
+ * needed neighbour points into NINF..NSUP; here a rank's context holds the
+ * contiguous index range that contains them (owned points plus halo,
+ * neighbour numbers local to it), which costs a few more exchanged points and
+ * gives the same results.
+ *  - wamgpu_set_owned (before wamgpu_prepare_propagation) makes the kernels
+ *    update only sea points i0..i1-1 (0-based).  CHECK_CFL then covers the
+ *    owned points, IMPLSCH integrates them, and PROPAGS writes them and
+ *    reads the halo points as the caller left them.
+ *  - wamgpu_set_counter installs the COUNTER agreed over all ranks: the
+ *    largest of the ranks' own values, which is CEILING of the global CFL
+ *    maximum as CHECK_CFL computes it over all processors
+ *    (propagation:2021-2130).
+ *  - wamgpu_propags_substep_dev runs one sub-step of IDELPRO/COUNTER seconds
+ *    from src to dst.  A band driver refreshes the halo of src before every
+ *    sub-step, as PROPAGS exchanges it before each one (propagation:
+ *    704-709).  The multi-sub-step entry points above do not exchange. */
+WAMGPU_API int wamgpu_set_owned(wamgpu_ctx* ctx, int i0, int i1);
+WAMGPU_API int wamgpu_set_counter(wamgpu_ctx* ctx, int counter);
+WAMGPU_API int wamgpu_propags_substep_dev(wamgpu_ctx* ctx, const void* src, void* dst, int ld, void* stream);
+
 /* Batched ensembles.  No single counterpart in the reference, where each
  * member is a separate WAMODEL run calling PROPAGS (propagation:635-829) and
  * IMPLSCH (source:374-700).  A batch advances many prepared member contexts

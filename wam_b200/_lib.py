@@ -47,6 +47,9 @@ SIGNATURES = {
     "wamgpu_sync": (c_int, [c_void_p]),
     "wamgpu_set_timing": (c_int, [c_void_p, c_int]),
     "wamgpu_get_timing": (c_int, [c_void_p, PF, PI]),
+    "wamgpu_set_owned": (c_int, [c_void_p, c_int, c_int]),
+    "wamgpu_set_counter": (c_int, [c_void_p, c_int]),
+    "wamgpu_propags_substep_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "wamgpu_batch_create": (c_int, [ctypes.POINTER(c_void_p), c_int, ctypes.POINTER(c_void_p)]),
     "wamgpu_batch_destroy": (c_int, [c_void_p]),
     "wamgpu_batch_last_error": (c_char_p, [c_void_p]),

@@ -58,6 +58,7 @@ struct wamgpu_ctx {
   int P = 8;  // sea points per IMPLSCH CTA
   // grid (reference convention, host)
   int nsea = 0, ny = 0, n_ext = 0;
+  int own0 = 0, own1 = -1;  // sea points this context updates ([own0, own1); own1 < 0: all), the rest are halo
   std::vector<int> klat, klon, kfromij;
   std::vector<float> wlat, sinph, cosph, dellam;
   std::vector<float> depth, u, v;
@@ -343,6 +344,7 @@ template <typename R> int prepare_prop(wamgpu_ctx* ctx, Impl<R>& I, float* total
   PropArgs<R>& A = I.pa;
   A.nsea = n; A.KL = KL; A.ML = ML; A.variant = var; A.reduced = c.reduced_grid; A.refr_d = c.refraction_d_run;
   A.spherical = c.spherical_run; A.counter = 1; A.rcounter = R(1); A.NDEPTH = ND;
+  A.i0 = ctx->own0; A.i1 = ctx->own1 < 0 ? n : ctx->own1;
   A.DELPH0 = (var == V_CART_DEEP) ? delpro / delphi : R(0.5) * delpro / delphi;
   A.DELTH0 = R(0.5) * delpro / t.DELTR;
   A.DELTHR = R(0.5) * delpro / t.DELTH;
@@ -398,6 +400,8 @@ template <typename R> int prepare_prop(wamgpu_ctx* ctx, Impl<R>& I, float* total
   R sg2max = cur ? mx(CFL_SG2) : R(0.1), sg2min = cur ? mn(CFL_SG2) : R(0.1);
   R summax = R(1.) - mn(CFL_SUM), summin = R(1.) - mx(CFL_SUM);
   R cmax = std::max({lat11max, lat12max, lon11max, lon12max, th1max, th2max, sg1max, sg2max, summax});
+  // the minimum follows CHECK_CFL's own expression (propagation:2013-2016),
+  // which lists COEF_LON_1_2_MIN twice and not COEF_LON_1_1_MIN
   R cmin = std::min({lat11min, lat12min, lon12min, lon12min, th1min, th2min, sg1min, sg2min, summin});
   ctx->cfl_min = cmin;
   if (cmin < R(0.)) {
@@ -461,14 +465,17 @@ int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u1
     return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_source first (ISNONLIN table)");
   if (!I.status.p) { CK(I.status.ensure(16), "alloc"); CK(cudaMemsetAsync(I.status.p, 0, 16, s), "memset"); }
   if (ctx->cfg.lcflx) CK(I.fluxes.ensure((size_t)7 * ctx->nsea * sizeof(R) + 16), "alloc");
+  // the owned sea points only (all of them unless wamgpu_set_owned narrowed the range)
+  const int p0 = ctx->own0, p1 = ctx->own1 < 0 ? ctx->nsea : ctx->own1;
   ImplArgs<R> a;
-  a.nsea = ctx->nsea; a.ld = ld;
-  a.fl3 = (R*)fl3; a.fl3_in = fl3_in ? (const R*)fl3_in : (const R*)fl3; a.u10 = (const R*)u10; a.udir = (const R*)udir; a.roairn = (const R*)roairn; a.wstar = (const R*)wstar;
-  a.depth = I.d_depth.template as<R>(); a.indep = I.d_indep.template as<int>();
-  a.tauw = (R*)tauw; a.ustar = (R*)ustar; a.z0 = (R*)z0;
-  a.fluxes = ctx->cfg.lcflx ? I.fluxes.template as<R>() : nullptr;
+  a.nsea = p1 - p0; a.ld = ld;
+  a.fl3 = (R*)fl3 + p0; a.fl3_in = (fl3_in ? (const R*)fl3_in : (const R*)fl3) + p0;
+  a.u10 = (const R*)u10 + p0; a.udir = (const R*)udir + p0; a.roairn = (const R*)roairn + p0; a.wstar = (const R*)wstar + p0;
+  a.depth = I.d_depth.template as<R>() + p0; a.indep = I.d_indep.template as<int>() + p0;
+  a.tauw = (R*)tauw + p0; a.ustar = (R*)ustar + p0; a.z0 = (R*)z0 + p0;
+  a.fluxes = ctx->cfg.lcflx ? I.fluxes.template as<R>() + p0 : nullptr;
   a.flx_ld = ctx->nsea;
-  a.enh = I.has_enh ? I.enh.template as<R>() : nullptr; a.enh_ld = ctx->nsea;
+  a.enh = I.has_enh ? I.enh.template as<R>() + p0 : nullptr; a.enh_ld = ctx->nsea;
   a.status = I.status.template as<int>();
   { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch"); }
   return WAMGPU_OK;
@@ -521,6 +528,26 @@ int static_scratch(wamgpu_ctx* ctx, void** out) {
 // PROPAGS with the F1 ping-pong spectrum in the fixed device array: no
 // allocation, no clearing (each scratch element read was written earlier in
 // the call), sizes above the array rejected before anything is queued.
+// One PROPAGS sub-step (IDELPRO/COUNTER seconds) from src to dst over the
+// owned sea points; halo points of dst are left as they were.
+template <typename R> int propags_substep_t(wamgpu_ctx* ctx, Impl<R>& I, const void* src, void* dst, int ld, cudaStream_t s) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  if (src == dst) return fail(ctx, WAMGPU_E_ARG, "a sub-step needs distinct source and destination spectra");
+  { TimedLaunch tl(ctx, 0, s); CK(launch_propags<R>(I.pa, (const R*)src, ld, (R*)dst, ld, s), "propags launch"); }
+  return WAMGPU_OK;
+}
+
+template <typename R> int set_counter_t(wamgpu_ctx* ctx, Impl<R>& I, int counter) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
+  if (counter < ctx->counter)
+    return fail(ctx, WAMGPU_E_ARG, "COUNTER below this grid's own CHECK_CFL value (" + std::to_string(ctx->counter) + ")");
+  ctx->total_cfl = ctx->total_cfl * ctx->counter / counter;
+  ctx->counter = counter;
+  I.pa.counter = counter; I.pa.rcounter = R(counter);
+  return WAMGPU_OK;
+}
+
 template <typename R> int propags_dev_static_t(wamgpu_ctx* ctx, Impl<R>& I, void* f3v, int ld, cudaStream_t s) {
   if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
   if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
@@ -919,7 +946,7 @@ template <typename R> int batch_build(wamgpu_batch* b, cudaStream_t s) {
         M.src = (it % 2 == 0) ? f3 : sc;
         M.dst = (it % 2 == 0) ? sc : f3;
         M.ld = b->st[g].ld;
-        M.nbi = (c->nsea + b->bs - 1) / b->bs;
+        M.nbi = (A.i1 - A.i0 + b->bs - 1) / b->bs;
         mem.push_back(M);
         first.push_back(first.back() + c->cfg.ml * M.nbi);
       }
@@ -1151,6 +1178,7 @@ int wamgpu_set_grid(wamgpu_ctx* ctx, int nsea, const int* klat, const int* klon,
   ctx->sinph.assign(sinph, sinph + ny); ctx->cosph.assign(cosph, cosph + ny); ctx->dellam.assign(dellam, dellam + ny);
   ctx->depth.assign(nsea, 999.0f); ctx->u.assign(nsea, 0.f); ctx->v.assign(nsea, 0.f);
   ctx->have_grid = true; ctx->prepared = false;
+  ctx->own0 = 0; ctx->own1 = -1;
   cudaSetDevice(ctx->cfg.device);
   return DISPATCH_CTX(ctx, set_grid_t);
 }
@@ -1400,6 +1428,28 @@ int wamgpu_batch_sync(wamgpu_batch* b) {
     if (rc) return bfail(b, rc, "member " + std::to_string(g) + ": " + b->members[g]->err);
   }
   return WAMGPU_OK;
+}
+
+// ---- latitude bands (one grid over several ranks) ------------------------------
+
+int wamgpu_set_owned(wamgpu_ctx* ctx, int i0, int i1) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!ctx->have_grid) return fail(ctx, WAMGPU_E_STATE, "set_grid first");
+  if (i0 < 0 || i1 < i0 || i1 > ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "owned range outside the grid");
+  ctx->own0 = i0; ctx->own1 = i1;
+  ctx->prepared = false;
+  return WAMGPU_OK;
+}
+
+int wamgpu_set_counter(wamgpu_ctx* ctx, int counter) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  return DISPATCH_CTX(ctx, set_counter_t, counter);
+}
+
+int wamgpu_propags_substep_dev(wamgpu_ctx* ctx, const void* src, void* dst, int ld, void* stream) {
+  if (!ctx || !ctx->impl || !src || !dst) return WAMGPU_E_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, propags_substep_t, src, dst, ld, s);
 }
 
 }  // extern "C"

@@ -45,8 +45,8 @@ __device__ __forceinline__ void propags_point(const PropArgs<R>& A, const R* __r
 template <typename R, int VAR, bool RED, bool REFRD>
 __global__ void __launch_bounds__(128) propags_kernel(const __grid_constant__ PropArgs<R> A, const R* __restrict__ f1,
                                                       int ld1, R* __restrict__ f3, int ld3, int m0) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= A.nsea) return;
+  const int i = A.i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.i1) return;
   propags_point<R, VAR, RED, REFRD>(A, f1, ld1, f3, ld3, i, m0 + blockIdx.y);
 }
 
@@ -75,8 +75,8 @@ __global__ void __launch_bounds__(BS) propags_batch_kernel(const PropMember<R>* 
   }
   __syncthreads();
   const int lb = (int)blockIdx.x - first[g], m = lb / sm.nbi, ib = lb - m * sm.nbi;
-  const int i = ib * BS + threadIdx.x;
-  if (i >= sm.A.nsea) return;
+  const int i = sm.A.i0 + ib * BS + threadIdx.x;
+  if (i >= sm.A.i1) return;
   propags_point<R, VAR, RED, REFRD>(sm.A, sm.src, sm.ld, sm.dst, sm.ld, i, m);
 }
 
@@ -87,11 +87,12 @@ __device__ __forceinline__ long long d2o(double d) { long long i = __double_as_l
 // ext[2*c] = max, ext[2*c+1] = min of coefficient class c (CflClass)
 template <typename R, int VAR, bool RED, bool REFRD>
 __global__ void __launch_bounds__(256) cfl_extrema_kernel(const __grid_constant__ PropArgs<R> A, long long* ext) {
-  const size_t n = (size_t)A.nsea * A.ML;
+  const int nown = A.i1 - A.i0;
+  const size_t n = (size_t)nown * A.ML;
   R mx[CFL_NCLASS], mn[CFL_NCLASS];
   for (int c = 0; c < CFL_NCLASS; ++c) { mx[c] = R(-1e30); mn[c] = R(1e30); }
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
-    const int i = (int)(t % A.nsea), m = (int)(t / A.nsea);
+    const int i = A.i0 + (int)(t % nown), m = (int)(t / nown);
     const Site<R, VAR, RED, REFRD> site(A, i, m);
     for (int k = 0; k < A.KL; ++k) {
       Coefs<R> c = site.coef(k);
@@ -139,7 +140,7 @@ cudaError_t dispatch(const PropArgs<R>& A, Args&&... args) {
 
 template <typename R, int V, bool RED, bool RD> struct PropLaunch {
   static cudaError_t run(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, int m0, int mcount, cudaStream_t s) {
-    dim3 grid((A.nsea + 127) / 128, mcount);
+    dim3 grid((A.i1 - A.i0 + 127) / 128, mcount);
     propags_kernel<R, V, RED, RD><<<grid, 128, 0, s>>>(A, f1, ld1, f3, ld3, m0);
     return cudaGetLastError();
   }
@@ -172,7 +173,7 @@ template <typename R>
 cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s, int m0, int mcount) {
   if (mcount < 0) mcount = A.ML - m0;
   if (m0 < 0 || mcount < 0 || m0 + mcount > A.ML) return cudaErrorInvalidValue;
-  if (A.nsea == 0 || mcount == 0) return cudaSuccess;
+  if (A.i1 <= A.i0 || mcount == 0) return cudaSuccess;
   return dispatch<R, PropLaunch>(A, f1, ld1, f3, ld3, m0, mcount, s);
 }
 
@@ -184,8 +185,8 @@ bool propags_planes_independent(int variant) {
 template <typename R>
 cudaError_t launch_cfl_extrema(const PropArgs<R>& A, long long* ext, int nsm, cudaStream_t s) {
   cfl_init_kernel<<<1, 32, 0, s>>>(ext);
-  if (A.nsea == 0) return cudaGetLastError();
-  size_t n = (size_t)A.nsea * A.ML;
+  if (A.i1 <= A.i0) return cudaGetLastError();
+  size_t n = (size_t)(A.i1 - A.i0) * A.ML;
   int blocks = (int)std::min<size_t>((n + 255) / 256, (size_t)nsm * 8);
   if (blocks < 1) blocks = 1;
   return dispatch<R, CflLaunch>(A, ext, blocks, s);

@@ -15,6 +15,7 @@ enum PropVariant : int {
 // followed by halo points) unless noted.
 template <typename R> struct PropArgs {
   int nsea, ld, KL, ML, variant, reduced, refr_d, spherical, counter, NDEPTH;
+  int i0, i1;         // sea points the kernels update (0-based, [i0, i1)); the rest are halo points
   R DELPH0, DELTH0, DELTHR, DELFR0, rcounter;
   const int* klat;    // [i + nsea*(ic + 2*j)]   (nsea entries per slot)
   const int* klon;    // [i + nsea*dir]

@@ -213,6 +213,22 @@ class WamModel:
                                            tauw.data_ptr(), ustar.data_ptr(), z0.data_ptr(), roairn.data_ptr(),
                                            wstar.data_ptr(), s), "step_dev")
 
+    # ---- latitude bands (one grid over several ranks) -----------------------
+    def set_owned(self, i0, i1):
+        """Only sea points i0..i1-1 are updated; the others are halo points."""
+        self._check(self.L.wamgpu_set_owned(self.h, int(i0), int(i1)), "set_owned")
+
+    def set_counter(self, counter):
+        """Install the COUNTER agreed over all ranks (not below this grid's own)."""
+        self._check(self.L.wamgpu_set_counter(self.h, int(counter)), "set_counter")
+        self.counter = int(counter)
+
+    def propags_substep_dev(self, src, dst, ld=None, stream=None):
+        """One PROPAGS sub-step src -> dst (device tensors shaped (ML, KL, ld))."""
+        ld = src.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        self._check(self.L.wamgpu_propags_substep_dev(self.h, src.data_ptr(), dst.data_ptr(), ld, s), "propags_substep")
+
     def set_timing(self, enable=True):
         self._check(self.L.wamgpu_set_timing(self.h, int(enable)), "set_timing")
 
