@@ -240,6 +240,39 @@ WAMGPU_API int wamgpu_batch_step(wamgpu_batch* b, void* stream);
 WAMGPU_API int wamgpu_batch_capture(wamgpu_batch* b, void* stream);
 WAMGPU_API int wamgpu_batch_sync(wamgpu_batch* b);
 
+/* Derivatives of one WAMODEL pass.  The reference has no tangent-linear or
+ * adjoint code; these differentiate its forward procedures as they stand, and
+ * are checked against central finite differences of the forward path and
+ * against each other (<TL dx, ly> = <dx, ADJ ly>).
+ *  - wamgpu_implsch_tl_dev: IMPLSCH (source:374-700) for ST4 (IPHYS=1) and
+ *    its tangent-linear in one pass.  Inputs FL3 (fl3_in), TAUW and U10 with
+ *    their perturbations dfl3_in, dtauw_in, du10; outputs the new spectrum
+ *    and TAUW with their perturbations.  UDIR, ROAIRN, WSTAR and the depth
+ *    are held fixed.  The branch decisions of the forward pass (MAX/MIN
+ *    selections, the high-frequency tail mask, the limiter) are frozen at
+ *    the base state, as a tangent-linear model takes them.
+ *  - wamgpu_implsch_adj_dev: the adjoint of the same map.  It recomputes the
+ *    forward pass from its inputs (the checkpoint: FL3, TAUW, U10 before
+ *    IMPLSCH) and maps lam_fl3 (in: adjoint of the new FL3, out: adjoint of
+ *    the old one), lam_tauw (in/out likewise) and lam_u10 (out, overwritten)
+ *    in place.
+ *  - wamgpu_propags_adj_dev: the transpose of PROPAGS (propagation:635-829),
+ *    which is linear in FL3: the COUNTER sub-steps in reverse order, each a
+ *    scatter of lam back to the points and bins it was gathered from.
+ *    scratch (ld x KL x ML values, NULL = a context-owned buffer) holds the
+ *    alternate sub-step; lam_f3 is updated in place.
+ * All three cover the whole grid of a context (no owned range), need
+ * wamgpu_prepare_propagation (and wamgpu_prepare_source with ISNONLIN != 0
+ * in shallow water), and work in the context's precision. */
+WAMGPU_API int wamgpu_implsch_tl_dev(wamgpu_ctx* ctx, const void* fl3_in, const void* dfl3_in, int ld,
+                                     const void* tauw_in, const void* dtauw_in, const void* u10, const void* du10,
+                                     const void* udir, const void* roairn, const void* wstar, void* fl3_out,
+                                     void* dfl3_out, void* tauw_out, void* dtauw_out, void* stream);
+WAMGPU_API int wamgpu_implsch_adj_dev(wamgpu_ctx* ctx, const void* fl3_in, int ld, const void* tauw_in,
+                                      const void* u10, const void* udir, const void* roairn, const void* wstar,
+                                      void* lam_fl3, void* lam_tauw, void* lam_u10, void* stream);
+WAMGPU_API int wamgpu_propags_adj_dev(wamgpu_ctx* ctx, void* lam_f3, int ld, void* scratch, void* stream);
+
 /* Synchronises the context stream; returns WAMGPU_E_NUMERIC if a kernel
  * reported non-finite output since the last call. */
 WAMGPU_API int wamgpu_sync(wamgpu_ctx* ctx);

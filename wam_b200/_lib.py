@@ -49,6 +49,9 @@ SIGNATURES = {
     "wamgpu_get_timing": (c_int, [c_void_p, PF, PI]),
     "wamgpu_set_owned": (c_int, [c_void_p, c_int, c_int]),
     "wamgpu_set_counter": (c_int, [c_void_p, c_int]),
+    "wamgpu_implsch_adj_dev": (c_int, [c_void_p] + [c_void_p, c_int] + [c_void_p] * 9),
+    "wamgpu_implsch_tl_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_int] + [c_void_p] * 12),
+    "wamgpu_propags_adj_dev": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "wamgpu_propags_substep_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "wamgpu_batch_create": (c_int, [ctypes.POINTER(c_void_p), c_int, ctypes.POINTER(c_void_p)]),
     "wamgpu_batch_destroy": (c_int, [c_void_p]),

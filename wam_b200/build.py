@@ -22,8 +22,9 @@ UNITS = {
     "implsch.cu": [],
     "propags.cu": ["-fmad=false"],
     "api.cu": [],
+    "adjoint.cu": [],
 }
-HEADERS = ["implsch.cuh", "propags.cuh", "propargs.hpp", "devmath.cuh", "kernels.hpp", "spectral_tables.hpp", "wamgpu_config.hpp"]
+HEADERS = ["implsch.cuh", "propags.cuh", "propargs.hpp", "devmath.cuh", "kernels.hpp", "adjoint.cuh", "spectral_tables.hpp", "wamgpu_config.hpp"]
 
 
 def _nvcc():

@@ -81,6 +81,7 @@ template <typename R> struct Impl : ImplBase {
   DevTables<R> dt{};
   PropArgs<R> pa{};
   bool has_enh = false;  // MAKE_SHALLOW_SNL factors uploaded to `enh` ([ij + nsea*(mc-1)])
+  DevBuf dwork, dmasks;  // work of the derivative kernels
   DevBuf small, ismall, tfak, tcgond, tsihkd, flminfr, enh, gom, fr, sinth, costh;
   // per-point metadata
   DevBuf d_klat, d_klon, d_wlat, d_dpsn, d_della0, d_drgm, d_indep, d_indep_g, d_ddphi, d_ddlam, d_duphi, d_dulam,
@@ -545,6 +546,96 @@ template <typename R> int set_counter_t(wamgpu_ctx* ctx, Impl<R>& I, int counter
   ctx->total_cfl = ctx->total_cfl * ctx->counter / counter;
   ctx->counter = counter;
   I.pa.counter = counter; I.pa.rcounter = R(counter);
+  return WAMGPU_OK;
+}
+
+// ---- derivatives (ST4): tangent-linear and adjoint ----------------------------
+
+// The source tables as the point-per-thread derivative code sees them.
+template <typename R> adj::ATabs<R> atabs_of(const DevTables<R>& d) {
+  adj::ATabs<R> A;
+  const SmallLayout& L = d.lay;
+  A.KL = d.KL; A.ML = d.ML; A.NDEPTH = d.NDEPTH; A.MFRSTLW = d.MFRSTLW; A.MLSTHG = d.MLSTHG; A.KFRH = d.KFRH;
+  A.NSDSNTH = d.NSDSNTH; A.shallow = d.shallow; A.isnonlin = d.isnonlin;
+  A.DELTH = d.DELTH; A.INV_LOG_CO = d.INV_LOG_CO; A.MO_TAIL = d.MO_TAIL; A.MM1_TAIL = d.MM1_TAIL; A.DELU = d.DELU;
+  A.DAL1 = d.DAL1; A.DAL2 = d.DAL2; A.X0TAUHF = d.X0TAUHF; A.BETAMAX = d.BETAMAX; A.ZALP = d.ZALP; A.ALPHA = d.ALPHA;
+  A.TAUWSHELTER = d.TAUWSHELTER; A.DELT = d.DELT;
+  const R* r = d.small;
+  A.FR = r + L.FR; A.DFIM = r + L.DFIM; A.DFIMOFR = r + L.DFIMOFR; A.FR5 = r + L.FR5; A.FRM5 = r + L.FRM5;
+  A.RHOWG = r + L.RHOWG_DFIM; A.TH = r + L.TH; A.COSTH = r + L.COSTH; A.SINTH = r + L.SINTH; A.DELFL = r + L.DELFL;
+  A.AF11 = r + L.AF11; A.RNL = r + L.RNLCOEF; A.SATW = r + L.SATW; A.WTAUHF = r + L.WTAUHF; A.SWELLFT = r + L.SWELLFT;
+  A.TFAK = d.TFAK; A.TCGOND = d.TCGOND; A.FLMINFR = d.FLMINFR;
+  const int* q = d.ismall;
+  A.K1W = q + L.K1W; A.K2W = q + L.K2W; A.K11W = q + L.K11W; A.K21W = q + L.K21W; A.INL = q + L.INLCOEF;
+  A.IKP = q + L.IKP; A.IKP1 = q + L.IKP1; A.IKM = q + L.IKM; A.IKM1 = q + L.IKM1; A.INDSAT = q + L.INDSAT;
+  return A;
+}
+
+template <typename R>
+int deriv_setup(wamgpu_ctx* ctx, Impl<R>& I, int ld, bool tl, DerivArgs<R>& a) {
+  if (ctx->cfg.iphys != 1) return fail(ctx, WAMGPU_E_ARG, "IMPLSCH derivatives are implemented for ST4 (IPHYS=1)");
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first (INDEP)");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  if (ctx->own0 != 0 || (ctx->own1 >= 0 && ctx->own1 != ctx->nsea))
+    return fail(ctx, WAMGPU_E_ARG, "derivatives cover the whole grid of a context (no owned range)");
+  if (ctx->cfg.shallow_run && ctx->cfg.isnonlin != 0 && !I.has_enh)
+    return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_source first (ISNONLIN table)");
+  const size_t n = (size_t)ctx->nsea;
+  CK(I.dwork.ensure(n * deriv_work_bytes<R>(ctx->cfg.kl, ctx->cfg.ml, tl) + 256), "alloc derivative work");
+  CK(I.dmasks.ensure(n * 2 * ctx->cfg.kl * ctx->cfg.ml + 256), "alloc derivative work");
+  std::memset(&a, 0, sizeof(a));
+  a.A = atabs_of(I.dt);
+  a.nsea = ctx->nsea; a.ld = ld;
+  a.depth = I.d_depth.template as<R>(); a.indep = I.d_indep.template as<int>();
+  a.enh = I.has_enh ? I.enh.template as<R>() : nullptr; a.enh_ld = ctx->nsea;
+  a.work = I.dwork.p; a.masks = I.dmasks.template as<uint8_t>();
+  return WAMGPU_OK;
+}
+
+template <typename R>
+int implsch_adj_t(wamgpu_ctx* ctx, Impl<R>& I, const void* fl3_in, int ld, const void* tauw_in, const void* u10,
+                  const void* udir, const void* roairn, const void* wstar, void* lam_fl3, void* lam_tauw, void* lam_u10,
+                  cudaStream_t s) {
+  DerivArgs<R> a;
+  int rc = deriv_setup<R>(ctx, I, ld, false, a);
+  if (rc) return rc;
+  a.fl3_in = (const R*)fl3_in; a.tauw_in = (const R*)tauw_in; a.u10 = (const R*)u10; a.udir = (const R*)udir;
+  a.roairn = (const R*)roairn; a.wstar = (const R*)wstar;
+  a.lam_fl3 = (R*)lam_fl3; a.lam_tauw = (R*)lam_tauw; a.lam_u10 = (R*)lam_u10;
+  { TimedLaunch tl(ctx, 1, s); CK(launch_implsch_adj<R>(a, s), "implsch adjoint launch"); }
+  return WAMGPU_OK;
+}
+
+template <typename R>
+int implsch_tl_t(wamgpu_ctx* ctx, Impl<R>& I, const void* fl3_in, const void* dfl3_in, int ld, const void* tauw_in,
+                 const void* dtauw_in, const void* u10, const void* du10, const void* udir, const void* roairn,
+                 const void* wstar, void* fl3_out, void* dfl3_out, void* tauw_out, void* dtauw_out, cudaStream_t s) {
+  DerivArgs<R> a;
+  int rc = deriv_setup<R>(ctx, I, ld, true, a);
+  if (rc) return rc;
+  a.fl3_in = (const R*)fl3_in; a.dfl3_in = (const R*)dfl3_in; a.tauw_in = (const R*)tauw_in;
+  a.dtauw_in = (const R*)dtauw_in; a.u10 = (const R*)u10; a.du10 = (const R*)du10; a.udir = (const R*)udir;
+  a.roairn = (const R*)roairn; a.wstar = (const R*)wstar;
+  a.fl3_out = (R*)fl3_out; a.dfl3_out = (R*)dfl3_out; a.tauw_out = (R*)tauw_out; a.dtauw_out = (R*)dtauw_out;
+  CK(launch_implsch_tl<R>(a, s), "implsch tangent-linear launch");
+  return WAMGPU_OK;
+}
+
+// Transpose of PROPAGS: the COUNTER sub-steps in reverse order, ping-pong
+// between lam and scratch (zeroed before each sub-step).
+template <typename R> int propags_adj_t(wamgpu_ctx* ctx, Impl<R>& I, void* lam, int ld, void* scratch, cudaStream_t s) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  const size_t bytes = (size_t)ld * ctx->cfg.kl * ctx->cfg.ml * sizeof(R);
+  R* sc = (R*)scratch;
+  if (!sc) { CK(I.scratch.ensure(bytes), "alloc scratch"); sc = I.scratch.template as<R>(); }
+  R* src = (R*)lam; R* dst = sc;
+  for (int it = 0; it < ctx->counter; ++it) {
+    CK(cudaMemsetAsync(dst, 0, bytes, s), "zero adjoint");
+    { TimedLaunch tl(ctx, 0, s); CK(launch_propags_adj<R>(I.pa, src, ld, dst, ld, s), "propags adjoint launch"); }
+    std::swap(src, dst);
+  }
+  if (src != (R*)lam) CK(cudaMemcpyAsync(lam, src, bytes, cudaMemcpyDeviceToDevice, s), "copy adjoint");
   return WAMGPU_OK;
 }
 
@@ -1450,6 +1541,37 @@ int wamgpu_propags_substep_dev(wamgpu_ctx* ctx, const void* src, void* dst, int 
   if (!ctx || !ctx->impl || !src || !dst) return WAMGPU_E_ARG;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   return DISPATCH_CTX(ctx, propags_substep_t, src, dst, ld, s);
+}
+
+// ---- derivatives --------------------------------------------------------------
+
+int wamgpu_implsch_adj_dev(wamgpu_ctx* ctx, const void* fl3_in, int ld, const void* tauw_in, const void* u10,
+                           const void* udir, const void* roairn, const void* wstar, void* lam_fl3, void* lam_tauw,
+                           void* lam_u10, void* stream) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!fl3_in || !tauw_in || !u10 || !udir || !roairn || !wstar || !lam_fl3 || !lam_tauw || !lam_u10)
+    return fail(ctx, WAMGPU_E_ARG, "null argument");
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, implsch_adj_t, fl3_in, ld, tauw_in, u10, udir, roairn, wstar, lam_fl3, lam_tauw, lam_u10, s);
+}
+
+int wamgpu_implsch_tl_dev(wamgpu_ctx* ctx, const void* fl3_in, const void* dfl3_in, int ld, const void* tauw_in,
+                          const void* dtauw_in, const void* u10, const void* du10, const void* udir, const void* roairn,
+                          const void* wstar, void* fl3_out, void* dfl3_out, void* tauw_out, void* dtauw_out,
+                          void* stream) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!fl3_in || !dfl3_in || !tauw_in || !dtauw_in || !u10 || !du10 || !udir || !roairn || !wstar || !fl3_out ||
+      !dfl3_out || !tauw_out || !dtauw_out)
+    return fail(ctx, WAMGPU_E_ARG, "null argument");
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, implsch_tl_t, fl3_in, dfl3_in, ld, tauw_in, dtauw_in, u10, du10, udir, roairn, wstar, fl3_out,
+                      dfl3_out, tauw_out, dtauw_out, s);
+}
+
+int wamgpu_propags_adj_dev(wamgpu_ctx* ctx, void* lam_f3, int ld, void* scratch, void* stream) {
+  if (!ctx || !ctx->impl || !lam_f3) return WAMGPU_E_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, propags_adj_t, lam_f3, ld, scratch, s);
 }
 
 }  // extern "C"

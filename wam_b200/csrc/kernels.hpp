@@ -5,6 +5,8 @@
 #include <cstring>
 #include <algorithm>
 #include "wamgpu_config.hpp"
+#include "propargs.hpp"
+#include "adjoint.cuh"
 
 namespace wamgpu {
 
@@ -62,5 +64,31 @@ cudaError_t launch_propags_batch(const PropArgs<R>& family, const PropMember<R>*
 template <typename R> cudaError_t launch_cfl_extrema(const PropArgs<R>& A, long long* ext, int nsm, cudaStream_t s);
 double cfl_decode(long long v, int precision);
 cudaError_t static_scratch_address(void** p);
+
+// Arguments of the IMPLSCH tangent-linear and adjoint kernels (ST4, one sea
+// point per thread).  work: deriv_work_bytes per point, masks: 2*KL*ML bytes
+// per point, both laid out with the sea point fastest.
+template <typename R> struct DerivArgs {
+  adj::ATabs<R> A;
+  int nsea, ld;
+  const R *fl3_in, *tauw_in, *u10, *udir, *roairn, *wstar, *depth;
+  const int* indep;
+  const R* enh;
+  int enh_ld;
+  void* work;
+  uint8_t* masks;
+  // adjoint: in = adjoints of the outputs, out = adjoints of the inputs
+  R *lam_fl3, *lam_tauw, *lam_u10;
+  // tangent-linear
+  const R *dfl3_in, *dtauw_in, *du10;
+  R *fl3_out, *dfl3_out, *tauw_out, *dtauw_out, *ustar_out, *z0_out;
+};
+template <typename R> size_t deriv_work_bytes(int KL, int ML, bool tl);
+template <typename R> cudaError_t launch_implsch_adj(const DerivArgs<R>& a, cudaStream_t s);
+template <typename R> cudaError_t launch_implsch_tl(const DerivArgs<R>& a, cudaStream_t s);
+// Transpose of one PROPAGS sub-step: lam_old (zeroed by the caller) +=
+// P^T lam_new, by atomic adds into the neighbours' bins.
+template <typename R>
+cudaError_t launch_propags_adj(const PropArgs<R>& A, const R* lam_new, int ld1, R* lam_old, int ld3, cudaStream_t s);
 
 }  // namespace wamgpu

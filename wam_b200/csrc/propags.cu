@@ -80,6 +80,59 @@ __global__ void __launch_bounds__(BS) propags_batch_kernel(const PropMember<R>* 
   propags_point<R, VAR, RED, REFRD>(sm.A, sm.src, sm.ld, sm.dst, sm.ld, i, m);
 }
 
+// Transpose of one sub-step, thread per (sea point i, frequency m): every
+// term c * F_old(source) of the forward stencil becomes lam_old(source) +=
+// c * lam_new(i, k, m).  The own point's direction neighbours (refraction)
+// and the point itself are summed in registers first; spatial and frequency
+// neighbours take atomic adds (lam_old zeroed by the caller).
+template <typename R, int VAR, bool RED, bool REFRD>
+__global__ void __launch_bounds__(128) propags_adj_kernel(const __grid_constant__ PropArgs<R> A,
+                                                          const R* __restrict__ lnew, int ld1, R* lold, int ld3) {
+  const int i = A.i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.i1) return;
+  const int m = blockIdx.y;
+  using S = Site<R, VAR, RED, REFRD>;
+  const S site(A, i, m);
+  const int KL = A.KL, ML = A.ML;
+  const size_t plane = (size_t)ld3 * KL;
+  const R* lm = lnew + (size_t)ld1 * KL * m;
+  R* om = lold + plane * m;
+  auto add = [&](int p1, int k, R v) { if (p1 != 0) atomicAdd(&om[(p1 - 1) + (size_t)ld3 * k], v); };
+  const bool theta = REFRD || S::SPH;
+  typename S::Win W = site.window(0);
+  R carry0 = 0, first_th2 = 0, prev_own = 0;  // own-point sums waiting for the next direction
+  for (int k = 0; k < KL; ++k) {
+    const Coefs<R> c = site.coef_w(W);
+    const R l = lm[i + (size_t)ld1 * k];
+    R own = c.sum * l + carry0;  // + th1 of direction k-1 (carried)
+    carry0 = 0;
+    if (!S::CUR) {
+      const bool ic0 = W.cs >= R(0.), is0 = W.sn >= R(0.);
+      add(ic0 ? site.s0 : site.n0, k, c.lat11 * l);
+      add(is0 ? site.w0 : site.e0, k, c.lon1 * l);
+      if (RED) add(ic0 ? site.s1 : site.n1, k, c.lat12 * l);
+    } else {
+      add(site.n0, k, c.lat21 * l); add(site.s0, k, c.lat11 * l); add(site.e0, k, c.lon2 * l); add(site.w0, k, c.lon1 * l);
+      if (RED) { add(site.n1, k, c.lat22 * l); add(site.s1, k, c.lat12 * l); }
+      const int mm = (m == 0) ? 0 : m - 1, mp = (m == ML - 1) ? ML - 1 : m + 1;
+      atomicAdd(&lold[i + (size_t)ld3 * k + plane * mp], c.sg1 * l);
+      atomicAdd(&lold[i + (size_t)ld3 * k + plane * mm], c.sg2 * l);
+    }
+    if (theta || S::CUR) {
+      // F_new(k) reads F_old(k+1) with th1 and F_old(k-1) with th2
+      carry0 = c.th1 * l;                 // -> direction k+1
+      if (k == 0) first_th2 = c.th2 * l;  // -> direction KL-1, added at the end
+      else prev_own = prev_own + c.th2 * l;
+    }
+    if (k > 0) atomicAdd(&om[i + (size_t)ld3 * (k - 1)], prev_own);
+    prev_own = own;
+    site.advance(W, k);
+  }
+  // direction KL-1 gets its own sum and th2 of direction 0; direction 0 gets th1 of KL-1
+  atomicAdd(&om[i + (size_t)ld3 * (KL - 1)], prev_own + first_th2);
+  if (theta || S::CUR) atomicAdd(&om[i], carry0);
+}
+
 // Order-preserving float <-> int mapping for atomic max/min of extrema.
 __device__ __forceinline__ int f2o(float f) { int i = __float_as_int(f); return i >= 0 ? i : i ^ 0x7fffffff; }
 __device__ __forceinline__ long long d2o(double d) { long long i = __double_as_longlong(d); return i >= 0 ? i : i ^ 0x7fffffffffffffffLL; }
@@ -169,6 +222,20 @@ cudaError_t launch_propags_batch(const PropArgs<R>& family, const PropMember<R>*
   return dispatch<R, PropBatchLaunch>(family, mem, first, nmem, nblocks, bs, s);
 }
 
+template <typename R, int V, bool RED, bool RD> struct PropAdjLaunch {
+  static cudaError_t run(const PropArgs<R>& A, const R* ln, int ld1, R* lo, int ld3, cudaStream_t s) {
+    dim3 grid((A.i1 - A.i0 + 127) / 128, A.ML);
+    propags_adj_kernel<R, V, RED, RD><<<grid, 128, 0, s>>>(A, ln, ld1, lo, ld3);
+    return cudaGetLastError();
+  }
+};
+
+template <typename R>
+cudaError_t launch_propags_adj(const PropArgs<R>& A, const R* lam_new, int ld1, R* lam_old, int ld3, cudaStream_t s) {
+  if (A.i1 <= A.i0) return cudaSuccess;
+  return dispatch<R, PropAdjLaunch>(A, lam_new, ld1, lam_old, ld3, s);
+}
+
 template <typename R>
 cudaError_t launch_propags(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, cudaStream_t s, int m0, int mcount) {
   if (mcount < 0) mcount = A.ML - m0;
@@ -215,6 +282,8 @@ template cudaError_t launch_propags_batch<float>(const PropArgs<float>&, const P
                                                  int, cudaStream_t);
 template cudaError_t launch_propags_batch<double>(const PropArgs<double>&, const PropMember<double>*, const int*, int,
                                                   int, int, cudaStream_t);
+template cudaError_t launch_propags_adj<float>(const PropArgs<float>&, const float*, int, float*, int, cudaStream_t);
+template cudaError_t launch_propags_adj<double>(const PropArgs<double>&, const double*, int, double*, int, cudaStream_t);
 template cudaError_t launch_cfl_extrema<float>(const PropArgs<float>&, long long*, int, cudaStream_t);
 template cudaError_t launch_cfl_extrema<double>(const PropArgs<double>&, long long*, int, cudaStream_t);
 

@@ -229,6 +229,35 @@ class WamModel:
         s = None if stream is None else ctypes.c_void_p(stream)
         self._check(self.L.wamgpu_propags_substep_dev(self.h, src.data_ptr(), dst.data_ptr(), ld, s), "propags_substep")
 
+    # ---- derivatives (ST4) ---------------------------------------------------
+    def implsch_tl_dev(self, fl3, dfl3, tauw, dtauw, u10, du10, udir, roairn, wstar,
+                       fl3_out, dfl3_out, tauw_out, dtauw_out, ld=None, stream=None):
+        """IMPLSCH and its tangent-linear: (FL3, TAUW, U10) + perturbations ->
+        new (FL3, TAUW) + perturbations. Spectra shaped (ML, KL, ld)."""
+        ld = fl3.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        p = lambda t: t.data_ptr()
+        self._check(self.L.wamgpu_implsch_tl_dev(self.h, p(fl3), p(dfl3), ld, p(tauw), p(dtauw), p(u10), p(du10),
+                                                 p(udir), p(roairn), p(wstar), p(fl3_out), p(dfl3_out), p(tauw_out),
+                                                 p(dtauw_out), s), "implsch_tl_dev")
+
+    def implsch_adj_dev(self, fl3, tauw, u10, udir, roairn, wstar, lam_fl3, lam_tauw, lam_u10, ld=None, stream=None):
+        """Adjoint of IMPLSCH at the checkpoint (FL3, TAUW, U10): lam_fl3 and
+        lam_tauw map in place from the new state's adjoints to the old
+        state's; lam_u10 is overwritten with the adjoint of U10."""
+        ld = fl3.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        p = lambda t: t.data_ptr()
+        self._check(self.L.wamgpu_implsch_adj_dev(self.h, p(fl3), ld, p(tauw), p(u10), p(udir), p(roairn), p(wstar),
+                                                  p(lam_fl3), p(lam_tauw), p(lam_u10), s), "implsch_adj_dev")
+
+    def propags_adj_dev(self, lam, ld=None, scratch=None, stream=None):
+        """Transpose of propags_dev (all COUNTER sub-steps), in place on lam."""
+        ld = lam.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        sc = None if scratch is None else ctypes.c_void_p(scratch.data_ptr())
+        self._check(self.L.wamgpu_propags_adj_dev(self.h, lam.data_ptr(), ld, sc, s), "propags_adj_dev")
+
     def set_timing(self, enable=True):
         self._check(self.L.wamgpu_set_timing(self.h, int(enable)), "set_timing")
 
