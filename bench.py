@@ -48,6 +48,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-batched", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true")
     return p.parse_args()
 
 
@@ -238,6 +239,95 @@ def batched_ensemble(dev, steps, warmup, n_members=32):
     return out
 
 
+def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242):
+    """Adjoint of one assimilation window on the 400x300 regional grid
+    (KL=36, ML=30, ST4, IDELPRO=120 s, IDELT=600 s), FP32.
+
+    The forward sweep runs `passes` WAMODEL passes and keeps one checkpoint
+    per pass (the spectrum entering IMPLSCH).  The cost is the squared Hs
+    misfit at n_obs seeded sea points against a perturbed-truth run (U10
+    +10%) with Hs noise of sigma 0.2 m.  The backward sweep, the IMPLSCH
+    adjoint and the PROPAGS transpose of every pass, gives the gradient with
+    respect to the initial spectrum, the initial TAUW and each pass's U10.
+    Device times by CUDA events: the plain forward pass (wamgpu_step_dev),
+    the checkpointed forward sweep, and the backward sweep."""
+    import torch
+    from wam_b200 import WamModel
+    from wam_b200.adjoint import WamPass, significant_wave_height, window_cost_and_grad
+    from wam_b200.synth import make_workload
+    w = make_workload("c2", device=dev.index)
+    m = WamModel(w.cfg)
+    m.set_grid(w.grid)
+    m.set_depth(w.depth)
+    _, counter = m.prepare_propagation()
+    m.prepare_source()
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    t = lambda a: torch.tensor(np.asarray(a, np.float32), device=dev)
+    f0 = w.spectrum_device(torch, dev)
+    u10, udir, tauw, roairn, wstar = (t(a) for a in (w.u10, w.udir, w.tauw, w.roairn, w.wstar))
+    ustar, z0 = t(w.ustar), t(w.z0)
+    nprop = w.cfg["idelt"] // w.cfg["idelpro"]
+    u_seq = [u10 * (1.0 + 0.05 * (p // 6)) for p in range(passes)]  # hourly changes of the forcing
+    gen = torch.Generator(device=dev).manual_seed(seed)
+    points = torch.randperm(w.nsea, generator=gen, device=dev)[:n_obs]
+    dfim = torch.tensor(m.table("DFIM"), device=dev, dtype=torch.float32)
+    with torch.no_grad():  # perturbed truth and observations
+        f, tw, obs = f0, tauw, []
+        for u in u_seq:
+            f, tw = WamPass.apply(f, tw, 1.1 * u, m, nprop, udir, roairn, wstar)
+            hs = significant_wave_height(f, dfim, points)
+            obs.append(hs + 0.2 * torch.randn(hs.shape, generator=gen, device=dev))
+    sh = stream.cuda_stream
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def plain():
+        f, sc, tw = f0.clone(), torch.empty_like(f0), tauw.clone()
+        torch.cuda.synchronize()
+        e0, e1 = ev(), ev()
+        e0.record(stream)
+        for u in u_seq:
+            m.step_dev(f, nprop, u, udir, tw, ustar, z0, roairn, wstar, scratch=sc, stream=sh)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / passes
+
+    for _ in range(warmup):
+        plain()
+    ms_plain = plain()
+    # one short window as warm-up, then the timed window
+    window_cost_and_grad(m, f0, tauw, u_seq[:2], udir, roairn, wstar, points, obs, nprop)
+    torch.cuda.synchronize()
+    fs = f0.detach().clone().requires_grad_(True)
+    ts = tauw.detach().clone().requires_grad_(True)
+    us = [u.detach().clone().requires_grad_(True) for u in u_seq]
+    e0, e1, e2 = ev(), ev(), ev()
+    e0.record(stream)
+    f, tw, J = fs, ts, torch.zeros((), device=dev)
+    for p, u in enumerate(us):
+        f, tw = WamPass.apply(f, tw, u, m, nprop, udir, roairn, wstar)
+        J = J + ((significant_wave_height(f, dfim, points) - obs[p]) ** 2).sum()
+    e1.record(stream)
+    J.backward()
+    e2.record(stream)
+    torch.cuda.synchronize()
+    ms_fwd = e0.elapsed_time(e1) / passes
+    ms_adj = e1.elapsed_time(e2) / passes
+    finite = bool(torch.isfinite(fs.grad).all()) and all(bool(torch.isfinite(u.grad).all()) for u in us)
+    bins = w.nsea * w.cfg["kl"] * w.cfg["ml"]
+    out = {"workload": f"c2: 400x300 regional, {w.nsea} sea points, ST4, KL=36 ML=30, IDELPRO=120 s IDELT=600 s, "
+                       f"{passes}-pass window, {n_obs} Hs observations",
+           "value": bins / (ms_adj / 1e3), "unit": UNIT + " (adjoint pass)", "ms_per_adjoint_pass": ms_adj,
+           "ms_per_forward_pass": ms_plain, "ms_per_checkpointed_forward_pass": ms_fwd,
+           "adjoint_over_forward": ms_adj / ms_plain, "counter": counter, "cost": float(J), "gradients_finite": finite,
+           "checkpoint_bytes": passes * bins * 4,
+           "how": "backward sweep = per pass wamgpu_implsch_adj_dev (recomputes IMPLSCH from its checkpoint) + "
+                  "IDELT/IDELPRO x wamgpu_propags_adj_dev; forward = wamgpu_step_dev"}
+    m.close()
+    torch.cuda.set_stream(torch.cuda.default_stream(dev))
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -370,6 +460,8 @@ def main():
                 "gpu_launches": launches, "clocks": clk.summary()}
         if not args.no_batched and world == 1:
             line["batched"] = batched_ensemble(dev, max(3, min(args.steps, 10)), max(3, args.warmup))
+        if not args.no_adjoint and world == 1:
+            line["adjoint"] = adjoint_window(dev, max(3, args.warmup))
         print(json.dumps(line), flush=True)
     m.close()
     if world > 1:

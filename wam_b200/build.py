@@ -24,7 +24,7 @@ UNITS = {
     "api.cu": [],
     "adjoint.cu": [],
 }
-HEADERS = ["implsch.cuh", "propags.cuh", "propargs.hpp", "devmath.cuh", "kernels.hpp", "adjoint.cuh", "spectral_tables.hpp", "wamgpu_config.hpp"]
+HEADERS = ["implsch.cuh", "propags.cuh", "propargs.hpp", "devmath.cuh", "kernels.hpp", "adjoint.cuh", "adjoint_warp.cuh", "spectral_tables.hpp", "wamgpu_config.hpp"]
 
 
 def _nvcc():

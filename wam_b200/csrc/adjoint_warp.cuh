@@ -1,0 +1,753 @@
+// Adjoint of IMPLSCH (ST4), one sea point per warp with the point's work
+// arrays in shared memory.
+//
+// The forward pass is recomputed inside the step with the forward kernel's own
+// lane-parallel routines (Src), recording what the reverse sweep needs: the
+// cut-off indices, AIRSEA's outputs, SINPUT's sheltering sums and SPOS sums per
+// frequency, the first wind-sea mask and the source terms SL/FL.  The reverse
+// sweep then runs the routines backwards with the lanes spread over the
+// directions of a frequency (or over all bins where the step is elementwise):
+// IMPHFTAIL, the implicit update, the DIA, SDISSIP_ARD, STRESSO and
+// SINPUT_ARD (second call on F1, then the first call on F0), the spectral
+// integrals and AIRSEA.  Scalar routines of one point (AIRSEA, TAU_PHI_HF,
+// WSIGSTAR) are differentiated by two dual-number passes, one per half-warp.
+// The statements follow the point-per-thread restatement in adjoint.cuh,
+// which is the same linearisation.
+//
+// Shared memory of one warp: the forward workspace (SF = {SL, FL} per bin,
+// F, 8 scratch rows, LL), then LAM (adjoint of the spectrum), 14 tape rows of
+// ML values and the first LLWS mask.  After the update's adjoint SF holds
+// {lambda_SL, lambda_FL}.  F holds F0, then F1 from the first IMPHFTAIL on;
+// once the reverse sweep is done with F1 it is reloaded with F0 from global
+// memory.
+#pragma once
+#include "adjoint.cuh"
+#include "implsch.cuh"
+
+namespace wamgpu {
+
+template <typename R> __host__ __device__ inline size_t adjw_lam_offset(int ld, int ML, int scr) {
+  return warp_ws_bytes<R>(ld, ML, 0, scr);
+}
+template <typename R> __host__ __device__ inline size_t adjw_at_offset(int ld, int ML, int scr) {
+  size_t b = adjw_lam_offset<R>(ld, ML, scr) + (size_t)ld * ML * sizeof(R);
+  return (b + 15) & ~size_t(15);
+}
+template <typename R> __host__ __device__ inline size_t adjw_ll1_offset(int ld, int ML, int scr) {
+  return adjw_at_offset<R>(ld, ML, scr) + ((14 * (size_t)ML * sizeof(R) + 15) & ~size_t(15));
+}
+template <typename R> __host__ __device__ inline size_t adjw_ws_bytes(int ld, int ML, int scr) {
+  return adjw_ll1_offset<R>(ld, ML, scr) + (((size_t)ld * ML + 15) & ~size_t(15));
+}
+
+template <typename R> struct AdjW {
+  using P_ = Phys<R>;
+  using R2 = typename Vec2<R>::type;
+  Src<R>& s;
+  const DevTables<R>& T;
+  const STabs<R>& S;
+  WarpWS<R>& w;
+  const adj::ATabs<R>& A;
+  const adj::PointIn<R>& P;
+  const int lane;
+  const R* F0g;     // the input spectrum in global memory (point ij, stride ldg)
+  const size_t ldg;
+  R *LAM, *AT;
+  uint8_t* LL1;
+  // recorded forward state
+  int mij = 1, mij2 = 1, ju = 1;
+  R us1 = 0, z01 = 0, tauw1 = 0, us2 = 0, z02 = 0, fmean = 0, fmeanws = 0, akmean = 0, fmx = 0;
+
+  __device__ AdjW(Src<R>& src, const adj::ATabs<R>& a, const adj::PointIn<R>& p, const R* f0g, size_t ldg_, R* lam, R* at,
+                  uint8_t* ll1)
+      : s(src), T(src.T), S(src.S), w(src.w), A(a), P(p), lane(src.lane), F0g(f0g), ldg(ldg_), LAM(lam), AT(at),
+        LL1(ll1) {}
+
+  __device__ int KL() const { return T.KL; }
+  __device__ int ML() const { return T.ML; }
+  // tape rows: sheltering sums (q = 0,1 XST of the two gust branches, 2,3 YST), SX, SY per call; LSX, LSY
+  __device__ R* shl_rows(int call) const { return AT + 4 * call * ML(); }
+  __device__ R* sx_row(int call) const { return AT + (8 + 2 * call) * ML(); }
+  __device__ R* sy_row(int call) const { return AT + (9 + 2 * call) * ML(); }
+  __device__ R* lsx_row() const { return AT + 12 * ML(); }
+  __device__ R* lsy_row() const { return AT + 13 * ML(); }
+  __device__ static R2 r2(R a, R b) { R2 v; v.x = a; v.y = b; return v; }
+
+  // ---- forward with recording --------------------------------------------------
+  __device__ void forward(R TAUW0) {
+    const int ml = ML(), ld = w.ld;
+    ju = min(300, max((int)lround((double)(s.U10 / T.DELU)), 1));
+    R emean, emeanws;
+    akmean = 0;
+    const bool need_ak = T.shallow && T.isnonlin == 0;
+    s.integrals(nullptr, emean, fmean, need_ak ? &akmean : nullptr);
+    s.airsea(TAUW0, us1, z01);
+    s.shl = shl_rows(0);
+    s.sinput_ard(us1, z01);
+    s.for_bins(ml, [&](int m, int k) { LL1[k + ld * m] = w.LL[k + ld * m]; });
+    for (int m = lane; m < ml; m += 32) { sx_row(0)[m] = w.t(1)[m]; sy_row(0)[m] = w.t(2)[m]; }
+    __syncwarp();
+    s.integrals(w.LL, emeanws, fmeanws, nullptr);
+    mij = s.frcutindex(fmean, fmeanws, us1);
+    R phiaw;
+    s.stresso_sums(us1, z01, mij, tauw1, phiaw);
+    s.airsea(tauw1, us2, z02);
+    s.imphftail(mij);  // F = F1 from here on
+    s.shl = shl_rows(1);
+    s.sinput_ard(us2, z02);
+    s.shl = nullptr;
+    for (int m = lane; m < ml; m += 32) { sx_row(1)[m] = w.t(1)[m]; sy_row(1)[m] = w.t(2)[m]; }
+    __syncwarp();
+    s.sdissip_ard();
+    s.snonlin(akmean);
+    fmx = dmax(fmeanws, fmean);
+    update_rows();
+    mij2 = cutoff_after_update();
+  }
+
+  // cos^2 spreading (row 2), limiter (3), floor (4) and SBOTTOM factor (6) of the update
+  __device__ void update_rows() const {
+    const int kl = KL(), ml = ML();
+    R *C2 = w.t(2), *LIM = w.t(3), *FMIN = w.t(4), *SBO = w.t(6);
+    for (int k = lane; k < kl; k += 32) { const R c = dmax(R(0.), dcos(S.TH[k] - s.UDIR)); C2[k] = c * c; }
+    const R cst = R(-2.0) * R(0.038) / P_::G;
+    for (int m = lane; m < ml; m += 32) {
+      LIM[m] = us2 * S.DELFL[m] * fmx;
+      FMIN[m] = __ldg(&T.FLMINFR[(ju - 1) + 300 * m]);
+      if (T.shallow) { const R wav = s.tfak(m); SBO[m] = cst * wav / dsinh(dmin(R(2.) * s.DEPTH * wav, R(50.))); }
+    }
+    __syncwarp();
+  }
+
+  // The update's output at bin (m, k), as the forward step forms it.
+  __device__ R updated(int m, int k) const {
+    const int p = k + w.ld * m;
+    const R f0 = w.F[p];
+    const R2 v = w.SF[p];
+    R sl = v.x, fl = v.y;
+    if (T.shallow) { sl = sl + w.t(6)[m] * f0; fl = fl + w.t(6)[m]; }
+    const R t1 = T.DELT * sl / dmax(R(1.), R(1.) - T.DELT * fl);
+    const R t3 = dmin(dabs(t1), w.t(3)[m]);
+    const R f = f0 + ((t1 >= R(0)) ? t3 : -t3);
+    return dmax(f, w.t(4)[m] * w.t(2)[k]);
+  }
+
+  // MIJ of the updated spectrum: the integrals (unmasked and with the second
+  // LLWS) of the update's output, formed without storing it.
+  __device__ int cutoff_after_update() const {
+    const int kl = KL(), ml = ML(), ld = w.ld;
+    R pe = 0, pf = 0, tail = 0, pew = 0, pfw = 0, tailw = 0;
+    for (int m = lane; m < ml; m += 32) {
+      R t = 0, tw = 0;
+      const uint8_t* mk = w.LL + ld * m;
+      for (int k = 0; k < kl; ++k) {
+        const R f = updated(m, k);
+        t = t + f;
+        tw = tw + (mk[k] ? f : R(0));
+      }
+      pe = pe + t * S.DFIM[m]; pf = pf + t * S.DFIMOFR[m];
+      pew = pew + tw * S.DFIM[m]; pfw = pfw + tw * S.DFIMOFR[m];
+      if (m == ml - 1) { tail = t; tailw = tw; }
+    }
+    pe = warp_sum(pe); pf = warp_sum(pf); pew = warp_sum(pew); pfw = warp_sum(pfw);
+    tail = __shfl_sync(0xffffffffu, tail, (ml - 1) & 31);
+    tailw = __shfl_sync(0xffffffffu, tailw, (ml - 1) & 31);
+    const R e = dmax(T.MO_TAIL * tail + pe, R(1.0E-12)), fm = e / dmax(T.MM1_TAIL * tail + pf, R(1.0E-12));
+    const R ew = dmax(T.MO_TAIL * tailw + pew, R(1.0E-12)), fmw = ew / dmax(T.MM1_TAIL * tailw + pfw, R(1.0E-12));
+    return s.frcutindex(fm, fmw, us2);
+  }
+
+  // ---- reverse sweep ---------------------------------------------------------------
+
+  // Jacobians of the two-input scalar routines: the two dual-number passes run
+  // on the two half-warps at once (their branch decisions follow the values,
+  // which both passes share) and are exchanged.
+  // du, dv: this lane's derivatives of the outputs (u, v) along input 0
+  // (lanes < 16) or input 1 (lanes >= 16).
+  __device__ adj::Jac2<R> jac_split(R du, R dv) const {
+    adj::Jac2<R> J;
+    const bool hi = lane >= 16;
+    const R ou = __shfl_xor_sync(0xffffffffu, du, 16), ov = __shfl_xor_sync(0xffffffffu, dv, 16);
+    J.d00 = hi ? ou : du; J.d10 = hi ? ov : dv;
+    J.d01 = hi ? du : ou; J.d11 = hi ? dv : ov;
+    return J;
+  }
+  // d(USTAR, Z0) / d(U10, TAUW) of AIRSEA
+  __device__ adj::Jac2<R> airsea_jac(R U10, R TAUW) const {
+    using D = adj::Dual<R>;
+    const bool hi = lane >= 16;
+    D us, z0;
+    adj::airsea(A, D(U10, hi ? R(0) : R(1)), D(TAUW, hi ? R(1) : R(0)), us, z0);
+    return jac_split(us.d, z0.d);
+  }
+  // d(TAUHF, PHIHF) / d(USTAR, Z0) of TAU_PHI_HF
+  __device__ adj::Jac2<R> tauphi_jac(int mj, R ustar, R z0) const {
+    using D = adj::Dual<R>;
+    const bool hi = lane >= 16;
+    D th, ph;
+    adj::tau_phi_hf(A, mj, D(ustar, hi ? R(0) : R(1)), D(z0, hi ? R(1) : R(0)), th, ph);
+    return jac_split(th.d, ph.d);
+  }
+  // d(WSIGSTAR) / d(USTAR) and / d(Z0)
+  __device__ void wsig_grad(R ustar, R z0, R& dus, R& dz0) const {
+    using D = adj::Dual<R>;
+    const bool hi = lane >= 16;
+    const D v = adj::wsigstar(P, D(ustar, hi ? R(0) : R(1)), D(z0, hi ? R(1) : R(0)));
+    const R o = __shfl_xor_sync(0xffffffffu, v.d, 16);
+    dus = hi ? o : v.d;
+    dz0 = hi ? v.d : o;
+  }
+
+  // IMPHFTAIL^T: rows m >= mij were copied from row mij-1 with a ratio.
+  __device__ void imphftail_adj(int mj) const {
+    const int kl = KL(), ml = ML(), ld = w.ld;
+    R* t = w.t(7);
+    for (int m = mj - 1 + lane; m < ml; m += 32) {
+      if (T.shallow) { const R akm1 = R(1.) / s.tfak(m); t[m] = (akm1 * akm1 * akm1) / s.tcgond(m); }
+      else t[m] = S.FRM5[m];
+    }
+    __syncwarp();
+    const R base = t[mj - 1];
+    for (int k = lane; k < kl; k += 32) {
+      R acc = LAM[k + ld * (mj - 1)];
+      for (int m = mj; m < ml; ++m) {
+        acc = acc + (t[m] / base) * LAM[k + ld * m];
+        LAM[k + ld * m] = R(0);
+      }
+      LAM[k + ld * (mj - 1)] = acc;
+    }
+    __syncwarp();
+  }
+
+  // The implicit update^T: LAM (output -> input spectrum) in place, SF
+  // replaced by {lambda_SL, lambda_FL}; adds to the adjoints of USTAR and FMX.
+  __device__ void update_adj(R& lus, R& lfmx) const {
+    const int ld = w.ld;
+    const R delt = T.DELT;
+    const R *C2 = w.t(2), *LIM = w.t(3), *FMIN = w.t(4), *SBO = w.t(6);
+    R aus = 0, afmx = 0;
+    s.for_bins(ML(), [&](int m, int k) {
+      const int p = k + ld * m;
+      const R f0 = w.F[p];
+      const R2 v = w.SF[p];
+      R sl = v.x, fl = v.y;
+      if (T.shallow) { sl = sl + SBO[m] * f0; fl = fl + SBO[m]; }
+      const R den_raw = R(1.) - delt * fl, den = dmax(R(1.), den_raw);
+      const R t1 = delt * sl / den, at1 = dabs(t1), lim = LIM[m];
+      const R t3 = dmin(at1, lim);
+      const R f = f0 + ((t1 >= R(0)) ? t3 : -t3);
+      const R lf = (f < FMIN[m] * C2[k]) ? R(0) : LAM[p];  // the floor holds when it is selected
+      R lf0 = lf, lt1 = 0;
+      const R lt3 = (t1 >= R(0)) ? lf : -lf;
+      if (lim < at1) { aus = aus + lt3 * S.DELFL[m] * fmx; afmx = afmx + lt3 * us2 * S.DELFL[m]; }
+      else lt1 = (t1 < R(0)) ? -lt3 : lt3;
+      const R lsl = lt1 * delt / den;
+      const R lfl = (R(1.) < den_raw) ? lt1 * t1 / den * delt : R(0);
+      if (T.shallow) lf0 = lf0 + SBO[m] * lsl;
+      LAM[p] = lf0;
+      w.SF[p] = r2(lsl, lfl);
+    });
+    lus = lus + warp_sum(aus);
+    lfmx = lfmx + warp_sum(afmx);
+    __syncwarp();
+  }
+
+  // SNONLIN^T (DIA), the transpose of the forward gather: for each MC the
+  // lanes first form, for their directions and both KH, the adjoints of the
+  // interaction's centre value and of its two partner sums from the adjoints
+  // of the nine targets, and leave them in a per-warp buffer; then every lane
+  // adds to its own direction column of the five gathered rows (IC, IP, IP1,
+  // IM, IM1) what the interactions that read that column owe it.  The partner
+  // tables are rotations (checked on the host), so the interaction that read
+  // column j through a table is found by rotating j back.  Returns the adjoint
+  // of AKMEAN (ISNONLIN = 0 in shallow water).
+  __device__ R snonlin_adj() const {
+    const int kl = KL(), ml = ML(), ld = w.ld;
+    const bool dyn = T.shallow && T.isnonlin == 0;
+    R enhfr = R(1), denh = R(0);
+    if (dyn) {
+      const adj::Dual<R> e = adj::snl_enhfr(A, P, adj::Dual<R>(akmean, R(1)));
+      enhfr = e.v; denh = e.d;
+    }
+    const int mfr1 = -T.MFRSTLW + 1, mfrl = ml - T.KFRH + mfr1;
+    const R2* SF = w.SF;
+    const R* F = w.F;
+    R* XF = w.T;       // [kh*kl + k]: adjoint of the centre value (times FTAIL)
+    R* XS = XF + 2 * kl;  // adjoint of SAP
+    R* XM = XS + 2 * kl;  // adjoint of SAM
+    int o1[2], o2[2], o11[2], o21[2];
+    for (int kh = 0; kh < 2; ++kh) {
+      o1[kh] = S.K1W[kl * kh] - 1; o2[kh] = S.K2W[kl * kh] - 1;
+      o11[kh] = S.K11W[kl * kh] - 1; o21[kh] = S.K21W[kl * kh] - 1;
+    }
+    auto rot = [kl](int k, int o) { const int t = k + o; return t >= kl ? t - kl : t; };
+    const int nsub = kl > 32 ? 2 : 1;
+    R lenh = 0;
+    for (int mc = 1; mc <= T.MLSTHG; ++mc) {
+      const int im = mc - T.MFRSTLW;
+      const int MP = S.IKP[im], MP1 = S.IKP1[im], MM = S.IKM[im], MM1 = S.IKM1[im];
+      const int* ic5 = S.INL + 5 * (mc - 1);
+      const int rIC = ld * (ic5[0] - 1), rIP = ld * (ic5[1] - 1), rIP1 = ld * (ic5[2] - 1), rIM = ld * (ic5[3] - 1),
+                rIM1 = ld * (ic5[4] - 1);
+      const R* rc = S.RNL + 25 * (mc - 1);
+      R ftemp = S.AF11[im];
+      if (T.shallow) ftemp = ftemp * (T.isnonlin == 0 ? enhfr : P.ENH[mc - 1]);
+      const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
+      const R ftail = (regime == 0) ? R(1) : rc[0];
+      const bool wMM = regime != 2, wMM1 = regime == 0 || (regime == 1 && MM1 <= ml) || (regime == 2 && MM1 >= 1);
+      const bool wMC = regime != 1 || (MM1 <= ml && mc <= ml);
+      const bool wMP = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml);
+      const bool wMP1 = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml && MP1 <= ml);
+      const int rMC = wMC ? ld * (mc - 1) : 0, rMM = wMM ? ld * (MM - 1) : 0, rMM1 = wMM1 ? ld * (MM1 - 1) : 0,
+                rMP = wMP ? ld * (MP - 1) : 0, rMP1 = wMP1 ? ld * (MP1 - 1) : 0;
+      const R g1 = rc[1], g2 = rc[2], g3 = rc[3], g4 = rc[4], g5 = rc[13], g6 = rc[14], g7 = rc[15], g8 = rc[16];
+      // 1. per interaction (k, kh) of this lane: adjoints of FIJ, SAP, SAM
+      for (int s_ = 0; s_ < nsub; ++s_) {
+        const int k = lane + 32 * s_;
+        if (k >= kl) break;
+        const R fij = F[k + rIC] * ftail;
+        const R2 vC = SF[k + rMC];
+        for (int kh = 0; kh < 2; ++kh) {
+          const int a1 = rot(k, o1[kh]), a11 = rot(k, o11[kh]), a2 = rot(k, o2[kh]), a21 = rot(k, o21[kh]);
+          const R sap = g1 * F[a1 + rIP] + g2 * F[a11 + rIP] + g3 * F[a1 + rIP1] + g4 * F[a11 + rIP1];
+          const R sam = g5 * F[a2 + rIM] + g6 * F[a21 + rIM] + g7 * F[a2 + rIM1] + g8 * F[a21 + rIM1];
+          R lad = 0, ldelad = 0, ldelap = 0, ldelam = 0;
+          if (wMC) { lad = lad - R(2.) * vC.x; ldelad = ldelad - R(2.) * vC.y; }
+          if (wMM) {
+            const R2 u = SF[a2 + rMM], u21 = SF[a21 + rMM];
+            lad = lad + (rc[20] * u.x + rc[19] * u21.x); ldelam = ldelam + (rc[23] * u.y + rc[24] * u21.y);
+          }
+          if (wMM1) {
+            const R2 u = SF[a2 + rMM1], u21 = SF[a21 + rMM1];
+            lad = lad + (rc[17] * u.x + rc[18] * u21.x); ldelam = ldelam + (rc[21] * u.y + rc[22] * u21.y);
+          }
+          if (wMP) {
+            const R2 u = SF[a1 + rMP], u11 = SF[a11 + rMP];
+            lad = lad + (rc[8] * u.x + rc[7] * u11.x); ldelap = ldelap + (rc[11] * u.y + rc[12] * u11.y);
+          }
+          if (wMP1) {
+            const R2 u = SF[a1 + rMP1], u11 = SF[a11 + rMP1];
+            lad = lad + (rc[5] * u.x + rc[6] * u11.x); ldelap = ldelap + (rc[9] * u.y + rc[10] * u11.y);
+          }
+          // ad = (fij S - 2P) ftemp fij, delad = (2 fij S - 2P) ftemp,
+          // delap = (fij - 2 sam) DAL1 ftemp fij, delam = (fij - 2 sap) DAL2 ftemp fij
+          const R S2 = sap + sam, P2 = sap * sam;
+          const R lfij = lad * ftemp * (R(2) * fij * S2 - R(2) * P2) + ldelad * R(2) * S2 * ftemp +
+                         ldelap * T.DAL1 * ftemp * (R(2) * fij - R(2) * sam) +
+                         ldelam * T.DAL2 * ftemp * (R(2) * fij - R(2) * sap);
+          const R lsap = lad * ftemp * fij * (fij - R(2) * sam) + ldelad * (R(2) * fij - R(2) * sam) * ftemp -
+                         ldelam * R(2) * T.DAL2 * ftemp * fij;
+          const R lsam = lad * ftemp * fij * (fij - R(2) * sap) + ldelad * (R(2) * fij - R(2) * sap) * ftemp -
+                         ldelap * R(2) * T.DAL1 * ftemp * fij;
+          if (dyn) {
+            const R lft = lad * (fij * S2 - R(2) * P2) * fij + ldelad * (R(2) * fij * S2 - R(2) * P2) +
+                          ldelap * (fij - R(2) * sam) * T.DAL1 * fij + ldelam * (fij - R(2) * sap) * T.DAL2 * fij;
+            lenh = lenh + lft * S.AF11[im];
+          }
+          XF[kl * kh + k] = lfij * ftail;
+          XS[kl * kh + k] = lsap;
+          XM[kl * kh + k] = lsam;
+        }
+      }
+      __syncwarp();
+      // 2. this lane's column j of the five gathered rows
+      for (int s_ = 0; s_ < nsub; ++s_) {
+        const int j = lane + 32 * s_;
+        if (j >= kl) break;
+        const R sp1 = XS[rot(j, kl - o1[0])] + XS[kl + rot(j, kl - o1[1])];
+        const R sp11 = XS[rot(j, kl - o11[0])] + XS[kl + rot(j, kl - o11[1])];
+        const R sm2 = XM[rot(j, kl - o2[0])] + XM[kl + rot(j, kl - o2[1])];
+        const R sm21 = XM[rot(j, kl - o21[0])] + XM[kl + rot(j, kl - o21[1])];
+        LAM[j + rIC] = LAM[j + rIC] + (XF[j] + XF[kl + j]);
+        LAM[j + rIP] = LAM[j + rIP] + (g1 * sp1 + g2 * sp11);
+        LAM[j + rIP1] = LAM[j + rIP1] + (g3 * sp1 + g4 * sp11);
+        LAM[j + rIM] = LAM[j + rIM] + (g5 * sm2 + g6 * sm21);
+        LAM[j + rIM1] = LAM[j + rIM1] + (g7 * sm2 + g8 * sm21);
+      }
+      __syncwarp();  // the next frequency overwrites the buffer
+    }
+    return warp_sum(lenh) * denh;
+  }
+
+  // SDISSIP_ARD^T.  The saturation window is a rotation of the directions
+  // (INDICESSAT(K, J) = K + J - NSDSNTH modulo KL, checked on the host), so
+  // the transposed window sum is gathered per column like the DIA.
+  __device__ void sdissip_adj() const {
+    const int kl = KL(), ml = ML(), nw = 2 * T.NSDSNTH + 1, ns = T.NSDSNTH, ld = w.ld;
+    const R tmp03 = R(1.0) / R(9.0E-4), c6 = R(0.3), c6m1 = R(1.) - c6;
+    R* LB = w.t(5);
+    for (int m = 0; m < ml; ++m) {
+      const R sig = P_::ZPI * S.FR[m];
+      R facsat;
+      if (T.shallow) { const R xk = s.tfak(m); facsat = (xk * xk * xk) * (R(1.0) / P_::ZPI) * s.tcgond(m); }
+      else { const R xk = sig * sig / P_::G; facsat = (xk * xk * xk) * (R(0.5) * (R(1.0) / P_::ZPI)) * P_::G / sig; }
+      const R* fm = w.F + ld * m;
+      R bth[2] = {0, 0}, bmax = 0;
+      int kmax = -1;
+      for (int s_ = 0; s_ < 2; ++s_) {
+        const int k = lane + 32 * s_;
+        if (k < kl) {
+          R acc = 0;
+          for (int j = 0; j < nw; ++j) acc = acc + S.SATW[k + kl * j] * fm[S.INDSAT[k + kl * j] - 1];
+          bth[s_] = acc * facsat;
+          if (bmax < bth[s_]) { bmax = bth[s_]; kmax = k; }
+        }
+      }
+      // the first direction of largest saturation (none while all are <= 0)
+      for (int o = 16; o > 0; o >>= 1) {
+        const R ob = __shfl_xor_sync(0xffffffffu, bmax, o);
+        const int ok = __shfl_xor_sync(0xffffffffu, kmax, o);
+        if (bmax < ob || (ob == bmax && ok >= 0 && (kmax < 0 || ok < kmax))) { bmax = ob; kmax = ok; }
+      }
+      const R d0raw = bmax * tmp03 - R(1.0), d0 = dmax(R(0.), d0raw);
+      const R temp1 = c6 * (d0 * d0), ssdsc2_sig = R(-2.2E-5) * sig;
+      R lt1 = 0, lb[2] = {0, 0};
+      for (int s_ = 0; s_ < 2; ++s_) {
+        const int k = lane + 32 * s_;
+        if (k < kl) {
+          const int b = k + ld * m;
+          const R ddraw = bth[s_] * tmp03 - R(1.0), dd = dmax(R(0.), ddraw);
+          const R d = ssdsc2_sig * (temp1 + c6m1 * (dd * dd));
+          const R2 v = w.SF[b];
+          LAM[b] = LAM[b] + d * v.x;
+          const R ldv = fm[k] * v.x + v.y;
+          lt1 = lt1 + ldv * ssdsc2_sig;
+          if (R(0.) < ddraw) lb[s_] = ldv * ssdsc2_sig * c6m1 * R(2) * dd * tmp03;
+        }
+      }
+      const R ltemp1 = warp_sum(lt1);
+      for (int s_ = 0; s_ < 2; ++s_) {
+        const int k = lane + 32 * s_;
+        if (k < kl) {
+          R v = lb[s_];
+          if (R(0.) < d0raw && k == kmax) v = v + ltemp1 * c6 * R(2) * d0 * tmp03;
+          LB[k] = v * facsat;
+        }
+      }
+      __syncwarp();
+      for (int s_ = 0; s_ < 2; ++s_) {
+        const int c = lane + 32 * s_;
+        if (c < kl) {
+          R acc = 0;
+          for (int j = 0; j < nw; ++j) {
+            int k = c - j + ns;
+            k = k < 0 ? k + kl : (k >= kl ? k - kl : k);
+            acc = acc + S.SATW[k + kl * j] * LB[k];
+          }
+          LAM[c + ld * m] = LAM[c + ld * m] + acc;
+        }
+      }
+      __syncwarp();
+    }
+  }
+
+  // STRESSO^T for TAUW of SINPUT call `call` (spectrum Fs): to the adjoints of
+  // its SPOS sums (rows LSX, LSY), of the cut-off row of the spectrum, of USTAR
+  // and of Z0.
+  __device__ void stresso_adj(int call, const R* Fs, R US, R Z0, R lTAU, R& lUS, R& lZ0) const {
+    const int kl = KL(), ml = ML(), ld = w.ld;
+    const R *SX = sx_row(call), *SY = sy_row(call);
+    R px = 0, py = 0;
+    for (int m = lane; m < mij; m += 32) {
+      const R cmr = s.cmw(m) * s.rhowgdfth(m, mij);
+      px = px + SX[m] * cmr;
+      py = py + SY[m] * cmr;
+    }
+    px = warp_sum(px); py = warp_sum(py);
+    const R gm1 = R(1.0) / P_::G;
+    const R cst = T.DELTH * ((P_::ZPI * P_::ZPI) * (P_::ZPI * P_::ZPI)) * gm1;
+    R t1 = 0;
+    for (int k = lane; k < kl; k += 32) {
+      const R cw = dmax(dcos(S.TH[k] - s.UDIR), R(0.));
+      t1 = t1 + Fs[k + ld * (mij - 1)] * (cw * cw * cw);
+    }
+    t1 = warp_sum(t1);
+    R tau1, phi1;
+    s.tau_phi_hf(mij, US, Z0, tau1, phi1);
+    const R kc = cst * S.FR5[mij - 1] * gm1;
+    const R tauhf = kc * t1 * tau1;
+    const R su = dsin(s.UDIR), cu = dcos(s.UDIR);
+    const R xs = px / P_::ROAIR + tauhf * su, ys = py / P_::ROAIR + tauhf * cu;
+    const R tw = dsqrt(xs * xs + ys * ys), cap = US * US - R(0.00001);
+    const R twc = dmin(tw, cap);
+    const R ltwc = (twc < R(0.)) ? R(0) : lTAU;
+    R ltw = 0;
+    if (cap < tw) lUS = lUS + ltwc * R(2) * US;
+    else ltw = ltwc;
+    const R lxs = tw > R(0) ? ltw * xs / tw : R(0), lys = tw > R(0) ? ltw * ys / tw : R(0);
+    const R lpx = lxs / P_::ROAIR, lpy = lys / P_::ROAIR, ltauhf = lxs * su + lys * cu;
+    const R lt1 = ltauhf * kc * tau1, ltau1 = ltauhf * kc * t1;
+    for (int k = lane; k < kl; k += 32) {
+      const R cw = dmax(dcos(S.TH[k] - s.UDIR), R(0.));
+      LAM[k + ld * (mij - 1)] = LAM[k + ld * (mij - 1)] + lt1 * (cw * cw * cw);
+    }
+    const adj::Jac2<R> J = tauphi_jac(mij, US, Z0);
+    lUS = lUS + ltau1 * J.d00;
+    lZ0 = lZ0 + ltau1 * J.d01;
+    R *LSX = lsx_row(), *LSY = lsy_row();
+    for (int m = lane; m < ml; m += 32) {
+      const R cmr = m < mij ? s.cmw(m) * s.rhowgdfth(m, mij) : R(0);
+      LSX[m] = lpx * cmr;
+      LSY[m] = lpy * cmr;
+    }
+    __syncwarp();
+  }
+
+  // SINPUT_ARD^T of call `call` on spectrum Fs.  lSF: adjoints of its SL/FL
+  // outputs (null for the first call, whose SL/FL the step overwrites); rows
+  // LSX/LSY: adjoints of its SPOS sums.  Adds to LAM and to the adjoints of
+  // USTAR and Z0.
+  __device__ void sinput_adj(int call, const R* Fs, R US, R Z0, const R2* lSF, R& lUS, R& lZ0) const {
+    const int kl = KL(), ml = ML(), ld = w.ld;
+    const R SWELLF = R(0.66), FU = R(0.022), FUD = R(-0.018), SWELLF4 = R(1.5E05), SWELLF5 = R(1.2), SWELLF7 = R(3.6E05);
+    const R const1 = T.BETAMAX / (P_::XKAPPA * P_::XKAPPA) / P_::ROWATER;
+    const R nu = P_::RNUAIR, rog = P_::ROWATER * P_::G;
+    const R delabm1 = R(200) / (R(8.0) - R(0.3));
+    const R shelter = dabs(T.TAUWSHELTER);
+    const R ROAIRN = s.ROAIRN;
+    // per-point prologue (recomputed)
+    const R sig_n = s.wsigstar(US, Z0);
+    R uo = 0, ao = 0;
+    for (int m = lane; m < ml; m += 32) {
+      R t = 0;
+      for (int k = 0; k < kl; ++k) t = t + Fs[k + ld * m];
+      const R sig = P_::ZPI * S.FR[m];
+      uo = uo + S.DFIM[m] * (sig * sig) * t;
+      ao = ao + S.DFIM[m] * t;
+    }
+    uo = warp_sum(uo); ao = warp_sum(ao);
+    const R tiny = sizeof(R) == 4 ? R(FLT_MIN) : R(DBL_MIN);
+    const R uorbt = R(2.0) * dsqrt(tiny + uo), aorb = R(2.0) * dsqrt(tiny + ao);
+    const R re = (R(4.0) / nu) * uorbt * aorb;
+    const R a1 = P_::RNUAIRM / dmax(US, R(0.0001)), a2 = R(0.04) * dmin(R(0.0005), Z0);
+    const R z0noz = dmax(a1, a2);
+    const R ratio = aorb / z0noz;
+    const R xi = (dlog10(dmax(ratio, R(3.0))) - R(0.3)) * delabm1;
+    const int ind = min(199, max(1, (int)xi));
+    const R deli1 = dmin(R(1.0), xi - R(ind));
+    const R fww = S.SWELLFT[ind - 1] * (R(1.0) - deli1) + S.SWELLFT[ind] * deli1;
+    const R temp2 = fww * uorbt;
+    const R zs = (re - SWELLF4) / SWELLF7, th = dtanh(zs);
+    const R smooth = R(0.5) * th, pturb = R(0.5) + smooth, pvisc = R(0.5) - smooth;
+    const R sgn[2] = {R(1), R(-1)};
+    R usg[2];
+    for (int g = 0; g < 2; ++g) { const R a = US * (R(1.0) + sgn[g] * sig_n); usg[g] = a * a; }
+    const R su = dsin(s.UDIR), cu = dcos(s.UDIR);
+    const R taux[2] = {usg[0] * su, usg[1] * su}, tauy[2] = {usg[0] * cu, usg[1] * cu};
+    const R rogoroair = rog / dmax(ROAIRN, R(1.0));
+    const R roairn_pvisc = ROAIRN * pvisc;
+    const R* shl = shl_rows(call);
+    const R *LSX = lsx_row(), *LSY = lsy_row();
+    // reverse over frequency with the adjoints of the sheltering sums
+    R lxst[2] = {0, 0}, lyst[2] = {0, 0}, ltaux[2] = {0, 0}, ltauy[2] = {0, 0};
+    R lpvisc = 0, lpturb = 0, ltemp2 = 0;  // lpturb, ltemp2: this lane's part
+    for (int m = ml - 1; m >= 0; --m) {
+      const R xst[2] = {shl[m], shl[ml + m]}, yst[2] = {shl[2 * ml + m], shl[3 * ml + m]};
+      const R sig = P_::ZPI * S.FR[m], sig2 = sig * sig;
+      R xk, cm;
+      if (T.shallow) { xk = s.tfak(m); cm = xk * (R(1.0) / sig); }
+      else { cm = sig / P_::G; xk = sig2 / P_::G; }
+      R tpx[2], tpy[2], ustp[2], usdirp[2], ucn[2], ucnz[2];
+      for (int g = 0; g < 2; ++g) {
+        tpx[g] = taux[g] - shelter * xst[g]; tpy[g] = tauy[g] - shelter * yst[g];
+        ustp[g] = dpow(tpx[g] * tpx[g] + tpy[g] * tpy[g], R(0.25));
+        usdirp[g] = datan2(tpx[g], tpy[g]);
+        ucn[g] = ustp[g] * cm;
+        ucnz[g] = P_::XKAPPA / (ucn[g] + T.ZALP);
+      }
+      const R constf = rogoroair * cm * S.DFIM[m];
+      const R zcn = dlog(xk * Z0);
+      const R cnsn = (sig * const1) * ROAIRN;
+      const R coef = -(SWELLF * R(16.) * sig2 / (P_::G * P_::ROWATER));
+      const R coef5 = -(SWELLF5 * R(2.) * dsqrt(R(2.) * nu * sig) / P_::ROWATER);
+      const R dstab1 = coef5 * roairn_pvisc * xk;
+      const R tmp1 = coef * ROAIRN;
+      const R lSX = LSX[m], lSY = LSY[m];
+      R q[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // lustp[2], lusdirp[2], lucn[2], lucnz[2], lzcn, ldstab1
+      for (int k = lane; k < kl; k += 32) {
+        const int b = k + ld * m;
+        const R f = Fs[b];
+        R c[2], ufac[2], slpu[2], zlog[2], xx[2];
+        bool act[2];
+        for (int g = 0; g < 2; ++g) {
+          c[g] = dcos(S.TH[k] - usdirp[g]);
+          ufac[g] = 0; act[g] = false; zlog[g] = 0; xx[g] = 0;
+          if (c[g] > R(0.01)) {
+            xx[g] = c[g] * ucn[g];
+            zlog[g] = zcn + ucnz[g] / c[g];
+            if (zlog[g] < R(0.0)) { const R z2x = zlog[g] * zlog[g] * xx[g]; ufac[g] = dexp(zlog[g]) * z2x * z2x; act[g] = true; }
+          }
+          slpu[g] = cnsn * ufac[g];
+        }
+        const R dst0 = dstab1 + pturb * (tmp1 * (temp2 + (FU + FUD * c[0]) * ustp[0]));
+        const R dst1 = dstab1 + pturb * (tmp1 * (temp2 + (FU + FUD * c[1]) * ustp[1]));
+        const R fl = R(0.5) * ((slpu[0] + dst0) + (slpu[1] + dst1));
+        R lsl = 0, lfl_out = 0;
+        if (lSF) { const R2 v = lSF[b]; lsl = v.x; lfl_out = v.y; }
+        const R lfl = lsl * f + lfl_out;
+        R lf = lsl * fl;
+        const R lspos = lSX * S.SINTH[k] + lSY * S.COSTH[k];
+        for (int g = 0; g < 2; ++g) {
+          const R lslpf = R(0.5) * lspos + lxst[g] * (constf * S.SINTH[k]) + lyst[g] * (constf * S.COSTH[k]);
+          const R lflp = R(0.5) * lfl;
+          const R lslpu = lflp + lslpf * f;
+          lf = lf + lslpf * slpu[g];
+          const R ldstab = lflp;
+          const R lufac = lslpu * cnsn;
+          q[9] = q[9] + ldstab;
+          lpturb = lpturb + ldstab * (tmp1 * (temp2 + (FU + FUD * c[g]) * ustp[g]));
+          ltemp2 = ltemp2 + ldstab * pturb * tmp1;
+          R lc = ldstab * pturb * tmp1 * FUD * ustp[g];
+          q[g] = q[g] + ldstab * pturb * tmp1 * (FU + FUD * c[g]);
+          if (act[g]) {
+            const R e = dexp(zlog[g]), z2x = zlog[g] * zlog[g] * xx[g];
+            const R lzlog = lufac * e * z2x * (z2x + R(4) * zlog[g] * xx[g]);
+            const R lx = lufac * e * R(2) * z2x * zlog[g] * zlog[g];
+            lc = lc + lx * ucn[g];
+            q[4 + g] = q[4 + g] + lx * c[g];
+            q[8] = q[8] + lzlog;
+            q[6 + g] = q[6 + g] + lzlog / c[g];
+            lc = lc - lzlog * ucnz[g] / (c[g] * c[g]);
+          }
+          q[2 + g] = q[2 + g] + lc * dsin(S.TH[k] - usdirp[g]);
+        }
+        LAM[b] = LAM[b] + lf;
+      }
+      for (int i = 0; i < 10; ++i) q[i] = warp_sum(q[i]);
+      for (int g = 0; g < 2; ++g) {
+        const R d = ucn[g] + T.ZALP;
+        const R lucn = q[4 + g] - q[6 + g] * P_::XKAPPA / (d * d);
+        const R lustp = q[g] + lucn * cm;
+        const R qq = tpx[g] * tpx[g] + tpy[g] * tpy[g];
+        R ltpx = 0, ltpy = 0;
+        if (qq > R(0)) {
+          const R lq = lustp * R(0.25) * dpow(qq, R(-0.75));
+          ltpx = lq * R(2) * tpx[g] + q[2 + g] * tpy[g] / qq;
+          ltpy = lq * R(2) * tpy[g] - q[2 + g] * tpx[g] / qq;
+        }
+        ltaux[g] = ltaux[g] + ltpx;
+        ltauy[g] = ltauy[g] + ltpy;
+        lxst[g] = lxst[g] - shelter * ltpx;
+        lyst[g] = lyst[g] - shelter * ltpy;
+      }
+      lZ0 = lZ0 + q[8] / Z0;
+      lpvisc = lpvisc + q[9] * coef5 * ROAIRN * xk;
+    }
+    lpturb = warp_sum(lpturb);
+    ltemp2 = warp_sum(ltemp2);
+    // prologue^T
+    R lsig_n = 0;
+    for (int g = 0; g < 2; ++g) {
+      const R lusg = ltaux[g] * su + ltauy[g] * cu;
+      const R a = US * (R(1.0) + sgn[g] * sig_n);
+      const R la = R(2) * a * lusg;
+      lUS = lUS + la * (R(1.0) + sgn[g] * sig_n);
+      lsig_n = lsig_n + la * US * sgn[g];
+    }
+    const R lsmooth = lpturb - lpvisc;
+    const R lre = lsmooth * R(0.5) * (R(1) - th * th) / SWELLF7;
+    R luorbt = ltemp2 * fww, laorb = 0;
+    const R lfww = ltemp2 * uorbt;
+    const R ldeli1 = lfww * (S.SWELLFT[ind] - S.SWELLFT[ind - 1]);
+    const R lxi = ((xi - R(ind)) < R(1.0)) ? ldeli1 : R(0);
+    R lz0noz = 0;
+    if (!(ratio < R(3.0))) {
+      const R lratio = lxi * delabm1 / (ratio * dlog(R(10)));
+      laorb = laorb + lratio / z0noz;
+      lz0noz = -lratio * aorb / (z0noz * z0noz);
+    }
+    if (!(a1 < a2)) { if (!(US < R(0.0001))) lUS = lUS - lz0noz * P_::RNUAIRM / (US * US); }
+    else if (Z0 < R(0.0005)) lZ0 = lZ0 + lz0noz * R(0.04);
+    luorbt = luorbt + lre * (R(4.0) / nu) * aorb;
+    laorb = laorb + lre * (R(4.0) / nu) * uorbt;
+    const R luo = luorbt / dsqrt(tiny + uo), lao = laorb / dsqrt(tiny + ao);
+    s.for_bins(ml, [&](int m, int k) {
+      const R sig = P_::ZPI * S.FR[m];
+      LAM[k + ld * m] = LAM[k + ld * m] + (luo * S.DFIM[m] * (sig * sig) + lao * S.DFIM[m]);
+    });
+    {
+      R dus, dz0;
+      wsig_grad(US, Z0, dus, dz0);
+      lUS = lUS + lsig_n * dus;
+      lZ0 = lZ0 + lsig_n * dz0;
+    }
+    __syncwarp();
+  }
+
+  // Adjoint of the spectral integrals of Fs (masked by `mask` when set) with
+  // respect to the spectrum, given the adjoints of FMEAN and AKMEAN.
+  __device__ void integrals_adj(const R* Fs, const uint8_t* mask, R lfm, R lak, bool with_ak) const {
+    const int kl = KL(), ml = ML(), ld = w.ld;
+    const R DEL2 = dsqrt(P_::G) / P_::ZPI;
+    R pe = 0, pf = 0, pa = 0, tail = 0;
+    for (int m = lane; m < ml; m += 32) {
+      R t = 0;
+      for (int k = 0; k < kl; ++k) { const int b = k + ld * m; if (!mask || mask[b]) t = t + Fs[b]; }
+      pe = pe + t * S.DFIM[m];
+      pf = pf + t * S.DFIMOFR[m];
+      if (with_ak) pa = pa + (T.shallow ? t / dsqrt(s.tfak(m)) * S.DFIM[m] : t * S.DFIMOFR[m] * DEL2);
+      if (m == ml - 1) tail = t;
+    }
+    pe = warp_sum(pe); pf = warp_sum(pf); pa = warp_sum(pa);
+    tail = __shfl_sync(0xffffffffu, tail, (ml - 1) & 31);
+    const R e_raw = T.MO_TAIL * tail + pe, emean = dmax(e_raw, R(1.0E-12));
+    const R den_raw = T.MM1_TAIL * tail + pf, den = dmax(den_raw, R(1.0E-12));
+    R lpe = 0, lpf = 0, lpa = 0, ltail = 0, le = 0;
+    if (with_ak && emean > R(1.0E-12)) {
+      const R wm = T.MM1_TAIL * DEL2 * tail + pa, qv = emean / wm;
+      const R lq = lak * R(2) * qv;
+      le = le + lq / wm;
+      const R lwm = -lq * emean / (wm * wm);
+      lpa = lwm; ltail = ltail + lwm * T.MM1_TAIL * DEL2;
+    }
+    le = le + lfm / den;
+    const R lden = -lfm * emean / (den * den);
+    if (den_raw >= R(1.0E-12)) { lpf = lden; ltail = ltail + lden * T.MM1_TAIL; }
+    if (e_raw >= R(1.0E-12)) { lpe = le; ltail = ltail + le * T.MO_TAIL; }
+    s.for_bins(ml, [&](int m, int k) {
+      const int b = k + ld * m;
+      R lt = lpe * S.DFIM[m] + lpf * S.DFIMOFR[m];
+      if (with_ak) lt = lt + lpa * (T.shallow ? S.DFIM[m] / dsqrt(s.tfak(m)) : S.DFIMOFR[m] * DEL2);
+      if (m == ml - 1) lt = lt + ltail;
+      if (!mask || mask[b]) LAM[b] = LAM[b] + lt;
+    });
+    __syncwarp();
+  }
+
+  // F <- F0 (the input spectrum), read back from global memory.
+  __device__ void reload_f0() const {
+    const int kl = KL(), ld = w.ld;
+    s.for_bins(ML(), [&](int m, int k) { w.F[k + ld * m] = __ldg(&F0g[ldg * (size_t)(k + kl * m)]); });
+    __syncwarp();
+  }
+
+  // The whole reverse sweep.  In: LAM = adjoint of the output spectrum, lTAUW =
+  // adjoint of the output TAUW.  Out: LAM = adjoint of the input spectrum,
+  // lTAUW0 and lU10.
+  __device__ void reverse(R TAUW0, R lTAUW, R& lTAUW0, R& lU10) {
+    imphftail_adj(mij2);
+    R lus2 = 0, lz02 = 0, lfmx = 0;
+    update_adj(lus2, lfmx);
+    const R lak = snonlin_adj();
+    sdissip_adj();
+    stresso_adj(1, w.F, us2, z02, lTAUW, lus2, lz02);
+    sinput_adj(1, w.F, us2, z02, w.SF, lus2, lz02);
+    imphftail_adj(mij);
+    reload_f0();
+    const adj::Jac2<R> J2 = airsea_jac(s.U10, tauw1);
+    lU10 = J2.d00 * lus2 + J2.d10 * lz02;
+    const R ltauw1 = J2.d01 * lus2 + J2.d11 * lz02;
+    R lus1 = 0, lz01 = 0;
+    stresso_adj(0, w.F, us1, z01, ltauw1, lus1, lz01);
+    sinput_adj(0, w.F, us1, z01, nullptr, lus1, lz01);
+    R lfmean = 0, lfmeanws = 0;
+    if (fmeanws < fmean) lfmean = lfmx; else lfmeanws = lfmx;
+    integrals_adj(w.F, nullptr, lfmean, lak, T.shallow && T.isnonlin == 0);
+    integrals_adj(w.F, LL1, lfmeanws, R(0), false);
+    const adj::Jac2<R> J1 = airsea_jac(s.U10, TAUW0);
+    lU10 = lU10 + J1.d00 * lus1 + J1.d10 * lz01;
+    lTAUW0 = J1.d01 * lus1 + J1.d11 * lz01;
+  }
+};
+
+}  // namespace wamgpu

@@ -580,9 +580,22 @@ int deriv_setup(wamgpu_ctx* ctx, Impl<R>& I, int ld, bool tl, DerivArgs<R>& a) {
     return fail(ctx, WAMGPU_E_ARG, "derivatives cover the whole grid of a context (no owned range)");
   if (ctx->cfg.shallow_run && ctx->cfg.isnonlin != 0 && !I.has_enh)
     return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_source first (ISNONLIN table)");
+  if (ctx->cfg.kl > 64) return fail(ctx, WAMGPU_E_ARG, "IMPLSCH derivatives support at most 64 directions");
+  {
+    // the adjoint gathers the transposed saturation window per direction
+    // column: INDICESSAT(K, J) must be the rotation K + J - NSDSNTH
+    const TableSet<R>& t = I.tab;
+    const int KL = t.KL, ns = t.NSDSNTH;
+    for (int j = 0; j < 2 * ns + 1; ++j)
+      for (int k = 0; k < KL; ++k)
+        if (t.INDICESSAT[k + KL * j] - 1 != ((k + j - ns) % KL + KL) % KL)
+          return fail(ctx, WAMGPU_E_ARG, "saturation window is not a rotation of the directions");
+  }
   const size_t n = (size_t)ctx->nsea;
-  CK(I.dwork.ensure(n * deriv_work_bytes<R>(ctx->cfg.kl, ctx->cfg.ml, tl) + 256), "alloc derivative work");
-  CK(I.dmasks.ensure(n * 2 * ctx->cfg.kl * ctx->cfg.ml + 256), "alloc derivative work");
+  if (tl) {
+    CK(I.dwork.ensure(n * deriv_work_bytes<R>(ctx->cfg.kl, ctx->cfg.ml) + 256), "alloc derivative work");
+    CK(I.dmasks.ensure(n * 2 * ctx->cfg.kl * ctx->cfg.ml + 256), "alloc derivative work");
+  }
   std::memset(&a, 0, sizeof(a));
   a.A = atabs_of(I.dt);
   a.nsea = ctx->nsea; a.ld = ld;
@@ -602,7 +615,7 @@ int implsch_adj_t(wamgpu_ctx* ctx, Impl<R>& I, const void* fl3_in, int ld, const
   a.fl3_in = (const R*)fl3_in; a.tauw_in = (const R*)tauw_in; a.u10 = (const R*)u10; a.udir = (const R*)udir;
   a.roairn = (const R*)roairn; a.wstar = (const R*)wstar;
   a.lam_fl3 = (R*)lam_fl3; a.lam_tauw = (R*)lam_tauw; a.lam_u10 = (R*)lam_u10;
-  { TimedLaunch tl(ctx, 1, s); CK(launch_implsch_adj<R>(a, s), "implsch adjoint launch"); }
+  { TimedLaunch tl(ctx, 1, s); CK(launch_implsch_adj<R>(I.dt, a, s), "implsch adjoint launch"); }
   return WAMGPU_OK;
 }
 

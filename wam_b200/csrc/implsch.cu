@@ -5,12 +5,6 @@
 
 namespace wamgpu {
 
-template <typename R>
-__host__ __device__ inline size_t tables_bytes(const SmallLayout& L) {
-  size_t b = (size_t)L.nreal * sizeof(R) + (size_t)L.nint * sizeof(int);
-  return (b + 15) & ~size_t(15);
-}
-
 // One CTA: sea points blk*P .. blk*P+P-1 of the launch's arguments.
 template <typename R, int P>
 __device__ __forceinline__ void implsch_cta(const DevTables<R>& T, const ImplArgs<R>& a, int blk, unsigned char* smem) {

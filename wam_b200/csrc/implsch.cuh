@@ -86,6 +86,12 @@ template <typename R> __host__ __device__ inline size_t ws_t_offset(int ld, int 
   return (b + 15) & ~size_t(15);
 }
 
+// Bytes of the small tables staged at the start of a CTA's shared memory.
+template <typename R> __host__ __device__ inline size_t tables_bytes(const SmallLayout& L) {
+  size_t b = (size_t)L.nreal * sizeof(R) + (size_t)L.nint * sizeof(int);
+  return (b + 15) & ~size_t(15);
+}
+
 // Per-point outputs of IMPLSCH beyond the spectrum.
 template <typename R> struct PointState {
   R TAUW, USTAR, Z0;
@@ -101,6 +107,9 @@ template <typename R> struct Src {
   const R U10, UDIR, ROAIRN, WSTAR, DEPTH;
   const R* ENH;  // MAKE_SHALLOW_SNL factors of the launch's points (ISNONLIN != 0), else null
   const int enh_ld;
+  // When set, SINPUT_ARD records the sheltering sums entering every
+  // frequency: rows XST0, XST1, YST0, YST1 of length ML (the adjoint's tape).
+  R* shl = nullptr;
   __device__ Src(const DevTables<R>& t, const STabs<R>& s, WarpWS<R>& ws, int l, int ij_, int indep, R u10, R udir,
                  R roairn, R wstar, R depth, const R* enh, int enh_ld_)
       : T(t), S(s), w(ws), lane(l), ij(ij_), INDEP(indep), U10(u10), UDIR(udir), ROAIRN(roairn), WSTAR(wstar), DEPTH(depth),
@@ -236,6 +245,7 @@ template <typename R> struct Src {
     R xst[2] = {0, 0}, yst[2] = {0, 0};
     R rogoroair = rog / dmax(ROAIRN, R(1.0)), roairn_pvisc = ROAIRN * pvisc;
     for (int m = 0; m < ml; ++m) {
+      if (shl && lane == 0) { shl[m] = xst[0]; shl[ml + m] = xst[1]; shl[2 * ml + m] = yst[0]; shl[3 * ml + m] = yst[1]; }
       R sig = P_::ZPI * S.FR[m], sig2 = sig * sig;
       R xk, cm;
       if (T.shallow) { xk = tfak(m); cm = xk * (R(1.0) / sig); }

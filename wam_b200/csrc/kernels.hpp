@@ -83,8 +83,8 @@ template <typename R> struct DerivArgs {
   const R *dfl3_in, *dtauw_in, *du10;
   R *fl3_out, *dfl3_out, *tauw_out, *dtauw_out, *ustar_out, *z0_out;
 };
-template <typename R> size_t deriv_work_bytes(int KL, int ML, bool tl);
-template <typename R> cudaError_t launch_implsch_adj(const DerivArgs<R>& a, cudaStream_t s);
+template <typename R> size_t deriv_work_bytes(int KL, int ML);
+template <typename R> cudaError_t launch_implsch_adj(const DevTables<R>& T, const DerivArgs<R>& a, cudaStream_t s);
 template <typename R> cudaError_t launch_implsch_tl(const DerivArgs<R>& a, cudaStream_t s);
 // Transpose of one PROPAGS sub-step: lam_old (zeroed by the caller) +=
 // P^T lam_new, by atomic adds into the neighbours' bins.
