@@ -34,7 +34,11 @@ template <typename R> __device__ adj::ATabs<R> atabs_view(const DevTables<R>& T,
 
 // CTA of P warps = P consecutive sea points.  The spectra and their adjoints
 // are staged into shared memory with consecutive threads on consecutive
-// points of one bin, and the adjoints written back the same way.
+// points of one bin, and the adjoints written back the same way.  The warps
+// of a CTA pass the phases of the step together (a CTA barrier after each):
+// the step's code is far larger than the instruction cache, and warps in
+// different phases would keep evicting each other's code.  A warp beyond the
+// last sea point repeats the last point and writes nothing.
 template <typename R, int P>
 __global__ void __launch_bounds__(P * 32) implsch_adj_kernel(const __grid_constant__ DevTables<R> T,
                                                              const __grid_constant__ DerivArgs<R> a) {
@@ -49,18 +53,17 @@ __global__ void __launch_bounds__(P * 32) implsch_adj_kernel(const __grid_consta
   unsigned char* ws0 = smem + tables_bytes<R>(T.lay);
   const size_t foff = ws_f_offset<R>(LD, ML), loff = adjw_lam_offset<R>(LD, ML, T.scr);
   const int ij0 = blockIdx.x * P;
+  const size_t ld = (size_t)a.ld;
   for (int idx = tid; idx < P * NS; idx += nthr) {
-    const int p = idx % P, b = idx / P, ij = ij0 + p;
+    const int p = idx % P, b = idx / P, ij = min(ij0 + p, a.nsea - 1);
     const int m = b / KL, k = b - m * KL;
-    if (ij < a.nsea) {
-      unsigned char* base = ws0 + p * wsb;
-      reinterpret_cast<R*>(base + foff)[k + LD * m] = a.fl3_in[ij + (size_t)a.ld * b];
-      reinterpret_cast<R*>(base + loff)[k + LD * m] = a.lam_fl3[ij + (size_t)a.ld * b];
-    }
+    unsigned char* base = ws0 + p * wsb;
+    reinterpret_cast<R*>(base + foff)[k + LD * m] = a.fl3_in[ij + ld * b];
+    reinterpret_cast<R*>(base + loff)[k + LD * m] = a.lam_fl3[ij + ld * b];
   }
   __syncthreads();
-  const int warp = tid >> 5, lane = tid & 31, ij = ij0 + warp;
-  if (ij < a.nsea) {
+  const int warp = tid >> 5, lane = tid & 31, ij = min(ij0 + warp, a.nsea - 1);
+  {
     STabs<R> S;
     S.bind(sR, sI, T.lay);
     WarpWS<R> w;
@@ -79,19 +82,19 @@ __global__ void __launch_bounds__(P * 32) implsch_adj_kernel(const __grid_consta
     pin.WSTAR = a.wstar[ij];
     pin.ENH.p = a.enh ? a.enh + ij : nullptr;
     pin.ENH.ld = (size_t)a.enh_ld;
-    AdjW<R> g(src, A, pin, a.fl3_in + ij, (size_t)a.ld, reinterpret_cast<R*>(base + loff),
+    AdjW<R> g(src, A, pin, a.fl3_in + ij, ld, reinterpret_cast<R*>(base + loff),
               reinterpret_cast<R*>(base + adjw_at_offset<R>(LD, ML, T.scr)), base + adjw_ll1_offset<R>(LD, ML, T.scr));
     const R tw0 = a.tauw_in[ij], ltw = a.lam_tauw[ij];
     g.forward(tw0);
     R lT0 = 0, lU = 0;
     g.reverse(tw0, ltw, lT0, lU);
-    if (lane == 0) { a.lam_tauw[ij] = lT0; a.lam_u10[ij] = lU; }
+    if (lane == 0 && ij0 + warp < a.nsea) { a.lam_tauw[ij] = lT0; a.lam_u10[ij] = lU; }
   }
   __syncthreads();
   for (int idx = tid; idx < P * NS; idx += nthr) {
-    const int p = idx % P, b = idx / P, ij = ij0 + p;
+    const int p = idx % P, b = idx / P, ijs = ij0 + p;
     const int m = b / KL, k = b - m * KL;
-    if (ij < a.nsea) a.lam_fl3[ij + (size_t)a.ld * b] = reinterpret_cast<R*>(ws0 + p * wsb + loff)[k + LD * m];
+    if (ijs < a.nsea) a.lam_fl3[ijs + ld * b] = reinterpret_cast<R*>(ws0 + p * wsb + loff)[k + LD * m];
   }
 }
 
@@ -114,20 +117,24 @@ template <typename R, int P> cudaError_t adj_set_smem(size_t bytes) {
   return e;
 }
 
-template <typename R, int P> cudaError_t adj_launch_one(const DevTables<R>& T, const DerivArgs<R>& a, cudaStream_t s) {
+template <typename R, int P>
+cudaError_t adj_launch_one(const DevTables<R>& T, const DerivArgs<R>& a, int ctas, cudaStream_t s) {
   const size_t bytes = adj_smem_bytes(T, P);
   cudaError_t e = adj_set_smem<R, P>(bytes);
   if (e != cudaSuccess) return e;
+  (void)ctas;
   implsch_adj_kernel<R, P><<<(a.nsea + P - 1) / P, P * 32, bytes, s>>>(T, a);
   return cudaGetLastError();
 }
 
 // Sea points per CTA: the compiled shape that keeps the most warps resident
-// per SM under the shared-memory budget (ties go to smaller CTAs).
-template <typename R> int adj_points_per_cta(const DevTables<R>& T, int dev) {
-  int optin = 0, persm = 0;
+// per SM under the shared-memory budget (ties go to smaller CTAs); `ctas`
+// receives the number of resident CTAs over the device.
+template <typename R> int adj_points_per_cta(const DevTables<R>& T, int dev, int& ctas) {
+  int optin = 0, persm = 0, nsm = 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
   if (cudaDeviceGetAttribute(&persm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
   const int cand32[] = {2, 4, 6, 8, 9}, cand64[] = {1, 2, 3, 4, 5};
   const int* cand = sizeof(R) == 4 ? cand32 : cand64;
   const int nc = 5;
@@ -135,8 +142,8 @@ template <typename R> int adj_points_per_cta(const DevTables<R>& T, int dev) {
   for (int i = 0; i < nc; ++i) {
     const size_t b = adj_smem_bytes(T, cand[i]);
     if (b > (size_t)optin) continue;
-    const int warps = cand[i] * (int)(persm / (b + 1024));
-    if (warps > best_warps) { best = cand[i]; best_warps = warps; }
+    const int per = (int)(persm / (b + 1024)), warps = cand[i] * per;
+    if (warps > best_warps) { best = cand[i]; best_warps = warps; ctas = per * nsm; }
   }
   return best;
 }
@@ -146,19 +153,20 @@ template <typename R> cudaError_t launch_implsch_adj(const DevTables<R>& T, cons
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  const int P = adj_points_per_cta(T, dev);
+  int ctas = 0;
+  const int P = adj_points_per_cta(T, dev, ctas);
   if constexpr (sizeof(R) == 4) {
-    if (P == 9) return adj_launch_one<R, 9>(T, a, s);
-    if (P == 8) return adj_launch_one<R, 8>(T, a, s);
-    if (P == 6) return adj_launch_one<R, 6>(T, a, s);
-    if (P == 4) return adj_launch_one<R, 4>(T, a, s);
-    if (P == 2) return adj_launch_one<R, 2>(T, a, s);
+    if (P == 9) return adj_launch_one<R, 9>(T, a, ctas, s);
+    if (P == 8) return adj_launch_one<R, 8>(T, a, ctas, s);
+    if (P == 6) return adj_launch_one<R, 6>(T, a, ctas, s);
+    if (P == 4) return adj_launch_one<R, 4>(T, a, ctas, s);
+    if (P == 2) return adj_launch_one<R, 2>(T, a, ctas, s);
   } else {
-    if (P == 5) return adj_launch_one<R, 5>(T, a, s);
-    if (P == 4) return adj_launch_one<R, 4>(T, a, s);
-    if (P == 3) return adj_launch_one<R, 3>(T, a, s);
-    if (P == 2) return adj_launch_one<R, 2>(T, a, s);
-    if (P == 1) return adj_launch_one<R, 1>(T, a, s);
+    if (P == 5) return adj_launch_one<R, 5>(T, a, ctas, s);
+    if (P == 4) return adj_launch_one<R, 4>(T, a, ctas, s);
+    if (P == 3) return adj_launch_one<R, 3>(T, a, ctas, s);
+    if (P == 2) return adj_launch_one<R, 2>(T, a, ctas, s);
+    if (P == 1) return adj_launch_one<R, 1>(T, a, ctas, s);
   }
   return cudaErrorInvalidConfiguration;  // one point's work arrays exceed the shared memory of a CTA
 }

@@ -72,6 +72,8 @@ template <typename R> struct AdjW {
   __device__ R* lsx_row() const { return AT + 12 * ML(); }
   __device__ R* lsy_row() const { return AT + 13 * ML(); }
   __device__ static R2 r2(R a, R b) { R2 v; v.x = a; v.y = b; return v; }
+  // end of a phase: every warp of the CTA runs the same sequence of phases
+  __device__ static void phase() { __syncthreads(); }
 
   // ---- forward with recording --------------------------------------------------
   __device__ void forward(R TAUW0) {
@@ -84,6 +86,7 @@ template <typename R> struct AdjW {
     s.airsea(TAUW0, us1, z01);
     s.shl = shl_rows(0);
     s.sinput_ard(us1, z01);
+    phase();
     s.for_bins(ml, [&](int m, int k) { LL1[k + ld * m] = w.LL[k + ld * m]; });
     for (int m = lane; m < ml; m += 32) { sx_row(0)[m] = w.t(1)[m]; sy_row(0)[m] = w.t(2)[m]; }
     __syncwarp();
@@ -93,13 +96,17 @@ template <typename R> struct AdjW {
     s.stresso_sums(us1, z01, mij, tauw1, phiaw);
     s.airsea(tauw1, us2, z02);
     s.imphftail(mij);  // F = F1 from here on
+    phase();
     s.shl = shl_rows(1);
     s.sinput_ard(us2, z02);
     s.shl = nullptr;
+    phase();
     for (int m = lane; m < ml; m += 32) { sx_row(1)[m] = w.t(1)[m]; sy_row(1)[m] = w.t(2)[m]; }
     __syncwarp();
     s.sdissip_ard();
+    phase();
     s.snonlin(akmean);
+    phase();
     fmx = dmax(fmeanws, fmean);
     update_rows();
     mij2 = cutoff_after_update();
@@ -388,7 +395,12 @@ template <typename R> struct AdjW {
         const int k = lane + 32 * s_;
         if (k < kl) {
           R acc = 0;
-          for (int j = 0; j < nw; ++j) acc = acc + S.SATW[k + kl * j] * fm[S.INDSAT[k + kl * j] - 1];
+          int src = k - ns;
+          src = src < 0 ? src + kl : src;
+          for (int j = 0; j < nw; ++j) {
+            acc = acc + S.SATW[k + kl * j] * fm[src];
+            src = src + 1 == kl ? 0 : src + 1;
+          }
           bth[s_] = acc * facsat;
           if (bmax < bth[s_]) { bmax = bth[s_]; kmax = k; }
         }
@@ -547,11 +559,17 @@ template <typename R> struct AdjW {
       R xk, cm;
       if (T.shallow) { xk = s.tfak(m); cm = xk * (R(1.0) / sig); }
       else { cm = sig / P_::G; xk = sig2 / P_::G; }
-      R tpx[2], tpy[2], ustp[2], usdirp[2], ucn[2], ucnz[2];
+      // cos and sin of the stress direction USDIRP = ATAN2(tpx, tpy) from the
+      // stress components; cos(TH - USDIRP) and sin(TH - USDIRP) per bin then
+      // follow from the direction tables
+      R tpx[2], tpy[2], ustp[2], cu_[2], su_[2], ucn[2], ucnz[2];
       for (int g = 0; g < 2; ++g) {
         tpx[g] = taux[g] - shelter * xst[g]; tpy[g] = tauy[g] - shelter * yst[g];
-        ustp[g] = dpow(tpx[g] * tpx[g] + tpy[g] * tpy[g], R(0.25));
-        usdirp[g] = datan2(tpx[g], tpy[g]);
+        const R qq = tpx[g] * tpx[g] + tpy[g] * tpy[g];
+        ustp[g] = dpow(qq, R(0.25));
+        const R rn = qq > R(0) ? R(1) / dsqrt(qq) : R(0);
+        cu_[g] = qq > R(0) ? tpy[g] * rn : R(1);
+        su_[g] = tpx[g] * rn;
         ucn[g] = ustp[g] * cm;
         ucnz[g] = P_::XKAPPA / (ucn[g] + T.ZALP);
       }
@@ -567,15 +585,22 @@ template <typename R> struct AdjW {
       for (int k = lane; k < kl; k += 32) {
         const int b = k + ld * m;
         const R f = Fs[b];
-        R c[2], ufac[2], slpu[2], zlog[2], xx[2];
+        const R sk = S.SINTH[k], ck = S.COSTH[k];
+        R c[2], ufac[2], slpu[2], zlog[2], xx[2], ez[2], rc[2];
         bool act[2];
         for (int g = 0; g < 2; ++g) {
-          c[g] = dcos(S.TH[k] - usdirp[g]);
-          ufac[g] = 0; act[g] = false; zlog[g] = 0; xx[g] = 0;
+          c[g] = ck * cu_[g] + sk * su_[g];
+          ufac[g] = 0; act[g] = false; zlog[g] = 0; xx[g] = 0; ez[g] = 0; rc[g] = 0;
           if (c[g] > R(0.01)) {
+            rc[g] = R(1) / c[g];
             xx[g] = c[g] * ucn[g];
-            zlog[g] = zcn + ucnz[g] / c[g];
-            if (zlog[g] < R(0.0)) { const R z2x = zlog[g] * zlog[g] * xx[g]; ufac[g] = dexp(zlog[g]) * z2x * z2x; act[g] = true; }
+            zlog[g] = zcn + ucnz[g] * rc[g];
+            if (zlog[g] < R(0.0)) {
+              const R z2x = zlog[g] * zlog[g] * xx[g];
+              ez[g] = dexp(zlog[g]);
+              ufac[g] = ez[g] * z2x * z2x;
+              act[g] = true;
+            }
           }
           slpu[g] = cnsn * ufac[g];
         }
@@ -600,16 +625,16 @@ template <typename R> struct AdjW {
           R lc = ldstab * pturb * tmp1 * FUD * ustp[g];
           q[g] = q[g] + ldstab * pturb * tmp1 * (FU + FUD * c[g]);
           if (act[g]) {
-            const R e = dexp(zlog[g]), z2x = zlog[g] * zlog[g] * xx[g];
+            const R e = ez[g], z2x = zlog[g] * zlog[g] * xx[g];
             const R lzlog = lufac * e * z2x * (z2x + R(4) * zlog[g] * xx[g]);
             const R lx = lufac * e * R(2) * z2x * zlog[g] * zlog[g];
             lc = lc + lx * ucn[g];
             q[4 + g] = q[4 + g] + lx * c[g];
             q[8] = q[8] + lzlog;
-            q[6 + g] = q[6 + g] + lzlog / c[g];
-            lc = lc - lzlog * ucnz[g] / (c[g] * c[g]);
+            q[6 + g] = q[6 + g] + lzlog * rc[g];
+            lc = lc - lzlog * ucnz[g] * (rc[g] * rc[g]);
           }
-          q[2 + g] = q[2 + g] + lc * dsin(S.TH[k] - usdirp[g]);
+          q[2 + g] = q[2 + g] + lc * (sk * cu_[g] - ck * su_[g]);  // sin(TH - USDIRP)
         }
         LAM[b] = LAM[b] + lf;
       }
@@ -728,10 +753,14 @@ template <typename R> struct AdjW {
     imphftail_adj(mij2);
     R lus2 = 0, lz02 = 0, lfmx = 0;
     update_adj(lus2, lfmx);
+    phase();
     const R lak = snonlin_adj();
+    phase();
     sdissip_adj();
+    phase();
     stresso_adj(1, w.F, us2, z02, lTAUW, lus2, lz02);
     sinput_adj(1, w.F, us2, z02, w.SF, lus2, lz02);
+    phase();
     imphftail_adj(mij);
     reload_f0();
     const adj::Jac2<R> J2 = airsea_jac(s.U10, tauw1);
@@ -739,7 +768,9 @@ template <typename R> struct AdjW {
     const R ltauw1 = J2.d01 * lus2 + J2.d11 * lz02;
     R lus1 = 0, lz01 = 0;
     stresso_adj(0, w.F, us1, z01, ltauw1, lus1, lz01);
+    phase();
     sinput_adj(0, w.F, us1, z01, nullptr, lus1, lz01);
+    phase();
     R lfmean = 0, lfmeanws = 0;
     if (fmeanws < fmean) lfmean = lfmx; else lfmeanws = lfmx;
     integrals_adj(w.F, nullptr, lfmean, lak, T.shallow && T.isnonlin == 0);
