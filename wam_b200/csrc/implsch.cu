@@ -20,13 +20,16 @@ __device__ __forceinline__ void implsch_cta(const DevTables<R>& T, const ImplArg
   const int ij0 = blk * P;
   // stage the P spectra: consecutive threads take consecutive points of one bin
   for (int idx = tid; idx < P * NS; idx += nthr) {
-    int p = idx % P, b = idx / P, ij = ij0 + p;
+    int p = idx % P, b = idx / P, ij = min(ij0 + p, a.nsea - 1);
     int m = b / KL, k = b - m * KL;
-    if (ij < a.nsea) reinterpret_cast<R*>(ws0 + p * wsb + foff)[k + LD * m] = a.fl3_in[ij + (size_t)a.ld * b];
+    reinterpret_cast<R*>(ws0 + p * wsb + foff)[k + LD * m] = a.fl3_in[ij + (size_t)a.ld * b];
   }
   __syncthreads();
-  const int warp = tid >> 5, lane = tid & 31, ij = ij0 + warp;
-  if (ij < a.nsea) {
+  // every warp runs the step (its phases end in CTA barriers); a warp past the
+  // last sea point repeats the last point and writes nothing
+  const int warp = tid >> 5, lane = tid & 31, ij = min(ij0 + warp, a.nsea - 1);
+  const bool real = ij0 + warp < a.nsea;
+  {
     STabs<R> S;
     S.bind(sR, sI, T.lay);
     WarpWS<R> w;
@@ -43,7 +46,7 @@ __device__ __forceinline__ void implsch_cta(const DevTables<R>& T, const ImplArg
     PointState<R> ps;
     ps.TAUW = a.tauw[ij];
     src.run(ps);
-    if (lane == 0) {
+    if (lane == 0 && real) {
       a.tauw[ij] = ps.TAUW; a.ustar[ij] = ps.USTAR; a.z0[ij] = ps.Z0;
       if (T.lcflx && a.fluxes)
         for (int q = 0; q < 7; ++q) a.fluxes[ij + (size_t)a.flx_ld * q] = ps.flx[q];

@@ -761,6 +761,11 @@ template <typename R> struct Src {
   }
 
   // ---- the whole IMPLSCH step for this point --------------------------------
+  // Every warp of the CTA runs the step (a warp past the last sea point
+  // repeats the last point), and the warps pass the phases together: the
+  // step's code is much larger than the instruction cache, and warps in
+  // different phases would keep evicting each other's code.
+  __device__ static void phase() { __syncthreads(); }
   __device__ void run(PointState<R>& ps) const {
     const int kl = KL(), ml = ML(), ld = w.ld;
     R TAUW = ps.TAUW, USTAR, Z0;
@@ -771,12 +776,13 @@ template <typename R> struct Src {
     else airsea(TAUW, USTAR, Z0);
     if (T.iphys == 1) sinput_ard(USTAR, Z0);
     else sinput_st6(USTAR, TAUW);
+    phase();
     integrals(w.LL, emeanws, fmeanws, nullptr);
     int mij = (T.iphys == 2) ? frcutindex_st6(fmean, USTAR) : frcutindex(fmean, fmeanws, USTAR);
     if (T.iphys == 2) { w3flx4(USTAR, Z0); }
     else { stresso_sums(USTAR, Z0, mij, TAUW, phiaw); airsea(TAUW, USTAR, Z0); }
     imphftail(mij);
-    if (T.iphys == 1) sinput_ard(USTAR, Z0);
+    if (T.iphys == 1) { sinput_ard(USTAR, Z0); phase(); }
     if (T.iphys == 1) stresso_sums(USTAR, Z0, mij, TAUW, phiaw);
     else if (T.lcflx) { R td; stresso_sp(USTAR, Z0, mij, td, phiaw); }
     if (T.lcflx) {  // SMIN = SL - SPOS, kept in SP from here on
@@ -785,7 +791,9 @@ template <typename R> struct Src {
     }
     if (T.iphys == 1) sdissip_ard();
     else sdissip_st6();
+    phase();
     snonlin(akmean);
+    phase();
     // SBOTTOM factor per frequency (scratch 6); SL_BOT = SBO*F is formed on the fly
     R* SBO = w.t(6);
     if (T.shallow) {
