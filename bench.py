@@ -49,6 +49,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
+    p.add_argument("--only", choices=["batched", "adjoint"], default=None,
+                   help="run only the batched-ensemble or the adjoint-window section and print its object "
+                        "(for profiling those kernels; not a bench line)")
     return p.parse_args()
 
 
@@ -239,7 +242,7 @@ def batched_ensemble(dev, steps, warmup, n_members=32):
     return out
 
 
-def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242):
+def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242, scale=1.0):
     """Adjoint of one assimilation window on the 400x300 regional grid
     (KL=36, ML=30, ST4, IDELPRO=120 s, IDELT=600 s), FP32.
 
@@ -255,7 +258,8 @@ def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242):
     from wam_b200 import WamModel
     from wam_b200.adjoint import WamPass, significant_wave_height, window_cost_and_grad
     from wam_b200.synth import make_workload
-    w = make_workload("c2", device=dev.index)
+    w = make_workload("c2", scale=scale, device=dev.index)
+    n_obs = min(n_obs, w.nsea)
     m = WamModel(w.cfg)
     m.set_grid(w.grid)
     m.set_depth(w.depth)
@@ -315,11 +319,13 @@ def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242):
     ms_adj = e1.elapsed_time(e2) / passes
     finite = bool(torch.isfinite(fs.grad).all()) and all(bool(torch.isfinite(u.grad).all()) for u in us)
     bins = w.nsea * w.cfg["kl"] * w.cfg["ml"]
-    out = {"workload": f"c2: 400x300 regional, {w.nsea} sea points, ST4, KL=36 ML=30, IDELPRO=120 s IDELT=600 s, "
+    grid = "400x300 regional" if scale == 1.0 else f"400x300 regional recipe at scale {scale}"
+    out = {"workload": f"c2: {grid}, {w.nsea} sea points, ST4, KL=36 ML=30, IDELPRO=120 s IDELT=600 s, "
                        f"{passes}-pass window, {n_obs} Hs observations",
            "value": bins / (ms_adj / 1e3), "unit": UNIT + " (adjoint pass)", "ms_per_adjoint_pass": ms_adj,
            "ms_per_forward_pass": ms_plain, "ms_per_checkpointed_forward_pass": ms_fwd,
-           "adjoint_over_forward": ms_adj / ms_plain, "counter": counter, "cost": float(J), "gradients_finite": finite,
+           "adjoint_over_forward": ms_adj / ms_plain, "counter": counter, "cost": float(J.detach()),
+           "gradients_finite": finite,
            "checkpoint_bytes": passes * bins * 4,
            "how": "backward sweep = per pass wamgpu_implsch_adj_dev (recomputes IMPLSCH from its checkpoint) + "
                   "IDELT/IDELPRO x wamgpu_propags_adj_dev; forward = wamgpu_step_dev"}
@@ -341,6 +347,14 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
+    if args.only:
+        dev = torch.device("cuda", local)
+        if args.only == "batched":
+            out = batched_ensemble(dev, max(3, min(args.steps, 10)), max(3, args.warmup))
+        else:
+            out = adjoint_window(dev, max(3, args.warmup), scale=args.scale)
+        print(json.dumps({"section": args.only, **out}), flush=True)
+        return
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
