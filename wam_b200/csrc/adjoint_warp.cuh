@@ -133,7 +133,7 @@ template <typename R> struct AdjW {
     const R2 v = w.SF[p];
     R sl = v.x, fl = v.y;
     if (T.shallow) { sl = sl + w.t(6)[m] * f0; fl = fl + w.t(6)[m]; }
-    const R t1 = T.DELT * sl / dmax(R(1.), R(1.) - T.DELT * fl);
+    const R t1 = fdiv(T.DELT * sl, dmax(R(1.), R(1.) - T.DELT * fl));
     const R t3 = dmin(dabs(t1), w.t(3)[m]);
     const R f = f0 + ((t1 >= R(0)) ? t3 : -t3);
     return dmax(f, w.t(4)[m] * w.t(2)[k]);
@@ -240,7 +240,8 @@ template <typename R> struct AdjW {
       R sl = v.x, fl = v.y;
       if (T.shallow) { sl = sl + SBO[m] * f0; fl = fl + SBO[m]; }
       const R den_raw = R(1.) - delt * fl, den = dmax(R(1.), den_raw);
-      const R t1 = delt * sl / den, at1 = dabs(t1), lim = LIM[m];
+      const R rden = fdiv(R(1.), den);  // den >= 1
+      const R t1 = fdiv(delt * sl, den), at1 = dabs(t1), lim = LIM[m];
       const R t3 = dmin(at1, lim);
       const R f = f0 + ((t1 >= R(0)) ? t3 : -t3);
       const R lf = (f < FMIN[m] * C2[k]) ? R(0) : LAM[p];  // the floor holds when it is selected
@@ -248,8 +249,8 @@ template <typename R> struct AdjW {
       const R lt3 = (t1 >= R(0)) ? lf : -lf;
       if (lim < at1) { aus = aus + lt3 * S.DELFL[m] * fmx; afmx = afmx + lt3 * us2 * S.DELFL[m]; }
       else lt1 = (t1 < R(0)) ? -lt3 : lt3;
-      const R lsl = lt1 * delt / den;
-      const R lfl = (R(1.) < den_raw) ? lt1 * t1 / den * delt : R(0);
+      const R lsl = lt1 * delt * rden;
+      const R lfl = (R(1.) < den_raw) ? lt1 * t1 * rden * delt : R(0);
       if (T.shallow) lf0 = lf0 + SBO[m] * lsl;
       LAM[p] = lf0;
       w.SF[p] = r2(lsl, lfl);

@@ -31,6 +31,12 @@ __device__ __forceinline__ double datan2(double y, double x) { return atan2(y, x
 __device__ __forceinline__ float dabs(float x) { return fabsf(x); }
 __device__ __forceinline__ double dabs(double x) { return fabs(x); }
 // Fortran MAX/MIN semantics for ordered operands
+// a / b through the hardware reciprocal path for FP32 (at most 2 ulp,
+// |b| in [2^-126, 2^126]); the precise division for FP64.  Used where the
+// divisor is bounded, as max(1, ...) is.
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+
 template <typename R> __device__ __forceinline__ R dmax(R a, R b) { return a < b ? b : a; }
 template <typename R> __device__ __forceinline__ R dmin(R a, R b) { return b < a ? b : a; }
 

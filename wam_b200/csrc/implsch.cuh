@@ -406,9 +406,12 @@ template <typename R> struct Src {
     }
     __syncwarp();
     const R base = t[mij - 1];
+    __syncwarp();
+    for (int m = mij + lane; m < ml; m += 32) t[m] = t[m] / base;  // ratio of row m to row mij-1
+    __syncwarp();
     for_bins(ml - mij, [&](int dm, int k) {
       const int m = mij + dm;
-      w.F[k + ld * m] = (t[m] / base) * w.F[k + ld * (mij - 1)];
+      w.F[k + ld * m] = t[m] * w.F[k + ld * (mij - 1)];
     });
     __syncwarp();
   }
@@ -598,13 +601,17 @@ template <typename R> struct Src {
     }
     __syncwarp();
     // growth rates per bin: D1 in SF.x, D2 in SF.y
+    // Only one of W1 (proj > 0) and W2 (proj < 0) is nonzero, and the other
+    // term is +0 whatever its tanh, so one tanh per bin gives the same D1, D2.
     for_bins(nk, [&](int m, int k) {
       R sig = P_::ZPI * S.FR[m], sqb = SQB[m];
       R proj = uproxy * CI10[m] * (S.COSTH[k] * cu + S.SINTH[k] * su) - R(1.);
       R w1 = dmax(R(0.), proj); w1 = w1 * w1;
       R w2 = dmin(R(0.), proj); w2 = w2 * w2;
-      R d1 = raw * sig * (R(2.8) - (R(1.) + dtanh(R(10.) * sqb * w1 - R(11.)))) * sqb * w1;
-      R d2 = raw * sig * R(0.09) * (R(2.8) - (R(1.) + dtanh(R(10.) * sqb * w2 - R(11.)))) * sqb * w2;
+      const bool up = proj > R(0.);
+      const R g = R(2.8) - (R(1.) + dtanh(R(10.) * sqb * (up ? w1 : w2) - R(11.)));
+      R d1 = up ? raw * sig * g * sqb * w1 : R(0.);
+      R d2 = up ? R(0.) : raw * sig * R(0.09) * g * sqb * w2;
       w.SF[k + ld * m] = r2(d1, d2);
     });
     __syncwarp();
@@ -845,7 +852,7 @@ template <typename R> struct Src {
       const R2 v = w.SF[p];
       R sl = v.x, fl = v.y;
       if (T.shallow) { sl = sl + SBO[m] * f0; fl = fl + SBO[m]; }
-      R t1 = delt * sl / dmax(R(1.), R(1.) - delt * fl);
+      R t1 = fdiv(delt * sl, dmax(R(1.), R(1.) - delt * fl));  // divisor >= 1
       R t3 = dmin(dabs(t1), LIM[m]);
       R f = f0 + ((t1 >= R(0)) ? t3 : -t3);
       w.F[p] = dmax(f, FMIN[m] * C2[k]);
