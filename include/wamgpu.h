@@ -273,6 +273,31 @@ WAMGPU_API int wamgpu_implsch_adj_dev(wamgpu_ctx* ctx, const void* fl3_in, int l
                                       void* lam_fl3, void* lam_tauw, void* lam_u10, void* stream);
 WAMGPU_API int wamgpu_propags_adj_dev(wamgpu_ctx* ctx, void* lam_f3, int ld, void* scratch, void* stream);
 
+/* Checkpointed assimilation windows, built on the derivative entry points
+ * (no reference counterpart).  A window of source steps runs forward with
+ * wamgpu_step_ckpt_dev, one checkpoint slot per step, and backward with
+ * wamgpu_step_adj_dev over the slots in reverse order; the driver adds its
+ * observation terms to lam_fl3 between steps.
+ *  - wamgpu_checkpoint_reserve keeps room on the device for n checkpoints of
+ *    spectra with leading dimension ld (n = 0 releases it).  A checkpoint is
+ *    the spectrum entering IMPLSCH, and TAUW and U10 before it:
+ *    ld*KL*ML + 2*NSEA values.
+ *  - wamgpu_step_ckpt_dev is wamgpu_step_dev (WAMODEL's PROP/PHYSICS pass,
+ *    wamodel.f90:286-360) that also stores checkpoint `slot`.
+ *  - wamgpu_step_adj_dev is the adjoint of that step: wamgpu_implsch_adj_dev
+ *    at the checkpoint, then nprop x wamgpu_propags_adj_dev.  lam_fl3 and
+ *    lam_tauw map in place from the step's output to its input; lam_u10
+ *    receives the adjoint of the step's U10.  scratch as for
+ *    wamgpu_propags_adj_dev.
+ * ld must be the one given to wamgpu_checkpoint_reserve. */
+WAMGPU_API int wamgpu_checkpoint_reserve(wamgpu_ctx* ctx, int n, int ld);
+WAMGPU_API int wamgpu_step_ckpt_dev(wamgpu_ctx* ctx, int slot, void* fl3, int ld, void* scratch, int nprop,
+                                    const void* u10, const void* udir, void* tauw, void* ustar, void* z0,
+                                    const void* roairn, const void* wstar, void* stream);
+WAMGPU_API int wamgpu_step_adj_dev(wamgpu_ctx* ctx, int slot, int nprop, void* lam_fl3, int ld, void* lam_tauw,
+                                   void* lam_u10, const void* udir, const void* roairn, const void* wstar,
+                                   void* scratch, void* stream);
+
 /* Synchronises the context stream; returns WAMGPU_E_NUMERIC if a kernel
  * reported non-finite output since the last call. */
 WAMGPU_API int wamgpu_sync(wamgpu_ctx* ctx);

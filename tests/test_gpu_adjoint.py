@@ -222,3 +222,56 @@ def test_window_gradient_matches_finite_differences(name, scale, passes):
     ad = float((gf * dF).sum() + (gt * dT).sum() + sum((a * b).sum() for a, b in zip(gu, dU)))
     assert abs(fd - ad) <= 1e-5 * abs(ad), (fd, ad)
     m.close()
+
+
+def test_checkpointed_window_through_the_c_abi_matches_autograd():
+    """wamgpu_step_ckpt_dev forward and wamgpu_step_adj_dev backward, with the
+    Hs misfit's adjoint added between steps, give the autograd harness's
+    gradients (FP64)."""
+    torch, dev = _torch()
+    from wam_b200._lib import WamgpuError
+    from wam_b200.adjoint import significant_wave_height, window_cost_and_grad
+    w, m, st, nprop = _spun_up("c0", 0.2, 8)
+    n, passes = w.nsea, 3
+    gen = torch.Generator(device=dev).manual_seed(5)
+    points = torch.randperm(n, generator=gen, device=dev)[: max(4, n // 8)]
+    us = [st["u10"] * (1.0 + 0.04 * p) for p in range(passes)]
+    dfim = torch.tensor(m.table("DFIM"), device=dev, dtype=torch.float64)
+    hs_obs = [None] * passes
+    J, gf, gt, gu = None, None, None, None
+    # observations: 5 % above a plain forward run
+    f, tw = st["f"].clone(), st["tauw"].clone()
+    ustar, z0, sc = torch.empty_like(tw), torch.empty_like(tw), torch.empty_like(f)
+    for p in range(passes):
+        m.step_dev(f, nprop, us[p], st["udir"], tw, ustar, z0, st["roairn"], st["wstar"], scratch=sc, stream=_s())
+        hs_obs[p] = 1.05 * significant_wave_height(f, dfim, points)
+    J, gf, gt, gu = window_cost_and_grad(m, st["f"], st["tauw"], us, st["udir"], st["roairn"], st["wstar"], points,
+                                         hs_obs, nprop)
+    # the same window through the checkpoint entry points
+    ld = st["f"].shape[-1]
+    m.checkpoint_reserve(passes, ld)
+    f, tw = st["f"].clone(), st["tauw"].clone()
+    hs = []
+    for p in range(passes):
+        m.step_ckpt_dev(p, f, nprop, us[p], st["udir"], tw, ustar, z0, st["roairn"], st["wstar"], scratch=sc, stream=_s())
+        hs.append(significant_wave_height(f, dfim, points))
+    J2 = sum(float(((h - o) ** 2).sum()) for h, o in zip(hs, hs_obs))
+    lam_f, lam_t = torch.zeros_like(st["f"]), torch.zeros_like(st["tauw"])
+    lam_u = [torch.empty_like(st["u10"]) for _ in range(passes)]
+    for p in reversed(range(passes)):
+        g = 16.0 * (hs[p] - hs_obs[p]) / hs[p]  # dJ/dE at the observed points, E = sum DFIM sum F
+        lam_f[:, :, points] += dfim[:, None, None] * g[None, None, :]
+        m.step_adj_dev(p, nprop, lam_f, lam_t, lam_u[p], st["udir"], st["roairn"], st["wstar"], scratch=sc, stream=_s())
+    torch.cuda.synchronize()
+    assert abs(J2 - float(J)) <= 1e-12 * float(J)
+    rel = lambda a, b: float((a - b).abs().max() / b.abs().max())
+    assert rel(lam_f, gf) < 1e-10 and rel(lam_t, gt) < 1e-10, (rel(lam_f, gf), rel(lam_t, gt))
+    for a, b in zip(lam_u, gu):
+        assert rel(a, b) < 1e-10
+    # slots and leading dimension are checked
+    with pytest.raises(WamgpuError, match="slot"):
+        m.step_adj_dev(passes, nprop, lam_f, lam_t, lam_u[0], st["udir"], st["roairn"], st["wstar"], stream=_s())
+    with pytest.raises(WamgpuError, match="ld differs"):
+        m.step_adj_dev(0, nprop, lam_f, lam_t, lam_u[0], st["udir"], st["roairn"], st["wstar"], ld=ld + 1, stream=_s())
+    m.checkpoint_reserve(0, ld)
+    m.close()

@@ -52,6 +52,9 @@ SIGNATURES = {
     "wamgpu_implsch_adj_dev": (c_int, [c_void_p] + [c_void_p, c_int] + [c_void_p] * 9),
     "wamgpu_implsch_tl_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_int] + [c_void_p] * 12),
     "wamgpu_propags_adj_dev": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "wamgpu_checkpoint_reserve": (c_int, [c_void_p, c_int, c_int]),
+    "wamgpu_step_ckpt_dev": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_int] + [c_void_p] * 8),
+    "wamgpu_step_adj_dev": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int] + [c_void_p] * 7),
     "wamgpu_propags_substep_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "wamgpu_batch_create": (c_int, [ctypes.POINTER(c_void_p), c_int, ctypes.POINTER(c_void_p)]),
     "wamgpu_batch_destroy": (c_int, [c_void_p]),

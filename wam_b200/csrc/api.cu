@@ -82,6 +82,8 @@ template <typename R> struct Impl : ImplBase {
   PropArgs<R> pa{};
   bool has_enh = false;  // MAKE_SHALLOW_SNL factors uploaded to `enh` ([ij + nsea*(mc-1)])
   DevBuf dwork, dmasks;  // work of the derivative kernels
+  DevBuf ckpt;           // checkpoints of an assimilation window
+  int nckpt = 0, ckpt_ld = 0;
   DevBuf small, ismall, tfak, tcgond, tsihkd, flminfr, enh, gom, fr, sinth, costh;
   // per-point metadata
   DevBuf d_klat, d_klon, d_wlat, d_dpsn, d_della0, d_drgm, d_indep, d_indep_g, d_ddphi, d_ddlam, d_duphi, d_dulam,
@@ -649,6 +651,77 @@ template <typename R> int propags_adj_t(wamgpu_ctx* ctx, Impl<R>& I, void* lam, 
     std::swap(src, dst);
   }
   if (src != (R*)lam) CK(cudaMemcpyAsync(lam, src, bytes, cudaMemcpyDeviceToDevice, s), "copy adjoint");
+  return WAMGPU_OK;
+}
+
+// ---- checkpointed assimilation windows ------------------------------------------
+
+// Slot q of the checkpoint store: the spectrum entering IMPLSCH (pitch
+// ckpt_ld), then TAUW before IMPLSCH and U10 (NSEA values each).
+template <typename R> R* ckpt_slot(const wamgpu_ctx* ctx, Impl<R>& I, int q) {
+  const size_t per = (size_t)I.ckpt_ld * ctx->cfg.kl * ctx->cfg.ml + 2 * (size_t)ctx->nsea;
+  return I.ckpt.template as<R>() + per * q;
+}
+
+template <typename R> int checkpoint_reserve_t(wamgpu_ctx* ctx, Impl<R>& I, int n, int ld) {
+  if (n < 0) return fail(ctx, WAMGPU_E_ARG, "negative number of checkpoints");
+  if (n == 0) { I.ckpt = DevBuf(); I.nckpt = 0; I.ckpt_ld = 0; return WAMGPU_OK; }
+  if (!ctx->have_grid) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_set_grid first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  const size_t per = (size_t)ld * ctx->cfg.kl * ctx->cfg.ml + 2 * (size_t)ctx->nsea;
+  CK(I.ckpt.ensure(per * n * sizeof(R)), "alloc checkpoints");
+  I.nckpt = n; I.ckpt_ld = ld;
+  return WAMGPU_OK;
+}
+
+template <typename R> int ckpt_check(wamgpu_ctx* ctx, Impl<R>& I, int slot, int ld, int nprop) {
+  if (slot < 0 || slot >= I.nckpt) return fail(ctx, WAMGPU_E_ARG, "checkpoint slot outside wamgpu_checkpoint_reserve's range");
+  if (ld != I.ckpt_ld) return fail(ctx, WAMGPU_E_ARG, "ld differs from the ld given to wamgpu_checkpoint_reserve");
+  if (nprop < 0) return fail(ctx, WAMGPU_E_ARG, "nprop < 0");
+  return WAMGPU_OK;
+}
+
+// wamgpu_step_dev that also stores checkpoint `slot`.
+template <typename R>
+int step_ckpt_dev_t(wamgpu_ctx* ctx, Impl<R>& I, int slot, void* f3v, int ld, void* scratch, int nprop, const void* u10,
+                    const void* udir, void* tauw, void* ustar, void* z0, const void* roairn, const void* wstar,
+                    cudaStream_t s) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
+  int rc = ckpt_check(ctx, I, slot, ld, nprop);
+  if (rc) return rc;
+  R* f3 = (R*)f3v;
+  const size_t nb = (size_t)ctx->cfg.kl * ctx->cfg.ml, bytes = (size_t)ld * nb * sizeof(R);
+  R* sc = (R*)scratch;
+  if (!sc) { CK(I.scratch.ensure(bytes), "alloc scratch"); sc = I.scratch.template as<R>(); }
+  R* src = f3; R* dst = sc;
+  for (int it = 0; it < nprop * ctx->counter; ++it) {
+    { TimedLaunch tl(ctx, 0, s); CK(launch_propags<R>(I.pa, src, ld, dst, ld, s), "propags launch"); }
+    std::swap(src, dst);
+  }
+  R* c = ckpt_slot(ctx, I, slot);
+  const size_t n = (size_t)ctx->nsea;
+  CK(cudaMemcpyAsync(c, src, bytes, cudaMemcpyDeviceToDevice, s), "checkpoint spectrum");
+  CK(cudaMemcpyAsync(c + (size_t)ld * nb, tauw, n * sizeof(R), cudaMemcpyDeviceToDevice, s), "checkpoint TAUW");
+  CK(cudaMemcpyAsync(c + (size_t)ld * nb + n, u10, n * sizeof(R), cudaMemcpyDeviceToDevice, s), "checkpoint U10");
+  return implsch_dev_t<R>(ctx, I, f3, ld, u10, udir, tauw, ustar, z0, roairn, wstar, s, src);
+}
+
+// The adjoint of the step stored in `slot`: IMPLSCH's adjoint at the
+// checkpoint, then the transposes of the step's nprop PROPAGS calls.
+template <typename R>
+int step_adj_dev_t(wamgpu_ctx* ctx, Impl<R>& I, int slot, int nprop, void* lam_fl3, int ld, void* lam_tauw, void* lam_u10,
+                   const void* udir, const void* roairn, const void* wstar, void* scratch, cudaStream_t s) {
+  int rc = ckpt_check(ctx, I, slot, ld, nprop);
+  if (rc) return rc;
+  const R* c = ckpt_slot(ctx, I, slot);
+  const size_t nb = (size_t)ctx->cfg.kl * ctx->cfg.ml;
+  rc = implsch_adj_t<R>(ctx, I, c, ld, c + (size_t)ld * nb, c + (size_t)ld * nb + ctx->nsea, udir, roairn, wstar, lam_fl3,
+                        lam_tauw, lam_u10, s);
+  if (rc) return rc;
+  for (int q = 0; q < nprop; ++q) {
+    rc = propags_adj_t<R>(ctx, I, lam_fl3, ld, scratch, s);
+    if (rc) return rc;
+  }
   return WAMGPU_OK;
 }
 
@@ -1585,6 +1658,28 @@ int wamgpu_propags_adj_dev(wamgpu_ctx* ctx, void* lam_f3, int ld, void* scratch,
   if (!ctx || !ctx->impl || !lam_f3) return WAMGPU_E_ARG;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   return DISPATCH_CTX(ctx, propags_adj_t, lam_f3, ld, scratch, s);
+}
+
+int wamgpu_checkpoint_reserve(wamgpu_ctx* ctx, int n, int ld) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  return DISPATCH_CTX(ctx, checkpoint_reserve_t, n, ld);
+}
+
+int wamgpu_step_ckpt_dev(wamgpu_ctx* ctx, int slot, void* fl3, int ld, void* scratch, int nprop, const void* u10,
+                         const void* udir, void* tauw, void* ustar, void* z0, const void* roairn, const void* wstar,
+                         void* stream) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!fl3 || !u10 || !udir || !tauw || !ustar || !z0 || !roairn || !wstar) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, step_ckpt_dev_t, slot, fl3, ld, scratch, nprop, u10, udir, tauw, ustar, z0, roairn, wstar, s);
+}
+
+int wamgpu_step_adj_dev(wamgpu_ctx* ctx, int slot, int nprop, void* lam_fl3, int ld, void* lam_tauw, void* lam_u10,
+                        const void* udir, const void* roairn, const void* wstar, void* scratch, void* stream) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  if (!lam_fl3 || !lam_tauw || !lam_u10 || !udir || !roairn || !wstar) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, step_adj_dev_t, slot, nprop, lam_fl3, ld, lam_tauw, lam_u10, udir, roairn, wstar, scratch, s);
 }
 
 }  // extern "C"

@@ -258,6 +258,31 @@ class WamModel:
         sc = None if scratch is None else ctypes.c_void_p(scratch.data_ptr())
         self._check(self.L.wamgpu_propags_adj_dev(self.h, lam.data_ptr(), ld, sc, s), "propags_adj_dev")
 
+    # ---- checkpointed assimilation windows --------------------------------------
+    def checkpoint_reserve(self, n, ld):
+        """Room for n checkpoints of spectra with leading dimension ld (0 releases)."""
+        self._check(self.L.wamgpu_checkpoint_reserve(self.h, int(n), int(ld)), "checkpoint_reserve")
+
+    def step_ckpt_dev(self, slot, fl3, nprop, u10, udir, tauw, ustar, z0, roairn, wstar, scratch=None, ld=None,
+                      stream=None):
+        """step_dev that also stores checkpoint `slot` (IMPLSCH's input spectrum, TAUW, U10)."""
+        ld = fl3.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        sc = None if scratch is None else ctypes.c_void_p(scratch.data_ptr())
+        p = lambda t: t.data_ptr()
+        self._check(self.L.wamgpu_step_ckpt_dev(self.h, int(slot), p(fl3), ld, sc, int(nprop), p(u10), p(udir), p(tauw),
+                                                p(ustar), p(z0), p(roairn), p(wstar), s), "step_ckpt_dev")
+
+    def step_adj_dev(self, slot, nprop, lam_fl3, lam_tauw, lam_u10, udir, roairn, wstar, scratch=None, ld=None,
+                     stream=None):
+        """Adjoint of the step stored in `slot`: lam_fl3, lam_tauw in place; lam_u10 written."""
+        ld = lam_fl3.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        sc = None if scratch is None else ctypes.c_void_p(scratch.data_ptr())
+        p = lambda t: t.data_ptr()
+        self._check(self.L.wamgpu_step_adj_dev(self.h, int(slot), int(nprop), p(lam_fl3), ld, p(lam_tauw), p(lam_u10),
+                                               p(udir), p(roairn), p(wstar), sc, s), "step_adj_dev")
+
     def set_timing(self, enable=True):
         self._check(self.L.wamgpu_set_timing(self.h, int(enable)), "set_timing")
 
