@@ -2,7 +2,8 @@
 // arrays in shared memory.
 //
 // The forward pass is recomputed inside the step with the forward kernel's own
-// lane-parallel routines (Src), recording what the reverse sweep needs: the
+// lane-parallel routines (Src; SINPUT_ARD in its tabled-direction form, which
+// the reverse sweep linearises), recording what the reverse sweep needs: the
 // cut-off indices, AIRSEA's outputs, SINPUT's sheltering sums and SPOS sums per
 // frequency, the first wind-sea mask and the source terms SL/FL.  The reverse
 // sweep then runs the routines backwards with the lanes spread over the
@@ -85,7 +86,7 @@ template <typename R> struct AdjW {
     s.integrals(nullptr, emean, fmean, need_ak ? &akmean : nullptr);
     s.airsea(TAUW0, us1, z01);
     s.shl = shl_rows(0);
-    s.sinput_ard(us1, z01);
+    s.template sinput_ard<true>(us1, z01);
     phase();
     s.for_bins(ml, [&](int m, int k) { LL1[k + ld * m] = w.LL[k + ld * m]; });
     for (int m = lane; m < ml; m += 32) { sx_row(0)[m] = w.t(1)[m]; sy_row(0)[m] = w.t(2)[m]; }
@@ -98,7 +99,7 @@ template <typename R> struct AdjW {
     s.imphftail(mij);  // F = F1 from here on
     phase();
     s.shl = shl_rows(1);
-    s.sinput_ard(us2, z02);
+    s.template sinput_ard<true>(us2, z02);
     s.shl = nullptr;
     phase();
     for (int m = lane; m < ml; m += 32) { sx_row(1)[m] = w.t(1)[m]; sy_row(1)[m] = w.t(2)[m]; }
@@ -567,7 +568,7 @@ template <typename R> struct AdjW {
       for (int g = 0; g < 2; ++g) {
         tpx[g] = taux[g] - shelter * xst[g]; tpy[g] = tauy[g] - shelter * yst[g];
         const R qq = tpx[g] * tpx[g] + tpy[g] * tpy[g];
-        ustp[g] = dpow(qq, R(0.25));
+        ustp[g] = dsqrt(dsqrt(qq));
         const R rn = qq > R(0) ? R(1) / dsqrt(qq) : R(0);
         cu_[g] = qq > R(0) ? tpy[g] * rn : R(1);
         su_[g] = tpx[g] * rn;
@@ -647,7 +648,7 @@ template <typename R> struct AdjW {
         const R qq = tpx[g] * tpx[g] + tpy[g] * tpy[g];
         R ltpx = 0, ltpy = 0;
         if (qq > R(0)) {
-          const R lq = lustp * R(0.25) * dpow(qq, R(-0.75));
+          const R lq = lustp * R(0.25) * (R(1) / (ustp[g] * ustp[g] * ustp[g]));  // d qq^(1/4) / d qq
           ltpx = lq * R(2) * tpx[g] + q[2 + g] * tpy[g] / qq;
           ltpy = lq * R(2) * tpy[g] - q[2 + g] * tpx[g] / qq;
         }

@@ -209,7 +209,12 @@ template <typename R> struct Src {
   // SINPUT_ARD: writes SL, FL, LL (and SP when kept) plus the per-frequency
   // sums of SPOS, SPOS*SIN, SPOS*COS that STRESSO integrates (scratch 0..2).
   // Sequential over frequency because of sheltering.
-  __device__ void sinput_ard(R USTAR, R Z0) const {
+  // TAB = false is the reference's statement order (the forward step).  TAB =
+  // true is the form the adjoint recomputes and linearises: the stress
+  // direction's cosine and sine come from the stress components, COS(TH(K) -
+  // USDIRP) from the direction tables, and (TPX^2+TPY^2)^(1/4) from two square
+  // roots; it agrees with the reference form to a few ulp.
+  template <bool TAB = false> __device__ void sinput_ard(R USTAR, R Z0) const {
     const int kl = KL(), ml = ML(), ld = w.ld;
     const R SWELLF = R(0.66), FU = R(0.022), FUD = R(-0.018), SWELLF4 = R(1.5E05), SWELLF5 = R(1.2), SWELLF7 = R(3.6E05);
     const R rog = P_::ROWATER * P_::G;
@@ -250,11 +255,21 @@ template <typename R> struct Src {
       R xk, cm;
       if (T.shallow) { xk = tfak(m); cm = xk * (R(1.0) / sig); }
       else { cm = sig / P_::G; xk = sig2 / P_::G; }
-      R ustp[2], usdirp[2], ucn[2], ucnz[2];
+      R ustp[2], usdirp[2], cu_[2], su_[2], ucn[2], ucnz[2];
       for (int g = 0; g < 2; ++g) {
         R tpx = taux[g] - shelter * xst[g], tpy = tauy[g] - shelter * yst[g];
-        ustp[g] = dpow(tpx * tpx + tpy * tpy, R(0.25));
-        usdirp[g] = datan2(tpx, tpy);
+        if constexpr (TAB) {
+          const R qq = tpx * tpx + tpy * tpy;
+          ustp[g] = dsqrt(dsqrt(qq));
+          const R rn = qq > R(0) ? R(1) / dsqrt(qq) : R(0);
+          cu_[g] = qq > R(0) ? tpy * rn : R(1);
+          su_[g] = tpx * rn;
+          usdirp[g] = R(0);
+        } else {
+          ustp[g] = dpow(tpx * tpx + tpy * tpy, R(0.25));
+          usdirp[g] = datan2(tpx, tpy);
+          cu_[g] = su_[g] = R(0);
+        }
         ucn[g] = ustp[g] * cm;
         ucnz[g] = P_::XKAPPA / (ucn[g] + T.ZALP);
       }
@@ -270,10 +285,12 @@ template <typename R> struct Src {
         R slp[2], flp[2];
         uint8_t ll = 0;
         for (int g = 0; g < 2; ++g) {
-          R c = dcos(S.TH[k] - usdirp[g]);
+          R c;
+          if constexpr (TAB) c = S.COSTH[k] * cu_[g] + S.SINTH[k] * su_[g];
+          else c = dcos(S.TH[k] - usdirp[g]);
           R ufac = 0;
           if (c > R(0.01)) {
-            R x = c * ucn[g], zlog = zcn + ucnz[g] / c;
+            R x = c * ucn[g], zlog = zcn + (TAB ? ucnz[g] * (R(1) / c) : ucnz[g] / c);
             if (zlog < R(0.0)) { R z2x = zlog * zlog * x; ufac = dexp(zlog) * z2x * z2x; ll = 1; }
           }
           R dstab = dstab1 + pturb * (tmp1 * (temp2 + (FU + FUD * c) * ustp[g]));
