@@ -244,19 +244,22 @@ def batched_ensemble(dev, steps, warmup, n_members=32):
 
 def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242, scale=1.0):
     """Adjoint of one assimilation window on the 400x300 regional grid
-    (KL=36, ML=30, ST4, IDELPRO=120 s, IDELT=600 s), FP32.
+    (KL=36, ML=30, ST4, IDELPRO=120 s, IDELT=600 s), FP32, through the C ABI
+    an assimilation driver calls.
 
-    The forward sweep runs `passes` WAMODEL passes and keeps one checkpoint
-    per pass (the spectrum entering IMPLSCH).  The cost is the squared Hs
-    misfit at n_obs seeded sea points against a perturbed-truth run (U10
-    +10%) with Hs noise of sigma 0.2 m.  The backward sweep, the IMPLSCH
-    adjoint and the PROPAGS transpose of every pass, gives the gradient with
-    respect to the initial spectrum, the initial TAUW and each pass's U10.
-    Device times by CUDA events: the plain forward pass (wamgpu_step_dev),
-    the checkpointed forward sweep, and the backward sweep."""
+    The forward sweep runs `passes` WAMODEL passes with wamgpu_step_ckpt_dev,
+    one checkpoint per pass (the spectrum entering IMPLSCH, TAUW, U10).  The
+    cost is the squared Hs misfit at n_obs seeded sea points against a
+    perturbed-truth run (U10 +10%) with Hs noise of sigma 0.2 m.  The backward
+    sweep adds each pass's misfit adjoint at the observed points and runs
+    wamgpu_step_adj_dev (the IMPLSCH adjoint from the checkpoint, then the
+    PROPAGS transposes), giving the gradient with respect to the initial
+    spectrum, the initial TAUW and each pass's U10.  Device times by CUDA
+    events: the plain forward pass (wamgpu_step_dev), the checkpointed forward
+    sweep and the backward sweep."""
     import torch
     from wam_b200 import WamModel
-    from wam_b200.adjoint import WamPass, significant_wave_height, window_cost_and_grad
+    from wam_b200.adjoint import significant_wave_height
     from wam_b200.synth import make_workload
     w = make_workload("c2", scale=scale, device=dev.index)
     n_obs = min(n_obs, w.nsea)
@@ -267,6 +270,7 @@ def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242, scale=1.0):
     m.prepare_source()
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
+    sh = stream.cuda_stream
     t = lambda a: torch.tensor(np.asarray(a, np.float32), device=dev)
     f0 = w.spectrum_device(torch, dev)
     u10, udir, tauw, roairn, wstar = (t(a) for a in (w.u10, w.udir, w.tauw, w.roairn, w.wstar))
@@ -276,17 +280,19 @@ def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242, scale=1.0):
     gen = torch.Generator(device=dev).manual_seed(seed)
     points = torch.randperm(w.nsea, generator=gen, device=dev)[:n_obs]
     dfim = torch.tensor(m.table("DFIM"), device=dev, dtype=torch.float32)
-    with torch.no_grad():  # perturbed truth and observations
-        f, tw, obs = f0, tauw, []
-        for u in u_seq:
-            f, tw = WamPass.apply(f, tw, 1.1 * u, m, nprop, udir, roairn, wstar)
-            hs = significant_wave_height(f, dfim, points)
-            obs.append(hs + 0.2 * torch.randn(hs.shape, generator=gen, device=dev))
-    sh = stream.cuda_stream
+    sc = torch.empty_like(f0)
+    # perturbed truth and observations
+    f, tw, obs = f0.clone(), tauw.clone(), []
+    for u in u_seq:
+        m.step_dev(f, nprop, 1.1 * u, udir, tw, ustar, z0, roairn, wstar, scratch=sc, stream=sh)
+        hs = significant_wave_height(f, dfim, points)
+        obs.append(hs + 0.2 * torch.randn(hs.shape, generator=gen, device=dev))
+    ld = f0.shape[-1]
+    m.checkpoint_reserve(passes, ld)
     ev = lambda: torch.cuda.Event(enable_timing=True)
 
     def plain():
-        f, sc, tw = f0.clone(), torch.empty_like(f0), tauw.clone()
+        f, tw = f0.clone(), tauw.clone()
         torch.cuda.synchronize()
         e0, e1 = ev(), ev()
         e0.record(stream)
@@ -296,39 +302,47 @@ def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242, scale=1.0):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / passes
 
+    def window(np_):
+        """One window of np_ passes: (cost, gradients, forward ms, backward ms)."""
+        f, tw = f0.clone(), tauw.clone()
+        lam_f, lam_t = torch.zeros_like(f0), torch.zeros_like(tauw)
+        lam_u = [torch.empty_like(u10) for _ in range(np_)]
+        torch.cuda.synchronize()
+        e0, e1, e2 = ev(), ev(), ev()
+        e0.record(stream)
+        hs = []
+        for p in range(np_):
+            m.step_ckpt_dev(p, f, nprop, u_seq[p], udir, tw, ustar, z0, roairn, wstar, scratch=sc, stream=sh)
+            hs.append(significant_wave_height(f, dfim, points))
+        e1.record(stream)
+        for p in reversed(range(np_)):
+            # dJ/dF at the observed points: J = sum (Hs - obs)^2, Hs = 4 sqrt(E), E = sum DFIM sum F
+            g = 16.0 * (hs[p] - obs[p]) / hs[p]
+            lam_f[:, :, points] += dfim[:, None, None] * g[None, None, :]
+            m.step_adj_dev(p, nprop, lam_f, lam_t, lam_u[p], udir, roairn, wstar, scratch=sc, stream=sh)
+        e2.record(stream)
+        torch.cuda.synchronize()
+        J = sum(float(((h - o) ** 2).sum()) for h, o in zip(hs, obs))
+        return J, lam_f, lam_t, lam_u, e0.elapsed_time(e1) / np_, e1.elapsed_time(e2) / np_
+
     for _ in range(warmup):
         plain()
     ms_plain = plain()
-    # one short window as warm-up, then the timed window
-    window_cost_and_grad(m, f0, tauw, u_seq[:2], udir, roairn, wstar, points, obs, nprop)
-    torch.cuda.synchronize()
-    fs = f0.detach().clone().requires_grad_(True)
-    ts = tauw.detach().clone().requires_grad_(True)
-    us = [u.detach().clone().requires_grad_(True) for u in u_seq]
-    e0, e1, e2 = ev(), ev(), ev()
-    e0.record(stream)
-    f, tw, J = fs, ts, torch.zeros((), device=dev)
-    for p, u in enumerate(us):
-        f, tw = WamPass.apply(f, tw, u, m, nprop, udir, roairn, wstar)
-        J = J + ((significant_wave_height(f, dfim, points) - obs[p]) ** 2).sum()
-    e1.record(stream)
-    J.backward()
-    e2.record(stream)
-    torch.cuda.synchronize()
-    ms_fwd = e0.elapsed_time(e1) / passes
-    ms_adj = e1.elapsed_time(e2) / passes
-    finite = bool(torch.isfinite(fs.grad).all()) and all(bool(torch.isfinite(u.grad).all()) for u in us)
+    window(2)  # warm-up
+    J, lam_f, lam_t, lam_u, ms_fwd, ms_adj = window(passes)
+    finite = bool(torch.isfinite(lam_f).all()) and all(bool(torch.isfinite(u).all()) for u in lam_u)
     bins = w.nsea * w.cfg["kl"] * w.cfg["ml"]
     grid = "400x300 regional" if scale == 1.0 else f"400x300 regional recipe at scale {scale}"
     out = {"workload": f"c2: {grid}, {w.nsea} sea points, ST4, KL=36 ML=30, IDELPRO=120 s IDELT=600 s, "
                        f"{passes}-pass window, {n_obs} Hs observations",
            "value": bins / (ms_adj / 1e3), "unit": UNIT + " (adjoint pass)", "ms_per_adjoint_pass": ms_adj,
            "ms_per_forward_pass": ms_plain, "ms_per_checkpointed_forward_pass": ms_fwd,
-           "adjoint_over_forward": ms_adj / ms_plain, "counter": counter, "cost": float(J.detach()),
-           "gradients_finite": finite,
-           "checkpoint_bytes": passes * bins * 4,
-           "how": "backward sweep = per pass wamgpu_implsch_adj_dev (recomputes IMPLSCH from its checkpoint) + "
-                  "IDELT/IDELPRO x wamgpu_propags_adj_dev; forward = wamgpu_step_dev"}
+           "adjoint_over_forward": ms_adj / ms_plain, "counter": counter, "cost": J, "gradients_finite": finite,
+           "checkpoint_bytes": passes * (bins + 2 * w.nsea) * 4,
+           "how": "C ABI: forward = wamgpu_step_ckpt_dev per pass; backward = the misfit adjoint at the observed "
+                  "points, then wamgpu_step_adj_dev per pass (IMPLSCH adjoint recomputing the source terms from "
+                  "the checkpoint, then IDELT/IDELPRO PROPAGS transposes); plain forward = wamgpu_step_dev"}
+    m.checkpoint_reserve(0, ld)
     m.close()
     torch.cuda.set_stream(torch.cuda.default_stream(dev))
     return out

@@ -91,10 +91,11 @@ __global__ void __launch_bounds__(P * 32) implsch_adj_kernel(const __grid_consta
     if (lane == 0 && ij0 + warp < a.nsea) { a.lam_tauw[ij] = lT0; a.lam_u10[ij] = lU; }
   }
   __syncthreads();
+  R* lout = a.lam_out ? a.lam_out : a.lam_fl3;
   for (int idx = tid; idx < P * NS; idx += nthr) {
     const int p = idx % P, b = idx / P, ijs = ij0 + p;
     const int m = b / KL, k = b - m * KL;
-    if (ijs < a.nsea) a.lam_fl3[ijs + ld * b] = reinterpret_cast<R*>(ws0 + p * wsb + loff)[k + LD * m];
+    if (ijs < a.nsea) lout[ijs + ld * b] = reinterpret_cast<R*>(ws0 + p * wsb + loff)[k + LD * m];
   }
 }
 

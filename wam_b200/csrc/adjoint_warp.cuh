@@ -188,22 +188,24 @@ template <typename R> struct AdjW {
     adj::airsea(A, D(U10, hi ? R(0) : R(1)), D(TAUW, hi ? R(1) : R(0)), us, z0);
     return jac_split(us.d, z0.d);
   }
-  // d(TAUHF, PHIHF) / d(USTAR, Z0) of TAU_PHI_HF
-  __device__ adj::Jac2<R> tauphi_jac(int mj, R ustar, R z0) const {
+  // d(TAUHF, PHIHF) / d(USTAR, Z0) of TAU_PHI_HF, and TAUHF itself
+  __device__ adj::Jac2<R> tauphi_jac(int mj, R ustar, R z0, R& tauhf) const {
     using D = adj::Dual<R>;
     const bool hi = lane >= 16;
     D th, ph;
     adj::tau_phi_hf(A, mj, D(ustar, hi ? R(0) : R(1)), D(z0, hi ? R(1) : R(0)), th, ph);
+    tauhf = th.v;
     return jac_split(th.d, ph.d);
   }
-  // d(WSIGSTAR) / d(USTAR) and / d(Z0)
-  __device__ void wsig_grad(R ustar, R z0, R& dus, R& dz0) const {
+  // WSIGSTAR and its derivatives with respect to USTAR and Z0
+  __device__ R wsig_grad(R ustar, R z0, R& dus, R& dz0) const {
     using D = adj::Dual<R>;
     const bool hi = lane >= 16;
     const D v = adj::wsigstar(P, D(ustar, hi ? R(0) : R(1)), D(z0, hi ? R(1) : R(0)));
     const R o = __shfl_xor_sync(0xffffffffu, v.d, 16);
     dus = hi ? o : v.d;
     dz0 = hi ? v.d : o;
+    return v.v;
   }
 
   // IMPHFTAIL^T: rows m >= mij were copied from row mij-1 with a ratio.
@@ -476,8 +478,8 @@ template <typename R> struct AdjW {
       t1 = t1 + Fs[k + ld * (mij - 1)] * (cw * cw * cw);
     }
     t1 = warp_sum(t1);
-    R tau1, phi1;
-    s.tau_phi_hf(mij, US, Z0, tau1, phi1);
+    R tau1;
+    const adj::Jac2<R> J = tauphi_jac(mij, US, Z0, tau1);
     const R kc = cst * S.FR5[mij - 1] * gm1;
     const R tauhf = kc * t1 * tau1;
     const R su = dsin(s.UDIR), cu = dcos(s.UDIR);
@@ -495,7 +497,6 @@ template <typename R> struct AdjW {
       const R cw = dmax(dcos(S.TH[k] - s.UDIR), R(0.));
       LAM[k + ld * (mij - 1)] = LAM[k + ld * (mij - 1)] + lt1 * (cw * cw * cw);
     }
-    const adj::Jac2<R> J = tauphi_jac(mij, US, Z0);
     lUS = lUS + ltau1 * J.d00;
     lZ0 = lZ0 + ltau1 * J.d01;
     R *LSX = lsx_row(), *LSY = lsy_row();
@@ -519,8 +520,9 @@ template <typename R> struct AdjW {
     const R delabm1 = R(200) / (R(8.0) - R(0.3));
     const R shelter = dabs(T.TAUWSHELTER);
     const R ROAIRN = s.ROAIRN;
-    // per-point prologue (recomputed)
-    const R sig_n = s.wsigstar(US, Z0);
+    // per-point prologue (recomputed); WSIGSTAR with its derivatives
+    R dsig_us, dsig_z0;
+    const R sig_n = wsig_grad(US, Z0, dsig_us, dsig_z0);
     R uo = 0, ao = 0;
     for (int m = lane; m < ml; m += 32) {
       R t = 0;
@@ -692,12 +694,8 @@ template <typename R> struct AdjW {
       const R sig = P_::ZPI * S.FR[m];
       LAM[k + ld * m] = LAM[k + ld * m] + (luo * S.DFIM[m] * (sig * sig) + lao * S.DFIM[m]);
     });
-    {
-      R dus, dz0;
-      wsig_grad(US, Z0, dus, dz0);
-      lUS = lUS + lsig_n * dus;
-      lZ0 = lZ0 + lsig_n * dz0;
-    }
+    lUS = lUS + lsig_n * dsig_us;
+    lZ0 = lZ0 + lsig_n * dsig_z0;
     __syncwarp();
   }
 

@@ -610,10 +610,11 @@ int deriv_setup(wamgpu_ctx* ctx, Impl<R>& I, int ld, bool tl, DerivArgs<R>& a) {
 template <typename R>
 int implsch_adj_t(wamgpu_ctx* ctx, Impl<R>& I, const void* fl3_in, int ld, const void* tauw_in, const void* u10,
                   const void* udir, const void* roairn, const void* wstar, void* lam_fl3, void* lam_tauw, void* lam_u10,
-                  cudaStream_t s) {
+                  cudaStream_t s, void* lam_out = nullptr) {
   DerivArgs<R> a;
   int rc = deriv_setup<R>(ctx, I, ld, false, a);
   if (rc) return rc;
+  a.lam_out = (R*)lam_out;
   a.fl3_in = (const R*)fl3_in; a.tauw_in = (const R*)tauw_in; a.u10 = (const R*)u10; a.udir = (const R*)udir;
   a.roairn = (const R*)roairn; a.wstar = (const R*)wstar;
   a.lam_fl3 = (R*)lam_fl3; a.lam_tauw = (R*)lam_tauw; a.lam_u10 = (R*)lam_u10;
@@ -713,14 +714,24 @@ int step_adj_dev_t(wamgpu_ctx* ctx, Impl<R>& I, int slot, int nprop, void* lam_f
                    const void* udir, const void* roairn, const void* wstar, void* scratch, cudaStream_t s) {
   int rc = ckpt_check(ctx, I, slot, ld, nprop);
   if (rc) return rc;
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
   const R* c = ckpt_slot(ctx, I, slot);
-  const size_t nb = (size_t)ctx->cfg.kl * ctx->cfg.ml;
-  rc = implsch_adj_t<R>(ctx, I, c, ld, c + (size_t)ld * nb, c + (size_t)ld * nb + ctx->nsea, udir, roairn, wstar, lam_fl3,
-                        lam_tauw, lam_u10, s);
+  const size_t nb = (size_t)ctx->cfg.kl * ctx->cfg.ml, bytes = (size_t)ld * nb * sizeof(R);
+  R* lam = (R*)lam_fl3;
+  R* sc = (R*)scratch;
+  if (!sc) { CK(I.scratch.ensure(bytes), "alloc scratch"); sc = I.scratch.template as<R>(); }
+  // the sub-steps ping-pong between lam and scratch; the IMPLSCH adjoint
+  // writes where the first one must start so that the last one ends in lam
+  const int nsub = nprop * ctx->counter;
+  R* src = (nsub % 2) ? sc : lam;
+  rc = implsch_adj_t<R>(ctx, I, c, ld, c + (size_t)ld * nb, c + (size_t)ld * nb + ctx->nsea, udir, roairn, wstar, lam,
+                        lam_tauw, lam_u10, s, src == lam ? nullptr : src);
   if (rc) return rc;
-  for (int q = 0; q < nprop; ++q) {
-    rc = propags_adj_t<R>(ctx, I, lam_fl3, ld, scratch, s);
-    if (rc) return rc;
+  R* dst = src == lam ? sc : lam;
+  for (int it = 0; it < nsub; ++it) {
+    CK(cudaMemsetAsync(dst, 0, bytes, s), "zero adjoint");
+    { TimedLaunch tl(ctx, 0, s); CK(launch_propags_adj<R>(I.pa, src, ld, dst, ld, s), "propags adjoint launch"); }
+    std::swap(src, dst);
   }
   return WAMGPU_OK;
 }

@@ -79,6 +79,7 @@ template <typename R> struct DerivArgs {
   uint8_t* masks;
   // adjoint: in = adjoints of the outputs, out = adjoints of the inputs
   R *lam_fl3, *lam_tauw, *lam_u10;
+  R* lam_out;  // where the adjoint kernel writes the input spectrum's adjoint (null: lam_fl3)
   // tangent-linear
   const R *dfl3_in, *dtauw_in, *du10;
   R *fl3_out, *dfl3_out, *tauw_out, *dtauw_out, *ustar_out, *z0_out;
