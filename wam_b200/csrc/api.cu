@@ -64,6 +64,7 @@ struct wamgpu_ctx {
   std::vector<float> depth, u, v;
   std::vector<int> indep;
   bool have_grid = false, prepared = false;
+  bool wncg_valid = false;  // the WN/CG rows match the current depth
   int counter = 1; double total_cfl = 0, cfl_min = 0; int variant = 0;
   std::unique_ptr<ImplBase> impl;
   // opt-in kernel timing: event pairs per kernel class (0 = PROPAGS, 1 = IMPLSCH)
@@ -83,6 +84,7 @@ template <typename R> struct Impl : ImplBase {
   bool has_enh = false;  // MAKE_SHALLOW_SNL factors uploaded to `enh` ([ij + nsea*(mc-1)])
   DevBuf dwork, dmasks;  // work of the derivative kernels
   DevBuf ckpt;           // checkpoints of an assimilation window
+  DevBuf wncg;           // ST6: WN and CG per (sea point, frequency), formed by wamgpu_prepare_source
   int nckpt = 0, ckpt_ld = 0;
   DevBuf small, ismall, tfak, tcgond, tsihkd, flminfr, enh, gom, fr, sinth, costh;
   // per-point metadata
@@ -442,6 +444,14 @@ template <typename R> int set_grid_t(wamgpu_ctx* ctx, Impl<R>& I) {
 // MAKE_SHALLOW_SNL (:975-1048)
 template <typename R> int prepare_source_t(wamgpu_ctx* ctx, Impl<R>& I) {
   const Config& c = ctx->cfg;
+  // ST6: WAVNU2 depends on the depth only, so its rows are formed once here
+  ctx->wncg_valid = false;
+  if (c.iphys == 2 && ctx->prepared) {
+    CK(I.wncg.ensure((size_t)ctx->nsea * 2 * c.ml * sizeof(R) + 16), "alloc WN/CG");
+    CK(launch_wavnu2<R>(I.dt, I.d_depth.template as<R>(), ctx->nsea, I.wncg.template as<R>(), ctx->stream), "WAVNU2");
+    CK(cudaStreamSynchronize(ctx->stream), "WAVNU2");
+    ctx->wncg_valid = true;
+  }
   I.has_enh = false;
   if (!(c.shallow_run && c.isnonlin != 0)) return WAMGPU_OK;
   const TableSet<R>& t = I.tab;
@@ -479,6 +489,7 @@ int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u1
   a.fluxes = ctx->cfg.lcflx ? I.fluxes.template as<R>() + p0 : nullptr;
   a.flx_ld = ctx->nsea;
   a.enh = I.has_enh ? I.enh.template as<R>() + p0 : nullptr; a.enh_ld = ctx->nsea;
+  a.wncg = ctx->wncg_valid ? I.wncg.template as<R>() + (size_t)p0 * 2 * ctx->cfg.ml : nullptr;
   a.status = I.status.template as<int>();
   { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch"); }
   return WAMGPU_OK;
@@ -898,6 +909,7 @@ int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float*
       a.flx_ld = n;
       a.status = I.status.template as<int>();
       a.enh = I.has_enh ? I.enh.template as<R>() + p0 : nullptr; a.enh_ld = n;
+      a.wncg = ctx->wncg_valid ? I.wncg.template as<R>() + (size_t)p0 * 2 * ctx->cfg.ml : nullptr;
       { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch"); }
     }
     CK(cudaEventRecord(ctx->xfer_ev[ngrp + q], s), "event");
@@ -1078,6 +1090,7 @@ int batch_impl_lists(wamgpu_batch* b, const std::vector<int>& Pin, std::vector<B
       a.fluxes = (c->cfg.lcflx && !tmp3) ? I.fluxes.template as<R>() : nullptr;
       a.flx_ld = c->nsea;
       a.enh = I.has_enh ? I.enh.template as<R>() : nullptr; a.enh_ld = c->nsea;
+      a.wncg = c->wncg_valid ? I.wncg.template as<R>() : nullptr;
       a.status = tmp_status ? tmp_status : I.status.template as<int>();
       first[q + 1] = first[q] + (c->nsea + P - 1) / P;
     }
@@ -1365,7 +1378,7 @@ int wamgpu_set_grid(wamgpu_ctx* ctx, int nsea, const int* klat, const int* klon,
   ctx->wlat.assign(wlat, wlat + 2 * (size_t)nsea); ctx->kfromij.assign(kfromij, kfromij + nsea);
   ctx->sinph.assign(sinph, sinph + ny); ctx->cosph.assign(cosph, cosph + ny); ctx->dellam.assign(dellam, dellam + ny);
   ctx->depth.assign(nsea, 999.0f); ctx->u.assign(nsea, 0.f); ctx->v.assign(nsea, 0.f);
-  ctx->have_grid = true; ctx->prepared = false;
+  ctx->have_grid = true; ctx->prepared = false; ctx->wncg_valid = false;
   ctx->own0 = 0; ctx->own1 = -1;
   cudaSetDevice(ctx->cfg.device);
   return DISPATCH_CTX(ctx, set_grid_t);
@@ -1377,6 +1390,7 @@ int wamgpu_set_depth(wamgpu_ctx* ctx, const float* depth) {
     if (!(depth[i] > 0.f) || !std::isfinite(depth[i])) return fail(ctx, WAMGPU_E_ARG, "depth must be positive and finite");
   ctx->depth.assign(depth, depth + ctx->nsea);
   ctx->prepared = false;
+  ctx->wncg_valid = false;
   return WAMGPU_OK;
 }
 

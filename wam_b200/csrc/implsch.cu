@@ -43,6 +43,7 @@ __device__ __forceinline__ void implsch_cta(const DevTables<R>& T, const ImplArg
     w.LL = reinterpret_cast<uint8_t*>(w.T + 8 * T.scr);
     Src<R> src(T, S, w, lane, ij, a.indep[ij], a.u10[ij], a.udir[ij], a.roairn[ij], a.wstar[ij], a.depth[ij], a.enh,
                a.enh_ld);
+    src.wncg = a.wncg ? a.wncg + (size_t)ij * 2 * T.ML : nullptr;
     PointState<R> ps;
     ps.TAUW = a.tauw[ij];
     src.run(ps);
@@ -98,6 +99,26 @@ __global__ void __launch_bounds__(P * 32) implsch_batch_kernel(const __grid_cons
   __syncthreads();
   implsch_cta<R, P>(T, sa, (int)blockIdx.x - first[g], smem);
 }
+
+template <typename R>
+__global__ void __launch_bounds__(256) wavnu2_kernel(const __grid_constant__ DevTables<R> T, const R* __restrict__ depth,
+                                                     int nsea, R* __restrict__ out) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const int ML = T.ML;
+  if (t >= (size_t)nsea * ML) return;
+  const int ij = (int)(t / ML), m = (int)(t - (size_t)ij * ML);
+  const R w0 = dabs(Phys<R>::ZPI * T.small[T.lay.FR + m]);
+  wavnu2_one(w0, depth[ij], out[(size_t)ij * 2 * ML + m], out[(size_t)ij * 2 * ML + ML + m]);
+}
+
+template <typename R> cudaError_t launch_wavnu2(const DevTables<R>& T, const R* depth, int nsea, R* out, cudaStream_t s) {
+  const size_t n = (size_t)nsea * T.ML;
+  if (n == 0) return cudaSuccess;
+  wavnu2_kernel<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(T, depth, nsea, out);
+  return cudaGetLastError();
+}
+template cudaError_t launch_wavnu2<float>(const DevTables<float>&, const float*, int, float*, cudaStream_t);
+template cudaError_t launch_wavnu2<double>(const DevTables<double>&, const double*, int, double*, cudaStream_t);
 
 template <typename R> size_t implsch_smem_bytes(const DevTables<R>& T, int P) {
   return tables_bytes<R>(T.lay) + (size_t)P * warp_ws_bytes<R>(T.ld, T.ML, T.need_sp, T.scr);

@@ -86,6 +86,26 @@ template <typename R> __host__ __device__ inline size_t ws_t_offset(int ld, int 
   return (b + 15) & ~size_t(15);
 }
 
+// WAVNU2 (:4343-4461) for one frequency: wavenumber and group velocity at
+// angular frequency w0 and depth H by Newton's method.
+template <typename R> __device__ __forceinline__ void wavnu2_one(R w0, R H, R& wn, R& cgv) {
+  using P_ = Phys<R>;
+  const R eps = R(1E-7);
+  R k = (w0 < dsqrt(P_::G / H)) ? w0 / dsqrt(P_::G * H) : w0 * w0 / P_::G;
+  R kold = 0;
+  for (int i = 0; i < 15; ++i) {
+    R dif = dabs(k - kold), rdif = (k != R(0)) ? dif / k : R(0);
+    if (dif < eps && rdif < eps) break;
+    kold = k;
+    R th = dtanh(kold * H);
+    R f1 = P_::G * kold * th - w0 * w0;
+    R fd = (kold * H > R(25)) ? P_::G * th : P_::G * th + P_::G * kold * H / (dcosh(kold * H) * dcosh(kold * H));
+    k = kold - f1 / fd;
+  }
+  wn = k;
+  cgv = (R(2) * k * H > R(25)) ? w0 / k * R(0.5) : w0 / k * R(0.5) * (R(1) + (R(2) * k * H / dsinh(R(2) * k * H)));
+}
+
 // Bytes of the small tables staged at the start of a CTA's shared memory.
 template <typename R> __host__ __device__ inline size_t tables_bytes(const SmallLayout& L) {
   size_t b = (size_t)L.nreal * sizeof(R) + (size_t)L.nint * sizeof(int);
@@ -110,6 +130,8 @@ template <typename R> struct Src {
   // When set, SINPUT_ARD records the sheltering sums entering every
   // frequency: rows XST0, XST1, YST0, YST1 of length ML (the adjoint's tape).
   R* shl = nullptr;
+  // ST6: this point's WN and CG rows formed once from the depth (WAVNU2), or null.
+  const R* wncg = nullptr;
   __device__ Src(const DevTables<R>& t, const STabs<R>& s, WarpWS<R>& ws, int l, int ij_, int indep, R u10, R udir,
                  R roairn, R wstar, R depth, const R* enh, int enh_ld_)
       : T(t), S(s), w(ws), lane(l), ij(ij_), INDEP(indep), U10(u10), UDIR(udir), ROAIRN(roairn), WSTAR(wstar), DEPTH(depth),
@@ -570,24 +592,14 @@ template <typename R> struct Src {
 
   // ---- ST6 ----------------------------------------------------------------
   // WAVNU2: wave number and group velocity per frequency -> scratch 0, 1
+  // The depth is fixed between preparations, so the rows are normally formed
+  // once per point (launch_wavnu2) and only read here.
   __device__ void wavnu2() const {
     R* WN = w.t(0); R* CG = w.t(1);
-    const R H = DEPTH, eps = R(1E-7);
-    for (int m = lane; m < ML(); m += 32) {
-      R w0 = dabs(P_::ZPI * S.FR[m]);
-      R k = (w0 < dsqrt(P_::G / H)) ? w0 / dsqrt(P_::G * H) : w0 * w0 / P_::G;
-      R kold = 0;
-      for (int i = 0; i < 15; ++i) {
-        R dif = dabs(k - kold), rdif = (k != R(0)) ? dif / k : R(0);
-        if (dif < eps && rdif < eps) break;
-        kold = k;
-        R th = dtanh(kold * H);
-        R f1 = P_::G * kold * th - w0 * w0;
-        R fd = (kold * H > R(25)) ? P_::G * th : P_::G * th + P_::G * kold * H / (dcosh(kold * H) * dcosh(kold * H));
-        k = kold - f1 / fd;
-      }
-      R cg = (R(2) * k * H > R(25)) ? w0 / k * R(0.5) : w0 / k * R(0.5) * (R(1) + (R(2) * k * H / dsinh(R(2) * k * H)));
-      WN[m] = k; CG[m] = cg;
+    if (wncg) {
+      for (int m = lane; m < ML(); m += 32) { WN[m] = wncg[m]; CG[m] = wncg[ML() + m]; }
+    } else {
+      for (int m = lane; m < ML(); m += 32) wavnu2_one(dabs(P_::ZPI * S.FR[m]), DEPTH, WN[m], CG[m]);
     }
     __syncwarp();
   }

@@ -26,10 +26,15 @@ template <typename R> struct ImplArgs {
   int flx_ld;  // leading dimension of fluxes (the full NSEA when a launch covers a range of points)
   const R* enh;  // MAKE_SHALLOW_SNL factors [ij + enh_ld*(mc-1)] when shallow && isnonlin != 0, else null
   int enh_ld;
+  const R* wncg;  // ST6: WN then CG (ML values each) per point [ij * 2*ML], or null (formed in the step)
   int* status; // bit 0: non-finite output
 };
 
 template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const ImplArgs<R>& a, int points_per_cta, cudaStream_t s);
+// WAVNU2's wavenumber and group velocity of every (sea point, frequency) from
+// the depth, the same routine the ST6 step uses: out[ij * 2*ML + m] = WN,
+// out[ij * 2*ML + ML + m] = CG.
+template <typename R> cudaError_t launch_wavnu2(const DevTables<R>& T, const R* depth, int nsea, R* out, cudaStream_t s);
 // Batched IMPLSCH over members that share their source tables T (one
 // spectral grid and physics configuration): CTA b works for member g with
 // first[g] <= b < first[g+1] (first[g] = sum of ceil(NSEA/P) over the members
