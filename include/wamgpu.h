@@ -158,12 +158,12 @@ WAMGPU_API int wamgpu_propags_dev_static(wamgpu_ctx* ctx, void* f3, int ld, void
  * nprop PROPAGS calls (IDELT/IDELPRO of them per source step) followed by
  * one IMPLSCH, with the spectrum resident on the device for the whole pass.
  * The _host form copies FL3 and the per-point fields in once and back once
- * (FP32 contexts), overlapping the copies with the kernels on a second
- * stream: without current refraction the spectrum goes up in groups of
- * frequency planes, each propagated as soon as it has arrived, and the
- * result comes down by sea-point ranges as IMPLSCH finishes them.  Host
- * buffers should be pinned for the copies to overlap.  The _dev form works
- * on caller-owned device buffers. */
+ * (FP32 contexts), in chunks of consecutive sea points: a chunk goes up on
+ * one copy stream, is propagated as soon as it and its neighbour chunks have
+ * arrived (the sub-steps of the chunks run as a wavefront), is integrated,
+ * and comes down on a second copy stream, so that both copy directions and
+ * the kernels overlap.  Host buffers should be pinned for the copies to
+ * overlap.  The _dev form works on caller-owned device buffers. */
 WAMGPU_API int wamgpu_step_dev(wamgpu_ctx* ctx, void* fl3, int ld, void* scratch, int nprop, const void* u10,
                                const void* udir, void* tauw, void* ustar, void* z0, const void* roairn,
                                const void* wstar, void* stream);

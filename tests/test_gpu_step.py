@@ -3,11 +3,11 @@ the C ABI. Each path runs one pass of the PROP/PHYSICS loop body
 (wamodel.f90:286-360) on the same inputs:
   A  nprop x wamgpu_propags_dev, then wamgpu_implsch_dev;
   B  wamgpu_step_dev;
-  C  wamgpu_step_host on host arrays, whose copies overlap the kernels by
-     frequency-plane groups and sea-point ranges.
+  C  wamgpu_step_host on host arrays, whose copies overlap the kernels in
+     chunks of sea points (PROPAGS sub-steps of the chunks as a wavefront).
 Results must be bit-identical (spectrum, TAUW, USTAR, Z0 and, with LCFLX,
-the flux arrays), for plane-independent propagation (split copies) and for
-current refraction (unsplit), over two consecutive passes."""
+the flux arrays), with and without current refraction, on grids cut into
+a few and into the maximum number of chunks, over two consecutive passes."""
 import numpy as np
 import pytest
 
@@ -30,10 +30,12 @@ def _model(w, currents=False, lcflx=False):
     return m
 
 
-CASES = [("c0", 0.25, False, False), ("c1", 0.02, False, False), ("c1", 0.02, False, True), ("c2", 0.05, True, False)]
+CASES = [("c0", 0.25, False, False), ("c1", 0.02, False, False), ("c1", 0.02, False, True), ("c2", 0.05, True, False),
+         ("c1", 0.1, True, False)]
 
 
-@pytest.mark.parametrize("name,scale,currents,lcflx", CASES, ids=["c0", "c1", "c1-lcflx", "c2-currents"])
+@pytest.mark.parametrize("name,scale,currents,lcflx", CASES,
+                         ids=["c0", "c1", "c1-lcflx", "c2-currents", "c1-32-chunks-currents"])
 def test_step_paths_identical(name, scale, currents, lcflx):
     import torch
     from wam_b200.synth import make_workload

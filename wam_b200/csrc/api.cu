@@ -52,12 +52,14 @@ struct wamgpu_ctx {
   Config cfg{};
   std::string err;
   cudaStream_t stream = nullptr;
-  cudaStream_t copy_stream = nullptr;  // host<->device copies overlapped with the kernels of a host-buffer step
+  cudaStream_t copy_stream = nullptr;  // host->device copies overlapped with the kernels of a host-buffer step
+  cudaStream_t down_stream = nullptr;  // device->host copies of a host-buffer step
   std::vector<cudaEvent_t> xfer_ev;     // ordering events between the two streams
   int nsm = 148;
   int P = 8;  // sea points per IMPLSCH CTA
   // grid (reference convention, host)
   int nsea = 0, ny = 0, n_ext = 0;
+  int halo = 0;  // largest |neighbour - point| over KLAT/KLON (sea point numbers)
   int own0 = 0, own1 = -1;  // sea points this context updates ([own0, own1); own1 < 0: all), the rest are halo
   std::vector<int> klat, klon, kfromij;
   std::vector<float> wlat, sinph, cosph, dellam;
@@ -833,16 +835,9 @@ int implsch_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, const float* u10, co
   return wamgpu_sync(ctx);
 }
 
-// Host-buffer form of one WAMODEL pass, with the copies overlapped:
-//  - without current refraction a PROPAGS sub-step of frequency plane m reads
-//    only plane m, so the spectrum goes up in groups of planes on the copy
-//    stream and each group is propagated (all nprop*COUNTER sub-steps) as
-//    soon as it has arrived;
-//  - IMPLSCH then runs over ranges of sea points, and each range's spectrum
-//    and TAUW/USTAR/Z0 go down on the copy stream while the next range is
-//    integrated.
-// Results are identical to the unsplit sequence: every kernel sees the same
-// inputs and writes the same elements.
+// Host-buffer form of one WAMODEL pass, with the copies overlapped (see the
+// chunk pipeline below).  Results are identical to the unsplit sequence:
+// every kernel sees the same inputs and writes the same elements.
 template <typename R>
 int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float* u10, const float* udir, float* tauw,
                 float* ustar, float* z0, const float* roairn, const float* wstar) {
@@ -867,36 +862,55 @@ int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float*
   R* f3 = I.fl3.template as<R>();
   R* sc = I.scratch.template as<R>();
   const int nsub = nprop * ctx->counter;
-  const bool split = n > 0 && nsub > 0 && propags_planes_independent(I.pa.variant);
-  const int ngrp = split ? std::min(ML, 6) : 1;
-  const int npart = n > 0 ? std::min(8, (n + 1023) / 1024) : 1;
-  if ((int)ctx->xfer_ev.size() < ngrp + npart)
-    for (int i = (int)ctx->xfer_ev.size(); i < ngrp + npart; ++i) {
+  // Chunks of consecutive sea points, each at least as wide as the largest
+  // neighbour distance, so that a sub-step of chunk q reads only chunks
+  // q-1..q+1.  Chunk q goes up on `c`, is propagated and integrated on `s`
+  // and comes down on `d`, so the two copy directions and the kernels overlap.
+  // The kernels are issued in the order of the key q + j - 1 (sub-step j of
+  // chunk q), ascending j within a key, with IMPLSCH of chunk q last under key
+  // q + nsub.  Sub-step j of chunk q then follows sub-step j-1 of chunks
+  // q-1..q+1, whose results it reads and whose input buffer it overwrites; it
+  // precedes sub-step j+1 of chunk q-1, which overwrites its input; and
+  // IMPLSCH of chunk q follows the last sub-step of chunks q-1..q+1.
+  const int width = std::max(ctx->halo, 1);
+  const int nq = n > 0 ? std::min(32, std::max(1, n / width)) : 1;
+  std::vector<int> lo(nq + 1);
+  for (int q = 0; q <= nq; ++q) lo[q] = (int)((long long)n * q / nq);
+  const int nev = 2 * nq;
+  if ((int)ctx->xfer_ev.size() < nev)
+    for (int i = (int)ctx->xfer_ev.size(); i < nev; ++i) {
       cudaEvent_t e;
       CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
       ctx->xfer_ev.push_back(e);
     }
-  // upload and propagate, plane group by plane group
-  R* fin = f3;
-  for (int g = 0; g < ngrp; ++g) {
-    const int m0 = (int)((long long)ML * g / ngrp), m1 = (int)((long long)ML * (g + 1) / ngrp);
-    if (split) {
-      CK(cudaMemcpyAsync(f3 + plane * m0, fl3 + plane * m0, plane * (m1 - m0) * 4, cudaMemcpyHostToDevice, c), "H2D");
-      CK(cudaEventRecord(ctx->xfer_ev[g], c), "event");
-      CK(cudaStreamWaitEvent(s, ctx->xfer_ev[g], 0), "wait");
-    } else {
-      CK(cudaMemcpyAsync(f3, fl3, nb * 4, cudaMemcpyHostToDevice, s), "H2D");
-    }
-    R* src = f3; R* dst = sc;
-    for (int it = 0; it < nsub; ++it) {
-      { TimedLaunch tl(ctx, 0, s); CK(launch_propags<R>(I.pa, src, n, dst, n, s, split ? m0 : 0, split ? m1 - m0 : -1), "propags launch"); }
-      std::swap(src, dst);
-    }
-    fin = src;
+  cudaStream_t d = ctx->down_stream;
+  // the spectrum chunk by chunk (the per-point fields went up on s above)
+  for (int q = 0; q < nq; ++q) {
+    const size_t w = (size_t)(lo[q + 1] - lo[q]) * 4;
+    if (w) CK(cudaMemcpy2DAsync(f3 + lo[q], (size_t)n * 4, fl3 + lo[q], (size_t)n * 4, w, (size_t)KL * ML,
+                                cudaMemcpyHostToDevice, c), "H2D");
+    CK(cudaEventRecord(ctx->xfer_ev[q], c), "event");
   }
-  // integrate and download, sea-point range by range
-  for (int q = 0; q < npart; ++q) {
-    const int p0 = (int)((long long)n * q / npart), p1 = (int)((long long)n * (q + 1) / npart);
+  R* buf[2] = {f3, sc};
+  const R* fin = buf[nsub % 2];  // the buffer the last sub-step writes
+  auto ready = [&](int q) -> int {  // chunk q and its neighbours are on the device
+    CK(cudaStreamWaitEvent(s, ctx->xfer_ev[std::min(q + 1, nq - 1)], 0), "wait");
+    return WAMGPU_OK;
+  };
+  const int last = (nq - 1) + nsub;
+  for (int t = 0; t <= last; ++t) {
+    for (int j = 1; j <= nsub; ++j) {
+      const int q = t - (j - 1);
+      if (q < 0 || q >= nq) continue;
+      if (j == 1) { int rc = ready(q); if (rc) return rc; }
+      PropArgs<R> A = I.pa;
+      A.i0 = lo[q]; A.i1 = lo[q + 1];
+      { TimedLaunch tl(ctx, 0, s); CK(launch_propags<R>(A, buf[(j - 1) % 2], n, buf[j % 2], n, s), "propags launch"); }
+    }
+    const int q = t - nsub;
+    if (q < 0 || q >= nq) continue;
+    if (nsub == 0) { int rc = ready(q); if (rc) return rc; }
+    const int p0 = lo[q], p1 = lo[q + 1];
     if (p1 > p0) {
       ImplArgs<R> a;
       a.nsea = p1 - p0; a.ld = n;
@@ -912,16 +926,17 @@ int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float*
       a.wncg = ctx->wncg_valid ? I.wncg.template as<R>() + (size_t)p0 * 2 * ctx->cfg.ml : nullptr;
       { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch"); }
     }
-    CK(cudaEventRecord(ctx->xfer_ev[ngrp + q], s), "event");
-    CK(cudaStreamWaitEvent(c, ctx->xfer_ev[ngrp + q], 0), "wait");
+    CK(cudaEventRecord(ctx->xfer_ev[nq + q], s), "event");
+    CK(cudaStreamWaitEvent(d, ctx->xfer_ev[nq + q], 0), "wait");
     if (p1 > p0) {
       const size_t w = (size_t)(p1 - p0) * 4;
-      CK(cudaMemcpy2DAsync(fl3 + p0, (size_t)n * 4, f3 + p0, (size_t)n * 4, w, (size_t)KL * ML, cudaMemcpyDeviceToHost, c), "D2H");
-      CK(cudaMemcpyAsync(tauw + p0, I.tauw.template as<R>() + p0, w, cudaMemcpyDeviceToHost, c), "D2H");
-      CK(cudaMemcpyAsync(ustar + p0, I.ustar.template as<R>() + p0, w, cudaMemcpyDeviceToHost, c), "D2H");
-      CK(cudaMemcpyAsync(z0 + p0, I.z0.template as<R>() + p0, w, cudaMemcpyDeviceToHost, c), "D2H");
+      CK(cudaMemcpy2DAsync(fl3 + p0, (size_t)n * 4, f3 + p0, (size_t)n * 4, w, (size_t)KL * ML, cudaMemcpyDeviceToHost, d), "D2H");
+      CK(cudaMemcpyAsync(tauw + p0, I.tauw.template as<R>() + p0, w, cudaMemcpyDeviceToHost, d), "D2H");
+      CK(cudaMemcpyAsync(ustar + p0, I.ustar.template as<R>() + p0, w, cudaMemcpyDeviceToHost, d), "D2H");
+      CK(cudaMemcpyAsync(z0 + p0, I.z0.template as<R>() + p0, w, cudaMemcpyDeviceToHost, d), "D2H");
     }
   }
+  CK(cudaStreamSynchronize(d), "step copies");
   CK(cudaStreamSynchronize(c), "step copies");
   CK(cudaStreamSynchronize(s), "step sync");
   return wamgpu_sync(ctx);
@@ -1319,6 +1334,7 @@ int wamgpu_create(const wamgpu_config* cfg, wamgpu_ctx** out) {
   if ((e = cudaSetDevice(c.device)) != cudaSuccess) return bail(cuda_fail(ctx, e, "cudaSetDevice"));
   if ((e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(cuda_fail(ctx, e, "stream"));
   if ((e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(cuda_fail(ctx, e, "stream"));
+  if ((e = cudaStreamCreateWithFlags(&ctx->down_stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(cuda_fail(ctx, e, "stream"));
   cudaDeviceGetAttribute(&ctx->nsm, cudaDevAttrMultiProcessorCount, c.device);
   int rc;
   if (c.precision == 8) { auto* I = new Impl<double>(); ctx->impl.reset(I); rc = build_tables<double>(ctx, *I); }
@@ -1332,11 +1348,13 @@ int wamgpu_destroy(wamgpu_ctx* ctx) {
   if (!ctx) return WAMGPU_OK;
   if (ctx->stream) { cudaSetDevice(ctx->cfg.device); cudaStreamSynchronize(ctx->stream); }
   if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
+  if (ctx->down_stream) cudaStreamSynchronize(ctx->down_stream);
   ctx->impl.reset();
   for (int c = 0; c < 2; ++c) for (auto& e : ctx->ev[c]) ctx->ev_pool.push_back(e);
   for (auto& e : ctx->ev_pool) { cudaEventDestroy(e.first); cudaEventDestroy(e.second); }
   for (auto e : ctx->xfer_ev) cudaEventDestroy(e);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->down_stream) cudaStreamDestroy(ctx->down_stream);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return WAMGPU_OK;
@@ -1374,6 +1392,11 @@ int wamgpu_set_grid(wamgpu_ctx* ctx, int nsea, const int* klat, const int* klon,
   for (int i = 0; i < 2 * nsea; ++i) if (klon[i] < 0 || klon[i] > nsea) return fail(ctx, WAMGPU_E_ARG, "KLON index out of range");
   for (int i = 0; i < nsea; ++i) if (kfromij[i] < 1 || kfromij[i] > ny) return fail(ctx, WAMGPU_E_ARG, "KFROMIJ out of range");
   ctx->nsea = nsea; ctx->ny = ny; ctx->n_ext = nsea;
+  ctx->halo = 0;
+  for (int q = 0; q < 4; ++q)
+    for (int i = 0; i < nsea; ++i) { const int p = klat[i + (size_t)nsea * q]; if (p > 0) ctx->halo = std::max(ctx->halo, std::abs(p - 1 - i)); }
+  for (int q = 0; q < 2; ++q)
+    for (int i = 0; i < nsea; ++i) { const int p = klon[i + (size_t)nsea * q]; if (p > 0) ctx->halo = std::max(ctx->halo, std::abs(p - 1 - i)); }
   ctx->klat.assign(klat, klat + 4 * (size_t)nsea); ctx->klon.assign(klon, klon + 2 * (size_t)nsea);
   ctx->wlat.assign(wlat, wlat + 2 * (size_t)nsea); ctx->kfromij.assign(kfromij, kfromij + nsea);
   ctx->sinph.assign(sinph, sinph + ny); ctx->cosph.assign(cosph, cosph + ny); ctx->dellam.assign(dellam, dellam + ny);
