@@ -1,23 +1,18 @@
-// Tangent-linear and adjoint of IMPLSCH for ST4 (IPHYS=1), one sea point per
-// thread.
+// Point-per-thread restatement of IMPLSCH for ST4 (IPHYS=1), templated on
+// the number type, for the tangent-linear model and the scalar routines the
+// adjoint differentiates.
 //
-// The forward kernel spreads a point over a warp.  The derivative kernels
-// instead walk one point's bins sequentially in one thread.  Every per-point
-// array lives in global memory with the sea point fastest ([bin * ld + ij]),
-// so the 32 threads of a warp always touch 32 consecutive addresses.
-//
-//  - `forward<R,T>` restates IMPLSCH (wam_source_module.f90:374-700, the
-//    ST4 branches) statement by statement.  T = R gives the values, with the
-//    intermediates the reverse sweep needs recorded on a per-point tape.
-//    T = Dual<R> gives the tangent-linear model (value and directional
-//    derivative of every statement).
-//  - `reverse<R>` is the hand-written adjoint.  It runs the routines
-//    backwards: IMPHFTAIL, the implicit update with its limiter and floor,
-//    SNONLIN (DIA), SDISSIP_ARD, SINPUT_ARD with the sheltering recursion
-//    over frequency, STRESSO, AIRSEA, and the spectral integrals.  The small
-//    scalar routines with two inputs (AIRSEA's Newton iteration, TAU_PHI_HF,
-//    WSIGSTAR) are differentiated by two forward passes of dual numbers
-//    inside the reverse sweep, which is exact for the computation as done.
+//  - `forward<R,T>` restates IMPLSCH (wam_source_module.f90:374-700, the ST4
+//    branches) statement by statement for one sea point, its per-point
+//    arrays in global memory with the sea point fastest ([bin * ld + ij]) so
+//    that the 32 threads of a warp touch 32 consecutive addresses.  T = R
+//    gives the values (with a tape of intermediates); T = Dual<R> gives the
+//    tangent-linear model: the value and the directional derivative of every
+//    statement.
+//  - The scalar routines with two inputs (AIRSEA's Newton iteration,
+//    TAU_PHI_HF, WSIGSTAR) are written once for any T, so the adjoint kernel
+//    (adjoint_warp.cuh) differentiates them by two dual-number passes, which
+//    is exact for the computation as done.
 //
 // Discrete decisions (the cut-off index MIJ, the wind-sea mask LLWS, JU,
 // branches of MAX/MIN and the limiter) are those of the forward state and are
@@ -634,486 +629,10 @@ WAHD void forward(const ATabs<R>& A, const PointIn<R>& P, Col<const T> F0, T TAU
 }
 
 
-// ---- reverse sweep ------------------------------------------------------------
+// ---- derivatives of the scalar routines ------------------------------------------
 
-// Jacobian of a scalar routine with two inputs by two dual passes.
-template <typename R> struct Jac2 { R d00, d01, d10, d11; };  // d(out_i)/d(in_j)
-
-template <typename R> WAHD Jac2<R> airsea_jac(const ATabs<R>& A, R U10, R TAUW) {
-  using D = Dual<R>;
-  D us, z0;
-  Jac2<R> J;
-  airsea(A, D(U10, R(1)), D(TAUW), us, z0); J.d00 = us.d; J.d10 = z0.d;
-  airsea(A, D(U10), D(TAUW, R(1)), us, z0); J.d01 = us.d; J.d11 = z0.d;
-  return J;  // outputs (USTAR, Z0), inputs (U10, TAUW)
-}
-template <typename R> WAHD Jac2<R> tauphi_jac(const ATabs<R>& A, int mij, R ustar, R z0) {
-  using D = Dual<R>;
-  D th, ph;
-  Jac2<R> J;
-  tau_phi_hf(A, mij, D(ustar, R(1)), D(z0), th, ph); J.d00 = th.d; J.d10 = ph.d;
-  tau_phi_hf(A, mij, D(ustar), D(z0, R(1)), th, ph); J.d01 = th.d; J.d11 = ph.d;
-  return J;  // outputs (tauhf, phihf), inputs (ustar, z0)
-}
-
-// IMPHFTAIL^T: rows m >= mij were overwritten from row mij-1.
-template <typename R> WAHD void imphftail_adj(const ATabs<R>& A, const PointIn<R>& P, Col<R> lam, int mij) {
-  const int kl = A.KL;
-  const R base = tail_ratio_row(A, P, mij - 1);
-  for (int m = mij; m < A.ML; ++m) {
-    const R r = tail_ratio_row(A, P, m) / base;
-    for (int k = 0; k < kl; ++k) {
-      lam[k + kl * (mij - 1)] = lam[k + kl * (mij - 1)] + r * lam[k + kl * m];
-      lam[k + kl * m] = R(0);
-    }
-  }
-}
-
-// Adjoint of the spectral integrals with respect to the spectrum, given the
-// adjoints of (emean, fmean, akmean) of the unmasked integrals.
-template <typename R, typename FC>
-WAHD void integrals_adj(const ATabs<R>& A, const PointIn<R>& P, FC F, Col<const uint8_t> mask, R lem, R lfm, R lak,
-                        bool with_ak, Col<R> lamF) {
-  using Ph = Phys<R>;
-  const int kl = A.KL, ml = A.ML;
-  R pe = 0, pf = 0, pa = 0, tail = 0;
-  const R DEL2 = msqrt(Ph::G) / Ph::ZPI;
-  for (int m = 0; m < ml; ++m) {
-    R t = 0;
-    for (int k = 0; k < kl; ++k) { const int b = k + kl * m; if (!mask.p || mask[b]) t = t + F[b]; }
-    pe = pe + t * A.DFIM[m];
-    pf = pf + t * A.DFIMOFR[m];
-    if (with_ak) pa = pa + (A.shallow ? t / msqrt(tfak(A, P, m)) * A.DFIM[m] : t * A.DFIMOFR[m] * DEL2);
-    if (m == ml - 1) tail = t;
-  }
-  const R e_raw = A.MO_TAIL * tail + pe;
-  const R emean = mmax(e_raw, R(1.0E-12));
-  const R den_raw = A.MM1_TAIL * tail + pf, den = mmax(den_raw, R(1.0E-12));
-  R lpe = 0, lpf = 0, lpa = 0, ltail = 0, le = lem;
-  // akmean = (emean/wm)^2 when emean > 1e-12
-  if (with_ak && emean > R(1.0E-12)) {
-    const R wm = A.MM1_TAIL * DEL2 * tail + pa, q = emean / wm;
-    const R lq = lak * R(2) * q;
-    le = le + lq / wm;
-    const R lwm = -lq * emean / (wm * wm);
-    lpa = lwm; ltail = ltail + lwm * A.MM1_TAIL * DEL2;
-  }
-  // fmean = emean / den
-  le = le + lfm / den;
-  const R lden = -lfm * emean / (den * den);
-  if (den_raw >= R(1.0E-12)) { lpf = lden; ltail = ltail + lden * A.MM1_TAIL; }
-  if (e_raw >= R(1.0E-12)) { lpe = le; ltail = ltail + le * A.MO_TAIL; }
-  for (int m = 0; m < ml; ++m) {
-    R lt = lpe * A.DFIM[m] + lpf * A.DFIMOFR[m];
-    if (with_ak) lt = lt + lpa * (A.shallow ? A.DFIM[m] / msqrt(tfak(A, P, m)) : A.DFIMOFR[m] * DEL2);
-    if (m == ml - 1) lt = lt + ltail;
-    for (int k = 0; k < kl; ++k) { const int b = k + kl * m; if (!mask.p || mask[b]) lamF[b] = lamF[b] + lt; }
-  }
-}
-
-// The implicit update^T.  Fw holds F1 (the update's input); lamF2 -> lamF1
-// (in place) and the adjoints of SL, FL; returns those of USTAR and fmx.
-template <typename R>
-WAHD void update_adj(const ATabs<R>& A, const PointIn<R>& P, Col<R> Fw, Col<R> SL, Col<R> FL, R USTAR, R fmx, int ju,
-                     Col<R> lam, Col<R> lSL, Col<R> lFL, R& lUSTAR, R& lfmx) {
-  const int kl = A.KL;
-  for (int m = 0; m < A.ML; ++m) {
-    const R sbo = A.shallow ? sbottom(A, P, m) : R(0);
-    const R lim = USTAR * A.DELFL[m] * fmx;
-    const R fmin = A.FLMINFR[(ju - 1) + 300 * m];
-    R llim = 0;
-    for (int k = 0; k < kl; ++k) {
-      const int b = k + kl * m;
-      const R c = mmax(R(0.), mcos(A.TH[k] - P.UDIR));
-      R f0 = Fw[b], sl = SL[b], fl = FL[b];
-      if (A.shallow) { sl = sl + sbo * f0; fl = fl + sbo; }
-      const R den_raw = R(1.) - A.DELT * fl, den = mmax(R(1.), den_raw);
-      const R t1 = A.DELT * sl / den;
-      const R at1 = mabs(t1);
-      const R t3 = mmin(at1, lim);
-      const R f = f0 + ((t1 >= R(0)) ? t3 : -t3);
-      const R lf = (f < fmin * (c * c)) ? R(0) : lam[b];  // the floor holds when it is selected
-      R lf0 = lf, lt1 = 0;
-      const R lt3 = (t1 >= R(0)) ? lf : -lf;
-      if (lim < at1) llim = llim + lt3;              // MIN selected the limiter
-      else lt1 = (t1 < R(0)) ? -lt3 : lt3;           // d|t1|/dt1
-      const R lsl = lt1 * A.DELT / den;
-      R lfl = 0;
-      if (R(1.) < den_raw) lfl = lt1 * t1 / den * A.DELT;  // d t1 / d fl = DELT*t1/den
-      if (A.shallow) lf0 = lf0 + sbo * lsl;
-      lam[b] = lf0;
-      lSL[b] = lSL[b] + lsl;
-      lFL[b] = lFL[b] + lfl;
-    }
-    lUSTAR = lUSTAR + llim * A.DELFL[m] * fmx;
-    lfmx = lfmx + llim * USTAR * A.DELFL[m];
-  }
-}
-
-// SNONLIN^T: adds to lamF (adjoint of the spectrum) from the adjoints of SL
-// and FL; returns the adjoint of AKMEAN.
-template <typename R>
-WAHD R snonlin_adj(const ATabs<R>& A, const PointIn<R>& P, Col<R> F, R AKMEAN, Col<R> lSL, Col<R> lFL, Col<R> lamF) {
-  const bool dyn = A.shallow && A.isnonlin == 0;
-  R lenh = 0;
-  R enhfr = R(1), denh = R(0);
-  if (dyn) {
-    Dual<R> e = snl_enhfr(A, P, Dual<R>(AKMEAN, R(1)));
-    enhfr = e.v; denh = e.d;
-  }
-  dia_for_each(A, [&](const DiaInt<R>& d) {
-    const R* rc = d.rc;
-    const R sap = d.g[0] * F[d.iP] + d.g[1] * F[d.iP_11] + d.g[2] * F[d.iP1] + d.g[3] * F[d.iP1_11];
-    const R sam = d.g[4] * F[d.iM] + d.g[5] * F[d.iM_21] + d.g[6] * F[d.iM1] + d.g[7] * F[d.iM1_21];
-    const R fij = F[d.iC] * d.ftail;
-    const R ftemp = dia_ftemp(A, P, d, enhfr);
-    R lad = 0, ldelad = 0, ldelap = 0, ldelam = 0;
-    if (d.wMC) { lad -= R(2.) * lSL[d.tC]; ldelad -= R(2.) * lFL[d.tC]; }
-    if (d.wMM) { lad += rc[20] * lSL[d.tMM] + rc[19] * lSL[d.tMM_21]; ldelam += rc[23] * lFL[d.tMM] + rc[24] * lFL[d.tMM_21]; }
-    if (d.wMM1) { lad += rc[17] * lSL[d.tMM1] + rc[18] * lSL[d.tMM1_21]; ldelam += rc[21] * lFL[d.tMM1] + rc[22] * lFL[d.tMM1_21]; }
-    if (d.wMP) { lad += rc[8] * lSL[d.tMP] + rc[7] * lSL[d.tMP_11]; ldelap += rc[11] * lFL[d.tMP] + rc[12] * lFL[d.tMP_11]; }
-    if (d.wMP1) { lad += rc[5] * lSL[d.tMP1] + rc[6] * lSL[d.tMP1_11]; ldelap += rc[9] * lFL[d.tMP1] + rc[10] * lFL[d.tMP1_11]; }
-    // ad = (fij S - 2P) ftemp fij, delad = (2 fij S - 2P) ftemp,
-    // delap = (fij - 2 sam) DAL1 ftemp fij, delam = (fij - 2 sap) DAL2 ftemp fij
-    const R S2 = sap + sam, P2 = sap * sam;
-    R lfij = lad * ftemp * (R(2) * fij * S2 - R(2) * P2) + ldelad * R(2) * S2 * ftemp +
-             ldelap * A.DAL1 * ftemp * (R(2) * fij - R(2) * sam) + ldelam * A.DAL2 * ftemp * (R(2) * fij - R(2) * sap);
-    R lsap = lad * ftemp * fij * (fij - R(2) * sam) + ldelad * (R(2) * fij - R(2) * sam) * ftemp -
-             ldelam * R(2) * A.DAL2 * ftemp * fij;
-    R lsam = lad * ftemp * fij * (fij - R(2) * sap) + ldelad * (R(2) * fij - R(2) * sap) * ftemp -
-             ldelap * R(2) * A.DAL1 * ftemp * fij;
-    if (dyn) {
-      const R lft = lad * (fij * S2 - R(2) * P2) * fij + ldelad * (R(2) * fij * S2 - R(2) * P2) +
-                    ldelap * (fij - R(2) * sam) * A.DAL1 * fij + ldelam * (fij - R(2) * sap) * A.DAL2 * fij;
-      lenh = lenh + lft * d.af11;
-    }
-    lamF[d.iC] += lfij * d.ftail;
-    lamF[d.iP] += d.g[0] * lsap; lamF[d.iP_11] += d.g[1] * lsap; lamF[d.iP1] += d.g[2] * lsap; lamF[d.iP1_11] += d.g[3] * lsap;
-    lamF[d.iM] += d.g[4] * lsam; lamF[d.iM_21] += d.g[5] * lsam; lamF[d.iM1] += d.g[6] * lsam; lamF[d.iM1_21] += d.g[7] * lsam;
-  });
-  return lenh * denh;
-}
-
-// SDISSIP_ARD^T: adds to lamF from the adjoints of SL and FL.
-template <typename R>
-WAHD void sdissip_adj(const ATabs<R>& A, const PointIn<R>& P, Col<R> F, Col<R> lSL, Col<R> lFL, Col<R> lamF) {
-  using Ph = Phys<R>;
-  const int kl = A.KL, nw = 2 * A.NSDSNTH + 1;
-  const R tmp03 = R(1.0) / R(9.0E-4), c6 = R(0.3), c6m1 = R(1.) - c6;
-  R bth[MAX_KL], lbth[MAX_KL];
-  for (int m = 0; m < A.ML; ++m) {
-    const R facsat = sds_facsat(A, P, m), ssdsc2_sig = R(-2.2E-5) * (Ph::ZPI * A.FR[m]);
-    R bmax = 0;
-    int kmax = -1;
-    for (int k = 0; k < kl; ++k) {
-      R acc = 0;
-      for (int j = 0; j < nw; ++j) acc = acc + A.SATW[k + kl * j] * F[(A.INDSAT[k + kl * j] - 1) + kl * m];
-      bth[k] = acc * facsat;
-      if (bmax < bth[k]) { bmax = bth[k]; kmax = k; }
-      lbth[k] = 0;
-    }
-    const R d0raw = bmax * tmp03 - R(1.0), d0 = mmax(R(0.), d0raw);
-    const R temp1 = c6 * (d0 * d0);
-    R ltemp1 = 0;
-    for (int k = 0; k < kl; ++k) {
-      const int b = k + kl * m;
-      const R ddraw = bth[k] * tmp03 - R(1.0), dd = mmax(R(0.), ddraw);
-      const R d = ssdsc2_sig * (temp1 + c6m1 * (dd * dd));
-      lamF[b] += d * lSL[b];
-      const R ld = F[b] * lSL[b] + lFL[b];
-      ltemp1 += ld * ssdsc2_sig;
-      if (R(0.) < ddraw) lbth[k] += ld * ssdsc2_sig * c6m1 * R(2) * dd * tmp03;
-    }
-    if (R(0.) < d0raw && kmax >= 0) lbth[kmax] += ltemp1 * c6 * R(2) * d0 * tmp03;
-    for (int k = 0; k < kl; ++k) {
-      const R lacc = lbth[k] * facsat;
-      for (int j = 0; j < nw; ++j) lamF[(A.INDSAT[k + kl * j] - 1) + kl * m] += A.SATW[k + kl * j] * lacc;
-    }
-  }
-}
-
-
-// STRESSO^T for TAUW: from its adjoint to those of the SPOS sums SX/SY
-// (lsx/lsy, per frequency), the spectrum at the cut-off row, USTAR and Z0.
-template <typename R, typename FC>
-WAHD void stresso_adj(const ATabs<R>& A, const PointIn<R>& P, FC F, int mij, R USTAR, R Z0, Col<R> tape, int call,
-                      R lTAUW, R* lsx, R* lsy, Col<R> lamF, R& lUS, R& lZ0) {
-  using Ph = Phys<R>;
-  const int kl = A.KL, ml = A.ML;
-  R px = 0, py = 0;
-  for (int m = 0; m < mij; ++m) {
-    const R cmr = cmw(A, P, m) * rhowgdfth(A, m, mij);
-    px = px + tape[tape_sin(call, 5, ml) + m] * cmr;
-    py = py + tape[tape_sin(call, 6, ml) + m] * cmr;
-  }
-  const R gm1 = R(1.0) / Ph::G;
-  const R cst = A.DELTH * ((Ph::ZPI * Ph::ZPI) * (Ph::ZPI * Ph::ZPI)) * gm1;
-  R t1 = 0;
-  for (int k = 0; k < kl; ++k) {
-    const R cw = mmax(mcos(A.TH[k] - P.UDIR), R(0.));
-    t1 = t1 + F[k + kl * (mij - 1)] * (cw * cw * cw);
-  }
-  R tau1, phi1;
-  tau_phi_hf(A, mij, USTAR, Z0, tau1, phi1);
-  const R kc = cst * A.FR5[mij - 1] * gm1;
-  const R tauhf = kc * t1 * tau1;
-  const R su = msin(P.UDIR), cu = mcos(P.UDIR);
-  const R xs = px / Ph::ROAIR + tauhf * su, ys = py / Ph::ROAIR + tauhf * cu;
-  const R tw = msqrt(xs * xs + ys * ys), cap = USTAR * USTAR - R(0.00001);
-  const R twc = mmin(tw, cap);
-  R ltwc = (twc < R(0.)) ? R(0) : lTAUW;
-  R ltw = 0;
-  if (cap < tw) lUS = lUS + ltwc * R(2) * USTAR;
-  else ltw = ltwc;
-  const R lxs = tw > R(0) ? ltw * xs / tw : R(0), lys = tw > R(0) ? ltw * ys / tw : R(0);
-  const R lpx = lxs / Ph::ROAIR, lpy = lys / Ph::ROAIR, ltauhf = lxs * su + lys * cu;
-  const R lt1 = ltauhf * kc * tau1, ltau1 = ltauhf * kc * t1;
-  for (int k = 0; k < kl; ++k) {
-    const R cw = mmax(mcos(A.TH[k] - P.UDIR), R(0.));
-    lamF[k + kl * (mij - 1)] += lt1 * (cw * cw * cw);
-  }
-  const Jac2<R> J = tauphi_jac(A, mij, USTAR, Z0);
-  lUS = lUS + ltau1 * J.d00;
-  lZ0 = lZ0 + ltau1 * J.d01;
-  for (int m = 0; m < ml; ++m) {
-    const R cmr = m < mij ? cmw(A, P, m) * rhowgdfth(A, m, mij) : R(0);
-    lsx[m] = lpx * cmr;
-    lsy[m] = lpy * cmr;
-  }
-}
-
-// SINPUT_ARD^T.  lSL/lFL: adjoints of the SL/FL outputs (null for the first
-// call, whose SL/FL the step overwrites); lsx/lsy: adjoints of the SPOS sums.
-// Adds to lamF; returns the adjoints of USTAR and Z0.
-template <typename R, typename FC>
-WAHD void sinput_adj(const ATabs<R>& A, const PointIn<R>& P, FC F, R USTAR, R Z0, Col<R> tape, int call, const Col<R>* lSL,
-                     const Col<R>* lFL, const R* lsx, const R* lsy, Col<R> lamF, R& lUS, R& lZ0) {
-  using Ph = Phys<R>;
-  using K = SinK<R>;
-  const int kl = A.KL, ml = A.ML;
-  const R const1 = A.BETAMAX / (Ph::XKAPPA * Ph::XKAPPA) / Ph::ROWATER;
-  const R nu = Ph::RNUAIR, rog = Ph::ROWATER * Ph::G;
-  const R delabm1 = R(200) / (R(8.0) - R(0.3));
-  const R shelter = mabs(A.TAUWSHELTER);
-  // per-point prologue (recomputed)
-  const R sig_n = wsigstar(P, USTAR, Z0);
-  R uo = 0, ao = 0;
-  for (int m = 0; m < ml; ++m) {
-    R t = 0;
-    for (int k = 0; k < kl; ++k) t = t + F[k + kl * m];
-    const R sig = Ph::ZPI * A.FR[m];
-    uo = uo + A.DFIM[m] * (sig * sig) * t;
-    ao = ao + A.DFIM[m] * t;
-  }
-  const R tiny = sizeof(R) == 4 ? R(FLT_MIN) : R(DBL_MIN);
-  const R uorbt = R(2.0) * msqrt(tiny + uo), aorb = R(2.0) * msqrt(tiny + ao);
-  const R re = (R(4.0) / nu) * uorbt * aorb;
-  const R a1 = Ph::RNUAIRM / mmax(USTAR, R(0.0001)), a2 = R(0.04) * mmin(R(0.0005), Z0);
-  const R z0noz = mmax(a1, a2);
-  const R ratio = aorb / z0noz;
-  const R xi = (mlog10(mmax(ratio, R(3.0))) - R(0.3)) * delabm1;
-  int ind = (int)xi;
-  ind = ind < 1 ? 1 : (ind > 199 ? 199 : ind);
-  const R deli1 = mmin(R(1.0), xi - R(ind));
-  const R fww = A.SWELLFT[ind - 1] * (R(1.0) - deli1) + A.SWELLFT[ind] * deli1;
-  const R temp2 = fww * uorbt;
-  const R zs = (re - K::SWELLF4) / K::SWELLF7, th = mtanh(zs);
-  const R smooth = R(0.5) * th, pturb = R(0.5) + smooth, pvisc = R(0.5) - smooth;
-  const R sgn[2] = {R(1), R(-1)};
-  R usg[2];
-  for (int g = 0; g < 2; ++g) { const R a = USTAR * (R(1.0) + sgn[g] * sig_n); usg[g] = a * a; }
-  const R su = msin(P.UDIR), cu = mcos(P.UDIR);
-  const R taux[2] = {usg[0] * su, usg[1] * su}, tauy[2] = {usg[0] * cu, usg[1] * cu};
-  const R rogoroair = rog / mmax(P.ROAIRN, R(1.0));
-  const R roairn_pvisc = P.ROAIRN * pvisc;
-  // reverse over frequency with the adjoints of the sheltering sums
-  R lxst[2] = {0, 0}, lyst[2] = {0, 0}, ltaux[2] = {0, 0}, ltauy[2] = {0, 0};
-  R lpturb = 0, lpvisc = 0, ltemp2 = 0, luo = 0, lao = 0;
-  for (int m = ml - 1; m >= 0; --m) {
-    const R xst[2] = {tape[tape_sin(call, 0, ml) + m], tape[tape_sin(call, 1, ml) + m]};
-    const R yst[2] = {tape[tape_sin(call, 2, ml) + m], tape[tape_sin(call, 3, ml) + m]};
-    const R sig = Ph::ZPI * A.FR[m], sig2 = sig * sig;
-    R xk, cm;
-    if (A.shallow) { xk = tfak(A, P, m); cm = xk * (R(1.0) / sig); }
-    else { cm = sig / Ph::G; xk = sig2 / Ph::G; }
-    R tpx[2], tpy[2], ustp[2], usdirp[2], ucn[2], ucnz[2];
-    for (int g = 0; g < 2; ++g) {
-      tpx[g] = taux[g] - shelter * xst[g]; tpy[g] = tauy[g] - shelter * yst[g];
-      ustp[g] = mpow(tpx[g] * tpx[g] + tpy[g] * tpy[g], R(0.25));
-      usdirp[g] = matan2(tpx[g], tpy[g]);
-      ucn[g] = ustp[g] * cm;
-      ucnz[g] = Ph::XKAPPA / (ucn[g] + A.ZALP);
-    }
-    const R constf = rogoroair * cm * A.DFIM[m];
-    const R zcn = mlog(xk * Z0);
-    const R cnsn = (sig * const1) * P.ROAIRN;
-    const R coef = -(K::SWELLF * R(16.) * sig2 / (Ph::G * Ph::ROWATER));
-    const R coef5 = -(K::SWELLF5 * R(2.) * msqrt(R(2.) * nu * sig) / Ph::ROWATER);
-    const R dstab1 = coef5 * roairn_pvisc * xk;
-    const R tmp1 = coef * P.ROAIRN;
-    const R lst = R(0);  // the step uses SX and SY only (STRESSO's PPHI feeds the flux module)
-    const R lSX = lsx ? lsx[m] : R(0), lSY = lsy ? lsy[m] : R(0);
-    R lustp[2] = {0, 0}, lusdirp[2] = {0, 0}, lucn[2] = {0, 0}, lucnz[2] = {0, 0}, lzcn = 0, ldstab1 = 0;
-    for (int k = 0; k < kl; ++k) {
-      const int b = k + kl * m;
-      const R f = F[b];
-      R c[2], ufac[2], dstab[2], slpu[2], zlog[2], xx[2];
-      bool act[2];
-      for (int g = 0; g < 2; ++g) {
-        c[g] = mcos(A.TH[k] - usdirp[g]);
-        ufac[g] = 0; act[g] = false; zlog[g] = 0; xx[g] = 0;
-        if (c[g] > R(0.01)) {
-          xx[g] = c[g] * ucn[g];
-          zlog[g] = zcn + ucnz[g] / c[g];
-          if (zlog[g] < R(0.0)) { const R z2x = zlog[g] * zlog[g] * xx[g]; ufac[g] = mexp(zlog[g]) * z2x * z2x; act[g] = true; }
-        }
-        dstab[g] = dstab1 + pturb * (tmp1 * (temp2 + (K::FU + K::FUD * c[g]) * ustp[g]));
-        slpu[g] = cnsn * ufac[g];
-      }
-      const R fl = R(0.5) * ((slpu[0] + dstab[0]) + (slpu[1] + dstab[1]));
-      const R lsl = lSL ? (*lSL)[b] : R(0), lfl_out = lFL ? (*lFL)[b] : R(0);
-      const R lfl = lsl * f + lfl_out;
-      R lf = lsl * fl;
-      const R lspos = lst + lSX * A.SINTH[k] + lSY * A.COSTH[k];
-      for (int g = 0; g < 2; ++g) {
-        const R lslpf = R(0.5) * lspos + lxst[g] * (constf * A.SINTH[k]) + lyst[g] * (constf * A.COSTH[k]);
-        const R lflp = R(0.5) * lfl;
-        const R lslpu = lflp + lslpf * f;
-        lf = lf + lslpf * slpu[g];
-        const R ldstab = lflp;
-        const R lufac = lslpu * cnsn;
-        ldstab1 = ldstab1 + ldstab;
-        lpturb = lpturb + ldstab * (tmp1 * (temp2 + (K::FU + K::FUD * c[g]) * ustp[g]));
-        ltemp2 = ltemp2 + ldstab * pturb * tmp1;
-        R lc = ldstab * pturb * tmp1 * K::FUD * ustp[g];
-        lustp[g] = lustp[g] + ldstab * pturb * tmp1 * (K::FU + K::FUD * c[g]);
-        if (act[g]) {
-          const R e = mexp(zlog[g]), z2x = zlog[g] * zlog[g] * xx[g];
-          const R lzlog = lufac * e * z2x * (z2x + R(4) * zlog[g] * xx[g]);
-          const R lx = lufac * e * R(2) * z2x * zlog[g] * zlog[g];
-          lc = lc + lx * ucn[g];
-          lucn[g] = lucn[g] + lx * c[g];
-          lzcn = lzcn + lzlog;
-          lucnz[g] = lucnz[g] + lzlog / c[g];
-          lc = lc - lzlog * ucnz[g] / (c[g] * c[g]);
-        }
-        lusdirp[g] = lusdirp[g] + lc * msin(A.TH[k] - usdirp[g]);
-      }
-      lamF[b] += lf;
-    }
-    for (int g = 0; g < 2; ++g) {
-      const R d = ucn[g] + A.ZALP;
-      lucn[g] = lucn[g] - lucnz[g] * Ph::XKAPPA / (d * d);
-      lustp[g] = lustp[g] + lucn[g] * cm;
-      const R q = tpx[g] * tpx[g] + tpy[g] * tpy[g];
-      R ltpx = 0, ltpy = 0;
-      if (q > R(0)) {
-        const R lq = lustp[g] * R(0.25) * mpow(q, R(-0.75));
-        ltpx = lq * R(2) * tpx[g] + lusdirp[g] * tpy[g] / q;
-        ltpy = lq * R(2) * tpy[g] - lusdirp[g] * tpx[g] / q;
-      }
-      ltaux[g] = ltaux[g] + ltpx;
-      ltauy[g] = ltauy[g] + ltpy;
-      lxst[g] = lxst[g] - shelter * ltpx;
-      lyst[g] = lyst[g] - shelter * ltpy;
-    }
-    lZ0 = lZ0 + lzcn / Z0;
-    lpvisc = lpvisc + ldstab1 * coef5 * P.ROAIRN * xk;
-  }
-  // prologue^T
-  R lsig_n = 0;
-  for (int g = 0; g < 2; ++g) {
-    const R lusg = ltaux[g] * su + ltauy[g] * cu;
-    const R a = USTAR * (R(1.0) + sgn[g] * sig_n);
-    const R la = R(2) * a * lusg;
-    lUS = lUS + la * (R(1.0) + sgn[g] * sig_n);
-    lsig_n = lsig_n + la * USTAR * sgn[g];
-  }
-  const R lsmooth = lpturb - lpvisc;
-  const R lre = lsmooth * R(0.5) * (R(1) - th * th) / K::SWELLF7;
-  R luorbt = ltemp2 * fww, laorb = 0;
-  const R lfww = ltemp2 * uorbt;
-  const R ldeli1 = lfww * (A.SWELLFT[ind] - A.SWELLFT[ind - 1]);
-  const R lxi = ((xi - R(ind)) < R(1.0)) ? ldeli1 : R(0);
-  R lz0noz = 0;
-  if (!(ratio < R(3.0))) {
-    const R lratio = lxi * delabm1 / (ratio * mlog(R(10)));
-    laorb = laorb + lratio / z0noz;
-    lz0noz = -lratio * aorb / (z0noz * z0noz);
-  }
-  if (!(a1 < a2)) { if (!(USTAR < R(0.0001))) lUS = lUS - lz0noz * Ph::RNUAIRM / (USTAR * USTAR); }
-  else if (Z0 < R(0.0005)) lZ0 = lZ0 + lz0noz * R(0.04);
-  luorbt = luorbt + lre * (R(4.0) / nu) * aorb;
-  laorb = laorb + lre * (R(4.0) / nu) * uorbt;
-  luo = luorbt / msqrt(tiny + uo);
-  lao = laorb / msqrt(tiny + ao);
-  for (int m = 0; m < ml; ++m) {
-    const R sig = Ph::ZPI * A.FR[m];
-    const R ltm = luo * A.DFIM[m] * (sig * sig) + lao * A.DFIM[m];
-    for (int k = 0; k < kl; ++k) lamF[k + kl * m] += ltm;
-  }
-  // WSIGSTAR by two dual passes
-  {
-    using D = Dual<R>;
-    const D a = wsigstar(P, D(USTAR, R(1)), D(Z0)), b = wsigstar(P, D(USTAR), D(Z0, R(1)));
-    lUS = lUS + lsig_n * a.d;
-    lZ0 = lZ0 + lsig_n * b.d;
-  }
-}
-
-// The whole IMPLSCH adjoint of one point.  In: lam = adjoint of the output
-// spectrum, lTAUW = adjoint of the output TAUW.  Out: lam = adjoint of the
-// input spectrum, lTAUW0 and lU10.  Work columns as for `forward`, plus lSL
-// and lFL.  USTAR and Z0 on entry do not enter the step (AIRSEA recomputes
-// them), so they have no adjoint.
-template <typename R>
-WAHD void reverse(const ATabs<R>& A, const PointIn<R>& P, Col<const R> F0, R TAUW0, R U10, Col<R> Fw, Col<R> SL, Col<R> FL,
-                  Col<uint8_t> LL1, Col<uint8_t> LL, Col<R> tape, Col<R> lam, Col<R> lSL, Col<R> lFL, R lTAUW,
-                  R& lTAUW0, R& lU10) {
-  const int kl = A.KL, ml = A.ML, n = kl * ml;
-  int it[TI_COUNT];
-  R tw, us, z0;
-  forward<R, R>(A, P, F0, TAUW0, U10, Fw, SL, FL, LL1, LL, tape, it, tw, us, z0);
-  const int mij = it[TI_MIJ], mij2 = it[TI_MIJ2], ju = it[TI_JU];
-  const R us1 = tape[tape_scalar(TS_USTAR1, ml)], z01 = tape[tape_scalar(TS_Z01, ml)];
-  const R tauw1 = tape[tape_scalar(TS_TAUW1, ml)];
-  const R us2 = tape[tape_scalar(TS_USTAR2, ml)], z02 = tape[tape_scalar(TS_Z02, ml)];
-  const R fmean = tape[tape_scalar(TS_FMEAN, ml)], fmeanws = tape[tape_scalar(TS_FMEANWS, ml)];
-  const R akmean = tape[tape_scalar(TS_AKMEAN, ml)];
-  const R fmx = mmax(fmeanws, fmean);
-  // F1 = F0 with the first tail
-  for (int b = 0; b < n; ++b) Fw[b] = F0[b];
-  imphftail(A, P, Fw, mij);
-  for (int b = 0; b < n; ++b) { lSL[b] = 0; lFL[b] = 0; }
-  // final tail, update, DIA, dissipation
-  imphftail_adj(A, P, lam, mij2);
-  R lus2 = 0, lz02 = 0, lfmx = 0;
-  update_adj(A, P, Fw, SL, FL, us2, fmx, ju, lam, lSL, lFL, lus2, lfmx);
-  const R lak = snonlin_adj(A, P, Fw, akmean, lSL, lFL, lam);
-  sdissip_adj(A, P, Fw, lSL, lFL, lam);
-  // second STRESSO and SINPUT on F1
-  R lsx[MAX_ML], lsy[MAX_ML];
-  stresso_adj(A, P, Fw, mij, us2, z02, tape, 1, lTAUW, lsx, lsy, lam, lus2, lz02);
-  sinput_adj(A, P, Fw, us2, z02, tape, 1, &lSL, &lFL, lsx, lsy, lam, lus2, lz02);
-  imphftail_adj(A, P, lam, mij);
-  // second AIRSEA, first STRESSO and SINPUT on F0
-  const Jac2<R> J2 = airsea_jac(A, U10, tauw1);
-  lU10 = J2.d00 * lus2 + J2.d10 * lz02;
-  const R ltauw1 = J2.d01 * lus2 + J2.d11 * lz02;
-  R lus1 = 0, lz01 = 0;
-  stresso_adj(A, P, F0, mij, us1, z01, tape, 0, ltauw1, lsx, lsy, lam, lus1, lz01);
-  sinput_adj(A, P, F0, us1, z01, tape, 0, (const Col<R>*)nullptr, (const Col<R>*)nullptr, lsx, lsy, lam, lus1, lz01);
-  // the integrals of the input spectrum (FMX and AKMEAN)
-  R lfmean = 0, lfmeanws = 0;
-  if (fmeanws < fmean) lfmean = lfmx; else lfmeanws = lfmx;
-  const Col<const uint8_t> nomask{nullptr, 0}, llc1{LL1.p, LL1.ld};
-  integrals_adj(A, P, F0, nomask, R(0), lfmean, lak, A.shallow && A.isnonlin == 0, lam);
-  integrals_adj(A, P, F0, llc1, R(0), lfmeanws, R(0), false, lam);
-  // first AIRSEA
-  const Jac2<R> J1 = airsea_jac(A, U10, TAUW0);
-  lU10 = lU10 + J1.d00 * lus1 + J1.d10 * lz01;
-  lTAUW0 = J1.d01 * lus1 + J1.d11 * lz01;
-}
+// Jacobian of a scalar routine with two inputs (d out_i / d in_j).
+template <typename R> struct Jac2 { R d00, d01, d10, d11; };
 
 }  // namespace adj
 }  // namespace wamgpu
