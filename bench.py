@@ -171,6 +171,39 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def transfer_bound(torch, dev, hf, reps=3):
+    """The host link for the e2e step's bytes: the pinned spectrum copied up
+    alone, down alone, and both at once on two streams (best of `reps`, wall
+    clock around synchronised copies).  The e2e step cannot beat the
+    concurrent figure."""
+    up_dst = torch.empty(hf.numel(), dtype=hf.dtype, device=dev)
+    down_src = torch.empty_like(up_dst)
+    down_dst = torch.empty(hf.numel(), dtype=hf.dtype, pin_memory=True)
+    src = hf.view(-1)
+    su, sd = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def timed(up, down):
+        best = None
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            if up:
+                with torch.cuda.stream(su):
+                    up_dst.copy_(src, non_blocking=True)
+            if down:
+                with torch.cuda.stream(sd):
+                    down_dst.copy_(down_src, non_blocking=True)
+            torch.cuda.synchronize()
+            t = time.perf_counter() - t0
+            best = t if best is None else min(best, t)
+        return best
+
+    nbytes = src.numel() * src.element_size()
+    t_up, t_down, t_both = timed(True, False), timed(False, True), timed(True, True)
+    return {"spectrum_bytes": nbytes, "h2d_gbs": nbytes / t_up / 1e9, "d2h_gbs": nbytes / t_down / 1e9,
+            "both_directions_ms": 1e3 * t_both, "sequential_ms": 1e3 * (t_up + t_down)}
+
+
 def batched_ensemble(dev, steps, warmup, n_members=32):
     """The 32-member ensemble (uneven regional grids, mixed KL/ML and ST4/ST6,
     900 s steps): one autotuned batched pass replayed from a CUDA graph per
@@ -465,7 +498,8 @@ def main():
         d2h = 4 * (n * KL * ML + 3 * n)
         e2e = {"value": bins * ksteps / dt, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "steps": ksteps, "ms_per_step": 1e3 * dt / ksteps,
-               "how": "wamgpu_step_host on pinned host FL3 + fields: H2D, 5 PROPAGS + IMPLSCH, D2H each step"}
+               "how": "wamgpu_step_host on pinned host FL3 + fields: H2D, 5 PROPAGS + IMPLSCH, D2H each step",
+               "transfer_bound": transfer_bound(torch, dev, hf)}
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
         r = cpu_reference(args, args.workload, 0.125, 15.0)
