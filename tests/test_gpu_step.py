@@ -35,7 +35,7 @@ CASES = [("c0", 0.25, False, False), ("c1", 0.02, False, False), ("c1", 0.02, Fa
 
 
 @pytest.mark.parametrize("name,scale,currents,lcflx", CASES,
-                         ids=["c0", "c1", "c1-lcflx", "c2-currents", "c1-32-chunks-currents"])
+                         ids=["c0", "c1", "c1-lcflx", "c2-currents", "c1-64-chunks-currents"])
 def test_step_paths_identical(name, scale, currents, lcflx):
     import torch
     from wam_b200.synth import make_workload

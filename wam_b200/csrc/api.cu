@@ -873,7 +873,7 @@ int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float*
   // precedes sub-step j+1 of chunk q-1, which overwrites its input; and
   // IMPLSCH of chunk q follows the last sub-step of chunks q-1..q+1.
   const int width = std::max(ctx->halo, 1);
-  const int nq = n > 0 ? std::min(32, std::max(1, n / width)) : 1;
+  const int nq = n > 0 ? std::min(64, std::max(1, n / width)) : 1;
   std::vector<int> lo(nq + 1);
   for (int q = 0; q <= nq; ++q) lo[q] = (int)((long long)n * q / nq);
   const int nev = 2 * nq;
