@@ -835,6 +835,11 @@ int implsch_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, const float* u10, co
   return wamgpu_sync(ctx);
 }
 
+// Chunks per host<->device copy piece of wamgpu_step_host.  One: pieces of
+// 2 and 4 chunks (longer copy rows) made the regional step 1-4 % slower, the
+// later first download costing more than the rows gained.
+constexpr int kChunksPerCopy = 1;
+
 // Host-buffer form of one WAMODEL pass, with the copies overlapped (see the
 // chunk pipeline below).  Results are identical to the unsplit sequence:
 // every kernel sees the same inputs and writes the same elements.
@@ -876,7 +881,10 @@ int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float*
   const int nq = n > 0 ? std::min(64, std::max(1, n / width)) : 1;
   std::vector<int> lo(nq + 1);
   for (int q = 0; q <= nq; ++q) lo[q] = (int)((long long)n * q / nq);
-  const int nev = 2 * nq;
+  // copies move pieces of kChunksPerCopy chunks
+  const int cpc = kChunksPerCopy, npc = (nq + cpc - 1) / cpc;
+  auto piece_lo = [&](int p) { return lo[std::min(nq, p * cpc)]; };
+  const int nev = 2 * npc;
   if ((int)ctx->xfer_ev.size() < nev)
     for (int i = (int)ctx->xfer_ev.size(); i < nev; ++i) {
       cudaEvent_t e;
@@ -884,17 +892,18 @@ int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float*
       ctx->xfer_ev.push_back(e);
     }
   cudaStream_t d = ctx->down_stream;
-  // the spectrum chunk by chunk (the per-point fields went up on s above)
-  for (int q = 0; q < nq; ++q) {
-    const size_t w = (size_t)(lo[q + 1] - lo[q]) * 4;
-    if (w) CK(cudaMemcpy2DAsync(f3 + lo[q], (size_t)n * 4, fl3 + lo[q], (size_t)n * 4, w, (size_t)KL * ML,
+  // the spectrum piece by piece (the per-point fields went up on s above)
+  for (int p = 0; p < npc; ++p) {
+    const int a0 = piece_lo(p);
+    const size_t w = (size_t)(piece_lo(p + 1) - a0) * 4;
+    if (w) CK(cudaMemcpy2DAsync(f3 + a0, (size_t)n * 4, fl3 + a0, (size_t)n * 4, w, (size_t)KL * ML,
                                 cudaMemcpyHostToDevice, c), "H2D");
-    CK(cudaEventRecord(ctx->xfer_ev[q], c), "event");
+    CK(cudaEventRecord(ctx->xfer_ev[p], c), "event");
   }
   R* buf[2] = {f3, sc};
   const R* fin = buf[nsub % 2];  // the buffer the last sub-step writes
   auto ready = [&](int q) -> int {  // chunk q and its neighbours are on the device
-    CK(cudaStreamWaitEvent(s, ctx->xfer_ev[std::min(q + 1, nq - 1)], 0), "wait");
+    CK(cudaStreamWaitEvent(s, ctx->xfer_ev[std::min(q + 1, nq - 1) / cpc], 0), "wait");
     return WAMGPU_OK;
   };
   const int last = (nq - 1) + nsub;
@@ -926,16 +935,19 @@ int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float*
       a.wncg = ctx->wncg_valid ? I.wncg.template as<R>() + (size_t)p0 * 2 * ctx->cfg.ml : nullptr;
       { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch"); }
     }
-    CK(cudaEventRecord(ctx->xfer_ev[nq + q], s), "event");
-    CK(cudaStreamWaitEvent(d, ctx->xfer_ev[nq + q], 0), "wait");
-    if (p1 > p0) {
-      const size_t w = (size_t)(p1 - p0) * 4;
-      CK(cudaMemcpy2DAsync(fl3 + p0, (size_t)n * 4, f3 + p0, (size_t)n * 4, w, (size_t)KL * ML, cudaMemcpyDeviceToHost, d), "D2H");
-      CK(cudaMemcpyAsync(tauw + p0, I.tauw.template as<R>() + p0, w, cudaMemcpyDeviceToHost, d), "D2H");
-      CK(cudaMemcpyAsync(ustar + p0, I.ustar.template as<R>() + p0, w, cudaMemcpyDeviceToHost, d), "D2H");
-      CK(cudaMemcpyAsync(z0 + p0, I.z0.template as<R>() + p0, w, cudaMemcpyDeviceToHost, d), "D2H");
+    if (q % cpc == cpc - 1 || q == nq - 1) {  // the last chunk of a piece: the piece goes down
+      const int pc = q / cpc, a0 = piece_lo(pc);
+      CK(cudaEventRecord(ctx->xfer_ev[npc + pc], s), "event");
+      CK(cudaStreamWaitEvent(d, ctx->xfer_ev[npc + pc], 0), "wait");
+      const size_t w = (size_t)(piece_lo(pc + 1) - a0) * 4;
+      if (w) CK(cudaMemcpy2DAsync(fl3 + a0, (size_t)n * 4, f3 + a0, (size_t)n * 4, w, (size_t)KL * ML,
+                                  cudaMemcpyDeviceToHost, d), "D2H");
     }
   }
+  // TAUW, USTAR, Z0 after the last piece (d follows the last IMPLSCH)
+  CK(cudaMemcpyAsync(tauw, I.tauw.template as<R>(), (size_t)n * 4, cudaMemcpyDeviceToHost, d), "D2H");
+  CK(cudaMemcpyAsync(ustar, I.ustar.template as<R>(), (size_t)n * 4, cudaMemcpyDeviceToHost, d), "D2H");
+  CK(cudaMemcpyAsync(z0, I.z0.template as<R>(), (size_t)n * 4, cudaMemcpyDeviceToHost, d), "D2H");
   CK(cudaStreamSynchronize(d), "step copies");
   CK(cudaStreamSynchronize(c), "step copies");
   CK(cudaStreamSynchronize(s), "step sync");
