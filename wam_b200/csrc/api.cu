@@ -880,7 +880,21 @@ int step_host_t(wamgpu_ctx* ctx, Impl<R>& I, float* fl3, int nprop, const float*
   const int width = std::max(ctx->halo, 1);
   const int nq = n > 0 ? std::min(64, std::max(1, n / width)) : 1;
   std::vector<int> lo(nq + 1);
-  for (int q = 0; q <= nq; ++q) lo[q] = (int)((long long)n * q / nq);
+  {
+    // The first nsub+2 chunks are small (a quarter of the others, and at least
+    // one neighbour distance), so that the first IMPLSCH, and with it the
+    // first download, starts after a few MB have gone up rather than after
+    // nsub+2 full chunks.  The other chunks share the rest evenly.
+    const int nsmall = std::min(nq - 1, nsub + 2);
+    const int small = std::max(width, n / (4 * nq));
+    if (nq > nsmall + 1 && (long long)small * nsmall < n / 2) {
+      for (int q = 0; q <= nsmall; ++q) lo[q] = q * small;
+      const int rest = n - lo[nsmall], nr = nq - nsmall;
+      for (int q = 1; q <= nr; ++q) lo[nsmall + q] = lo[nsmall] + (int)((long long)rest * q / nr);
+    } else {
+      for (int q = 0; q <= nq; ++q) lo[q] = (int)((long long)n * q / nq);
+    }
+  }
   // copies move pieces of kChunksPerCopy chunks
   const int cpc = kChunksPerCopy, npc = (nq + cpc - 1) / cpc;
   auto piece_lo = [&](int p) { return lo[std::min(nq, p * cpc)]; };
