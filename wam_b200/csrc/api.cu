@@ -1,6 +1,7 @@
 // C ABI of libwamgpu (declarations and reference citations in include/wamgpu.h).
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <climits>
 #include <functional>
 #include <cmath>
 #include <cstdio>
@@ -194,6 +195,38 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
   d.ld = t.KL | 1;
   d.scr = (std::max(std::max(t.ML, t.KL), nk10) + 31) / 32 * 32;
   d.need_sp = c.lcflx ? 1 : 0;
+  // The DIA forms the interactions of the directions beyond the first 32
+  // (NX = KL - 32) for a batch of consecutive MCs in one pass.  The batch's
+  // slots take 8*NX reals per MC of scratch after the 8*KL of the per-MC
+  // buffer, and the batch updates its target rows one kind (MC, MM, MM1, MP,
+  // MP1) at a time, so the rows that one kind writes must be distinct within
+  // a batch: strictly increasing in MC.  Otherwise the batch is one MC.
+  d.dia_batch = 1;
+  if (t.KL > 32) {
+    const int nx = t.KL - 32, ML = t.ML, mfr1 = -t.MFRSTLW + 1, mfrl = ML - t.KFRH + mfr1;
+    int b = 32 / nx;
+    while (b > 1 && 8 * t.KL + 8 * nx * b > 8 * d.scr) --b;
+    if (8 * t.KL + 8 * nx * b > 8 * d.scr) d.scr = ((8 * t.KL + 8 * nx * b + 7) / 8 + 31) / 32 * 32;
+    int last[5] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN};
+    bool mono = true;
+    for (int mc = 1; mc <= t.MLSTHG; ++mc) {
+      const int i = mc - t.MFRSTLW, MP = t.IKP[i], MP1 = t.IKP1[i], MM = t.IKM[i], MM1 = t.IKM1[i];
+      const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
+      const bool wr[5] = {regime != 1 || (MM1 <= ML && mc <= ML), regime != 2,
+                          regime == 0 || (regime == 1 && MM1 <= ML) || (regime == 2 && MM1 >= 1),
+                          regime != 1 || (MM1 <= ML && mc <= ML && MP <= ML),
+                          regime != 1 || (MM1 <= ML && mc <= ML && MP <= ML && MP1 <= ML)};
+      const int row[5] = {mc, MM, MM1, MP, MP1};
+      for (int q = 0; q < 5; ++q)
+        if (wr[q]) {
+          if (row[q] <= last[q]) mono = false;
+          last[q] = row[q];
+        }
+    }
+    if (!mono) b = 1;
+    const int nbatch = (t.MLSTHG + b - 1) / b;
+    d.dia_batch = nbatch > 0 ? (t.MLSTHG + nbatch - 1) / nbatch : 1;  // the same batch count, evenly filled
+  }
   d.iphys = c.iphys; d.shallow = c.shallow_run; d.isnonlin = c.isnonlin; d.lcflx = c.lcflx;
   d.DELTH = t.DELTH; d.DELTR = t.DELTR; d.INV_LOG_CO = t.INV_LOG_CO; d.MO_TAIL = t.MO_TAIL; d.MM1_TAIL = t.MM1_TAIL;
   d.DELU = t.DELU; d.DAL1 = t.DAL1; d.DAL2 = t.DAL2; d.X0TAUHF = t.X0TAUHF;

@@ -507,17 +507,66 @@ template <typename R> struct Src {
   // rotated back.  The target rows of one MC are distinct (checked on the
   // host), and no two lanes write the same column, so the only ordering
   // needed is around the buffer.
+  //
+  // With KL > 32 the directions 32..KL-1 (NX of them) would take a second,
+  // mostly idle pass per MC.  They are done for a batch of T.dia_batch
+  // consecutive MCs at once, one lane per (MC of the batch, direction):
+  //   - before the batch, one pass forms their interactions for every MC of
+  //     the batch into the batch slots;
+  //   - each MC's pass copies its slot into the buffer and, once the buffer
+  //     is complete, leaves in the slot the four KH-summed gathers that the
+  //     columns 32..KL-1 need;
+  //   - after the batch, one pass updates those columns of the five target
+  //     rows, one row kind at a time.  The rows of one kind are distinct
+  //     within a batch (strictly increasing in MC, checked on the host), and
+  //     the kinds are separated by barriers, so no two lanes write one bin
+  //     at once.
+  // The columns 32..KL-1 thus add the contributions of a batch kind by kind
+  // rather than MC by MC: a different FP association, like the gather form.
+  struct DiaMc {
+    const R* rc;
+    R ftemp, ftail;
+    int rIC, rIP, rIP1, rIM, rIM1;       // gathered rows (offsets)
+    int rMC, rMM, rMM1, rMP, rMP1;       // target rows (offsets; row 0 where not written)
+    bool wMC, wMM, wMM1, wMP, wMP1;      // which targets this MC writes
+  };
+  __device__ DiaMc dia_mc(int mc, R enhfr, int mfr1, int mfrl) const {
+    const int ml = ML(), ld = w.ld;
+    DiaMc d;
+    const int im = mc - T.MFRSTLW;
+    const int MP = S.IKP[im], MP1 = S.IKP1[im], MM = S.IKM[im], MM1 = S.IKM1[im];
+    const int* ic5 = S.INL + 5 * (mc - 1);
+    d.rIC = ld * (ic5[0] - 1); d.rIP = ld * (ic5[1] - 1); d.rIP1 = ld * (ic5[2] - 1);
+    d.rIM = ld * (ic5[3] - 1); d.rIM1 = ld * (ic5[4] - 1);
+    d.rc = S.RNL + 25 * (mc - 1);
+    d.ftemp = S.AF11[im];
+    if (T.shallow) d.ftemp = d.ftemp * (T.isnonlin == 0 ? enhfr : __ldg(&ENH[ij + (size_t)enh_ld * (mc - 1)]));
+    const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
+    d.ftail = (regime == 0) ? R(1) : d.rc[0];
+    d.wMM = regime != 2;
+    d.wMM1 = regime == 0 || (regime == 1 && MM1 <= ml) || (regime == 2 && MM1 >= 1);
+    d.wMC = regime != 1 || (MM1 <= ml && mc <= ml);
+    d.wMP = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml);
+    d.wMP1 = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml && MP1 <= ml);
+    // rows this MC does not write are clamped to row 0, so the loads never
+    // leave the spectrum
+    d.rMC = d.wMC ? ld * (mc - 1) : 0; d.rMM = d.wMM ? ld * (MM - 1) : 0; d.rMM1 = d.wMM1 ? ld * (MM1 - 1) : 0;
+    d.rMP = d.wMP ? ld * (MP - 1) : 0; d.rMP1 = d.wMP1 ? ld * (MP1 - 1) : 0;
+    return d;
+  }
+
   __device__ void snonlin(R AKMEAN) const {
-    const int kl = KL(), ml = ML(), ld = w.ld;
+    const int kl = KL(), ld = w.ld;
     R enhfr = R(1);
     if (T.shallow && T.isnonlin == 0) {
       enhfr = dmax(R(0.75) * DEPTH * AKMEAN, R(.5));
       enhfr = R(1.) + (R(5.5) / enhfr) * (R(1.) - R(.833) * enhfr) * dexp(R(-1.25) * enhfr);
     }
-    const int mfr1 = -T.MFRSTLW + 1, mfrl = ml - T.KFRH + mfr1;
+    const int mfr1 = -T.MFRSTLW + 1, mfrl = ML() - T.KFRH + mfr1;
     R2* SF = w.SF; const R* F = w.F;
     R2* XM = reinterpret_cast<R2*>(w.T);  // [kh*kl + k] = {AD, DELAM}
     R2* XP = XM + 2 * kl;                 // [kh*kl + k] = {AD, DELAP}
+    R2* XB = XP + 2 * kl;                 // batch slots, 4*NX per MC of the batch
     // rotation offsets of the partner tables, per KH (warp-uniform)
     int o1[2], o2[2], o11[2], o21[2];
     for (int kh = 0; kh < 2; ++kh) {
@@ -525,68 +574,118 @@ template <typename R> struct Src {
       o11[kh] = S.K11W[kl * kh] - 1; o21[kh] = S.K21W[kl * kh] - 1;
     }
     auto rot = [kl](int k, int o) { const int t = k + o; return t >= kl ? t - kl : t; };
-    const int nsub = kl > 32 ? 2 : 1;
-    for (int mc = 1; mc <= T.MLSTHG; ++mc) {
-      const int im = mc - T.MFRSTLW;
-      const int MP = S.IKP[im], MP1 = S.IKP1[im], MM = S.IKM[im], MM1 = S.IKM1[im];
-      const int* ic5 = S.INL + 5 * (mc - 1);
-      const int rIC = ld * (ic5[0] - 1), rIP = ld * (ic5[1] - 1), rIP1 = ld * (ic5[2] - 1), rIM = ld * (ic5[3] - 1),
-                rIM1 = ld * (ic5[4] - 1);
-      const R* rc = S.RNL + 25 * (mc - 1);
-      R ftemp = S.AF11[im];
-      if (T.shallow) ftemp = ftemp * (T.isnonlin == 0 ? enhfr : __ldg(&ENH[ij + (size_t)enh_ld * (mc - 1)]));
-      const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
-      const R ftail = (regime == 0) ? R(1) : rc[0];
-      // which targets this frequency writes (uniform over the warp)
-      const bool wMM = regime != 2, wMM1 = regime == 0 || (regime == 1 && MM1 <= ml) || (regime == 2 && MM1 >= 1);
-      const bool wMC = regime != 1 || (MM1 <= ml && mc <= ml);
-      const bool wMP = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml);
-      const bool wMP1 = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml && MP1 <= ml);
-      // row offsets of targets this frequency does not write are clamped to row 0,
-      // so the loads below never leave the spectrum
-      const int rMC = wMC ? ld * (mc - 1) : 0, rMM = wMM ? ld * (MM - 1) : 0, rMM1 = wMM1 ? ld * (MM1 - 1) : 0,
-                rMP = wMP ? ld * (MP - 1) : 0, rMP1 = wMP1 ? ld * (MP1 - 1) : 0;
+    // interactions of direction k at one MC, both KH: {AD, DELAM} to xm[kh*skh],
+    // {AD, DELAP} to xp[kh*skh]; AD and DELAD summed over KH to adc, delc
+    auto interact = [&](const DiaMc& d, int k, R2* xm, R2* xp, int skh, R& adc, R& delc) {
+      const R* rc = d.rc;
       const R g1 = rc[1], g2 = rc[2], g3 = rc[3], g4 = rc[4], g5 = rc[13], g6 = rc[14], g7 = rc[15], g8 = rc[16];
-      // 1. interactions (both KH) of this lane's directions
-      R adc[2] = {R(0), R(0)}, delc[2] = {R(0), R(0)};  // centre: AD and DELAD summed over KH
-      for (int s = 0; s < nsub; ++s) {
-        const int k = lane + 32 * s;
-        if (k >= kl) break;
-        const R fij = F[k + rIC] * ftail;
-        for (int kh = 0; kh < 2; ++kh) {
-          const int a1 = rot(k, o1[kh]), a11 = rot(k, o11[kh]), a2 = rot(k, o2[kh]), a21 = rot(k, o21[kh]);
-          R sap = g1 * F[a1 + rIP] + g2 * F[a11 + rIP] + g3 * F[a1 + rIP1] + g4 * F[a11 + rIP1];
-          R sam = g5 * F[a2 + rIM] + g6 * F[a21 + rIM] + g7 * F[a2 + rIM1] + g8 * F[a21 + rIM1];
-          R fad1 = fij * (sap + sam);
-          R fad2 = fad1 - R(2.) * sap * sam;
-          fad1 = fad1 + fad2;
-          R fcen = ftemp * fij;
-          const R ad = fad2 * fcen;
-          adc[s] = adc[s] + ad;
-          delc[s] = delc[s] + fad1 * ftemp;
-          XM[kl * kh + k] = r2(ad, (fij - R(2.) * sap) * T.DAL2 * fcen);
-          XP[kl * kh + k] = r2(ad, (fij - R(2.) * sam) * T.DAL1 * fcen);
+      const R fij = F[k + d.rIC] * d.ftail;
+      adc = R(0); delc = R(0);
+      for (int kh = 0; kh < 2; ++kh) {
+        const int a1 = rot(k, o1[kh]), a11 = rot(k, o11[kh]), a2 = rot(k, o2[kh]), a21 = rot(k, o21[kh]);
+        R sap = g1 * F[a1 + d.rIP] + g2 * F[a11 + d.rIP] + g3 * F[a1 + d.rIP1] + g4 * F[a11 + d.rIP1];
+        R sam = g5 * F[a2 + d.rIM] + g6 * F[a21 + d.rIM] + g7 * F[a2 + d.rIM1] + g8 * F[a21 + d.rIM1];
+        R fad1 = fij * (sap + sam);
+        R fad2 = fad1 - R(2.) * sap * sam;
+        fad1 = fad1 + fad2;
+        R fcen = d.ftemp * fij;
+        const R ad = fad2 * fcen;
+        adc = adc + ad;
+        delc = delc + fad1 * d.ftemp;
+        xm[skh * kh] = r2(ad, (fij - R(2.) * sap) * T.DAL2 * fcen);
+        xp[skh * kh] = r2(ad, (fij - R(2.) * sam) * T.DAL1 * fcen);
+      }
+    };
+    // the five target-row updates of column j from the KH-summed gathers
+    // {a2, d2} (K2W), {a21, d21} (K21W), {a1, d1} (K1W), {a11, d11} (K11W)
+    auto upd_mm = [&](const DiaMc& d, R2& v, R a2, R d2, R a21, R d21) {
+      const R* rc = d.rc; v.x = v.x + (a2 * rc[20] + a21 * rc[19]); v.y = v.y + (d2 * rc[23] + d21 * rc[24]); };
+    auto upd_mm1 = [&](const DiaMc& d, R2& v, R a2, R d2, R a21, R d21) {
+      const R* rc = d.rc; v.x = v.x + (a2 * rc[17] + a21 * rc[18]); v.y = v.y + (d2 * rc[21] + d21 * rc[22]); };
+    auto upd_mp = [&](const DiaMc& d, R2& v, R a1, R d1, R a11, R d11) {
+      const R* rc = d.rc; v.x = v.x + (a1 * rc[8] + a11 * rc[7]); v.y = v.y + (d1 * rc[11] + d11 * rc[12]); };
+    auto upd_mp1 = [&](const DiaMc& d, R2& v, R a1, R d1, R a11, R d11) {
+      const R* rc = d.rc; v.x = v.x + (a1 * rc[5] + a11 * rc[6]); v.y = v.y + (d1 * rc[9] + d11 * rc[10]); };
+
+    const int kmain = kl < 32 ? kl : 32;          // directions of the per-MC pass (lane = k)
+    const int nx = kl > 32 ? kl - 32 : 0;         // directions done per batch
+    const int bsz = max(1, nx > 0 ? T.dia_batch : T.MLSTHG);
+    // this lane's batch item (MC lb of the batch, direction 32 + lx), and its
+    // slot entry i = lane < 4*NX: the copy target in the buffer, and the two
+    // buffer entries whose sum the columns 32..KL-1 need
+    const int lb = nx > 0 ? lane / nx : 0, lx = nx > 0 ? lane - lb * nx : 0;
+    int cdst = 0, sa = 0, sb = 0;
+    if (lane < 4 * nx) {
+      const int q = lane / nx, part = q >> 1, kh = q & 1, j = 32 + lx;
+      cdst = part * 2 * kl + kh * kl + j;  // slot layout [XM|XP][kh][x]
+      const int oa = q == 0 ? o2[0] : q == 1 ? o21[0] : q == 2 ? o1[0] : o11[0];
+      const int ob = q == 0 ? o2[1] : q == 1 ? o21[1] : q == 2 ? o1[1] : o11[1];
+      const int base = q < 2 ? 0 : 2 * kl;  // K2W, K21W read XM; K1W, K11W read XP
+      sa = base + rot(j, kl - oa); sb = base + kl + rot(j, kl - ob);
+    }
+    for (int mc0 = 1; mc0 <= T.MLSTHG; mc0 += bsz) {
+      const int nb = min(bsz, T.MLSTHG - mc0 + 1);
+      const bool lact = nx > 0 && lb < nb;
+      R ladc = R(0), ldelc = R(0);
+      if (nx > 0) {
+        if (lact) {
+          const DiaMc d = dia_mc(mc0 + lb, enhfr, mfr1, mfrl);
+          R2* xs = XB + 4 * nx * lb + lx;
+          interact(d, 32 + lx, xs, xs + 2 * nx, nx, ladc, ldelc);
         }
+        __syncwarp();
       }
-      __syncwarp();
-      // 2. this lane's column j of the five target rows
-      for (int s = 0; s < nsub; ++s) {
-        const int j = lane + 32 * s;
-        if (j >= kl) break;
-        const R2 m2a = XM[rot(j, kl - o2[0])], m2b = XM[kl + rot(j, kl - o2[1])];
-        const R2 m21a = XM[rot(j, kl - o21[0])], m21b = XM[kl + rot(j, kl - o21[1])];
-        const R2 p1a = XP[rot(j, kl - o1[0])], p1b = XP[kl + rot(j, kl - o1[1])];
-        const R2 p11a = XP[rot(j, kl - o11[0])], p11b = XP[kl + rot(j, kl - o11[1])];
-        R2 vC = SF[j + rMC], vM = SF[j + rMM], vM1 = SF[j + rMM1], vP = SF[j + rMP], vP1 = SF[j + rMP1];
-        const R a2 = m2a.x + m2b.x, d2 = m2a.y + m2b.y, a21 = m21a.x + m21b.x, d21 = m21a.y + m21b.y;
-        const R a1 = p1a.x + p1b.x, d1 = p1a.y + p1b.y, a11 = p11a.x + p11b.x, d11 = p11a.y + p11b.y;
-        if (wMC) { vC.x = vC.x - R(2.) * adc[s]; vC.y = vC.y - R(2.) * delc[s]; SF[j + rMC] = vC; }
-        if (wMM) { vM.x = vM.x + (a2 * rc[20] + a21 * rc[19]); vM.y = vM.y + (d2 * rc[23] + d21 * rc[24]); SF[j + rMM] = vM; }
-        if (wMM1) { vM1.x = vM1.x + (a2 * rc[17] + a21 * rc[18]); vM1.y = vM1.y + (d2 * rc[21] + d21 * rc[22]); SF[j + rMM1] = vM1; }
-        if (wMP) { vP.x = vP.x + (a1 * rc[8] + a11 * rc[7]); vP.y = vP.y + (d1 * rc[11] + d11 * rc[12]); SF[j + rMP] = vP; }
-        if (wMP1) { vP1.x = vP1.x + (a1 * rc[5] + a11 * rc[6]); vP1.y = vP1.y + (d1 * rc[9] + d11 * rc[10]); SF[j + rMP1] = vP1; }
+      for (int b = 0; b < nb; ++b) {
+        const DiaMc d = dia_mc(mc0 + b, enhfr, mfr1, mfrl);
+        // 1. interactions (both KH) of this lane's direction; the batch's
+        // directions come from the slot
+        R adc = R(0), delc = R(0);
+        if (lane < kmain) interact(d, lane, XM + lane, XP + lane, kl, adc, delc);
+        if (lane < 4 * nx) XM[cdst] = XB[4 * nx * b + lane];
+        __syncwarp();
+        // 2. this lane's column j of the five target rows
+        if (lane < kmain) {
+          const int j = lane;
+          const R2 m2a = XM[rot(j, kl - o2[0])], m2b = XM[kl + rot(j, kl - o2[1])];
+          const R2 m21a = XM[rot(j, kl - o21[0])], m21b = XM[kl + rot(j, kl - o21[1])];
+          const R2 p1a = XP[rot(j, kl - o1[0])], p1b = XP[kl + rot(j, kl - o1[1])];
+          const R2 p11a = XP[rot(j, kl - o11[0])], p11b = XP[kl + rot(j, kl - o11[1])];
+          R2 vC = SF[j + d.rMC], vM = SF[j + d.rMM], vM1 = SF[j + d.rMM1], vP = SF[j + d.rMP], vP1 = SF[j + d.rMP1];
+          const R a2 = m2a.x + m2b.x, d2 = m2a.y + m2b.y, a21 = m21a.x + m21b.x, d21 = m21a.y + m21b.y;
+          const R a1 = p1a.x + p1b.x, d1 = p1a.y + p1b.y, a11 = p11a.x + p11b.x, d11 = p11a.y + p11b.y;
+          if (d.wMC) { vC.x = vC.x - R(2.) * adc; vC.y = vC.y - R(2.) * delc; SF[j + d.rMC] = vC; }
+          if (d.wMM) { upd_mm(d, vM, a2, d2, a21, d21); SF[j + d.rMM] = vM; }
+          if (d.wMM1) { upd_mm1(d, vM1, a2, d2, a21, d21); SF[j + d.rMM1] = vM1; }
+          if (d.wMP) { upd_mp(d, vP, a1, d1, a11, d11); SF[j + d.rMP] = vP; }
+          if (d.wMP1) { upd_mp1(d, vP1, a1, d1, a11, d11); SF[j + d.rMP1] = vP1; }
+        }
+        if (lane < 4 * nx) {
+          const R2 u = XM[sa], v = XM[sb];
+          XB[4 * nx * b + lane] = r2(u.x + v.x, u.y + v.y);
+        }
+        __syncwarp();  // the next MC overwrites the buffer
       }
-      __syncwarp();  // the next frequency overwrites XM / XP
+      if (nx > 0) {
+        // 3. the columns 32..KL-1 of the batch's target rows, one kind at a time
+        const int j = 32 + lx;
+        DiaMc d;
+        R2 s2, s21, s1, s11;
+        if (lact) {
+          d = dia_mc(mc0 + lb, enhfr, mfr1, mfrl);
+          const R2* xs = XB + 4 * nx * lb + lx;
+          s2 = xs[0]; s21 = xs[nx]; s1 = xs[2 * nx]; s11 = xs[3 * nx];
+        }
+        if (lact && d.wMC) { R2 v = SF[j + d.rMC]; v.x = v.x - R(2.) * ladc; v.y = v.y - R(2.) * ldelc; SF[j + d.rMC] = v; }
+        __syncwarp();
+        if (lact && d.wMM) { R2 v = SF[j + d.rMM]; upd_mm(d, v, s2.x, s2.y, s21.x, s21.y); SF[j + d.rMM] = v; }
+        __syncwarp();
+        if (lact && d.wMM1) { R2 v = SF[j + d.rMM1]; upd_mm1(d, v, s2.x, s2.y, s21.x, s21.y); SF[j + d.rMM1] = v; }
+        __syncwarp();
+        if (lact && d.wMP) { R2 v = SF[j + d.rMP]; upd_mp(d, v, s1.x, s1.y, s11.x, s11.y); SF[j + d.rMP] = v; }
+        __syncwarp();
+        if (lact && d.wMP1) { R2 v = SF[j + d.rMP1]; upd_mp1(d, v, s1.x, s1.y, s11.x, s11.y); SF[j + d.rMP1] = v; }
+        __syncwarp();  // the next batch overwrites the slots
+      }
     }
   }
 
