@@ -266,116 +266,180 @@ template <typename R> struct AdjW {
   // SNONLIN^T (DIA), the transpose of the forward gather: for each MC the
   // lanes first form, for their directions and both KH, the adjoints of the
   // interaction's centre value and of its two partner sums from the adjoints
-  // of the nine targets, and leave them in a per-warp buffer; then every lane
-  // adds to its own direction column of the five gathered rows (IC, IP, IP1,
-  // IM, IM1) what the interactions that read that column owe it.  The partner
-  // tables are rotations (checked on the host), so the interaction that read
-  // column j through a table is found by rotating j back.  Returns the adjoint
-  // of AKMEAN (ISNONLIN = 0 in shallow water).
+  // of the nine targets, and leave the partner-sum adjoints in a per-warp
+  // buffer; then every lane adds to its own direction column of the five
+  // gathered rows (IC, IP, IP1, IM, IM1) what the interactions that read that
+  // column owe it.  The partner tables are rotations (checked on the host), so
+  // the interaction that read column j through a table is found by rotating j
+  // back.  Returns the adjoint of AKMEAN (ISNONLIN = 0 in shallow water).
+  //
+  // With KL > 32 the directions 32..KL-1 are done for a batch of consecutive
+  // MCs at once, as in the forward DIA: one pass forms their adjoints for
+  // every MC of the batch into the batch slots; each MC's pass copies its
+  // slot into the buffer and leaves there the four KH-summed partner adjoints
+  // that the columns 32..KL-1 gather; one pass after the batch adds to those
+  // columns of the five gathered rows, one row kind at a time.  The gathered
+  // rows repeat at both ends of the frequency range (rows clamped to 1 and
+  // ML), so the host cuts the batches wherever one kind would add twice to a
+  // row (T.dia_adj_starts).
+  __device__ bool adj_batch_start(int mc) const {
+    return mc > 128 || ((T.dia_adj_starts[(mc - 1) >> 6] >> ((mc - 1) & 63)) & 1ull);
+  }
   __device__ R snonlin_adj() const {
-    const int kl = KL(), ml = ML(), ld = w.ld;
+    const int kl = KL(), ld = w.ld;
     const bool dyn = T.shallow && T.isnonlin == 0;
     R enhfr = R(1), denh = R(0);
     if (dyn) {
       const adj::Dual<R> e = adj::snl_enhfr(A, P, adj::Dual<R>(akmean, R(1)));
       enhfr = e.v; denh = e.d;
     }
-    const int mfr1 = -T.MFRSTLW + 1, mfrl = ml - T.KFRH + mfr1;
+    const int mfr1 = -T.MFRSTLW + 1, mfrl = ML() - T.KFRH + mfr1;
     const R2* SF = w.SF;
     const R* F = w.F;
-    R* XF = w.T;       // [kh*kl + k]: adjoint of the centre value (times FTAIL)
-    R* XS = XF + 2 * kl;  // adjoint of SAP
+    R* XS = w.T;          // [kh*kl + k]: adjoint of SAP
     R* XM = XS + 2 * kl;  // adjoint of SAM
+    R* XB = XM + 2 * kl;  // batch slots, 4*NX per MC of the batch
     int o1[2], o2[2], o11[2], o21[2];
     for (int kh = 0; kh < 2; ++kh) {
       o1[kh] = S.K1W[kl * kh] - 1; o2[kh] = S.K2W[kl * kh] - 1;
       o11[kh] = S.K11W[kl * kh] - 1; o21[kh] = S.K21W[kl * kh] - 1;
     }
     auto rot = [kl](int k, int o) { const int t = k + o; return t >= kl ? t - kl : t; };
-    const int nsub = kl > 32 ? 2 : 1;
     R lenh = 0;
-    for (int mc = 1; mc <= T.MLSTHG; ++mc) {
-      const int im = mc - T.MFRSTLW;
-      const int MP = S.IKP[im], MP1 = S.IKP1[im], MM = S.IKM[im], MM1 = S.IKM1[im];
-      const int* ic5 = S.INL + 5 * (mc - 1);
-      const int rIC = ld * (ic5[0] - 1), rIP = ld * (ic5[1] - 1), rIP1 = ld * (ic5[2] - 1), rIM = ld * (ic5[3] - 1),
-                rIM1 = ld * (ic5[4] - 1);
-      const R* rc = S.RNL + 25 * (mc - 1);
-      R ftemp = S.AF11[im];
-      if (T.shallow) ftemp = ftemp * (T.isnonlin == 0 ? enhfr : P.ENH[mc - 1]);
-      const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
-      const R ftail = (regime == 0) ? R(1) : rc[0];
-      const bool wMM = regime != 2, wMM1 = regime == 0 || (regime == 1 && MM1 <= ml) || (regime == 2 && MM1 >= 1);
-      const bool wMC = regime != 1 || (MM1 <= ml && mc <= ml);
-      const bool wMP = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml);
-      const bool wMP1 = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml && MP1 <= ml);
-      const int rMC = wMC ? ld * (mc - 1) : 0, rMM = wMM ? ld * (MM - 1) : 0, rMM1 = wMM1 ? ld * (MM1 - 1) : 0,
-                rMP = wMP ? ld * (MP - 1) : 0, rMP1 = wMP1 ? ld * (MP1 - 1) : 0;
+    // adjoints of direction k's interactions at one MC, both KH: SAP to
+    // xs[kh*skh], SAM to xm[kh*skh]; FIJ's (times FTAIL) summed over KH
+    // returned
+    auto interact = [&](const typename Src<R>::DiaMc& d, int mc, int k, R* xs, R* xm, int skh) -> R {
+      const R* rc = d.rc;
       const R g1 = rc[1], g2 = rc[2], g3 = rc[3], g4 = rc[4], g5 = rc[13], g6 = rc[14], g7 = rc[15], g8 = rc[16];
-      // 1. per interaction (k, kh) of this lane: adjoints of FIJ, SAP, SAM
-      for (int s_ = 0; s_ < nsub; ++s_) {
-        const int k = lane + 32 * s_;
-        if (k >= kl) break;
-        const R fij = F[k + rIC] * ftail;
-        const R2 vC = SF[k + rMC];
-        for (int kh = 0; kh < 2; ++kh) {
-          const int a1 = rot(k, o1[kh]), a11 = rot(k, o11[kh]), a2 = rot(k, o2[kh]), a21 = rot(k, o21[kh]);
-          const R sap = g1 * F[a1 + rIP] + g2 * F[a11 + rIP] + g3 * F[a1 + rIP1] + g4 * F[a11 + rIP1];
-          const R sam = g5 * F[a2 + rIM] + g6 * F[a21 + rIM] + g7 * F[a2 + rIM1] + g8 * F[a21 + rIM1];
-          R lad = 0, ldelad = 0, ldelap = 0, ldelam = 0;
-          if (wMC) { lad = lad - R(2.) * vC.x; ldelad = ldelad - R(2.) * vC.y; }
-          if (wMM) {
-            const R2 u = SF[a2 + rMM], u21 = SF[a21 + rMM];
-            lad = lad + (rc[20] * u.x + rc[19] * u21.x); ldelam = ldelam + (rc[23] * u.y + rc[24] * u21.y);
-          }
-          if (wMM1) {
-            const R2 u = SF[a2 + rMM1], u21 = SF[a21 + rMM1];
-            lad = lad + (rc[17] * u.x + rc[18] * u21.x); ldelam = ldelam + (rc[21] * u.y + rc[22] * u21.y);
-          }
-          if (wMP) {
-            const R2 u = SF[a1 + rMP], u11 = SF[a11 + rMP];
-            lad = lad + (rc[8] * u.x + rc[7] * u11.x); ldelap = ldelap + (rc[11] * u.y + rc[12] * u11.y);
-          }
-          if (wMP1) {
-            const R2 u = SF[a1 + rMP1], u11 = SF[a11 + rMP1];
-            lad = lad + (rc[5] * u.x + rc[6] * u11.x); ldelap = ldelap + (rc[9] * u.y + rc[10] * u11.y);
-          }
-          // ad = (fij S - 2P) ftemp fij, delad = (2 fij S - 2P) ftemp,
-          // delap = (fij - 2 sam) DAL1 ftemp fij, delam = (fij - 2 sap) DAL2 ftemp fij
-          const R S2 = sap + sam, P2 = sap * sam;
-          const R lfij = lad * ftemp * (R(2) * fij * S2 - R(2) * P2) + ldelad * R(2) * S2 * ftemp +
-                         ldelap * T.DAL1 * ftemp * (R(2) * fij - R(2) * sam) +
-                         ldelam * T.DAL2 * ftemp * (R(2) * fij - R(2) * sap);
-          const R lsap = lad * ftemp * fij * (fij - R(2) * sam) + ldelad * (R(2) * fij - R(2) * sam) * ftemp -
-                         ldelam * R(2) * T.DAL2 * ftemp * fij;
-          const R lsam = lad * ftemp * fij * (fij - R(2) * sap) + ldelad * (R(2) * fij - R(2) * sap) * ftemp -
-                         ldelap * R(2) * T.DAL1 * ftemp * fij;
-          if (dyn) {
-            const R lft = lad * (fij * S2 - R(2) * P2) * fij + ldelad * (R(2) * fij * S2 - R(2) * P2) +
-                          ldelap * (fij - R(2) * sam) * T.DAL1 * fij + ldelam * (fij - R(2) * sap) * T.DAL2 * fij;
-            lenh = lenh + lft * S.AF11[im];
-          }
-          XF[kl * kh + k] = lfij * ftail;
-          XS[kl * kh + k] = lsap;
-          XM[kl * kh + k] = lsam;
+      const R ftemp = d.ftemp, ftail = d.ftail;
+      const R fij = F[k + d.rIC] * ftail;
+      const R2 vC = SF[k + d.rMC];
+      R xf[2];
+      for (int kh = 0; kh < 2; ++kh) {
+        const int a1 = rot(k, o1[kh]), a11 = rot(k, o11[kh]), a2 = rot(k, o2[kh]), a21 = rot(k, o21[kh]);
+        const R sap = g1 * F[a1 + d.rIP] + g2 * F[a11 + d.rIP] + g3 * F[a1 + d.rIP1] + g4 * F[a11 + d.rIP1];
+        const R sam = g5 * F[a2 + d.rIM] + g6 * F[a21 + d.rIM] + g7 * F[a2 + d.rIM1] + g8 * F[a21 + d.rIM1];
+        R lad = 0, ldelad = 0, ldelap = 0, ldelam = 0;
+        if (d.wMC) { lad = lad - R(2.) * vC.x; ldelad = ldelad - R(2.) * vC.y; }
+        if (d.wMM) {
+          const R2 u = SF[a2 + d.rMM], u21 = SF[a21 + d.rMM];
+          lad = lad + (rc[20] * u.x + rc[19] * u21.x); ldelam = ldelam + (rc[23] * u.y + rc[24] * u21.y);
         }
+        if (d.wMM1) {
+          const R2 u = SF[a2 + d.rMM1], u21 = SF[a21 + d.rMM1];
+          lad = lad + (rc[17] * u.x + rc[18] * u21.x); ldelam = ldelam + (rc[21] * u.y + rc[22] * u21.y);
+        }
+        if (d.wMP) {
+          const R2 u = SF[a1 + d.rMP], u11 = SF[a11 + d.rMP];
+          lad = lad + (rc[8] * u.x + rc[7] * u11.x); ldelap = ldelap + (rc[11] * u.y + rc[12] * u11.y);
+        }
+        if (d.wMP1) {
+          const R2 u = SF[a1 + d.rMP1], u11 = SF[a11 + d.rMP1];
+          lad = lad + (rc[5] * u.x + rc[6] * u11.x); ldelap = ldelap + (rc[9] * u.y + rc[10] * u11.y);
+        }
+        // ad = (fij S - 2P) ftemp fij, delad = (2 fij S - 2P) ftemp,
+        // delap = (fij - 2 sam) DAL1 ftemp fij, delam = (fij - 2 sap) DAL2 ftemp fij
+        const R S2 = sap + sam, P2 = sap * sam;
+        const R lfij = lad * ftemp * (R(2) * fij * S2 - R(2) * P2) + ldelad * R(2) * S2 * ftemp +
+                       ldelap * T.DAL1 * ftemp * (R(2) * fij - R(2) * sam) +
+                       ldelam * T.DAL2 * ftemp * (R(2) * fij - R(2) * sap);
+        const R lsap = lad * ftemp * fij * (fij - R(2) * sam) + ldelad * (R(2) * fij - R(2) * sam) * ftemp -
+                       ldelam * R(2) * T.DAL2 * ftemp * fij;
+        const R lsam = lad * ftemp * fij * (fij - R(2) * sap) + ldelad * (R(2) * fij - R(2) * sap) * ftemp -
+                       ldelap * R(2) * T.DAL1 * ftemp * fij;
+        if (dyn) {
+          const R lft = lad * (fij * S2 - R(2) * P2) * fij + ldelad * (R(2) * fij * S2 - R(2) * P2) +
+                        ldelap * (fij - R(2) * sam) * T.DAL1 * fij + ldelam * (fij - R(2) * sap) * T.DAL2 * fij;
+          lenh = lenh + lft * S.AF11[mc - T.MFRSTLW];
+        }
+        xf[kh] = lfij * ftail;
+        xs[skh * kh] = lsap;
+        xm[skh * kh] = lsam;
       }
-      __syncwarp();
-      // 2. this lane's column j of the five gathered rows
-      for (int s_ = 0; s_ < nsub; ++s_) {
-        const int j = lane + 32 * s_;
-        if (j >= kl) break;
-        const R sp1 = XS[rot(j, kl - o1[0])] + XS[kl + rot(j, kl - o1[1])];
-        const R sp11 = XS[rot(j, kl - o11[0])] + XS[kl + rot(j, kl - o11[1])];
-        const R sm2 = XM[rot(j, kl - o2[0])] + XM[kl + rot(j, kl - o2[1])];
-        const R sm21 = XM[rot(j, kl - o21[0])] + XM[kl + rot(j, kl - o21[1])];
-        LAM[j + rIC] = LAM[j + rIC] + (XF[j] + XF[kl + j]);
-        LAM[j + rIP] = LAM[j + rIP] + (g1 * sp1 + g2 * sp11);
-        LAM[j + rIP1] = LAM[j + rIP1] + (g3 * sp1 + g4 * sp11);
-        LAM[j + rIM] = LAM[j + rIM] + (g5 * sm2 + g6 * sm21);
-        LAM[j + rIM1] = LAM[j + rIM1] + (g7 * sm2 + g8 * sm21);
+      return xf[0] + xf[1];
+    };
+
+    const int kmain = kl < 32 ? kl : 32;  // directions of the per-MC pass (lane = k)
+    const int nx = kl > 32 ? kl - 32 : 0;
+    // this lane's batch item (MC lb of the batch, direction 32 + lx), and its
+    // slot entry i = lane < 4*NX: the copy target in the buffer, and the two
+    // buffer entries whose sum the columns 32..KL-1 need
+    const int lb = nx > 0 ? lane / nx : 0, lx = nx > 0 ? lane - lb * nx : 0;
+    int cdst = 0, sa = 0, sb = 0;
+    if (lane < 4 * nx) {
+      const int q = lane / nx, j = 32 + lx;
+      cdst = (q >> 1) * 2 * kl + (q & 1) * kl + j;  // slot layout [XS|XM][kh][x]
+      const int oa = q == 0 ? o1[0] : q == 1 ? o11[0] : q == 2 ? o2[0] : o21[0];
+      const int ob = q == 0 ? o1[1] : q == 1 ? o11[1] : q == 2 ? o2[1] : o21[1];
+      const int base = q < 2 ? 0 : 2 * kl;  // K1W, K11W read XS; K2W, K21W read XM
+      sa = base + rot(j, kl - oa); sb = base + kl + rot(j, kl - ob);
+    }
+    for (int mc0 = 1, nb = 0; mc0 <= T.MLSTHG; mc0 += nb) {
+      nb = 1;
+      if (nx == 0) nb = T.MLSTHG;
+      else while (mc0 + nb <= T.MLSTHG && !adj_batch_start(mc0 + nb)) ++nb;
+      const bool lact = nx > 0 && lb < nb;
+      R lxf = R(0);
+      if (nx > 0) {
+        if (lact) {
+          const int mc = mc0 + lb;
+          R* xs = XB + 4 * nx * lb + lx;
+          lxf = interact(s.dia_mc(mc, enhfr, mfr1, mfrl), mc, 32 + lx, xs, xs + 2 * nx, nx);
+        }
+        __syncwarp();
       }
-      __syncwarp();  // the next frequency overwrites the buffer
+      for (int b = 0; b < nb; ++b) {
+        const int mc = mc0 + b;
+        const typename Src<R>::DiaMc d = s.dia_mc(mc, enhfr, mfr1, mfrl);
+        // 1. per interaction (k, kh) of this lane: adjoints of FIJ, SAP, SAM;
+        // the batch's directions come from the slot
+        R xfc = R(0);
+        if (lane < kmain) xfc = interact(d, mc, lane, XS + lane, XM + lane, kl);
+        if (lane < 4 * nx) XS[cdst] = XB[4 * nx * b + lane];
+        __syncwarp();
+        // 2. this lane's column j of the five gathered rows
+        if (lane < kmain) {
+          const int j = lane;
+          const R* rc = d.rc;
+          const R sp1 = XS[rot(j, kl - o1[0])] + XS[kl + rot(j, kl - o1[1])];
+          const R sp11 = XS[rot(j, kl - o11[0])] + XS[kl + rot(j, kl - o11[1])];
+          const R sm2 = XM[rot(j, kl - o2[0])] + XM[kl + rot(j, kl - o2[1])];
+          const R sm21 = XM[rot(j, kl - o21[0])] + XM[kl + rot(j, kl - o21[1])];
+          LAM[j + d.rIC] = LAM[j + d.rIC] + xfc;
+          LAM[j + d.rIP] = LAM[j + d.rIP] + (rc[1] * sp1 + rc[2] * sp11);
+          LAM[j + d.rIP1] = LAM[j + d.rIP1] + (rc[3] * sp1 + rc[4] * sp11);
+          LAM[j + d.rIM] = LAM[j + d.rIM] + (rc[13] * sm2 + rc[14] * sm21);
+          LAM[j + d.rIM1] = LAM[j + d.rIM1] + (rc[15] * sm2 + rc[16] * sm21);
+        }
+        if (lane < 4 * nx) XB[4 * nx * b + lane] = XS[sa] + XS[sb];
+        __syncwarp();  // the next MC overwrites the buffer
+      }
+      if (nx > 0) {
+        // 3. the columns 32..KL-1 of the batch's gathered rows, one kind at a time
+        const int j = 32 + lx;
+        int rIC = 0, rIP = 0, rIP1 = 0, rIM = 0, rIM1 = 0;
+        R vP = 0, vP1 = 0, vM = 0, vM1 = 0;
+        if (lact) {
+          const typename Src<R>::DiaMc d = s.dia_mc(mc0 + lb, enhfr, mfr1, mfrl);
+          const R* rc = d.rc;
+          const R* xs = XB + 4 * nx * lb + lx;
+          const R sp1 = xs[0], sp11 = xs[nx], sm2 = xs[2 * nx], sm21 = xs[3 * nx];
+          rIC = d.rIC; rIP = d.rIP; rIP1 = d.rIP1; rIM = d.rIM; rIM1 = d.rIM1;
+          vP = rc[1] * sp1 + rc[2] * sp11; vP1 = rc[3] * sp1 + rc[4] * sp11;
+          vM = rc[13] * sm2 + rc[14] * sm21; vM1 = rc[15] * sm2 + rc[16] * sm21;
+        }
+        if (lact) LAM[j + rIC] = LAM[j + rIC] + lxf;
+        __syncwarp();
+        if (lact) LAM[j + rIP] = LAM[j + rIP] + vP;
+        __syncwarp();
+        if (lact) LAM[j + rIP1] = LAM[j + rIP1] + vP1;
+        __syncwarp();
+        if (lact) LAM[j + rIM] = LAM[j + rIM] + vM;
+        __syncwarp();
+        if (lact) LAM[j + rIM1] = LAM[j + rIM1] + vM1;
+        __syncwarp();  // the next batch overwrites the slots
+      }
     }
     return warp_sum(lenh) * denh;
   }

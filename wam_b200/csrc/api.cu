@@ -227,6 +227,25 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
     const int nbatch = (t.MLSTHG + b - 1) / b;
     d.dia_batch = nbatch > 0 ? (t.MLSTHG + nbatch - 1) / nbatch : 1;  // the same batch count, evenly filled
   }
+  // The DIA^T batches the same directions but adds to the gathered rows (IC,
+  // IP, IP1, IM, IM1 of INLCOEF), which repeat where they are clamped to the
+  // ends of the spectrum.  A batch holds at most as many MCs as its slots
+  // (4*NX reals each after the 6*KL of the per-MC buffer) and the lanes allow,
+  // and a new batch starts wherever a kind's row equals the previous MC's.
+  d.dia_adj_starts[0] = d.dia_adj_starts[1] = ~0ull;
+  if (t.KL > 32) {
+    const int nx = t.KL - 32;
+    const int bmax = std::max(1, std::min(32 / nx, (8 * d.scr - 6 * t.KL) / (4 * nx)));
+    d.dia_adj_starts[0] = d.dia_adj_starts[1] = 0;
+    int nb = 0;
+    for (int mc = 1; mc <= t.MLSTHG && mc <= 128; ++mc) {
+      bool cut = nb == 0 || nb == bmax;
+      if (!cut)
+        for (int q = 0; q < 5; ++q) cut = cut || t.INLCOEF[5 * (mc - 1) + q] == t.INLCOEF[5 * (mc - 2) + q];
+      if (cut) { d.dia_adj_starts[(mc - 1) >> 6] |= 1ull << ((mc - 1) & 63); nb = 0; }
+      ++nb;
+    }
+  }
   d.iphys = c.iphys; d.shallow = c.shallow_run; d.isnonlin = c.isnonlin; d.lcflx = c.lcflx;
   d.DELTH = t.DELTH; d.DELTR = t.DELTR; d.INV_LOG_CO = t.INV_LOG_CO; d.MO_TAIL = t.MO_TAIL; d.MM1_TAIL = t.MM1_TAIL;
   d.DELU = t.DELU; d.DAL1 = t.DAL1; d.DAL2 = t.DAL2; d.X0TAUHF = t.X0TAUHF;

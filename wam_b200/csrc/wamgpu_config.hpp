@@ -30,6 +30,7 @@ template <typename R> struct DevTables {
   int KL, ML, NS, NDEPTH, MFRSTLW, MLSTHG, KFRH, NSDSNTH, NK10;
   int ld, scr, need_sp;  // shared-memory row stride (odd, >= KL), scratch row length, SPOS array kept
   int dia_batch;         // MCs per batch of the DIA's directions beyond the first 32 (KL > 32)
+  unsigned long long dia_adj_starts[2];  // DIA^T: bit MC-1 set where a batch starts (MC <= 128; every later MC starts one)
   int iphys, shallow, isnonlin, lcflx;
   R DELTH, DELTR, INV_LOG_CO, MO_TAIL, MM1_TAIL, DELU, DAL1, DAL2, X0TAUHF;
   R BETAMAX, ZALP, ALPHA, TAUWSHELTER, CDFAC, DELT;
