@@ -446,78 +446,107 @@ template <typename R> struct AdjW {
 
   // SDISSIP_ARD^T.  The saturation window is a rotation of the directions
   // (INDICESSAT(K, J) = K + J - NSDSNTH modulo KL, checked on the host), so
-  // the transposed window sum is gathered per column like the DIA.
+  // the transposed window sum is gathered per column like the DIA.  With
+  // KL > 32 the directions 32..KL-1 are grouped over frequencies as in the
+  // forward: before a group, one lane per (frequency, extra direction) forms
+  // what does not depend on the frequency's maximum; after it, their
+  // whitecapping adjoint and transposed window sum.  Each frequency of the
+  // group keeps its row of the window's adjoint sources (LB) for that.
   __device__ void sdissip_adj() const {
     const int kl = KL(), ml = ML(), nw = 2 * T.NSDSNTH + 1, ns = T.NSDSNTH, ld = w.ld;
     const R tmp03 = R(1.0) / R(9.0E-4), c6 = R(0.3), c6m1 = R(1.) - c6;
-    R* LB = w.t(5);
-    for (int m = 0; m < ml; ++m) {
-      const R sig = P_::ZPI * S.FR[m];
-      R facsat;
-      if (T.shallow) { const R xk = s.tfak(m); facsat = (xk * xk * xk) * (R(1.0) / P_::ZPI) * s.tcgond(m); }
-      else { const R xk = sig * sig / P_::G; facsat = (xk * xk * xk) * (R(0.5) * (R(1.0) / P_::ZPI)) * P_::G / sig; }
-      const R* fm = w.F + ld * m;
-      R bth[2] = {0, 0}, bmax = 0;
-      int kmax = -1;
-      for (int s_ = 0; s_ < 2; ++s_) {
-        const int k = lane + 32 * s_;
-        if (k < kl) {
-          R acc = 0;
-          int src = k - ns;
-          src = src < 0 ? src + kl : src;
-          for (int j = 0; j < nw; ++j) {
-            acc = acc + S.SATW[k + kl * j] * fm[src];
-            src = src + 1 == kl ? 0 : src + 1;
-          }
-          bth[s_] = acc * facsat;
-          if (bmax < bth[s_]) { bmax = bth[s_]; kmax = k; }
+    const int nx = kl > 32 ? kl - 32 : 0;
+    // a group holds at most as many frequencies as the scratch rows have LB
+    // rows (8*scr reals), for every KL
+    const int gcap = (8 * w.scr) / kl;
+    const int gsz = min(nx > 0 ? 32 / nx : ml, gcap);
+    const int lg = nx > 0 ? lane / nx : 0, lx = nx > 0 ? lane - lg * nx : 0;
+    R* LBG = w.T;  // [g*kl + k]: LB of frequency m0 + g, g < gsz
+    auto window = [&](int k, const R* fm) {
+      R acc = 0;
+      int src = k - ns;
+      src = src < 0 ? src + kl : src;
+      for (int j = 0; j < nw; ++j) {
+        acc = acc + S.SATW[k + kl * j] * fm[src];
+        src = src + 1 == kl ? 0 : src + 1;
+      }
+      return acc;
+    };
+    auto window_t = [&](int c, const R* lbr) {
+      R acc = 0;
+      for (int j = 0; j < nw; ++j) {
+        int k = c - j + ns;
+        k = k < 0 ? k + kl : (k >= kl ? k - kl : k);
+        acc = acc + S.SATW[k + kl * j] * lbr[k];
+      }
+      return acc;
+    };
+    for (int m0 = 0; m0 < ml; m0 += gsz) {
+      const int ng = min(gsz, ml - m0);
+      const bool lact = nx > 0 && lg < ng;
+      // this lane's extra bin (32 + lx, m0 + lg): saturation, its share of
+      // the TEMP1 adjoint and its own window source
+      R bthx = 0, ltx = 0, lbx = 0, temp1x = 0;
+      if (lact) {
+        const int m = m0 + lg, b = 32 + lx + ld * m;
+        const R ss = R(-2.2E-5) * (P_::ZPI * S.FR[m]);
+        bthx = window(32 + lx, w.F + ld * m) * s.sat_facsat(m);
+        const R2 v = w.SF[b];
+        const R ldv = w.F[b] * v.x + v.y;
+        ltx = ldv * ss;
+        const R ddraw = bthx * tmp03 - R(1.0), dd = dmax(R(0.), ddraw);
+        if (R(0.) < ddraw) lbx = ldv * ss * c6m1 * R(2) * dd * tmp03;
+      }
+      for (int g = 0; g < ng; ++g) {
+        const int m = m0 + g;
+        const R sig = P_::ZPI * S.FR[m], facsat = s.sat_facsat(m);
+        const R* fm = w.F + ld * m;
+        const bool own = lact && lg == g;
+        R bth = 0, bmax = 0;
+        int kmax = -1;
+        if (lane < kl) {
+          bth = window(lane, fm) * facsat;
+          if (bmax < bth) { bmax = bth; kmax = lane; }
         }
-      }
-      // the first direction of largest saturation (none while all are <= 0)
-      for (int o = 16; o > 0; o >>= 1) {
-        const R ob = __shfl_xor_sync(0xffffffffu, bmax, o);
-        const int ok = __shfl_xor_sync(0xffffffffu, kmax, o);
-        if (bmax < ob || (ob == bmax && ok >= 0 && (kmax < 0 || ok < kmax))) { bmax = ob; kmax = ok; }
-      }
-      const R d0raw = bmax * tmp03 - R(1.0), d0 = dmax(R(0.), d0raw);
-      const R temp1 = c6 * (d0 * d0), ssdsc2_sig = R(-2.2E-5) * sig;
-      R lt1 = 0, lb[2] = {0, 0};
-      for (int s_ = 0; s_ < 2; ++s_) {
-        const int k = lane + 32 * s_;
-        if (k < kl) {
-          const int b = k + ld * m;
-          const R ddraw = bth[s_] * tmp03 - R(1.0), dd = dmax(R(0.), ddraw);
+        if (own && bmax < bthx) { bmax = bthx; kmax = 32 + lx; }
+        // the first direction of largest saturation (none while all are <= 0)
+        for (int o = 16; o > 0; o >>= 1) {
+          const R ob = __shfl_xor_sync(0xffffffffu, bmax, o);
+          const int ok = __shfl_xor_sync(0xffffffffu, kmax, o);
+          if (bmax < ob || (ob == bmax && ok >= 0 && (kmax < 0 || ok < kmax))) { bmax = ob; kmax = ok; }
+        }
+        const R d0raw = bmax * tmp03 - R(1.0), d0 = dmax(R(0.), d0raw);
+        const R temp1 = c6 * (d0 * d0), ssdsc2_sig = R(-2.2E-5) * sig;
+        if (own) temp1x = temp1;
+        R lt1 = 0, lb = 0;
+        if (lane < kl) {
+          const int b = lane + ld * m;
+          const R ddraw = bth * tmp03 - R(1.0), dd = dmax(R(0.), ddraw);
           const R d = ssdsc2_sig * (temp1 + c6m1 * (dd * dd));
           const R2 v = w.SF[b];
           LAM[b] = LAM[b] + d * v.x;
-          const R ldv = fm[k] * v.x + v.y;
-          lt1 = lt1 + ldv * ssdsc2_sig;
-          if (R(0.) < ddraw) lb[s_] = ldv * ssdsc2_sig * c6m1 * R(2) * dd * tmp03;
+          const R ldv = fm[lane] * v.x + v.y;
+          lt1 = ldv * ssdsc2_sig;
+          if (R(0.) < ddraw) lb = ldv * ssdsc2_sig * c6m1 * R(2) * dd * tmp03;
         }
+        if (own) lt1 = lt1 + ltx;
+        const R ltemp1 = warp_sum(lt1);
+        const R lt1s = ltemp1 * c6 * R(2) * d0 * tmp03;
+        R* LB = LBG + g * kl;
+        if (lane < kl) LB[lane] = ((R(0.) < d0raw && lane == kmax) ? lb + lt1s : lb) * facsat;
+        if (own) LB[32 + lx] = ((R(0.) < d0raw && 32 + lx == kmax) ? lbx + lt1s : lbx) * facsat;
+        __syncwarp();
+        if (lane < kl) LAM[lane + ld * m] = LAM[lane + ld * m] + window_t(lane, LB);
       }
-      const R ltemp1 = warp_sum(lt1);
-      for (int s_ = 0; s_ < 2; ++s_) {
-        const int k = lane + 32 * s_;
-        if (k < kl) {
-          R v = lb[s_];
-          if (R(0.) < d0raw && k == kmax) v = v + ltemp1 * c6 * R(2) * d0 * tmp03;
-          LB[k] = v * facsat;
-        }
+      if (lact) {
+        const int m = m0 + lg, c = 32 + lx, b = c + ld * m;
+        const R ss = R(-2.2E-5) * (P_::ZPI * S.FR[m]);
+        const R dd = dmax(R(0.), bthx * tmp03 - R(1.0));
+        const R d = ss * (temp1x + c6m1 * (dd * dd));
+        LAM[b] = LAM[b] + d * w.SF[b].x;
+        LAM[b] = LAM[b] + window_t(c, LBG + lg * kl);
       }
-      __syncwarp();
-      for (int s_ = 0; s_ < 2; ++s_) {
-        const int c = lane + 32 * s_;
-        if (c < kl) {
-          R acc = 0;
-          for (int j = 0; j < nw; ++j) {
-            int k = c - j + ns;
-            k = k < 0 ? k + kl : (k >= kl ? k - kl : k);
-            acc = acc + S.SATW[k + kl * j] * LB[k];
-          }
-          LAM[c + ld * m] = LAM[c + ld * m] + acc;
-        }
-      }
-      __syncwarp();
+      __syncwarp();  // the next group overwrites the LB rows
     }
   }
 

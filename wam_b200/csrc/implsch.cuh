@@ -456,40 +456,60 @@ template <typename R> struct Src {
   }
 
   // SDISSIP_ARD: saturation-based whitecapping (SSDSC3 = SSDSC5 = 0).
+  //
+  // Frequency by frequency, lane k forms the saturation of direction k.  With
+  // KL > 32 the directions 32..KL-1 (NX of them) are done for a group of
+  // 32/NX frequencies at once, one lane per (frequency of the group,
+  // direction): their saturations before the group, their whitecapping after
+  // it.  The lanes holding a frequency's extra directions add them to that
+  // frequency's maximum.  The maximum is exact and every bin keeps its own
+  // formula, so the results do not depend on the grouping.
+  __device__ R sat_facsat(int m) const {
+    const R sig = P_::ZPI * S.FR[m];
+    if (T.shallow) { const R xk = tfak(m); return (xk * xk * xk) * (R(1.0) / P_::ZPI) * tcgond(m); }
+    const R xk = sig * sig / P_::G;
+    return (xk * xk * xk) * (R(0.5) * (R(1.0) / P_::ZPI)) * P_::G / sig;
+  }
+  // saturation window sum of bin (k, m), without FACSAT
+  __device__ R sat_window(int k, int m) const {
+    const int kl = KL(), nw = 2 * T.NSDSNTH + 1;
+    const R* fm = w.F + w.ld * m;
+    R acc = 0;
+    for (int j = 0; j < nw; ++j) acc = acc + S.SATW[k + kl * j] * fm[S.INDSAT[k + kl * j] - 1];
+    return acc;
+  }
   __device__ void sdissip_ard() const {
-    const int kl = KL(), ml = ML(), nw = 2 * T.NSDSNTH + 1, ld = w.ld;
+    const int kl = KL(), ml = ML(), ld = w.ld;
     const R tmp03 = R(1.0) / R(9.0E-4), c6 = R(0.3), c6m1 = R(1.) - c6;
-    for (int m = 0; m < ml; ++m) {
-      R sig = P_::ZPI * S.FR[m], facsat;
-      if (T.shallow) { R xk = tfak(m); facsat = (xk * xk * xk) * (R(1.0) / P_::ZPI) * tcgond(m); }
-      else { R xk = sig * sig / P_::G; facsat = (xk * xk * xk) * (R(0.5) * (R(1.0) / P_::ZPI)) * P_::G / sig; }
-      const R* fm = w.F + ld * m;
-      R bth[2] = {0, 0}, bmax = 0;
-      for (int s = 0; s < 2; ++s) {
-        int k = lane + 32 * s;
-        if (k < kl) {
-          R acc = 0;
-          for (int j = 0; j < nw; ++j) acc = acc + S.SATW[k + kl * j] * fm[S.INDSAT[k + kl * j] - 1];
-          bth[s] = acc * facsat;
-          bmax = dmax(bmax, bth[s]);
-        }
+    const int nx = kl > 32 ? kl - 32 : 0, gsz = nx > 0 ? 32 / nx : ml;
+    const int lg = nx > 0 ? lane / nx : 0, lx = nx > 0 ? lane - lg * nx : 0;
+    auto whitecap = [&](int k, int m, R bth, R temp1, R ssdsc2_sig) {
+      R dd = dmax(R(0.), bth * tmp03 - R(1.0));
+      R d = ssdsc2_sig * (temp1 + c6m1 * (dd * dd));
+      int b = k + ld * m;
+      R2 v = w.SF[b];
+      v.x = v.x + d * w.F[b];
+      v.y = v.y + d;
+      w.SF[b] = v;
+    };
+    for (int m0 = 0; m0 < ml; m0 += gsz) {
+      const int ng = min(gsz, ml - m0);
+      const bool lact = nx > 0 && lg < ng;
+      R bthx = 0, temp1x = 0;  // this lane's extra direction: saturation, TEMP1 of its frequency
+      if (lact) bthx = sat_window(32 + lx, m0 + lg) * sat_facsat(m0 + lg);
+      for (int g = 0; g < ng; ++g) {
+        const int m = m0 + g;
+        const R sig = P_::ZPI * S.FR[m], facsat = sat_facsat(m);
+        R bth = 0, bmax = 0;
+        if (lane < kl) { bth = sat_window(lane, m) * facsat; bmax = dmax(bmax, bth); }
+        if (lact && lg == g) bmax = dmax(bmax, bthx);
+        bmax = warp_max(bmax);
+        R d0 = dmax(R(0.), bmax * tmp03 - R(1.0));
+        R temp1 = c6 * (d0 * d0);
+        if (lg == g) temp1x = temp1;
+        if (lane < kl) whitecap(lane, m, bth, temp1, R(-2.2E-5) * sig);
       }
-      bmax = warp_max(bmax);
-      R d0 = dmax(R(0.), bmax * tmp03 - R(1.0));
-      R temp1 = c6 * (d0 * d0);
-      R ssdsc2_sig = R(-2.2E-5) * sig;
-      for (int s = 0; s < 2; ++s) {
-        int k = lane + 32 * s;
-        if (k < kl) {
-          R dd = dmax(R(0.), bth[s] * tmp03 - R(1.0));
-          R d = ssdsc2_sig * (temp1 + c6m1 * (dd * dd));
-          int b = k + ld * m;
-          R2 v = w.SF[b];
-          v.x = v.x + d * w.F[b];
-          v.y = v.y + d;
-          w.SF[b] = v;
-        }
-      }
+      if (lact) whitecap(32 + lx, m0 + lg, bthx, temp1x, R(-2.2E-5) * (P_::ZPI * S.FR[m0 + lg]));
     }
     __syncwarp();
   }
