@@ -486,7 +486,7 @@ template <typename R, class Fn> WAHD void dia_for_each(const ATabs<R>& A, Fn&& f
     const int im = mc - A.MFRSTLW;
     const int MP = A.IKP[im], MP1 = A.IKP1[im], MM = A.IKM[im], MM1 = A.IKM1[im];
     const int* ic5 = A.INL + 5 * (mc - 1);
-    const R* rc = A.RNL + 25 * (mc - 1);
+    const R* rc = A.RNL + RNL_STRIDE * (mc - 1);
     const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
     d.mc = mc; d.rc = rc; d.af11 = A.AF11[im];
     d.ftail = (regime == 0) ? R(1) : rc[0];
@@ -496,7 +496,7 @@ template <typename R, class Fn> WAHD void dia_for_each(const ATabs<R>& A, Fn&& f
     d.wMP = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml);
     d.wMP1 = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml && MP1 <= ml);
     const int g_idx[8] = {1, 2, 3, 4, 13, 14, 15, 16};
-    for (int q = 0; q < 8; ++q) d.g[q] = rc[g_idx[q]];
+    for (int q = 0; q < 8; ++q) d.g[q] = rc[rnl_slot(g_idx[q])];
     for (int kh = 0; kh < 2; ++kh)
       for (int k = 0; k < kl; ++k) {
         const int a1 = A.K1W[k + kl * kh] - 1, a2 = A.K2W[k + kl * kh] - 1, a11 = A.K11W[k + kl * kh] - 1,
@@ -538,20 +538,20 @@ WAHD void snonlin(const ATabs<R>& A, const PointIn<R>& P, Col<T> F, T AKMEAN, Co
     T delap = (fij - R(2.) * sam) * A.DAL1 * fcen, delam = (fij - R(2.) * sap) * A.DAL2 * fcen;
     if (d.wMC) { SL[d.tC] = SL[d.tC] - R(2.) * ad; FL[d.tC] = FL[d.tC] - R(2.) * delad; }
     if (d.wMM) {
-      SL[d.tMM] = SL[d.tMM] + ad * rc[20]; FL[d.tMM] = FL[d.tMM] + delam * rc[23];
-      SL[d.tMM_21] = SL[d.tMM_21] + ad * rc[19]; FL[d.tMM_21] = FL[d.tMM_21] + delam * rc[24];
+      SL[d.tMM] = SL[d.tMM] + ad * rc[rnl_slot(20)]; FL[d.tMM] = FL[d.tMM] + delam * rc[rnl_slot(23)];
+      SL[d.tMM_21] = SL[d.tMM_21] + ad * rc[rnl_slot(19)]; FL[d.tMM_21] = FL[d.tMM_21] + delam * rc[rnl_slot(24)];
     }
     if (d.wMM1) {
-      SL[d.tMM1] = SL[d.tMM1] + ad * rc[17]; FL[d.tMM1] = FL[d.tMM1] + delam * rc[21];
-      SL[d.tMM1_21] = SL[d.tMM1_21] + ad * rc[18]; FL[d.tMM1_21] = FL[d.tMM1_21] + delam * rc[22];
+      SL[d.tMM1] = SL[d.tMM1] + ad * rc[rnl_slot(17)]; FL[d.tMM1] = FL[d.tMM1] + delam * rc[rnl_slot(21)];
+      SL[d.tMM1_21] = SL[d.tMM1_21] + ad * rc[rnl_slot(18)]; FL[d.tMM1_21] = FL[d.tMM1_21] + delam * rc[rnl_slot(22)];
     }
     if (d.wMP) {
-      SL[d.tMP] = SL[d.tMP] + ad * rc[8]; FL[d.tMP] = FL[d.tMP] + delap * rc[11];
-      SL[d.tMP_11] = SL[d.tMP_11] + ad * rc[7]; FL[d.tMP_11] = FL[d.tMP_11] + delap * rc[12];
+      SL[d.tMP] = SL[d.tMP] + ad * rc[rnl_slot(8)]; FL[d.tMP] = FL[d.tMP] + delap * rc[rnl_slot(11)];
+      SL[d.tMP_11] = SL[d.tMP_11] + ad * rc[rnl_slot(7)]; FL[d.tMP_11] = FL[d.tMP_11] + delap * rc[rnl_slot(12)];
     }
     if (d.wMP1) {
-      SL[d.tMP1] = SL[d.tMP1] + ad * rc[5]; FL[d.tMP1] = FL[d.tMP1] + delap * rc[9];
-      SL[d.tMP1_11] = SL[d.tMP1_11] + ad * rc[6]; FL[d.tMP1_11] = FL[d.tMP1_11] + delap * rc[10];
+      SL[d.tMP1] = SL[d.tMP1] + ad * rc[rnl_slot(5)]; FL[d.tMP1] = FL[d.tMP1] + delap * rc[rnl_slot(9)];
+      SL[d.tMP1_11] = SL[d.tMP1_11] + ad * rc[rnl_slot(6)]; FL[d.tMP1_11] = FL[d.tMP1_11] + delap * rc[rnl_slot(10)];
     }
   });
 }

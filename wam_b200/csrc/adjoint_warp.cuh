@@ -310,8 +310,8 @@ template <typename R> struct AdjW {
     // xs[kh*skh], SAM to xm[kh*skh]; FIJ's (times FTAIL) summed over KH
     // returned
     auto interact = [&](const typename Src<R>::DiaMc& d, int mc, int k, R* xs, R* xm, int skh) -> R {
-      const R* rc = d.rc;
-      const R g1 = rc[1], g2 = rc[2], g3 = rc[3], g4 = rc[4], g5 = rc[13], g6 = rc[14], g7 = rc[15], g8 = rc[16];
+      const Quad<R> c0 = ld4(d.rc), c1 = ld4(d.rc + 4);  // RNLCOEF slots (rnl_slot)
+      const R g1 = c0.b, g2 = c0.c, g3 = c0.d, g4 = c1.a, g5 = c1.b, g6 = c1.c, g7 = c1.d, g8 = d.rc[8];
       const R ftemp = d.ftemp, ftail = d.ftail;
       const R fij = F[k + d.rIC] * ftail;
       const R2 vC = SF[k + d.rMC];
@@ -322,21 +322,26 @@ template <typename R> struct AdjW {
         const R sam = g5 * F[a2 + d.rIM] + g6 * F[a21 + d.rIM] + g7 * F[a2 + d.rIM1] + g8 * F[a21 + d.rIM1];
         R lad = 0, ldelad = 0, ldelap = 0, ldelam = 0;
         if (d.wMC) { lad = lad - R(2.) * vC.x; ldelad = ldelad - R(2.) * vC.y; }
+        // target weights per row kind: slots 12 MM, 16 MM1, 20 MP, 24 MP1
         if (d.wMM) {
           const R2 u = SF[a2 + d.rMM], u21 = SF[a21 + d.rMM];
-          lad = lad + (rc[20] * u.x + rc[19] * u21.x); ldelam = ldelam + (rc[23] * u.y + rc[24] * u21.y);
+          const Quad<R> c = ld4(d.rc + 12);
+          lad = lad + (c.a * u.x + c.b * u21.x); ldelam = ldelam + (c.c * u.y + c.d * u21.y);
         }
         if (d.wMM1) {
           const R2 u = SF[a2 + d.rMM1], u21 = SF[a21 + d.rMM1];
-          lad = lad + (rc[17] * u.x + rc[18] * u21.x); ldelam = ldelam + (rc[21] * u.y + rc[22] * u21.y);
+          const Quad<R> c = ld4(d.rc + 16);
+          lad = lad + (c.a * u.x + c.b * u21.x); ldelam = ldelam + (c.c * u.y + c.d * u21.y);
         }
         if (d.wMP) {
           const R2 u = SF[a1 + d.rMP], u11 = SF[a11 + d.rMP];
-          lad = lad + (rc[8] * u.x + rc[7] * u11.x); ldelap = ldelap + (rc[11] * u.y + rc[12] * u11.y);
+          const Quad<R> c = ld4(d.rc + 20);
+          lad = lad + (c.a * u.x + c.b * u11.x); ldelap = ldelap + (c.c * u.y + c.d * u11.y);
         }
         if (d.wMP1) {
           const R2 u = SF[a1 + d.rMP1], u11 = SF[a11 + d.rMP1];
-          lad = lad + (rc[5] * u.x + rc[6] * u11.x); ldelap = ldelap + (rc[9] * u.y + rc[10] * u11.y);
+          const Quad<R> c = ld4(d.rc + 24);
+          lad = lad + (c.a * u.x + c.b * u11.x); ldelap = ldelap + (c.c * u.y + c.d * u11.y);
         }
         // ad = (fij S - 2P) ftemp fij, delad = (2 fij S - 2P) ftemp,
         // delap = (fij - 2 sam) DAL1 ftemp fij, delam = (fij - 2 sap) DAL2 ftemp fij
@@ -401,16 +406,17 @@ template <typename R> struct AdjW {
         // 2. this lane's column j of the five gathered rows
         if (lane < kmain) {
           const int j = lane;
-          const R* rc = d.rc;
+          const Quad<R> c0 = ld4(d.rc), c1 = ld4(d.rc + 4);
+          const R g8 = d.rc[8];
           const R sp1 = XS[rot(j, kl - o1[0])] + XS[kl + rot(j, kl - o1[1])];
           const R sp11 = XS[rot(j, kl - o11[0])] + XS[kl + rot(j, kl - o11[1])];
           const R sm2 = XM[rot(j, kl - o2[0])] + XM[kl + rot(j, kl - o2[1])];
           const R sm21 = XM[rot(j, kl - o21[0])] + XM[kl + rot(j, kl - o21[1])];
           LAM[j + d.rIC] = LAM[j + d.rIC] + xfc;
-          LAM[j + d.rIP] = LAM[j + d.rIP] + (rc[1] * sp1 + rc[2] * sp11);
-          LAM[j + d.rIP1] = LAM[j + d.rIP1] + (rc[3] * sp1 + rc[4] * sp11);
-          LAM[j + d.rIM] = LAM[j + d.rIM] + (rc[13] * sm2 + rc[14] * sm21);
-          LAM[j + d.rIM1] = LAM[j + d.rIM1] + (rc[15] * sm2 + rc[16] * sm21);
+          LAM[j + d.rIP] = LAM[j + d.rIP] + (c0.b * sp1 + c0.c * sp11);
+          LAM[j + d.rIP1] = LAM[j + d.rIP1] + (c0.d * sp1 + c1.a * sp11);
+          LAM[j + d.rIM] = LAM[j + d.rIM] + (c1.b * sm2 + c1.c * sm21);
+          LAM[j + d.rIM1] = LAM[j + d.rIM1] + (c1.d * sm2 + g8 * sm21);
         }
         if (lane < 4 * nx) XB[4 * nx * b + lane] = XS[sa] + XS[sb];
         __syncwarp();  // the next MC overwrites the buffer
@@ -422,12 +428,13 @@ template <typename R> struct AdjW {
         R vP = 0, vP1 = 0, vM = 0, vM1 = 0;
         if (lact) {
           const typename Src<R>::DiaMc d = s.dia_mc(mc0 + lb, enhfr, mfr1, mfrl);
-          const R* rc = d.rc;
+          const Quad<R> c0 = ld4(d.rc), c1 = ld4(d.rc + 4);
+          const R g8 = d.rc[8];
           const R* xs = XB + 4 * nx * lb + lx;
           const R sp1 = xs[0], sp11 = xs[nx], sm2 = xs[2 * nx], sm21 = xs[3 * nx];
           rIC = d.rIC; rIP = d.rIP; rIP1 = d.rIP1; rIM = d.rIM; rIM1 = d.rIM1;
-          vP = rc[1] * sp1 + rc[2] * sp11; vP1 = rc[3] * sp1 + rc[4] * sp11;
-          vM = rc[13] * sm2 + rc[14] * sm21; vM1 = rc[15] * sm2 + rc[16] * sm21;
+          vP = c0.b * sp1 + c0.c * sp11; vP1 = c0.d * sp1 + c1.a * sp11;
+          vM = c1.b * sm2 + c1.c * sm21; vM1 = c1.d * sm2 + g8 * sm21;
         }
         if (lact) LAM[j + rIC] = LAM[j + rIC] + lxf;
         __syncwarp();

@@ -168,7 +168,14 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
   }
   putr(L.FR, t.FR); putr(L.DF, t.DF); putr(L.DFIM, t.DFIM); putr(L.DFIMOFR, t.DFIMOFR); putr(L.FR5, t.FR5);
   putr(L.FRM5, t.FRM5); putr(L.RHOWG_DFIM, t.RHOWG_DFIM); putr(L.TH, t.TH); putr(L.COSTH, t.COSTH);
-  putr(L.SINTH, t.SINTH); putr(L.DELFL, delfl); putr(L.AF11, t.AF11); putr(L.RNLCOEF, t.RNLCOEF);
+  putr(L.SINTH, t.SINTH); putr(L.DELFL, delfl); putr(L.AF11, t.AF11);
+  {  // RNLCOEF regrouped (rnl_slot), each MC's block 16-byte aligned
+    std::vector<R> rn((size_t)RNL_STRIDE * t.MLSTHG, R(0));
+    for (int mc = 0; mc < t.MLSTHG; ++mc)
+      for (int i = 0; i < 25; ++i) rn[(size_t)RNL_STRIDE * mc + rnl_slot(i)] = t.RNLCOEF[25 * mc + i];
+    while (sr.size() % 4) sr.push_back(R(0));
+    putr(L.RNLCOEF, rn);
+  }
   putr(L.SATW, t.SATWEIGHTS); putr(L.WTAUHF, t.WTAUHF); putr(L.SWELLFT, t.SWELLFT);
   putr(L.SIG10, sig10); putr(L.DSII10, dsii10);
   L.nreal = (int)sr.size();

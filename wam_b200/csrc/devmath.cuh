@@ -44,6 +44,16 @@ template <typename R> __device__ __forceinline__ R warp_sum(R v) {
   for (int o = 16; o > 0; o >>= 1) v = v + __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+// Four consecutive reals from a 16-byte aligned address.
+template <typename R> struct Quad { R a, b, c, d; };
+__device__ __forceinline__ Quad<float> ld4(const float* p) {
+  const float4 v = *reinterpret_cast<const float4*>(p);
+  return {v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ Quad<double> ld4(const double* p) {
+  const double2 u = *reinterpret_cast<const double2*>(p), v = *reinterpret_cast<const double2*>(p + 2);
+  return {u.x, u.y, v.x, v.y};
+}
 template <typename R> __device__ __forceinline__ R warp_max(R v) {
   for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;

@@ -558,7 +558,7 @@ template <typename R> struct Src {
     const int* ic5 = S.INL + 5 * (mc - 1);
     d.rIC = ld * (ic5[0] - 1); d.rIP = ld * (ic5[1] - 1); d.rIP1 = ld * (ic5[2] - 1);
     d.rIM = ld * (ic5[3] - 1); d.rIM1 = ld * (ic5[4] - 1);
-    d.rc = S.RNL + 25 * (mc - 1);
+    d.rc = S.RNL + RNL_STRIDE * (mc - 1);
     d.ftemp = S.AF11[im];
     if (T.shallow) d.ftemp = d.ftemp * (T.isnonlin == 0 ? enhfr : __ldg(&ENH[ij + (size_t)enh_ld * (mc - 1)]));
     const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
@@ -597,8 +597,8 @@ template <typename R> struct Src {
     // interactions of direction k at one MC, both KH: {AD, DELAM} to xm[kh*skh],
     // {AD, DELAP} to xp[kh*skh]; AD and DELAD summed over KH to adc, delc
     auto interact = [&](const DiaMc& d, int k, R2* xm, R2* xp, int skh, R& adc, R& delc) {
-      const R* rc = d.rc;
-      const R g1 = rc[1], g2 = rc[2], g3 = rc[3], g4 = rc[4], g5 = rc[13], g6 = rc[14], g7 = rc[15], g8 = rc[16];
+      const Quad<R> c0 = ld4(d.rc), c1 = ld4(d.rc + 4);  // slots of RNLCOEF 0-4, 13-15
+      const R g1 = c0.b, g2 = c0.c, g3 = c0.d, g4 = c1.a, g5 = c1.b, g6 = c1.c, g7 = c1.d, g8 = d.rc[8];
       const R fij = F[k + d.rIC] * d.ftail;
       adc = R(0); delc = R(0);
       for (int kh = 0; kh < 2; ++kh) {
@@ -616,16 +616,13 @@ template <typename R> struct Src {
         xp[skh * kh] = r2(ad, (fij - R(2.) * sam) * T.DAL1 * fcen);
       }
     };
-    // the five target-row updates of column j from the KH-summed gathers
-    // {a2, d2} (K2W), {a21, d21} (K21W), {a1, d1} (K1W), {a11, d11} (K11W)
-    auto upd_mm = [&](const DiaMc& d, R2& v, R a2, R d2, R a21, R d21) {
-      const R* rc = d.rc; v.x = v.x + (a2 * rc[20] + a21 * rc[19]); v.y = v.y + (d2 * rc[23] + d21 * rc[24]); };
-    auto upd_mm1 = [&](const DiaMc& d, R2& v, R a2, R d2, R a21, R d21) {
-      const R* rc = d.rc; v.x = v.x + (a2 * rc[17] + a21 * rc[18]); v.y = v.y + (d2 * rc[21] + d21 * rc[22]); };
-    auto upd_mp = [&](const DiaMc& d, R2& v, R a1, R d1, R a11, R d11) {
-      const R* rc = d.rc; v.x = v.x + (a1 * rc[8] + a11 * rc[7]); v.y = v.y + (d1 * rc[11] + d11 * rc[12]); };
-    auto upd_mp1 = [&](const DiaMc& d, R2& v, R a1, R d1, R a11, R d11) {
-      const R* rc = d.rc; v.x = v.x + (a1 * rc[5] + a11 * rc[6]); v.y = v.y + (d1 * rc[9] + d11 * rc[10]); };
+    // the target-row updates of column j from the KH-summed gathers
+    // {a, dl} and {b, dm} of the kind's two partner tables, with the kind's
+    // four weights (RNLCOEF slots 12 MM, 16 MM1, 20 MP, 24 MP1)
+    auto upd = [&](const DiaMc& d, int slot, R2& v, R a, R dl, R b, R dm) {
+      const Quad<R> c = ld4(d.rc + slot);
+      v.x = v.x + (a * c.a + b * c.b); v.y = v.y + (dl * c.c + dm * c.d);
+    };
 
     const int kmain = kl < 32 ? kl : 32;          // directions of the per-MC pass (lane = k)
     const int nx = kl > 32 ? kl - 32 : 0;         // directions done per batch
@@ -674,10 +671,10 @@ template <typename R> struct Src {
           const R a2 = m2a.x + m2b.x, d2 = m2a.y + m2b.y, a21 = m21a.x + m21b.x, d21 = m21a.y + m21b.y;
           const R a1 = p1a.x + p1b.x, d1 = p1a.y + p1b.y, a11 = p11a.x + p11b.x, d11 = p11a.y + p11b.y;
           if (d.wMC) { vC.x = vC.x - R(2.) * adc; vC.y = vC.y - R(2.) * delc; SF[j + d.rMC] = vC; }
-          if (d.wMM) { upd_mm(d, vM, a2, d2, a21, d21); SF[j + d.rMM] = vM; }
-          if (d.wMM1) { upd_mm1(d, vM1, a2, d2, a21, d21); SF[j + d.rMM1] = vM1; }
-          if (d.wMP) { upd_mp(d, vP, a1, d1, a11, d11); SF[j + d.rMP] = vP; }
-          if (d.wMP1) { upd_mp1(d, vP1, a1, d1, a11, d11); SF[j + d.rMP1] = vP1; }
+          if (d.wMM) { upd(d, 12, vM, a2, d2, a21, d21); SF[j + d.rMM] = vM; }
+          if (d.wMM1) { upd(d, 16, vM1, a2, d2, a21, d21); SF[j + d.rMM1] = vM1; }
+          if (d.wMP) { upd(d, 20, vP, a1, d1, a11, d11); SF[j + d.rMP] = vP; }
+          if (d.wMP1) { upd(d, 24, vP1, a1, d1, a11, d11); SF[j + d.rMP1] = vP1; }
         }
         if (lane < 4 * nx) {
           const R2 u = XM[sa], v = XM[sb];
@@ -697,13 +694,13 @@ template <typename R> struct Src {
         }
         if (lact && d.wMC) { R2 v = SF[j + d.rMC]; v.x = v.x - R(2.) * ladc; v.y = v.y - R(2.) * ldelc; SF[j + d.rMC] = v; }
         __syncwarp();
-        if (lact && d.wMM) { R2 v = SF[j + d.rMM]; upd_mm(d, v, s2.x, s2.y, s21.x, s21.y); SF[j + d.rMM] = v; }
+        if (lact && d.wMM) { R2 v = SF[j + d.rMM]; upd(d, 12, v, s2.x, s2.y, s21.x, s21.y); SF[j + d.rMM] = v; }
         __syncwarp();
-        if (lact && d.wMM1) { R2 v = SF[j + d.rMM1]; upd_mm1(d, v, s2.x, s2.y, s21.x, s21.y); SF[j + d.rMM1] = v; }
+        if (lact && d.wMM1) { R2 v = SF[j + d.rMM1]; upd(d, 16, v, s2.x, s2.y, s21.x, s21.y); SF[j + d.rMM1] = v; }
         __syncwarp();
-        if (lact && d.wMP) { R2 v = SF[j + d.rMP]; upd_mp(d, v, s1.x, s1.y, s11.x, s11.y); SF[j + d.rMP] = v; }
+        if (lact && d.wMP) { R2 v = SF[j + d.rMP]; upd(d, 20, v, s1.x, s1.y, s11.x, s11.y); SF[j + d.rMP] = v; }
         __syncwarp();
-        if (lact && d.wMP1) { R2 v = SF[j + d.rMP1]; upd_mp1(d, v, s1.x, s1.y, s11.x, s11.y); SF[j + d.rMP1] = v; }
+        if (lact && d.wMP1) { R2 v = SF[j + d.rMP1]; upd(d, 24, v, s1.x, s1.y, s11.x, s11.y); SF[j + d.rMP1] = v; }
         __syncwarp();  // the next batch overwrites the slots
       }
     }

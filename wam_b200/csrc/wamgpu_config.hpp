@@ -13,6 +13,18 @@ constexpr int MAX_ML = 48;
 constexpr int MAX_NK10 = 96;   // ST6 frequency axis extended to 10 Hz (LFACTOR)
 constexpr int SCR = 96;        // per-warp per-frequency scratch length (>= MAX_ML, MAX_KL, MAX_NK10)
 
+// The DIA coefficients RNLCOEF(1:25, MC) are stored RNL_STRIDE per MC,
+// grouped for 4-wide loads: {0, 1, 2, 3}, {4, 13, 14, 15}, {16, -, -, -}
+// (the tail factor and the weights of the eight gathers), then the target
+// weights of each row kind: MM {20, 19, 23, 24}, MM1 {17, 18, 21, 22},
+// MP {8, 7, 11, 12}, MP1 {5, 6, 9, 10} (0-based reference indices).  Each
+// MC's block starts 16-byte aligned.  rnl_slot(i) is the slot of index i.
+constexpr int RNL_STRIDE = 28;
+__host__ __device__ constexpr int rnl_slot(int i) {
+  constexpr int slot[25] = {0, 1, 2, 3, 4, 24, 25, 21, 20, 26, 27, 22, 23, 5, 6, 7, 8, 16, 17, 13, 12, 18, 19, 14, 15};
+  return slot[i];
+}
+
 // Offsets (in elements) of the small tables inside the packed blocks that
 // every IMPLSCH CTA stages into shared memory.
 struct SmallLayout {
