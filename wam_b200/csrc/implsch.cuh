@@ -801,13 +801,27 @@ template <typename R> struct Src {
       bool over = false;
       R rtau = err / R(90.), drtau = R(2.0);
       int sgn = (err >= R(0)) ? 1 : -1;
+      // this lane's points of the 10 Hz axis (i = lane + 32 q) stay in
+      // registers over the iterations; LF is stored once, from the last one
+      constexpr int NQ = (MAX_NK10 + 31) / 32;
+      R qx[NQ], qy[NQ], qc[NQ], qd[NQ], qa[NQ], qf[NQ];
+#pragma unroll
+      for (int q = 0; q < NQ; ++q) {
+        const int i = lane + 32 * q;
+        const bool in = i < nk10;
+        qx[q] = in ? SDX[i] : R(0); qy[q] = in ? SDY[i] : R(0); qc[q] = in ? CI10[i] : R(0);
+        qd[q] = in ? DS10[i] : R(0); qa[q] = R(1.0) - uproxy * qc[q]; qf[q] = R(1.0);
+      }
       for (int it = 0; it < 80; ++it) {
         px = 0; py = 0;
-        for (int i = lane; i < nk10; i += 32) {
-          R lf = dmin(R(1.0), dexp((R(1.0) - uproxy * CI10[i]) * rtau));
-          if (i < nk) LF[i] = lf;
-          px = px + (SDX[i] * lf) * CI10[i] * DS10[i];
-          py = py + (SDY[i] * lf) * CI10[i] * DS10[i];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          if (lane + 32 * q < nk10) {
+            const R lf = dmin(R(1.0), dexp(qa[q] * rtau));
+            qf[q] = lf;
+            px = px + (qx[q] * lf) * qc[q] * qd[q];
+            py = py + (qy[q] * lf) * qc[q] * qd[q];
+          }
         }
         tauwx = gro * warp_sum(px); tauwy = gro * warp_sum(py);
         tau = dsqrt((tvx + tauwx) * (tvx + tauwx) + (tvy + tauwy) * (tvy + tauwy));
@@ -819,6 +833,9 @@ template <typename R> struct Src {
         rtau = (sgn > 0) ? rtau * drtau : rtau * (R(1) / drtau);
         if (dabs(err) < R(1.54E-4)) break;
       }
+#pragma unroll
+      for (int q = 0; q < NQ; ++q)
+        if (lane + 32 * q < nk) LF[lane + 32 * q] = qf[q];
     }
     __syncwarp();
     R sumlf = 0;
