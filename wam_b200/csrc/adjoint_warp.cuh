@@ -293,7 +293,6 @@ template <typename R> struct AdjW {
       const adj::Dual<R> e = adj::snl_enhfr(A, P, adj::Dual<R>(akmean, R(1)));
       enhfr = e.v; denh = e.d;
     }
-    const int mfr1 = -T.MFRSTLW + 1, mfrl = ML() - T.KFRH + mfr1;
     const R2* SF = w.SF;
     const R* F = w.F;
     R* XS = w.T;          // [kh*kl + k]: adjoint of SAP
@@ -390,13 +389,13 @@ template <typename R> struct AdjW {
         if (lact) {
           const int mc = mc0 + lb;
           R* xs = XB + 4 * nx * lb + lx;
-          lxf = interact(s.dia_mc(mc, enhfr, mfr1, mfrl), mc, 32 + lx, xs, xs + 2 * nx, nx);
+          lxf = interact(s.dia_mc(mc, enhfr), mc, 32 + lx, xs, xs + 2 * nx, nx);
         }
         __syncwarp();
       }
       for (int b = 0; b < nb; ++b) {
         const int mc = mc0 + b;
-        const typename Src<R>::DiaMc d = s.dia_mc(mc, enhfr, mfr1, mfrl);
+        const typename Src<R>::DiaMc d = s.dia_mc(mc, enhfr);
         // 1. per interaction (k, kh) of this lane: adjoints of FIJ, SAP, SAM;
         // the batch's directions come from the slot
         R xfc = R(0);
@@ -427,7 +426,7 @@ template <typename R> struct AdjW {
         int rIC = 0, rIP = 0, rIP1 = 0, rIM = 0, rIM1 = 0;
         R vP = 0, vP1 = 0, vM = 0, vM1 = 0;
         if (lact) {
-          const typename Src<R>::DiaMc d = s.dia_mc(mc0 + lb, enhfr, mfr1, mfrl);
+          const typename Src<R>::DiaMc d = s.dia_mc(mc0 + lb, enhfr);
           const Quad<R> c0 = ld4(d.rc), c1 = ld4(d.rc + 4);
           const R g8 = d.rc[8];
           const R* xs = XB + 4 * nx * lb + lx;

@@ -90,6 +90,7 @@ template <typename R> struct Impl : ImplBase {
   DevBuf wncg;           // ST6: WN and CG per (sea point, frequency), formed by wamgpu_prepare_source
   int nckpt = 0, ckpt_ld = 0;
   DevBuf small, ismall, tfak, tcgond, tsihkd, flminfr, enh, gom, fr, sinth, costh;
+  DevBuf diamc;          // per-MC DIA rows and write masks (DevTables::diamc)
   // per-point metadata
   DevBuf d_klat, d_klon, d_wlat, d_dpsn, d_della0, d_drgm, d_indep, d_indep_g, d_ddphi, d_ddlam, d_duphi, d_dulam,
       d_dvphi, d_dvlam, d_u, d_v, d_depth;
@@ -296,6 +297,33 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
           if (rows[x] == rows[y] && in(rows[x]) && in(rows[y]))
             return fail(ctx, WAMGPU_E_ARG, "DIA target rows coincide; unsupported frequency ratio");
     }
+  }
+  // Per-MC DIA bookkeeping, point-independent, as the kernels read it: three
+  // int4 per MC = {IC, IP, IP1, IM} and {IM1, MC, MM, MM1} row offsets (the
+  // gathered rows of INLCOEF, the target rows; row 0 where not written), then
+  // {MP, MP1} offsets, the write flags (1 MC, 2 MM, 4 MM1, 8 MP, 16 MP1; 32 =
+  // interior MC, FTAIL 1) and the AF11 index.  The regimes follow the
+  // interior (:2890), high-tail (:2942) and low-tail (:2999) branches.
+  {
+    const int ML = t.ML, ld = d.ld, mfr1 = -t.MFRSTLW + 1, mfrl = ML - t.KFRH + mfr1;
+    std::vector<int> dm((size_t)12 * std::max(1, t.MLSTHG), 0);
+    for (int mc = 1; mc <= t.MLSTHG; ++mc) {
+      const int im = mc - t.MFRSTLW, MP = t.IKP[im], MP1 = t.IKP1[im], MM = t.IKM[im], MM1 = t.IKM1[im];
+      const int* ic5 = &t.INLCOEF[5 * (mc - 1)];
+      const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
+      const bool wMM = regime != 2, wMM1 = regime == 0 || (regime == 1 && MM1 <= ML) || (regime == 2 && MM1 >= 1);
+      const bool wMC = regime != 1 || (MM1 <= ML && mc <= ML);
+      const bool wMP = regime != 1 || (MM1 <= ML && mc <= ML && MP <= ML);
+      const bool wMP1 = regime != 1 || (MM1 <= ML && mc <= ML && MP <= ML && MP1 <= ML);
+      int* e = &dm[(size_t)12 * (mc - 1)];
+      for (int q = 0; q < 5; ++q) e[q] = ld * (ic5[q] - 1);
+      e[5] = wMC ? ld * (mc - 1) : 0; e[6] = wMM ? ld * (MM - 1) : 0; e[7] = wMM1 ? ld * (MM1 - 1) : 0;
+      e[8] = wMP ? ld * (MP - 1) : 0; e[9] = wMP1 ? ld * (MP1 - 1) : 0;
+      e[10] = (wMC ? 1 : 0) | (wMM ? 2 : 0) | (wMM1 ? 4 : 0) | (wMP ? 8 : 0) | (wMP1 ? 16 : 0) | (regime == 0 ? 32 : 0);
+      e[11] = im;
+    }
+    CK(upload(I.diamc, dm, ctx->stream), "upload tables");
+    d.diamc = I.diamc.template as<int4>();
   }
   // CTA shape: the number of sea points per CTA that keeps the most warps
   // resident per SM under the shared-memory budget (ties go to larger CTAs,

@@ -550,28 +550,17 @@ template <typename R> struct Src {
     int rMC, rMM, rMM1, rMP, rMP1;       // target rows (offsets; row 0 where not written)
     bool wMC, wMM, wMM1, wMP, wMP1;      // which targets this MC writes
   };
-  __device__ DiaMc dia_mc(int mc, R enhfr, int mfr1, int mfrl) const {
-    const int ml = ML(), ld = w.ld;
+  __device__ DiaMc dia_mc(int mc, R enhfr) const {
     DiaMc d;
-    const int im = mc - T.MFRSTLW;
-    const int MP = S.IKP[im], MP1 = S.IKP1[im], MM = S.IKM[im], MM1 = S.IKM1[im];
-    const int* ic5 = S.INL + 5 * (mc - 1);
-    d.rIC = ld * (ic5[0] - 1); d.rIP = ld * (ic5[1] - 1); d.rIP1 = ld * (ic5[2] - 1);
-    d.rIM = ld * (ic5[3] - 1); d.rIM1 = ld * (ic5[4] - 1);
+    const int4* e = T.diamc + 3 * (mc - 1);
+    const int4 a = __ldg(e), b = __ldg(e + 1), c = __ldg(e + 2);
+    d.rIC = a.x; d.rIP = a.y; d.rIP1 = a.z; d.rIM = a.w; d.rIM1 = b.x;
+    d.rMC = b.y; d.rMM = b.z; d.rMM1 = b.w; d.rMP = c.x; d.rMP1 = c.y;
+    d.wMC = c.z & 1; d.wMM = c.z & 2; d.wMM1 = c.z & 4; d.wMP = c.z & 8; d.wMP1 = c.z & 16;
     d.rc = S.RNL + RNL_STRIDE * (mc - 1);
-    d.ftemp = S.AF11[im];
+    d.ftail = (c.z & 32) ? R(1) : d.rc[0];
+    d.ftemp = S.AF11[c.w];
     if (T.shallow) d.ftemp = d.ftemp * (T.isnonlin == 0 ? enhfr : __ldg(&ENH[ij + (size_t)enh_ld * (mc - 1)]));
-    const int regime = (mc > mfr1 && mc < mfrl) ? 0 : (mc >= mfrl ? 1 : 2);
-    d.ftail = (regime == 0) ? R(1) : d.rc[0];
-    d.wMM = regime != 2;
-    d.wMM1 = regime == 0 || (regime == 1 && MM1 <= ml) || (regime == 2 && MM1 >= 1);
-    d.wMC = regime != 1 || (MM1 <= ml && mc <= ml);
-    d.wMP = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml);
-    d.wMP1 = regime != 1 || (MM1 <= ml && mc <= ml && MP <= ml && MP1 <= ml);
-    // rows this MC does not write are clamped to row 0, so the loads never
-    // leave the spectrum
-    d.rMC = d.wMC ? ld * (mc - 1) : 0; d.rMM = d.wMM ? ld * (MM - 1) : 0; d.rMM1 = d.wMM1 ? ld * (MM1 - 1) : 0;
-    d.rMP = d.wMP ? ld * (MP - 1) : 0; d.rMP1 = d.wMP1 ? ld * (MP1 - 1) : 0;
     return d;
   }
 
@@ -582,7 +571,6 @@ template <typename R> struct Src {
       enhfr = dmax(R(0.75) * DEPTH * AKMEAN, R(.5));
       enhfr = R(1.) + (R(5.5) / enhfr) * (R(1.) - R(.833) * enhfr) * dexp(R(-1.25) * enhfr);
     }
-    const int mfr1 = -T.MFRSTLW + 1, mfrl = ML() - T.KFRH + mfr1;
     R2* SF = w.SF; const R* F = w.F;
     R2* XM = reinterpret_cast<R2*>(w.T);  // [kh*kl + k] = {AD, DELAM}
     R2* XP = XM + 2 * kl;                 // [kh*kl + k] = {AD, DELAP}
@@ -646,14 +634,14 @@ template <typename R> struct Src {
       R ladc = R(0), ldelc = R(0);
       if (nx > 0) {
         if (lact) {
-          const DiaMc d = dia_mc(mc0 + lb, enhfr, mfr1, mfrl);
+          const DiaMc d = dia_mc(mc0 + lb, enhfr);
           R2* xs = XB + 4 * nx * lb + lx;
           interact(d, 32 + lx, xs, xs + 2 * nx, nx, ladc, ldelc);
         }
         __syncwarp();
       }
       for (int b = 0; b < nb; ++b) {
-        const DiaMc d = dia_mc(mc0 + b, enhfr, mfr1, mfrl);
+        const DiaMc d = dia_mc(mc0 + b, enhfr);
         // 1. interactions (both KH) of this lane's direction; the batch's
         // directions come from the slot
         R adc = R(0), delc = R(0);
@@ -688,7 +676,7 @@ template <typename R> struct Src {
         DiaMc d;
         R2 s2, s21, s1, s11;
         if (lact) {
-          d = dia_mc(mc0 + lb, enhfr, mfr1, mfrl);
+          d = dia_mc(mc0 + lb, enhfr);
           const R2* xs = XB + 4 * nx * lb + lx;
           s2 = xs[0]; s21 = xs[nx]; s1 = xs[2 * nx]; s11 = xs[3 * nx];
         }

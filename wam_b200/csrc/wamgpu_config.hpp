@@ -52,6 +52,7 @@ template <typename R> struct DevTables {
   const R* TFAK;       // [(jd) + NDEPTH*m], jd 0-based
   const R* TCGOND;
   const R* FLMINFR;    // [(ju) + 300*m], ju 0-based
+  const int4* diamc;   // per MC: 3 int4 of DIA row offsets, write flags and the AF11 index
 };
 
 }  // namespace wamgpu
