@@ -285,7 +285,9 @@ template <typename R> struct AdjW {
   __device__ bool adj_batch_start(int mc) const {
     return mc > 128 || ((T.dia_adj_starts[(mc - 1) >> 6] >> ((mc - 1) & 63)) & 1ull);
   }
-  __device__ R snonlin_adj() const {
+  // WIDE: KL > 40, as in the forward DIA.
+  __device__ R snonlin_adj() const { return KL() > 40 ? snonlin_adj_t<true>() : snonlin_adj_t<false>(); }
+  template <bool WIDE> __device__ R snonlin_adj_t() const {
     const int kl = KL(), ld = w.ld;
     const bool dyn = T.shallow && T.isnonlin == 0;
     R enhfr = R(1), denh = R(0);
@@ -367,18 +369,13 @@ template <typename R> struct AdjW {
     const int kmain = kl < 32 ? kl : 32;  // directions of the per-MC pass (lane = k)
     const int nx = kl > 32 ? kl - 32 : 0;
     // this lane's batch item (MC lb of the batch, direction 32 + lx), and its
-    // slot entry i = lane < 4*NX: the copy target in the buffer, and the two
-    // buffer entries whose sum the columns 32..KL-1 need
+    // slot entry i = lane < 4*NX (the adjoint's part of T.dslot): the copy
+    // target in the buffer, and the two buffer entries whose sum the columns
+    // 32..KL-1 need.  With NX > 8 the entries 32 and up are read where used.
     const int lb = nx > 0 ? lane / nx : 0, lx = nx > 0 ? lane - lb * nx : 0;
+    const int4* aslot = T.dslot + 4 * nx;
     int cdst = 0, sa = 0, sb = 0;
-    if (lane < 4 * nx) {
-      const int q = lane / nx, j = 32 + lx;
-      cdst = (q >> 1) * 2 * kl + (q & 1) * kl + j;  // slot layout [XS|XM][kh][x]
-      const int oa = q == 0 ? o1[0] : q == 1 ? o11[0] : q == 2 ? o2[0] : o21[0];
-      const int ob = q == 0 ? o1[1] : q == 1 ? o11[1] : q == 2 ? o2[1] : o21[1];
-      const int base = q < 2 ? 0 : 2 * kl;  // K1W, K11W read XS; K2W, K21W read XM
-      sa = base + rot(j, kl - oa); sb = base + kl + rot(j, kl - ob);
-    }
+    if (lane < 4 * nx) { const int4 e = __ldg(aslot + lane); cdst = e.x; sa = e.y; sb = e.z; }
     for (int mc0 = 1, nb = 0; mc0 <= T.MLSTHG; mc0 += nb) {
       nb = 1;
       if (nx == 0) nb = T.MLSTHG;
@@ -401,6 +398,8 @@ template <typename R> struct AdjW {
         R xfc = R(0);
         if (lane < kmain) xfc = interact(d, mc, lane, XS + lane, XM + lane, kl);
         if (lane < 4 * nx) XS[cdst] = XB[4 * nx * b + lane];
+        if (WIDE)
+          for (int i = lane + 32; i < 4 * nx; i += 32) XS[__ldg(aslot + i).x] = XB[4 * nx * b + i];
         __syncwarp();
         // 2. this lane's column j of the five gathered rows
         if (lane < kmain) {
@@ -418,6 +417,11 @@ template <typename R> struct AdjW {
           LAM[j + d.rIM1] = LAM[j + d.rIM1] + (c1.d * sm2 + g8 * sm21);
         }
         if (lane < 4 * nx) XB[4 * nx * b + lane] = XS[sa] + XS[sb];
+        if (WIDE)
+          for (int i = lane + 32; i < 4 * nx; i += 32) {
+            const int4 e = __ldg(aslot + i);
+            XB[4 * nx * b + i] = XS[e.y] + XS[e.z];
+          }
         __syncwarp();  // the next MC overwrites the buffer
       }
       if (nx > 0) {

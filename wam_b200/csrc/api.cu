@@ -91,6 +91,7 @@ template <typename R> struct Impl : ImplBase {
   int nckpt = 0, ckpt_ld = 0;
   DevBuf small, ismall, tfak, tcgond, tsihkd, flminfr, enh, gom, fr, sinth, costh;
   DevBuf diamc;          // per-MC DIA rows and write masks (DevTables::diamc)
+  DevBuf dslot;          // DIA batch slot entries (DevTables::dslot)
   // per-point metadata
   DevBuf d_klat, d_klon, d_wlat, d_dpsn, d_della0, d_drgm, d_indep, d_indep_g, d_ddphi, d_ddlam, d_duphi, d_dulam,
       d_dvphi, d_dvlam, d_u, d_v, d_depth;
@@ -324,6 +325,32 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
     }
     CK(upload(I.diamc, dm, ctx->stream), "upload tables");
     d.diamc = I.diamc.template as<int4>();
+  }
+  // DIA batch slots (KL > 32, NX = KL - 32 directions per MC of a batch).
+  // Entry i < 4*NX of a slot, as int4: where the per-MC pass copies it in the
+  // buffer, and the two buffer entries whose sum (over KH) the columns
+  // 32..KL-1 gather through one partner table, then 0.  Entry i = (table q,
+  // direction 32 + x) with q = i / NX.  The forward's buffer is {XM | XP}
+  // [kh][k] (q: K2W, K21W read XM; K1W, K11W read XP); the adjoint's is
+  // {XS | XM} (q: K1W, K11W read XS; K2W, K21W read XM).  A source column is
+  // the target column rotated back by the table's offset.
+  {
+    const int KL = t.KL, nx = KL > 32 ? KL - 32 : 0;
+    std::vector<int> ds((size_t)32 * std::max(1, nx), 0);
+    auto rot = [KL](int k, int o) { const int v = k + o; return v >= KL ? v - KL : v; };
+    auto put = [&](int e, const std::vector<int>* const tabs[4], int i) {
+      const int q = i / nx, j = 32 + (i - q * nx), kh = q & 1, base = q < 2 ? 0 : 2 * KL;
+      const std::vector<int>& tb = *tabs[q];
+      int* v = &ds[(size_t)4 * e];
+      v[0] = (q >> 1) * 2 * KL + kh * KL + j;
+      v[1] = base + rot(j, KL - (tb[0] - 1));
+      v[2] = base + KL + rot(j, KL - (tb[KL] - 1));
+    };
+    const std::vector<int>* const fw[4] = {&t.K2W, &t.K21W, &t.K1W, &t.K11W};
+    const std::vector<int>* const ad[4] = {&t.K1W, &t.K11W, &t.K2W, &t.K21W};
+    for (int i = 0; i < 4 * nx; ++i) { put(i, fw, i); put(4 * nx + i, ad, i); }
+    CK(upload(I.dslot, ds, ctx->stream), "upload tables");
+    d.dslot = I.dslot.template as<int4>();
   }
   // CTA shape: the number of sea points per CTA that keeps the most warps
   // resident per SM under the shared-memory budget (ties go to larger CTAs,

@@ -564,7 +564,14 @@ template <typename R> struct Src {
     return d;
   }
 
+  // WIDE: more than 8 directions beyond the first 32 (KL > 40), so a batch
+  // slot has more entries than lanes.  The common shapes compile without that
+  // code in the MC loop.
   __device__ void snonlin(R AKMEAN) const {
+    if (KL() > 40) snonlin_t<true>(AKMEAN);
+    else snonlin_t<false>(AKMEAN);
+  }
+  template <bool WIDE> __device__ void snonlin_t(R AKMEAN) const {
     const int kl = KL(), ld = w.ld;
     R enhfr = R(1);
     if (T.shallow && T.isnonlin == 0) {
@@ -616,18 +623,12 @@ template <typename R> struct Src {
     const int nx = kl > 32 ? kl - 32 : 0;         // directions done per batch
     const int bsz = max(1, nx > 0 ? T.dia_batch : T.MLSTHG);
     // this lane's batch item (MC lb of the batch, direction 32 + lx), and its
-    // slot entry i = lane < 4*NX: the copy target in the buffer, and the two
-    // buffer entries whose sum the columns 32..KL-1 need
+    // slot entry i = lane < 4*NX (T.dslot): the copy target in the buffer,
+    // and the two buffer entries whose sum the columns 32..KL-1 need.  With
+    // NX > 8 the entries 32 and up are read from the table where used.
     const int lb = nx > 0 ? lane / nx : 0, lx = nx > 0 ? lane - lb * nx : 0;
     int cdst = 0, sa = 0, sb = 0;
-    if (lane < 4 * nx) {
-      const int q = lane / nx, part = q >> 1, kh = q & 1, j = 32 + lx;
-      cdst = part * 2 * kl + kh * kl + j;  // slot layout [XM|XP][kh][x]
-      const int oa = q == 0 ? o2[0] : q == 1 ? o21[0] : q == 2 ? o1[0] : o11[0];
-      const int ob = q == 0 ? o2[1] : q == 1 ? o21[1] : q == 2 ? o1[1] : o11[1];
-      const int base = q < 2 ? 0 : 2 * kl;  // K2W, K21W read XM; K1W, K11W read XP
-      sa = base + rot(j, kl - oa); sb = base + kl + rot(j, kl - ob);
-    }
+    if (lane < 4 * nx) { const int4 e = __ldg(T.dslot + lane); cdst = e.x; sa = e.y; sb = e.z; }
     for (int mc0 = 1; mc0 <= T.MLSTHG; mc0 += bsz) {
       const int nb = min(bsz, T.MLSTHG - mc0 + 1);
       const bool lact = nx > 0 && lb < nb;
@@ -647,6 +648,8 @@ template <typename R> struct Src {
         R adc = R(0), delc = R(0);
         if (lane < kmain) interact(d, lane, XM + lane, XP + lane, kl, adc, delc);
         if (lane < 4 * nx) XM[cdst] = XB[4 * nx * b + lane];
+        if (WIDE)
+          for (int i = lane + 32; i < 4 * nx; i += 32) XM[__ldg(T.dslot + i).x] = XB[4 * nx * b + i];
         __syncwarp();
         // 2. this lane's column j of the five target rows
         if (lane < kmain) {
@@ -668,6 +671,12 @@ template <typename R> struct Src {
           const R2 u = XM[sa], v = XM[sb];
           XB[4 * nx * b + lane] = r2(u.x + v.x, u.y + v.y);
         }
+        if (WIDE)
+          for (int i = lane + 32; i < 4 * nx; i += 32) {
+            const int4 e = __ldg(T.dslot + i);
+            const R2 u = XM[e.y], v = XM[e.z];
+            XB[4 * nx * b + i] = r2(u.x + v.x, u.y + v.y);
+          }
         __syncwarp();  // the next MC overwrites the buffer
       }
       if (nx > 0) {

@@ -53,6 +53,7 @@ template <typename R> struct DevTables {
   const R* TCGOND;
   const R* FLMINFR;    // [(ju) + 300*m], ju 0-based
   const int4* diamc;   // per MC: 3 int4 of DIA row offsets, write flags and the AF11 index
+  const int4* dslot;   // KL > 32: DIA batch slot entries, 4*(KL-32) for the forward, then as many for the adjoint
 };
 
 }  // namespace wamgpu

@@ -122,6 +122,27 @@ def _finish(name, cfg, g, depth_grid, u_grid, v_grid, rng, seed_fn=None, **kw):
     return Workload(name, cfg, g, depth, u10, udir, e_fm, d_fk, **kw)
 
 
+def make_direction_variant(kl, iphys, seed=1234, scale=0.25, precision=4, device=0):
+    """The small open-ocean grid of "c0" with KL directions and ST4 (iphys=1)
+    or ST6 (iphys=2) source terms.  The direction count decides how the source
+    kernels split the directions of a sea point over a warp's 32 lanes (the
+    DIA and SDISSIP_ARD take the directions beyond the first 32 in batches
+    over frequencies), so the parity tests run KL = 33, 48 and 64 besides the
+    configurations' 24 and 36."""
+    rng = np.random.default_rng(seed)
+    nx, ny = max(8, int(60 * scale)), max(6, int(40 * scale))
+    sea = blob_mask(rng, nx, ny, 0.10, 3)
+    g = regular_grid(sea, 20.0, -40.0, 40.0 / ny, 60.0 / nx)
+    cfg = make_config(kl, 25, 0.04177, iphys, 900, 900, g["delphi"], shallow_run=False, spherical_run=True,
+                      betamax=1.42 if iphys == 1 else 1.20, precision=precision, device=device)
+    depth = np.full((nx, ny), 4000.0)
+    spd = 5 + 15 * _unit(_smooth(rng.random((nx, ny)), 3))
+    drc = 2 * math.pi * _unit(_smooth(rng.random((nx, ny)), 3))
+    u, v = spd * np.sin(drc), spd * np.cos(drc)
+    g["_mask"] = sea
+    return _finish(f"c0/kl{kl}/st{4 if iphys == 1 else 6}", cfg, g, depth, u, v, rng, n_src_steps=48, sub_steps=1)
+
+
 def make_workload(name, seed=1234, scale=1.0, precision=4, device=0):
     rng = np.random.default_rng(seed)
     if name == "c0":
