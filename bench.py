@@ -15,8 +15,8 @@ path); the spectrum (3.3 GB) is far larger than L2, so no flush is needed.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl wamgpu|reference]
 
 --impl reference times the CPU restatement of the reference (oracle/, the
-reference's Fortran cannot be compiled in this image) on a bounded sample of
-the same workload recipe with all host threads.  With N>1 (torchrun), every
+reference's Fortran cannot be compiled on these machines) with all host
+threads on latitude bands of the same workload grid (same config line).  With N>1 (torchrun), every
 rank runs its own replica of the workload (weak scaling, no collective).
 """
 import argparse
@@ -118,55 +118,122 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_reference(args, wl_name, scale, budget_s, steps=None):
-    """The oracle (CPU restatement) on a bounded sample of the workload recipe."""
-    from oracle.oracle import Oracle
-    from wam_b200.synth import make_workload
-    w = make_workload(wl_name, scale=scale)
-    o = Oracle(w.cfg)
-    o.set_grid(w.grid)
-    o.set_fields(w.depth)
-    o.prepare_propagation()
-    o.prepare_source()
-    indep = o.indep()
-    f = w.spectrum_f().astype(float)
-    tw, us, zz = (a.astype(float) for a in (w.tauw, w.ustar, w.z0))
-    nthreads = os.cpu_count() or 1
-    n_done, t_tot = 0, 0.0
-    while (steps is None and t_tot < budget_s) or (steps is not None and n_done < steps):
+def workload_config(name, scale, nsea, kl, ml):
+    """The `config` of both arms: the workload, its sea points and bins per point."""
+    if name == "c1" and scale == 1.0:
+        desc = ("c1: 0.1 deg 1200x900 regional, ST6, KL=36 ML=30, IDELPRO=120 s IDELT=600 s "
+                "(5 PROPAGS + 1 IMPLSCH per step)")
+    else:
+        desc = f"{name} at scale {scale}"
+    return {"workload": desc, "nsea": int(nsea), "bins_per_point": int(kl * ml)}
+
+
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+class CpuSample:
+    """The oracle (the CPU restatement of the reference) on bands of the
+    full workload grid: each band is a contiguous range of the south-to-north
+    ordered sea points with the halo rows its propagation reads, prepared once
+    (PREPARE_PROPAGATION with its stored coefficient arrays, as the reference
+    does) and kept resident in the oracle's REAL precision.  One CPU step runs
+    one band's WAMODEL pass (IDELT/IDELPRO PROPAGS calls, then IMPLSCH over
+    every point of the band) on all host threads; the bands take turns.  The
+    bins counted are all the points the pass updates, halo rows included."""
+
+    def __init__(self, name, scale, nbands=64, sample_bands=(8, 24, 40, 56)):
+        from oracle.oracle import Oracle
+        from wam_b200.halo import local_grid, partition
+        from wam_b200.synth import make_workload
+        w = make_workload(name, scale=scale)
+        self.w = w
+        self.nprop = w.cfg["idelt"] // w.cfg["idelpro"]
+        self.nthreads = os.cpu_count() or 1
+        parts = partition(w.grid, nbands)
+        self.bands = []
+        f_all = None
+        for q in sample_bands:
+            p = parts[min(q, nbands - 1)]
+            a, b = p["ninf"], p["nsup"]
+            o = Oracle(w.cfg)
+            o.set_grid(local_grid(w.grid, p))
+            o.set_fields(w.depth[a:b])
+            o.prepare_propagation()
+            o.prepare_source()
+            e = w.e_fm[a:b]
+            d = w.d_fk[a:b]
+            f = np.asfortranarray(e[:, None, :] * d[:, :, None])
+            sl = lambda x: np.asarray(x)[a:b]
+            o.resident_set(f, sl(w.u10), sl(w.udir), sl(w.tauw), sl(w.ustar), sl(w.z0), sl(w.roairn), sl(w.wstar),
+                           sl(w.depth))
+            self.bands.append((o, b - a))
+        self.i = 0
+
+    def step(self):
+        """One band's pass; returns (bins updated, seconds)."""
+        o, n = self.bands[self.i % len(self.bands)]
+        self.i += 1
         t0 = time.perf_counter()
-        for _ in range(w.sub_steps):
-            f = o.propags(f)
-        f, tw, us, zz, _ = o.implsch(f, w.u10, w.udir, tw, us, zz, w.roairn, w.wstar, w.depth, indep,
-                                     nthreads=nthreads)
-        t_tot += time.perf_counter() - t0
-        n_done += 1
-    bins = w.nsea * w.cfg["kl"] * w.cfg["ml"]
-    return dict(value=bins * n_done / t_tot, nsea=w.nsea, steps=n_done, seconds=t_tot, cores=nthreads,
-                grid=f"{w.grid['nx']}x{w.grid['ny']}")
+        o.resident_step(self.nprop, self.nthreads)
+        dt = time.perf_counter() - t0
+        return n * self.w.cfg["kl"] * self.w.cfg["ml"], dt
+
+    def describe(self, nsteps, seconds):
+        pts = [n for _, n in self.bands]
+        return (f"{len(pts)} latitude bands of the full {self.w.grid['nx']}x{self.w.grid['ny']} grid "
+                f"({min(pts)}-{max(pts)} sea points each, halo rows included) taking turns, {nsteps} WAMODEL "
+                f"passes ({self.nprop} PROPAGS + IMPLSCH) in {seconds:.1f} s on {self.nthreads} host threads "
+                f"({cpu_model()})")
+
+
+def cpu_baseline(name, scale, budget_s):
+    """cpu_baseline object of the GPU arm: the oracle sample for ~budget_s seconds."""
+    cs = CpuSample(name, scale)
+    cs.step()  # warm
+    bins = secs = 0.0
+    n = 0
+    while secs < budget_s:
+        b, dt = cs.step()
+        bins += b
+        secs += dt
+        n += 1
+    return {"value": bins / secs, "unit": UNIT, "cores": cs.nthreads, "kind": "port", "cpu": cpu_model(),
+            "sample": cs.describe(n, secs)}
 
 
 def run_reference(args):
+    """The reference arm: the CPU restatement of the reference's path (the
+    Fortran reference cannot be built on these machines) timed on the host
+    cores on bands of the same workload grid, same config and metric as the
+    GPU arm.  Rank 0 alone runs it under torchrun."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    # sample: the workload recipe at 1/8 linear scale (~12k sea points), one step per timed step
-    per_step = []
-    for i in range(args.warmup + args.steps):
-        r = cpu_reference(args, args.workload, 0.125, 0.0, steps=1)
-        if i >= args.warmup:
-            per_step.append(r)
-    secs = sum(r["seconds"] for r in per_step)
-    bins = per_step[0]["nsea"] * 36 * 30
-    val = bins * len(per_step) / secs
+    cs = CpuSample(args.workload, args.scale)
+    for _ in range(args.warmup):
+        cs.step()
+    bins = secs = 0.0
+    for _ in range(args.steps):
+        b, dt = cs.step()
+        bins += b
+        secs += dt
+    val = bins / secs
+    w = cs.w
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / len(per_step),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic (seeded)",
-            "config": {"workload": f"{args.workload} recipe at 1/8 linear scale ({per_step[0]['grid']}, "
-                                   f"{per_step[0]['nsea']} sea points): 5 PROPAGS + 1 IMPLSCH per step"},
-            "cpu_baseline": {"value": val, "unit": UNIT, "cores": per_step[0]["cores"], "kind": "port",
-                             "sample": f"{per_step[0]['nsea']} sea points x {len(per_step)} source steps"},
+            "data": "synthetic (seeded fields; no dataset for this path)",
+            "config": workload_config(args.workload, args.scale, w.nsea, w.cfg["kl"], w.cfg["ml"]),
+            "cpu_baseline": {"value": val, "unit": UNIT, "cores": cs.nthreads, "kind": "port", "cpu": cpu_model(),
+                             "sample": cs.describe(args.steps, secs)},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -502,22 +569,15 @@ def main():
                "transfer_bound": transfer_bound(torch, dev, hf)}
     cpu = None
     if not args.no_cpu_baseline and rank == 0 and world == 1:
-        r = cpu_reference(args, args.workload, 0.125, 15.0)
-        cpu = {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": "port",
-               "sample": f"{args.workload} recipe at 1/8 scale ({r['grid']}, {r['nsea']} sea points), "
-                         f"{r['steps']} source steps (5 PROPAGS + IMPLSCH) in {r['seconds']:.1f} s"}
+        cpu = cpu_baseline(args.workload, args.scale, 15.0)
     if rank == 0:
         launches = sum(v["launches"] for v in kernels.values())
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fields; no dataset for this path)",
-                "config": {"workload": f"{args.workload}: 0.1 deg 1200x900 regional, ST6, KL=36 ML=30, "
-                                       f"IDELPRO=120 s IDELT=600 s (5 PROPAGS + 1 IMPLSCH per step)"
-                                       if args.workload == "c1" and args.scale == 1.0 else
-                                       f"{args.workload} at scale {args.scale}",
-                           "nsea": n, "bins_per_point": KL * ML, "counter": counter, "total_cfl": cfl,
-                           "l2": "spectrum 3.3 GB >> 126 MB L2, no flush needed",
-                           "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+                "config": workload_config(args.workload, args.scale, n, KL, ML),
+                "run": {"counter": counter, "total_cfl": cfl, "l2": "spectrum 3.3 GB >> 126 MB L2, no flush needed",
+                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
                 "roofline": roof, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e,
                 "gpu_launches": launches, "clocks": clk.summary()}
         if not args.no_batched and world == 1:

@@ -41,7 +41,8 @@ extern "C" {
 #define WAMGPU_E_CFL -4       /* negative propagation coefficient (CHECK_CFL) */
 #define WAMGPU_E_NOMEM -5     /* device allocation failed                     */
 #define WAMGPU_E_NUMERIC -6   /* non-finite values detected in outputs        */
-#define WAMGPU_E_TIMEOUT -7   /* a bounded device wait expired                */
+#define WAMGPU_E_TIMEOUT -7   /* reserved: a bounded device wait expired; no  */
+                              /* entry point returns it yet                   */
 
 typedef struct wamgpu_ctx wamgpu_ctx;
 
@@ -146,7 +147,13 @@ WAMGPU_API int wamgpu_propags_dev(wamgpu_ctx* ctx, void* f3, int ld, void* scrat
  *    (cudaGetSymbolAddress, which may load the module) and keeps it for the
  *    process; make that first call before any stream capture.
  *  - Nothing is allocated, freed or cleared: every scratch element a call
- *    reads it wrote earlier in the same call.
+ *    reads it wrote earlier in the same call.  This holds for the whole
+ *    grid only, so a context with an owned range (wamgpu_set_owned) is
+ *    rejected with WAMGPU_E_ARG; a band driver sub-steps with
+ *    wamgpu_propags_substep_dev instead.
+ *  - The looked-up address belongs to the device's primary context: do not
+ *    use the library across a cudaDeviceReset (which invalidates every
+ *    context and buffer of the library as well).
  *  - There is ONE array per device: calls whose GPU work overlaps (other
  *    streams, other contexts on the same device) race on it; order them on
  *    one stream.
@@ -297,6 +304,65 @@ WAMGPU_API int wamgpu_step_ckpt_dev(wamgpu_ctx* ctx, int slot, void* fl3, int ld
 WAMGPU_API int wamgpu_step_adj_dev(wamgpu_ctx* ctx, int slot, int nprop, void* lam_fl3, int ld, void* lam_tauw,
                                    void* lam_u10, const void* udir, const void* roairn, const void* wstar,
                                    void* scratch, void* stream);
+
+/* Test diagnostics of IMPLSCH's integer decisions.  No counterpart in the
+ * reference, where they live in local arrays of IMPLSCH
+ * (wam_source_module.f90:440-462); they let a test compare them one by one
+ * with another implementation.  While set, every IMPLSCH launch of the
+ * context (wamgpu_implsch_*, wamgpu_step_*) writes, for sea point ij
+ * (0-based), decisions[ij + ld*q] with
+ *   q = 0  JU, NINT(U10/DELU) clamped to 1..JUMAX (source:498),
+ *   q = 1  MIJ of the first FRCUTINDEX call (source:563; ST6 :5447-5515),
+ *   q = 2  MIJ of the last call, after the update (source:697),
+ *   q = 3  LFACTOR iterations (ST6, source:4647-4672; 0 when the stress
+ *          needs no reduction, -1 for ST4);
+ * and, when llws is not NULL, llws[ij + ld*(b + KL*ML*q)] for bin
+ * b = (K-1) + KL*(M-1): the LLWS mask of the first (q = 0) and of the last
+ * (q = 1) SINPUT call.  Device pointers of the context's device; ld >= NSEA.
+ * decisions = NULL switches the diagnostics off.  The production step
+ * writes none of this. */
+WAMGPU_API int wamgpu_set_diagnostics(wamgpu_ctx* ctx, int* decisions, unsigned char* llws, int ld);
+
+/* PUT_ICE (FL3, INDICATOR) and PUT_DRY (FL3, INDICATOR) on device data
+ * (PUT_ICE_SPEC wam_ice_module.f90:312-324, PUT_DRY_SPEC
+ * wam_topo_module.f90:557-569; called by WAMODEL at wamodel.f90:380-397),
+ * and their parameter-block forms PUT_ICE_PAR / PUT_DRY_PAR (:283-308,
+ * :529-553).  data holds nrows rows of ld values with the sea point fastest
+ * (a spectrum: nrows = KL*ML; an output block: one row per parameter);
+ * points is a device array of n 1-based sea point numbers (IJ_ICE, IJ_DRY).
+ * Every row of every listed point becomes `value` (converted to the
+ * context's precision); points outside the owned range are skipped, as the
+ * reference skips those outside NIJS..NIJL.  This keeps a WAMODEL pass with
+ * ice or dry points on the device. */
+WAMGPU_API int wamgpu_put_points_dev(wamgpu_ctx* ctx, void* data, int ld, int nrows, const int* points, int n,
+                                     double value, void* stream);
+
+/* COMPUTE_OUTPUT_PARAMETER (wam_output_module.f90:481-640) on the device:
+ * the integrated parameters of every owned sea point from the resident
+ * spectrum, so that an output step reads WAMGPU_OUT_NPARAM values per point
+ * instead of the whole spectrum.  block[ij + block_ld*(IP-1)] receives the
+ * reference's output parameter IP (CFLAG_P numbering):
+ *   1 U10 [m/s], 2 wind direction [deg], 3 USTAR [m/s], 4 drag coefficient,
+ *   5 Charnock parameter (CHARNOCK_PAR, wam_interface_module.f90:159),
+ *   6 water depth [m] (999 in deep water), 7 current speed [m/s],
+ *   8 current direction [deg], 9 significant wave height Hs [m]
+ *   (TOTAL_ENERGY :1342), 10 peak period [s] (PEAK_PERIOD :741),
+ *   11 mean period 1/FM [s] (FEMEAN :207), 12 TM1 and 13 TM2 [s]
+ *   (TM1_TM2_PERIODS :1152), 14 mean direction and 15 directional spread
+ *   [deg] (MEAN_DIRECTION :412), 16 normalised wave stress, 32 Z0 [m],
+ *   40 mean square slope (MEANSQS :639).
+ * The other parameters up to WAMGPU_OUT_NPARAM (swell separation, kurtosis,
+ * radiation stress, Stokes drift) are not computed and are set to 0.
+ * from != 0 gives directions the waves and wind come from (the reference's
+ * default orientation_of_directions), 0 directions they go to.  When USTAR
+ * is zero at every point, AIRSEA (wam_source_module.f90:868-971) first sets
+ * USTAR and Z0 from U10 and TAUW, as the reference does.  Device pointers in
+ * the context's precision, spectrum and fields as for wamgpu_implsch_dev;
+ * currents and depth are the context's own. */
+#define WAMGPU_OUT_NPARAM 40
+WAMGPU_API int wamgpu_output_parameters_dev(wamgpu_ctx* ctx, const void* fl3, int ld, const void* u10,
+                                            const void* udir, const void* tauw, void* ustar, void* z0, int from,
+                                            void* block, int block_ld, void* stream);
 
 /* Synchronises the context stream; returns WAMGPU_E_NUMERIC if a kernel
  * reported non-finite output since the last call. */

@@ -58,7 +58,13 @@ def lib():
         L.oracle_get_coef.argtypes = [vp, ctypes.c_char_p, dp]
         L.oracle_implsch.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, ip, dp,
                                      ctypes.c_int]
+        L.oracle_implsch_diag.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, dp, dp, dp, dp, dp, ip, dp,
+                                          ctypes.c_int, ip, dp, ctypes.POINTER(ctypes.c_ubyte)]
         L.oracle_propags.argtypes = [vp, dp]
+        L.oracle_resident_set.argtypes = [vp] + [dp] * 9
+        L.oracle_output_params.argtypes = [vp, ctypes.c_int] + [dp] * 9 + [ip, ctypes.c_int, dp]
+        L.oracle_resident_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.oracle_resident_get.argtypes = [vp, dp, dp, dp, dp]
         L.oracle_grid_create.restype = vp
         L.oracle_grid_create.argtypes = [ctypes.POINTER(GridDef), ctypes.c_char_p]
         L.oracle_grid_destroy.argtypes = [vp]
@@ -184,7 +190,78 @@ class Oracle:
                               nthreads)
         return f, tw, us, zz, (fl.reshape(7, nsea) if fl is not None else None)
 
+    def implsch_diag(self, fl3, u10, udir, tauw, ustar, z0, roairn, wstar, depth, indep, lcflx=False, nthreads=0):
+        """implsch() plus the step's integer decisions: returns (fl3, tauw, ustar, z0, fluxes, diag) where diag
+        holds JU, MIJ1, MIJ2 (first and last FRCUTINDEX), LFIT (LFACTOR iterations, -1 for ST4), the REAL values
+        they were rounded from (JU_ARG, MIJ1_ARG, MIJ2_ARG), the smallest relative distance of the LFACTOR |ERR|
+        from its exit threshold over the iterations (LF_MARGIN) and the LLWS masks of the first and the last
+        SINPUT call (LLWS1, LLWS2: uint8 arrays shaped like FL3)."""
+        nsea = fl3.shape[0]
+        f = np.array(fl3, dtype=float, order="F")
+        tw, us, zz = (np.array(a, dtype=float) for a in (tauw, ustar, z0))
+        fl = np.zeros(7 * nsea) if lcflx else None
+        idg = np.zeros(4 * nsea, np.int32)
+        fdg = np.zeros(4 * nsea)
+        ll = np.zeros(2 * nsea * self.kl * self.ml, np.uint8)
+        self.L.oracle_implsch_diag(self.h, nsea, nsea, _d(f), _d(np.ascontiguousarray(u10, float)),
+                                   _d(np.ascontiguousarray(udir, float)), _d(tw), _d(us), _d(zz),
+                                   _d(np.ascontiguousarray(roairn, float)), _d(np.ascontiguousarray(wstar, float)),
+                                   _d(np.ascontiguousarray(depth, float)), _i(np.ascontiguousarray(indep, np.int32)),
+                                   _d(fl), nthreads, _i(idg), _d(fdg), ll.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)))
+        idg, fdg = idg.reshape(4, nsea), fdg.reshape(4, nsea)
+        ll = ll.reshape(2, self.ml, self.kl, nsea)
+        diag = dict(JU=idg[0], MIJ1=idg[1], MIJ2=idg[2], LFIT=idg[3], JU_ARG=fdg[0], MIJ1_ARG=fdg[1], MIJ2_ARG=fdg[2],
+                    LF_MARGIN=fdg[3], LLWS1=np.asfortranarray(ll[0].transpose(2, 1, 0)),
+                    LLWS2=np.asfortranarray(ll[1].transpose(2, 1, 0)))
+        return f, tw, us, zz, (fl.reshape(7, nsea) if fl is not None else None), diag
+
+    def output_params(self, fl3, u10, udir, ustar, tauw, z0, depth, u=None, v=None, indep=None, from_=True):
+        """COMPUTE_OUTPUT_PARAMETER: returns (block[40, nsea] with row IP-1 = parameter IP, ustar, z0)."""
+        nsea = fl3.shape[0]
+        f = np.asfortranarray(fl3, float)
+        us, zz = np.array(ustar, float), np.array(z0, float)
+        c = lambda a: None if a is None else np.ascontiguousarray(a, float)
+        out = np.zeros(40 * nsea)
+        ind = np.ascontiguousarray(indep if indep is not None else self.indep(), np.int32)
+        self.L.oracle_output_params(self.h, nsea, _d(f), _d(c(u10)), _d(c(udir)), _d(us), _d(c(tauw)), _d(zz),
+                                    _d(c(depth)), _d(c(u)), _d(c(v)), _i(ind), int(bool(from_)), _d(out))
+        return out.reshape(40, nsea), us, zz
+
+    def resident_set(self, fl3, u10, udir, tauw, ustar, z0, roairn, wstar, depth):
+        """Keep a model state inside the oracle in its own precision (the timed CPU baseline)."""
+        c = lambda a: np.ascontiguousarray(a, float)
+        self._res = [np.asfortranarray(fl3, float)] + [c(a) for a in (u10, udir, tauw, ustar, z0, roairn, wstar, depth)]
+        self.L.oracle_resident_set(self.h, *[_d(a) for a in self._res])
+
+    def resident_step(self, nprop, nthreads=0):
+        """One WAMODEL pass on the resident state: nprop PROPAGS, then IMPLSCH (all host threads when 0)."""
+        rc = self.L.oracle_resident_step(self.h, int(nprop), int(nthreads or os.cpu_count() or 1))
+        if rc != 0:
+            raise RuntimeError("oracle_resident_step: no resident state")
+
+    def resident_get(self):
+        """(fl3, tauw, ustar, z0) of the resident state."""
+        n = self.nsea
+        f = np.zeros((n, self.kl, self.ml), order="F")
+        tw, us, zz = np.zeros(n), np.zeros(n), np.zeros(n)
+        self.L.oracle_resident_get(self.h, _d(f), _d(tw), _d(us), _d(zz))
+        return f, tw, us, zz
+
     def propags(self, fl3):
         f = np.array(fl3, dtype=float, order="F")
         self.L.oracle_propags(self.h, _d(f))
         return f
+
+
+def put_points(data, points, value, nijs=1, nijl=None):
+    """PUT_ICE_SPEC / PUT_DRY_SPEC (wam_ice_module.f90:312-324,
+    wam_topo_module.f90:557-569) and the PUT_*_PAR forms: for every 1-based
+    sea point of the list (IJ_ICE / IJ_DRY) inside NIJS..NIJL, all values of
+    that point (data[ij-1, ...], sea point first) become `value`.  Returns a
+    modified copy."""
+    out = np.array(data, copy=True, order="F")
+    nijl = out.shape[0] if nijl is None else nijl
+    for ij in np.asarray(points).reshape(-1):
+        if nijs <= ij <= nijl:
+            out[ij - 1, ...] = value
+    return out

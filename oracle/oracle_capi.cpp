@@ -12,6 +12,7 @@
 #include "oracle_grid.hpp"
 #include "oracle_source.hpp"
 #include "oracle_prop.hpp"
+#include "oracle_output.hpp"
 
 using namespace wamo;
 
@@ -23,8 +24,10 @@ struct OracleBase {
 template <typename R> struct Oracle : OracleBase {
   OracleConfig cfg;
   FreDir<R> fd; ShallowTables<R> sh; MinEnergy<R> me; DiaTables<R> dia; SourceTables<R> st;
-  SourceModel<R> src; PropModel<R> prop;
+  SourceModel<R> src; PropModel<R> prop; OutputModel<R> outm;
   std::vector<R> depth_src;  // depth of the points passed to prepare_source
+  // resident REAL state of the timed CPU baseline (oracle_resident_*)
+  std::vector<R> rF, rU10, rUDIR, rTAUW, rUSTAR, rZ0, rROAIRN, rWSTAR, rDEPTH;
   explicit Oracle(const OracleConfig& c) : cfg(c) {
     precision = sizeof(R);
     fd.build(c.kl, c.ml, R(c.fr1), c.iref);
@@ -37,6 +40,7 @@ template <typename R> struct Oracle : OracleBase {
     src.cfg = c; src.fd = &fd; src.sh = &sh; src.me = &me; src.dia = &dia; src.st = &st;
     src.BETAMAX = betamax; src.ZALP = zalp; src.ALPHA = alpha; src.TAUWSHELTER = tauwshelter; src.CDFAC = R(c.cdfac);
     prop.cfg = c; prop.fd = &fd; prop.sh = &sh;
+    outm.fd = &fd; outm.sh = &sh; outm.shallow = c.shallow_run != 0;
   }
 };
 
@@ -83,7 +87,8 @@ template <typename R> static int get_itable_t(Oracle<R>* o, const std::string& n
 
 template <typename R> static void implsch_t(Oracle<R>* o, int nsea, int ld, double* fl3, const double* u10, const double* udir,
                                             double* tauw, double* ustar, double* z0, const double* roairn, const double* wstar,
-                                            const double* depth, const int* indep, double* fluxes, int nthreads) {
+                                            const double* depth, const int* indep, double* fluxes, int nthreads,
+                                            int* idiag = nullptr, double* fdiag = nullptr, unsigned char* llws = nullptr) {
   const int kl = o->fd.KL, ml = o->fd.ML;
   if (nthreads <= 0) nthreads = (int)std::max(1u, std::thread::hardware_concurrency());
   std::atomic<int> next(0);
@@ -96,8 +101,20 @@ template <typename R> static void implsch_t(Oracle<R>* o, int nsea, int ld, doub
       for (int k = 0; k < kl; ++k) F[k + kl * m] = R(fl3[ij + (size_t)ld * (k + (size_t)kl * m)]);
     R tw = R(tauw[ij]), us = R(ustar[ij]), zz = R(z0[ij]);
     typename SourceModel<R>::Fluxes fx{};
+    typename SourceModel<R>::Diag dg{};
+    std::vector<uint8_t> m1, m2;
+    if (llws) { m1.resize((size_t)kl * ml); m2.resize((size_t)kl * ml); dg.LLWS1 = m1.data(); dg.LLWS2 = m2.data(); }
     o->src.implsch_point(F.data(), R(u10[ij]), R(udir[ij]), tw, us, zz, R(roairn[ij]), R(wstar[ij]), R(depth[ij]), indep[ij],
-                         ij, fluxes ? &fx : nullptr);
+                         ij, fluxes ? &fx : nullptr, (idiag || fdiag || llws) ? &dg : nullptr);
+    if (idiag) { idiag[ij] = dg.JU; idiag[ij + nsea] = dg.MIJ1; idiag[ij + 2 * (size_t)nsea] = dg.MIJ2; idiag[ij + 3 * (size_t)nsea] = dg.LFIT; }
+    if (fdiag) {
+      fdiag[ij] = dg.JU_ARG; fdiag[ij + nsea] = dg.MIJ1_ARG; fdiag[ij + 2 * (size_t)nsea] = dg.MIJ2_ARG;
+      fdiag[ij + 3 * (size_t)nsea] = dg.LF_MARGIN;
+    }
+    if (llws) {
+      const size_t ns = (size_t)kl * ml;
+      for (size_t b = 0; b < ns; ++b) { llws[ij + nsea * b] = m1[b]; llws[ij + nsea * (b + ns)] = m2[b]; }
+    }
     for (int m = 0; m < ml; ++m)
       for (int k = 0; k < kl; ++k) fl3[ij + (size_t)ld * (k + (size_t)kl * m)] = (double)F[k + kl * m];
     tauw[ij] = tw; ustar[ij] = us; z0[ij] = zz;
@@ -108,6 +125,32 @@ template <typename R> static void implsch_t(Oracle<R>* o, int nsea, int ld, doub
   }
   };
   if (nthreads == 1) { work(); return; }
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nthreads; ++t) pool.emplace_back(work);
+  for (auto& t : pool) t.join();
+}
+
+// One WAMODEL pass (wamodel.f90:286-360) on the resident state: nprop
+// PROPAGS calls, then IMPLSCH over every sea point, with nthreads host
+// threads (planes of PROPAGS, sea points of IMPLSCH) and no conversions.
+template <typename R> static void resident_step_t(Oracle<R>* o, int nprop, int nthreads) {
+  const int kl = o->fd.KL, ml = o->fd.ML, nsea = o->prop.NSEA;
+  R* FL3 = o->rF.data();
+  for (int p = 0; p < nprop; ++p) o->prop.propags(FL3, nthreads);
+  const int* indep = &o->prop.INDEP[1];
+  std::atomic<int> next(0);
+  auto work = [&]() {
+    std::vector<R> F((size_t)kl * ml);
+    for (int ij; (ij = next.fetch_add(1)) < nsea;) {
+      for (int m = 0; m < ml; ++m)
+        for (int k = 0; k < kl; ++k) F[k + kl * m] = FL3[ij + (size_t)nsea * (k + (size_t)kl * m)];
+      o->src.implsch_point(F.data(), o->rU10[ij], o->rUDIR[ij], o->rTAUW[ij], o->rUSTAR[ij], o->rZ0[ij], o->rROAIRN[ij],
+                           o->rWSTAR[ij], o->rDEPTH[ij], indep[ij], ij, nullptr);
+      for (int m = 0; m < ml; ++m)
+        for (int k = 0; k < kl; ++k) FL3[ij + (size_t)nsea * (k + (size_t)kl * m)] = F[k + kl * m];
+    }
+  };
+  if (nthreads <= 1) { work(); return; }
   std::vector<std::thread> pool;
   for (int t = 0; t < nthreads; ++t) pool.emplace_back(work);
   for (auto& t : pool) t.join();
@@ -125,6 +168,65 @@ void oracle_destroy(void* h) { delete (OracleBase*)h; }
 
 #define DISPATCH(h, call) \
   (((OracleBase*)(h))->precision == 8 ? (call((Oracle<double>*)(h))) : (call((Oracle<float>*)(h))))
+
+// Resident state for the timed CPU baseline: FL3(IJ,K,M) of NSEA points and
+// the per-point fields, converted once to the oracle's precision.
+int oracle_resident_set(void* h, const double* fl3, const double* u10, const double* udir, const double* tauw,
+                        const double* ustar, const double* z0, const double* roairn, const double* wstar,
+                        const double* depth) {
+  auto f = [&](auto* o) {
+    using RR = typename std::decay<decltype(o->fd.FR[0])>::type;
+    const size_t n = (size_t)o->prop.NSEA, nb = n * o->fd.KL * o->fd.ML;
+    auto cv = [](const double* a, size_t m) { std::vector<RR> v(m); for (size_t i = 0; i < m; ++i) v[i] = RR(a[i]); return v; };
+    o->rF = cv(fl3, nb); o->rU10 = cv(u10, n); o->rUDIR = cv(udir, n); o->rTAUW = cv(tauw, n); o->rUSTAR = cv(ustar, n);
+    o->rZ0 = cv(z0, n); o->rROAIRN = cv(roairn, n); o->rWSTAR = cv(wstar, n); o->rDEPTH = cv(depth, n);
+    return 0;
+  };
+  return DISPATCH(h, f);
+}
+int oracle_resident_step(void* h, int nprop, int nthreads) {
+  auto f = [&](auto* o) {
+    if (o->rF.size() != (size_t)o->prop.NSEA * o->fd.KL * o->fd.ML) return -1;
+    resident_step_t(o, nprop, nthreads);
+    return 0;
+  };
+  return DISPATCH(h, f);
+}
+int oracle_resident_get(void* h, double* fl3, double* tauw, double* ustar, double* z0) {
+  auto f = [&](auto* o) {
+    for (size_t i = 0; i < o->rF.size(); ++i) fl3[i] = (double)o->rF[i];
+    for (size_t i = 0; i < o->rTAUW.size(); ++i) { tauw[i] = o->rTAUW[i]; ustar[i] = o->rUSTAR[i]; z0[i] = o->rZ0[i]; }
+    return 0;
+  };
+  return DISPATCH(h, f);
+}
+
+// COMPUTE_OUTPUT_PARAMETER (wam_output_module.f90:481-640) for nsea points:
+// out[ij + nsea*(IP-1)], IP = 1..40 (parameters not restated stay 0).
+// ustar and z0 are in/out: AIRSEA sets them when USTAR is zero everywhere.
+int oracle_output_params(void* h, int nsea, const double* fl3, const double* u10, const double* udir, double* ustar,
+                         const double* tauw, double* z0, const double* depth, const double* u, const double* v,
+                         const int* indep, int from, double* out) {
+  auto f = [&](auto* o) {
+    using RR = typename std::decay<decltype(o->fd.FR[0])>::type;
+    const int kl = o->fd.KL, ml = o->fd.ML;
+    double mx = 0;
+    for (int i = 0; i < nsea; ++i) mx = std::max(mx, ustar[i]);
+    o->outm.from = from != 0;
+    std::vector<RR> F((size_t)kl * ml), P(OUT_NPARAM);
+    for (int ij = 0; ij < nsea; ++ij) {
+      for (int m = 0; m < ml; ++m)
+        for (int k = 0; k < kl; ++k) F[k + kl * m] = RR(fl3[ij + (size_t)nsea * (k + (size_t)kl * m)]);
+      RR us = RR(ustar[ij]), zz = RR(z0[ij]);
+      if (mx == 0) { o->src.airsea(RR(u10[ij]), RR(tauw[ij]), us, zz); ustar[ij] = us; z0[ij] = zz; }
+      o->outm.point(F.data(), RR(u10[ij]), RR(udir[ij]), us, RR(tauw[ij]), zz, RR(depth[ij]), u ? RR(u[ij]) : RR(0),
+                    v ? RR(v[ij]) : RR(0), indep[ij], P.data());
+      for (int p = 0; p < OUT_NPARAM; ++p) out[ij + (size_t)nsea * p] = (double)P[p];
+    }
+    return 0;
+  };
+  return DISPATCH(h, f);
+}
 
 int oracle_get_table(void* h, const char* name, double* out) {
   std::string n(name);
@@ -213,6 +315,22 @@ int oracle_implsch(void* h, int nsea, int ld, double* fl3, const double* u10, co
   return DISPATCH(h, f);
 }
 
+// oracle_implsch that also returns the step's integer decisions: idiag
+// (4 blocks of nsea: JU, MIJ of the first and of the last FRCUTINDEX call,
+// LFACTOR iterations), fdiag (the REAL values they were rounded from, and
+// the smallest relative distance of the LFACTOR |ERR| from its exit threshold) and llws (2 planes of KL*ML blocks of nsea: the
+// LLWS masks of the first and of the last SINPUT call), each optional.
+int oracle_implsch_diag(void* h, int nsea, int ld, double* fl3, const double* u10, const double* udir, double* tauw,
+                        double* ustar, double* z0, const double* roairn, const double* wstar, const double* depth,
+                        const int* indep, double* fluxes, int nthreads, int* idiag, double* fdiag, unsigned char* llws) {
+  auto f = [&](auto* o) {
+    implsch_t(o, nsea, ld, fl3, u10, udir, tauw, ustar, z0, roairn, wstar, depth, indep, fluxes, nthreads, idiag, fdiag,
+              llws);
+    return 0;
+  };
+  return DISPATCH(h, f);
+}
+
 // One PROPAGS call (COUNTER sub-steps) on F3(IJ,K,M), leading dimension NSEA.
 int oracle_propags(void* h, double* f3) {
   auto f = [&](auto* o) {
@@ -220,7 +338,7 @@ int oracle_propags(void* h, double* f3) {
     size_t n = (size_t)o->prop.NSEA * o->fd.KL * o->fd.ML;
     std::vector<RR> F(n);
     for (size_t i = 0; i < n; ++i) F[i] = RR(f3[i]);
-    o->prop.propags(F.data());
+    o->prop.propags(F.data(), (int)std::max(1u, std::thread::hardware_concurrency()));
     for (size_t i = 0; i < n; ++i) f3[i] = (double)F[i];
     return 0;
   };

@@ -8,6 +8,8 @@
 // Point-indexed arrays carry that land slot at index 0 (1-based points).
 // L_OBSTRUCTION and dry points (PUT_DRY) are not restated.
 #pragma once
+#include <atomic>
+#include <thread>
 #include "oracle_tables.hpp"
 
 namespace wamo {
@@ -526,19 +528,30 @@ template <typename R> struct PropModel {
   }
 
   // PROPAGS :635-829 on F3[(ij-1) + NSEA*((k-1) + KL*(m-1))]
-  void propags(R* F3) {
+  // nthreads > 1 spreads the (direction, frequency) planes of each sub-step
+  // over host threads; every plane is computed as in the serial loops, so
+  // the result does not depend on the thread count.
+  void propags(R* F3, int nthreads = 1) {
     std::vector<R> F1((size_t)(NSEA + 1) * KL * ML);
     auto f1 = [&](int ij, int k, int m) -> R& { return F1[ij + (size_t)(NSEA + 1) * ((k - 1) + (size_t)KL * (m - 1))]; };
+    auto planes = [&](auto&& fn) {  // fn(k, m) for every plane
+      const int n = KL * ML;
+      if (nthreads <= 1) { for (int q = 0; q < n; ++q) fn(q % KL + 1, q / KL + 1); return; }
+      std::atomic<int> next(0);
+      std::vector<std::thread> pool;
+      for (int t = 0; t < nthreads; ++t)
+        pool.emplace_back([&]() { for (int q; (q = next.fetch_add(1)) < n;) fn(q % KL + 1, q / KL + 1); });
+      for (auto& t : pool) t.join();
+    };
     for (int it = 0; it < COUNTER; ++it) {
-      for (int m = 1; m <= ML; ++m)
-        for (int k = 1; k <= KL; ++k) {
-          f1(0, k, m) = R(0.);
-          for (int ij = 1; ij <= NSEA; ++ij) f1(ij, k, m) = F3[b(ij, k, m)];
-        }
+      planes([&](int k, int m) {
+        f1(0, k, m) = R(0.);
+        for (int ij = 1; ij <= NSEA; ++ij) f1(ij, k, m) = F3[b(ij, k, m)];
+      });
       if (cfg.refraction_c_run) {
-        for (int m = 1; m <= ML; ++m) {
+        planes([&](int k, int m) {
           int MM = mpm(m, -1), MP = mpm(m, 1);
-          for (int k = 1; k <= KL; ++k) {
+          {
             int KP = kpm(k, 1), KM = kpm(k, -1);
             for (int ij = 1; ij <= NSEA; ++ij) {
               R v = csum(ij, k, m) * f1(ij, k, m) + lat(ij, k, m, 2, 1) * f1(klat(ij, 2, 1), k, m) +
@@ -550,11 +563,11 @@ template <typename R> struct PropModel {
               F3[b(ij, k, m)] = v;
             }
           }
-        }
+        });
       } else {
-        for (int k = 1; k <= KL; ++k) {
+        planes([&](int k, int m) {
           int KP = kpm(k, 1), KM = kpm(k, -1), IS = jxo(k, 1), IC = jyo(k, 1);
-          for (int m = 1; m <= ML; ++m)
+          {
             for (int ij = 1; ij <= NSEA; ++ij) {
               R v = csum(ij, k, m) * f1(ij, k, m) + lat(ij, k, m, 1, 1) * f1(klat(ij, IC, 1), k, m) +
                     lon(ij, k, m, 1) * f1(klon(ij, IS), k, m);
@@ -563,7 +576,8 @@ template <typename R> struct PropModel {
               if (cfg.reduced_grid) v = v + lat(ij, k, m, 1, 2) * f1(klat(ij, IC, 2), k, m);
               F3[b(ij, k, m)] = v;
             }
-        }
+          }
+        });
       }
     }
   }

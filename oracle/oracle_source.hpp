@@ -250,8 +250,12 @@ template <typename R> struct SourceModel {
   }
 
   // ---- LFACTOR :4465-4700 ------------------------------------------------------
+  // nit (optional): iterations run (0 when the stress needs no reduction);
+  // margin: the smallest relative distance of |ERR| from the exit threshold
+  // 1.54E-4 over the iterations run (how close the count came to changing).
   void lfactor(const std::vector<R>& S /*[k + KL*m]*/, const std::vector<R>& CINV, R U10, R USTAR, R USDIR, R ROAIRN,
-               const std::vector<R>& SIG, const std::vector<R>& DSII, std::vector<R>& LFACT, R& TAUWX, R& TAUWY) const {
+               const std::vector<R>& SIG, const std::vector<R>& DSII, std::vector<R>& LFACT, R& TAUWX, R& TAUWY,
+               int* nit = nullptr, double* margin = nullptr) const {
     const int NTH = KL(), NK = ML();
     const R SIN6WS = R(32.); const int ITERMAX = 80;
     int NK10 = nk10hz(SIG);
@@ -280,13 +284,15 @@ template <typename R> struct SourceModel {
     R TAU_TOT = ipow(USTAR, 2) * ROAIRN;
     R TAU_VIS = std::max(R(0.0), -(R(5.0E-5) * U10) + R(1.1E-3)) * ipow(U10, 2) * ROAIRN;
     TAU_VIS = std::min(R(0.95) * TAU_TOT, TAU_VIS);
-    R TAUVX = TAU_VIS * std::cos(USDIR), TAUVY = TAU_VIS * std::sin(USDIR);
+    R TAUVX = TAU_VIS * crcos(USDIR), TAUVY = TAU_VIS * crsin(USDIR);
     TAUWX = tauwinds(SDX, CINV10, DSII10);
     TAUWY = tauwinds(SDY, CINV10, DSII10);
     R TAUX = TAUVX + TAUWX, TAUY = TAUVY + TAUWY;
     R TAU = std::sqrt(ipow(TAUX, 2) + ipow(TAUY, 2));
     R ERR = (TAU - TAU_TOT) / TAU_TOT;
     for (auto& v : LF10) v = R(1.0);
+    int NIT = 0;
+    double MARGIN = 1e30;
     if (TAU > TAU_TOT) {
       bool OVERSHOT = false;
       R RTAU = ERR / R(90.);
@@ -296,7 +302,8 @@ template <typename R> struct SourceModel {
       for (int i = 0; i < NK10; ++i) UCINV10[i] = R(1.0) - (UPROXY * CINV10[i]);
       std::vector<R> tx(NK10), ty(NK10);
       for (int it = 1; it <= ITERMAX; ++it) {
-        for (int i = 0; i < NK10; ++i) LF10[i] = std::min(R(1.0), std::exp(UCINV10[i] * RTAU));
+        NIT = it;
+        for (int i = 0; i < NK10; ++i) LF10[i] = std::min(R(1.0), crexp(UCINV10[i] * RTAU));
         for (int i = 0; i < NK10; ++i) { tx[i] = SDX[i] * LF10[i]; ty[i] = SDY[i] * LF10[i]; }
         TAUWX = tauwinds(tx, CINV10, DSII10);
         TAUWY = tauwinds(ty, CINV10, DSII10);
@@ -308,9 +315,12 @@ template <typename R> struct SourceModel {
         if (SIGN_NEW != SIGN_OLD) OVERSHOT = true;
         if (OVERSHOT) DRTAU = std::max(R(0.5) * (R(1.0) + DRTAU), R(1.00010));
         RTAU = RTAU * ipow(DRTAU, SIGN_NEW);
+        MARGIN = std::min(MARGIN, std::fabs(std::fabs((double)ERR) - (double)R(1.54E-4)) / (double)R(1.54E-4));
         if (std::fabs(ERR) < R(1.54E-4)) break;
       }
     }
+    if (nit) *nit = NIT;
+    if (margin) *margin = MARGIN;
     LFACT.resize(NK);
     for (int i = 0; i < NK; ++i) LFACT[i] = LF10[i];
   }
@@ -347,12 +357,12 @@ template <typename R> struct SourceModel {
 
   // ---- SINPUT_ST6 :4704-4925 --------------------------------------------------
   void sinput_st6(const R* F, const R* CGG, const R* WN, R UABS, R USTAR, R USDIR, R ROAIRN, R& TAUW, R& TAUNW,
-                  R* SL, R* SPOS, R* FL) const {
+                  R* SL, R* SPOS, R* FL, int* nit = nullptr, double* margin = nullptr) const {
     const int NTH = KL(), NK = ML();
     const R SIN6WS = R(32.), SIN6A0 = R(0.09);
     std::vector<R> SIG(NK), DSII(NK);
     for (int m = 0; m < NK; ++m) { SIG[m] = C_::ZPI * fd->FR[m]; DSII[m] = C_::ZPI * fd->DF[m]; }
-    R COSU = std::cos(USDIR), SINU = std::sin(USDIR);
+    R COSU = crcos(USDIR), SINU = crsin(USDIR);
     R TAUNWX = 0, TAUNWY = 0, TAUWX = 0, TAUWY = 0;
     R UPROXY = SIN6WS * USTAR;
     const int NS = NTH * NK;
@@ -389,7 +399,7 @@ template <typename R> struct SourceModel {
       }
     for (int ik = 0; ik < NK; ++ik) CINV[ik] = CINV2[NTH * ik];
     for (int i = 0; i < NS; ++i) { int ik = i / NTH; SDENSIG[i] = S[i] * SIG[ik] / CGG[ik]; }
-    lfactor(SDENSIG, CINV, UABS, USTAR, USDIR, ROAIRN, SIG, DSII, LFACT, TAUWX, TAUWY);
+    lfactor(SDENSIG, CINV, UABS, USTAR, USDIR, ROAIRN, SIG, DSII, LFACT, TAUWX, TAUWY, nit, margin);
     R sumlf = 0; for (int ik = 0; ik < NK; ++ik) sumlf = sumlf + LFACT[ik];
     if (sumlf < R(NK)) {
       for (int i = 0; i < NS; ++i) D[i] = D[i] * LFACT[i / NTH];
@@ -429,44 +439,49 @@ template <typename R> struct SourceModel {
         R RDIF = (Kk != R(0)) ? DIF / Kk : R(0);
         if (DIF < EPS && RDIF < EPS) { conv = true; break; }
         KOLD = Kk;
-        R F1 = C_::G * KOLD * std::tanh(KOLD * H) - ipow(W0, 2);
+        R F1 = C_::G * KOLD * crtanh(KOLD * H) - ipow(W0, 2);
         R FD;
-        if (KOLD * H > R(25)) FD = C_::G * std::tanh(KOLD * H);
-        else FD = C_::G * std::tanh(KOLD * H) + C_::G * KOLD * H / ipow(std::cosh(KOLD * H), 2);
+        if (KOLD * H > R(25)) FD = C_::G * crtanh(KOLD * H);
+        else FD = C_::G * crtanh(KOLD * H) + C_::G * KOLD * H / ipow(crcosh(KOLD * H), 2);
         Kk = KOLD - F1 / FD;
       }
       (void)conv;
       if (R(2) * Kk * H > R(25)) CG = W0 / Kk * R(0.5);
-      else CG = W0 / Kk * R(0.5) * (R(1) + (R(2) * Kk * H / std::sinh(R(2) * Kk * H)));
+      else CG = W0 / Kk * R(0.5) * (R(1) + (R(2) * Kk * H / crsinh(R(2) * Kk * H)));
       if (SIG < R(0.0)) { Kk = -Kk; CG = -CG; }
       WN[m] = Kk; CGG[m] = CG;
     }
   }
 
   // ---- FRCUTINDEX :3569-3647 and FRCUTINDEX_ST6 :5447-5515 -----------------------
-  int frcutindex(R FM, R FMWS, R USTAR) const {
+  // arg (optional) receives the REAL value that NINT / INT rounds.
+  int frcutindex(R FM, R FMWS, R USTAR, double* arg = nullptr) const {
     const R EPSUS = R(1.0E-6), FRIC = R(28.0), TAILFACTOR = R(2.5), TAILFACTOR_PM = R(3.0);
     R FPMH = TAILFACTOR / fd->FR[0];
     R FPPM = TAILFACTOR_PM * C_::G / (FRIC * C_::ZPI * fd->FR[0]);
     R FM2 = std::max(FMWS, FM) * FPMH;
     R FPM = FPPM / std::max(USTAR, EPSUS);
     R FPM4 = std::max(FM2, FPM);
-    int MIJ = nint_f(std::log10(FPM4) * fd->INV_LOG_CO) + 1;
+    R X = crlog10(FPM4) * fd->INV_LOG_CO;
+    if (arg) *arg = (double)X;
+    int MIJ = nint_f(X) + 1;
     return std::min(std::max(1, MIJ), ML());
   }
-  int frcutindex_st6(R FMEAN, R USTAR) const {
+  int frcutindex_st6(R FMEAN, R USTAR, double* arg = nullptr) const {
     const int NK = ML();
     const R SIN6FC = R(6.);
     R FXFM = SIN6FC; FXFM = FXFM * C_::ZPI;
     R FXPM = R(4.0); FXPM = FXPM * C_::G / R(28.);
     R SIGNK = C_::ZPI * fd->FR[NK - 1];
     R FHIGH = std::max(FXFM * FMEAN, FXPM / USTAR);
-    R FACTI1 = R(1.) / std::log(C_::CO);
-    R FACTI2 = R(1.) - std::log(C_::ZPI * fd->FR[0]) * FACTI1;
-    int NKH = std::min(NK, int_f(FACTI2 + FACTI1 * std::log(std::max(R(1.E-7), FHIGH))));
+    R FACTI1 = R(1.) / crlog(C_::CO);
+    R FACTI2 = R(1.) - crlog(C_::ZPI * fd->FR[0]) * FACTI1;
+    int NKH = std::min(NK, int_f(FACTI2 + FACTI1 * crlog(std::max(R(1.E-7), FHIGH))));
     int NKH1 = std::min(NK, NKH + 1);
     FHIGH = std::min(SIGNK, std::max(FXFM * FMEAN, FXPM / USTAR));
-    NKH = std::max(2, std::min(NKH1, int_f(FACTI2 + FACTI1 * std::log(std::max(R(1.E-7), FHIGH)))));
+    R X = FACTI2 + FACTI1 * crlog(std::max(R(1.E-7), FHIGH));
+    if (arg) *arg = (double)X;
+    NKH = std::max(2, std::min(NKH1, int_f(X)));
     return NKH;
   }
 
@@ -823,15 +838,30 @@ template <typename R> struct SourceModel {
     }
   }
 
+  // Integer decisions of one IMPLSCH call and the REAL values they were
+  // rounded from: JU (NINT(U10/DELU), :498), the cut-off index MIJ of the
+  // first FRCUTINDEX call (:563) and of the last (:697), the LFACTOR
+  // iteration count (ST6, :4647-4672; 0 without reduction, -1 for ST4) with
+  // the smallest relative distance of |ERR| from its exit threshold, and the
+  // wind-sea masks LLWS of the first SINPUT call and of the last one (the
+  // mask of the final integrals).
+  struct Diag {
+    int JU, MIJ1, MIJ2, LFIT;
+    double JU_ARG, MIJ1_ARG, MIJ2_ARG, LF_MARGIN;
+    uint8_t* LLWS1;  // KL*ML, or null
+    uint8_t* LLWS2;
+  };
+
   // ---- IMPLSCH :374-700, one sea point -------------------------------------------------------
   // F: spectrum of the point [k + KL*m], updated in place.
   void implsch_point(R* F, R U10, R UDIR, R& TAUW, R& USTAR, R& Z0, R ROAIRN, R WSTAR, R DEPTH, int INDEP, int ij,
-                     Fluxes* flx) const {
+                     Fluxes* flx, Diag* dg = nullptr) const {
     const int kl = KL(), ml = ML(), NS = kl * ml;
     std::vector<R> SL(NS), FL(NS), SPOS(NS), SMIN, SL_BOT, SPRD(kl), WN(ml), CGG(ml);
     std::vector<uint8_t> LLWS(NS);
     for (int k = 0; k < kl; ++k) SPRD[k] = ipow(std::max(R(0.), std::cos(fd->TH[k] - UDIR)), 2);
-    int JU = std::min(C_::JUMAX, std::max(nint_f(U10 / me->DELU), 1));
+    const R JU_ARG = U10 / me->DELU;
+    int JU = std::min(C_::JUMAX, std::max(nint_f(JU_ARG), 1));
     R EMEAN = total_energy(F, nullptr);
     R FMEAN = femean(F, EMEAN, nullptr);
     R AKMEAN = wm1(F, EMEAN, INDEP);
@@ -839,14 +869,18 @@ template <typename R> struct SourceModel {
     R CD, TAUNW = 0, TAUW_DUMMY, PHIAW;
     if (cfg.iphys == 2) w3flx4(U10, USTAR, Z0, CD);
     else airsea(U10, TAUW, USTAR, Z0);
+    int LFIT = -1; double LF_MARGIN = 1e30, MIJ_ARG = 0;
     if (cfg.iphys == 1) sinput_ard(F, SL.data(), SPOS.data(), FL.data(), USTAR, UDIR, Z0, ROAIRN, WSTAR, INDEP, LLWS.data());
     else {
-      sinput_st6(F, CGG.data(), WN.data(), U10, USTAR, UDIR, ROAIRN, TAUW, TAUNW, SL.data(), SPOS.data(), FL.data());
+      sinput_st6(F, CGG.data(), WN.data(), U10, USTAR, UDIR, ROAIRN, TAUW, TAUNW, SL.data(), SPOS.data(), FL.data(),
+                 &LFIT, &LF_MARGIN);
       for (int i = 0; i < NS; ++i) LLWS[i] = SPOS[i] > R(0);
     }
+    if (dg && dg->LLWS1) std::copy(LLWS.begin(), LLWS.end(), dg->LLWS1);
     R EMEANWS = total_energy(F, LLWS.data());
     R FMEANWS = femean(F, EMEANWS, LLWS.data());
-    int MIJ = (cfg.iphys == 2) ? frcutindex_st6(FMEAN, USTAR) : frcutindex(FMEAN, FMEANWS, USTAR);
+    int MIJ = (cfg.iphys == 2) ? frcutindex_st6(FMEAN, USTAR, &MIJ_ARG) : frcutindex(FMEAN, FMEANWS, USTAR, &MIJ_ARG);
+    if (dg) { dg->JU = JU; dg->JU_ARG = (double)JU_ARG; dg->MIJ1 = MIJ; dg->MIJ1_ARG = MIJ_ARG; dg->LFIT = LFIT; dg->LF_MARGIN = LF_MARGIN; }
     if (cfg.iphys == 2) { stresso(F, SPOS.data(), USTAR, UDIR, Z0, MIJ, TAUW_DUMMY, PHIAW, INDEP); w3flx4(U10, USTAR, Z0, CD); }
     else { stresso(F, SPOS.data(), USTAR, UDIR, Z0, MIJ, TAUW, PHIAW, INDEP); airsea(U10, TAUW, USTAR, Z0); }
     imphftail(MIJ, INDEP, F);
@@ -885,7 +919,11 @@ template <typename R> struct SourceModel {
     FMEAN = femean(F, EMEAN, nullptr);
     EMEANWS = total_energy(F, LLWS.data());
     FMEANWS = femean(F, EMEANWS, LLWS.data());
-    MIJ = (cfg.iphys == 2) ? frcutindex_st6(FMEAN, USTAR) : frcutindex(FMEAN, FMEANWS, USTAR);
+    MIJ = (cfg.iphys == 2) ? frcutindex_st6(FMEAN, USTAR, &MIJ_ARG) : frcutindex(FMEAN, FMEANWS, USTAR, &MIJ_ARG);
+    if (dg) {
+      dg->MIJ2 = MIJ; dg->MIJ2_ARG = MIJ_ARG;
+      if (dg->LLWS2) std::copy(LLWS.begin(), LLWS.end(), dg->LLWS2);
+    }
     imphftail(MIJ, INDEP, F);
   }
 };

@@ -35,6 +35,23 @@ template <typename R> inline R ipow(R x, int n) {
   }
   return result;
 }
+// Correctly rounded REAL intrinsics for the values that decide an integer:
+// the cut-off index MIJ (LOG10 in FRCUTINDEX, LOG in FRCUTINDEX_ST6), the
+// LFACTOR iteration (EXP, and COS/SIN of the wind direction) and the
+// wavenumbers and group velocities of WAVNU2 that enter it (TANH, COSH, SINH).  The Fortran
+// standard leaves the accuracy of LOG10, EXP, ... processor dependent; glibc's
+// single-precision log10f, for one, is off by one ulp for about 7% of its
+// arguments.  Evaluating these few per-point values in double and rounding
+// once gives the correctly rounded REAL result, which the GPU kernels compute
+// the same way, so equal inputs give equal decisions on both sides.
+template <typename R> inline R crlog10(R x) { return R(std::log10((double)x)); }
+template <typename R> inline R crlog(R x) { return R(std::log((double)x)); }
+template <typename R> inline R crexp(R x) { return R(std::exp((double)x)); }
+template <typename R> inline R crcos(R x) { return R(std::cos((double)x)); }
+template <typename R> inline R crsin(R x) { return R(std::sin((double)x)); }
+template <typename R> inline R crtanh(R x) { return R(std::tanh((double)x)); }
+template <typename R> inline R crcosh(R x) { return R(std::cosh((double)x)); }
+template <typename R> inline R crsinh(R x) { return R(std::sinh((double)x)); }
 inline int nint_f(double x) { return (int)std::lround(x); }           // NINT
 inline int int_f(double x) { return (int)std::trunc(x); }            // INT
 template <typename R> inline R fsign(R a, R b) { return b >= R(0) ? std::fabs(a) : -std::fabs(a); }

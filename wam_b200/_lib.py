@@ -45,6 +45,10 @@ SIGNATURES = {
     "wamgpu_step_host": (c_int, [c_void_p, PF, c_int, PF, PF, PF, PF, PF, PF, PF]),
     "wamgpu_get_fluxes": (c_int, [c_void_p, PF]),
     "wamgpu_sync": (c_int, [c_void_p]),
+    "wamgpu_set_diagnostics": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "wamgpu_put_points_dev": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, ctypes.c_double, c_void_p]),
+    "wamgpu_output_parameters_dev": (c_int, [c_void_p, c_void_p, c_int] + [c_void_p] * 5 + [c_int, c_void_p, c_int,
+                                                                                             c_void_p]),
     "wamgpu_set_timing": (c_int, [c_void_p, c_int]),
     "wamgpu_get_timing": (c_int, [c_void_p, PF, PI]),
     "wamgpu_set_owned": (c_int, [c_void_p, c_int, c_int]),

@@ -23,6 +23,7 @@ UNITS = {
     "propags.cu": ["-fmad=false"],
     "api.cu": [],
     "adjoint.cu": [],
+    "output.cu": ["-fmad=false"],
 }
 HEADERS = ["implsch.cuh", "propags.cuh", "propargs.hpp", "devmath.cuh", "kernels.hpp", "adjoint.cuh", "adjoint_warp.cuh", "spectral_tables.hpp", "wamgpu_config.hpp"]
 

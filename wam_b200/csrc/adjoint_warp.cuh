@@ -141,10 +141,13 @@ template <typename R> struct AdjW {
   }
 
   // MIJ of the updated spectrum: the integrals (unmasked and with the second
-  // LLWS) of the update's output, formed without storing it.
+  // LLWS) of the update's output, formed without storing it, with the
+  // frequency sums in order as the forward step forms them (scratch rows 0,
+  // 1, 5 and 7; rows 2, 3, 4 and 6 hold the update's factors).
   __device__ int cutoff_after_update() const {
     const int kl = KL(), ml = ML(), ld = w.ld;
-    R pe = 0, pf = 0, tail = 0, pew = 0, pfw = 0, tailw = 0;
+    R *TE = w.t(0), *TF = w.t(1), *TEW = w.t(5), *TFW = w.t(7);
+    R tail = 0, tailw = 0;
     for (int m = lane; m < ml; m += 32) {
       R t = 0, tw = 0;
       const uint8_t* mk = w.LL + ld * m;
@@ -153,15 +156,18 @@ template <typename R> struct AdjW {
         t = t + f;
         tw = tw + (mk[k] ? f : R(0));
       }
-      pe = pe + t * S.DFIM[m]; pf = pf + t * S.DFIMOFR[m];
-      pew = pew + tw * S.DFIM[m]; pfw = pfw + tw * S.DFIMOFR[m];
+      TE[m] = rmul(t, S.DFIM[m]); TF[m] = rmul(t, S.DFIMOFR[m]);
+      TEW[m] = rmul(tw, S.DFIM[m]); TFW[m] = rmul(tw, S.DFIMOFR[m]);
       if (m == ml - 1) { tail = t; tailw = tw; }
     }
-    pe = warp_sum(pe); pf = warp_sum(pf); pew = warp_sum(pew); pfw = warp_sum(pfw);
     tail = __shfl_sync(0xffffffffu, tail, (ml - 1) & 31);
     tailw = __shfl_sync(0xffffffffu, tailw, (ml - 1) & 31);
-    const R e = dmax(T.MO_TAIL * tail + pe, R(1.0E-12)), fm = e / dmax(T.MM1_TAIL * tail + pf, R(1.0E-12));
-    const R ew = dmax(T.MO_TAIL * tailw + pew, R(1.0E-12)), fmw = ew / dmax(T.MM1_TAIL * tailw + pfw, R(1.0E-12));
+    R* rows[4] = {TE, TF, TEW, TFW};
+    const R init[4] = {rmul(T.MO_TAIL, tail), rmul(T.MM1_TAIL, tail), rmul(T.MO_TAIL, tailw), rmul(T.MM1_TAIL, tailw)};
+    R sum[4];
+    s.template ordered_sums<4>(rows, init, ml, sum);
+    const R e = dmax(sum[0], R(1.0E-12)), fm = e / dmax(sum[1], R(1.0E-12));
+    const R ew = dmax(sum[2], R(1.0E-12)), fmw = ew / dmax(sum[3], R(1.0E-12));
     return s.frcutindex(fm, fmw, us2);
   }
 

@@ -69,6 +69,10 @@ struct wamgpu_ctx {
   bool have_grid = false, prepared = false;
   bool wncg_valid = false;  // the WN/CG rows match the current depth
   int counter = 1; double total_cfl = 0, cfl_min = 0; int variant = 0;
+  // test diagnostics of IMPLSCH's integer decisions (wamgpu_set_diagnostics)
+  int* diag = nullptr;
+  unsigned char* diag_ll = nullptr;
+  int diag_ld = 0;
   std::unique_ptr<ImplBase> impl;
   // opt-in kernel timing: event pairs per kernel class (0 = PROPAGS, 1 = IMPLSCH)
   bool timing = false;
@@ -90,6 +94,8 @@ template <typename R> struct Impl : ImplBase {
   DevBuf wncg;           // ST6: WN and CG per (sea point, frequency), formed by wamgpu_prepare_source
   int nckpt = 0, ckpt_ld = 0;
   DevBuf small, ismall, tfak, tcgond, tsihkd, flminfr, enh, gom, fr, sinth, costh;
+  DevBuf outtab;         // integrated output: DFIM_FR, DFIM_FR2, MEANSQS deep-water weights (ML each)
+  DevBuf ustar_max;      // MAXVAL(USTAR) word of the output step
   DevBuf diamc;          // per-MC DIA rows and write masks (DevTables::diamc)
   DevBuf dslot;          // DIA batch slot entries (DevTables::dslot)
   // per-point metadata
@@ -197,6 +203,14 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
   CK(upload(I.fr, t.FR, s), "upload tables");
   CK(upload(I.sinth, t.SINTH, s), "upload tables");
   CK(upload(I.costh, t.COSTH, s), "upload tables");
+  {
+    // MEANSQS deep-water weights FD(M) = DFIM(M)*(ZPI*FR(M))**4/G**2 (wam_interface_module.f90:721)
+    std::vector<R> ot(t.DFIM_FR);
+    ot.insert(ot.end(), t.DFIM_FR2.begin(), t.DFIM_FR2.end());
+    for (int m = 0; m < t.ML; ++m)
+      ot.push_back(t.DFIM[m] * powi(Phys<R>::ZPI * t.FR[m], 4) / powi(Phys<R>::G, 2));
+    CK(upload(I.outtab, ot, s), "upload tables");
+  }
   DevTables<R>& d = I.dt;
   d.KL = t.KL; d.ML = t.ML; d.NS = t.KL * t.ML; d.NDEPTH = t.NDEPTH; d.MFRSTLW = t.MFRSTLW; d.MLSTHG = t.MLSTHG;
   d.KFRH = t.KFRH; d.NSDSNTH = t.NSDSNTH;
@@ -607,6 +621,11 @@ int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u1
   a.enh = I.has_enh ? I.enh.template as<R>() + p0 : nullptr; a.enh_ld = ctx->nsea;
   a.wncg = ctx->wncg_valid ? I.wncg.template as<R>() + (size_t)p0 * 2 * ctx->cfg.ml : nullptr;
   a.status = I.status.template as<int>();
+  if (ctx->diag) {
+    a.diag = ctx->diag + p0;
+    a.diag_ll = ctx->diag_ll ? ctx->diag_ll + p0 : nullptr;
+    a.diag_ld = ctx->diag_ld;
+  }
   { TimedLaunch tl(ctx, 1, s); CK(launch_implsch<R>(I.dt, a, ctx->P, s), "implsch launch"); }
   return WAMGPU_OK;
 }
@@ -866,6 +885,13 @@ int step_adj_dev_t(wamgpu_ctx* ctx, Impl<R>& I, int slot, int nprop, void* lam_f
 template <typename R> int propags_dev_static_t(wamgpu_ctx* ctx, Impl<R>& I, void* f3v, int ld, cudaStream_t s) {
   if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
   if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  // With an owned range the sub-steps write only the owned points of the
+  // scratch, and the next sub-step would read halo points of it that this
+  // call never wrote (whatever an earlier call left in the shared array).
+  if (ctx->own0 != 0 || (ctx->own1 >= 0 && ctx->own1 != ctx->nsea))
+    return fail(ctx, WAMGPU_E_ARG,
+                "wamgpu_propags_dev_static covers the whole grid; with an owned range (wamgpu_set_owned) use "
+                "wamgpu_propags_substep_dev and refresh the halo between sub-steps");
   const size_t bytes = (size_t)ld * ctx->cfg.kl * ctx->cfg.ml * sizeof(R);
   if (bytes > (size_t)WAMGPU_STATIC_SCRATCH_BYTES)
     return fail(ctx, WAMGPU_E_ARG, "spectrum of " + std::to_string(bytes) + " bytes exceeds the static PROPAGS scratch of " +
@@ -906,6 +932,62 @@ int step_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* f3v, int ld, void* scratch, in
     std::swap(src, dst);
   }
   return implsch_dev_t<R>(ctx, I, f3, ld, u10, udir, tauw, ustar, z0, roairn, wstar, s, src);
+}
+
+// COMPUTE_OUTPUT_PARAMETER (wam_output_module.f90:481-640) for the owned
+// sea points: the integrated parameters into block[ij + block_ld*(IP-1)].
+template <typename R>
+int output_params_t(wamgpu_ctx* ctx, Impl<R>& I, const void* fl3, int ld, const void* u10, const void* udir,
+                    const void* tauw, void* ustar, void* z0, int from, void* block, int block_ld, cudaStream_t s) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first (INDEP, currents)");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  if (block_ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "block_ld < nsea");
+  if (!fl3 || !u10 || !udir || !tauw || !ustar || !z0 || !block) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  const int p0 = ctx->own0, p1 = ctx->own1 < 0 ? ctx->nsea : ctx->own1;
+  const DevTables<R>& d = I.dt;
+  OutArgs<R> a;
+  a.nsea = p1 - p0; a.ld = ld; a.KL = d.KL; a.ML = d.ML; a.NDEPTH = d.NDEPTH; a.shallow = d.shallow;
+  a.from = from ? 1 : 0;
+  a.fl3 = (const R*)fl3 + p0;
+  a.u10 = (const R*)u10 + p0; a.udir = (const R*)udir + p0; a.tauw = (const R*)tauw + p0;
+  a.depth = I.d_depth.template as<R>() + p0;
+  a.u = I.d_u.template as<R>() + p0;  // zero unless wamgpu_set_current gave currents
+  a.v = I.d_v.template as<R>() + p0;
+  a.ustar = (R*)ustar + p0; a.z0 = (R*)z0 + p0;
+  a.indep = I.d_indep.template as<int>() + p0;
+  a.block = (R*)block + p0; a.block_ld = block_ld;
+  const R* r = d.small;
+  a.FR = r + d.lay.FR; a.DFIM = r + d.lay.DFIM; a.DFIMOFR = r + d.lay.DFIMOFR;
+  a.SINTH = r + d.lay.SINTH; a.COSTH = r + d.lay.COSTH;
+  const R* ot = I.outtab.template as<R>();
+  a.DFIM_FR = ot; a.DFIM_FR2 = ot + d.ML; a.MSSFD = ot + 2 * d.ML;
+  a.TFAK = d.TFAK;
+  a.MO_TAIL = d.MO_TAIL; a.MM1_TAIL = d.MM1_TAIL;
+  a.MP1_TAIL = R(I.tab.MP1_TAIL); a.MP2_TAIL = R(I.tab.MP2_TAIL);
+  a.A = atabs_of(d);
+  a.ustar_max = nullptr;
+  CK(I.ustar_max.ensure(16), "alloc");
+  // parameters that are not computed stay 0
+  for (int p = 0; p < WAMGPU_OUT_NPARAM; ++p)
+    CK(cudaMemsetAsync((R*)block + p0 + (size_t)block_ld * p, 0, (size_t)(p1 - p0) * sizeof(R), s), "memset block");
+  CK(launch_output<R>(a, I.ustar_max.template as<unsigned long long>(), s), "output launch");
+  return WAMGPU_OK;
+}
+
+// PUT_ICE (wam_ice_module.f90:312-324) / PUT_DRY (wam_topo_module.f90:557-569)
+// on device data of nrows rows (a spectrum: KL*ML rows; a parameter block:
+// its parameters), skipping listed points outside the owned range as the
+// reference skips those outside NIJS..NIJL.
+template <typename R>
+int put_points_t(wamgpu_ctx* ctx, Impl<R>& I, void* data, int ld, int nrows, const int* points, int n, double value,
+                 cudaStream_t s) {
+  (void)I;
+  if (!ctx->have_grid) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_set_grid first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  if (nrows < 0 || n < 0 || (n > 0 && (!points || !data))) return fail(ctx, WAMGPU_E_ARG, "bad point list");
+  const int lo = ctx->own0 + 1, hi = ctx->own1 < 0 ? ctx->nsea : ctx->own1;
+  CK(launch_put_points<R>((R*)data, (size_t)ld, nrows, points, n, lo, hi, R(value), s), "put points launch");
+  return WAMGPU_OK;
 }
 
 template <typename R> std::vector<R> to_r(const float* p, size_t n) {
@@ -1674,6 +1756,30 @@ int wamgpu_get_timing(wamgpu_ctx* ctx, float* ms, int* count) {
     }
     ctx->ev[c].clear();
   }
+  return WAMGPU_OK;
+}
+
+int wamgpu_output_parameters_dev(wamgpu_ctx* ctx, const void* fl3, int ld, const void* u10, const void* udir,
+                                 const void* tauw, void* ustar, void* z0, int from, void* block, int block_ld,
+                                 void* stream) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, output_params_t, fl3, ld, u10, udir, tauw, ustar, z0, from, block, block_ld, s);
+}
+
+int wamgpu_put_points_dev(wamgpu_ctx* ctx, void* data, int ld, int nrows, const int* points, int n, double value,
+                          void* stream) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, put_points_t, data, ld, nrows, points, n, value, s);
+}
+
+int wamgpu_set_diagnostics(wamgpu_ctx* ctx, int* decisions, unsigned char* llws, int ld) {
+  if (!ctx) return WAMGPU_E_ARG;
+  if (!decisions) { ctx->diag = nullptr; ctx->diag_ll = nullptr; ctx->diag_ld = 0; return WAMGPU_OK; }
+  if (!ctx->have_grid) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_set_grid first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "diagnostics: ld < nsea");
+  ctx->diag = decisions; ctx->diag_ll = llws; ctx->diag_ld = ld;
   return WAMGPU_OK;
 }
 

@@ -37,6 +37,39 @@ __device__ __forceinline__ double dabs(double x) { return fabs(x); }
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
 
+// Separately rounded products and sums (never contracted into an FMA), for
+// the expressions whose last bit decides an integer on the reference's
+// separate-operation arithmetic: the spectral integrals behind the cut-off
+// index, the stress sums of the LFACTOR iteration, the drag law of u*.
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+// Correctly rounded single-precision transcendentals (evaluated in double,
+// rounded once) for the same per-point values: the cut-off index's LOG10 /
+// LOG, the LFACTOR exponentials and wind-direction cosines, and WAVNU2's
+// dispersion relation.  The CPU oracle evaluates them the same way, so equal
+// inputs give equal integer decisions.  In double precision they are the
+// functions themselves.
+__device__ __forceinline__ float crlog10(float x) { return (float)log10((double)x); }
+__device__ __forceinline__ double crlog10(double x) { return log10(x); }
+__device__ __forceinline__ float crlog(float x) { return (float)log((double)x); }
+__device__ __forceinline__ double crlog(double x) { return log(x); }
+__device__ __forceinline__ float crexp(float x) { return (float)exp((double)x); }
+__device__ __forceinline__ double crexp(double x) { return exp(x); }
+__device__ __forceinline__ float crcos(float x) { return (float)cos((double)x); }
+__device__ __forceinline__ double crcos(double x) { return cos(x); }
+__device__ __forceinline__ float crsin(float x) { return (float)sin((double)x); }
+__device__ __forceinline__ double crsin(double x) { return sin(x); }
+__device__ __forceinline__ float crtanh(float x) { return (float)tanh((double)x); }
+__device__ __forceinline__ double crtanh(double x) { return tanh(x); }
+__device__ __forceinline__ float crcosh(float x) { return (float)cosh((double)x); }
+__device__ __forceinline__ double crcosh(double x) { return cosh(x); }
+__device__ __forceinline__ float crsinh(float x) { return (float)sinh((double)x); }
+__device__ __forceinline__ double crsinh(double x) { return sinh(x); }
+
 template <typename R> __device__ __forceinline__ R dmax(R a, R b) { return a < b ? b : a; }
 template <typename R> __device__ __forceinline__ R dmin(R a, R b) { return b < a ? b : a; }
 

@@ -44,11 +44,16 @@ __device__ __forceinline__ void implsch_cta(const DevTables<R>& T, const ImplArg
     Src<R> src(T, S, w, lane, ij, a.indep[ij], a.u10[ij], a.udir[ij], a.roairn[ij], a.wstar[ij], a.depth[ij], a.enh,
                a.enh_ld);
     src.wncg = a.wncg ? a.wncg + (size_t)ij * 2 * T.ML : nullptr;
+    if (a.diag_ll && real) { src.dll = a.diag_ll + ij; src.dll_ld = (size_t)a.diag_ld; }
     PointState<R> ps;
     ps.TAUW = a.tauw[ij];
     src.run(ps);
     if (lane == 0 && real) {
       a.tauw[ij] = ps.TAUW; a.ustar[ij] = ps.USTAR; a.z0[ij] = ps.Z0;
+      if (a.diag) {
+        a.diag[ij] = ps.JU; a.diag[ij + (size_t)a.diag_ld] = ps.MIJ1;
+        a.diag[ij + 2 * (size_t)a.diag_ld] = ps.MIJ2; a.diag[ij + 3 * (size_t)a.diag_ld] = ps.LFIT;
+      }
       if (T.lcflx && a.fluxes)
         for (int q = 0; q < 7; ++q) a.fluxes[ij + (size_t)a.flx_ld * q] = ps.flx[q];
       if (!isfinite(ps.TAUW) || !isfinite(ps.USTAR) || !isfinite(ps.Z0)) atomicOr(a.status, 1);

@@ -88,6 +88,9 @@ template <typename R> __host__ __device__ inline size_t ws_t_offset(int ld, int 
 
 // WAVNU2 (:4343-4461) for one frequency: wavenumber and group velocity at
 // angular frequency w0 and depth H by Newton's method.
+// The hyperbolic functions are correctly rounded and nothing is contracted,
+// so WN and CG equal the oracle's bit for bit; they are formed once per
+// depth, outside the step.
 template <typename R> __device__ __forceinline__ void wavnu2_one(R w0, R H, R& wn, R& cgv) {
   using P_ = Phys<R>;
   const R eps = R(1E-7);
@@ -97,13 +100,15 @@ template <typename R> __device__ __forceinline__ void wavnu2_one(R w0, R H, R& w
     R dif = dabs(k - kold), rdif = (k != R(0)) ? dif / k : R(0);
     if (dif < eps && rdif < eps) break;
     kold = k;
-    R th = dtanh(kold * H);
-    R f1 = P_::G * kold * th - w0 * w0;
-    R fd = (kold * H > R(25)) ? P_::G * th : P_::G * th + P_::G * kold * H / (dcosh(kold * H) * dcosh(kold * H));
+    const R kh = kold * H, th = crtanh(kh);
+    R f1 = rsub(rmul(P_::G * kold, th), rmul(w0, w0));
+    R ch = crcosh(kh);
+    R fd = (kh > R(25)) ? P_::G * th : radd(rmul(P_::G, th), (P_::G * kold * H) / (ch * ch));
     k = kold - f1 / fd;
   }
   wn = k;
-  cgv = (R(2) * k * H > R(25)) ? w0 / k * R(0.5) : w0 / k * R(0.5) * (R(1) + (R(2) * k * H / dsinh(R(2) * k * H)));
+  cgv = (R(2) * k * H > R(25)) ? w0 / k * R(0.5)
+                               : w0 / k * R(0.5) * (R(1) + (R(2) * k * H / crsinh(R(2) * k * H)));
 }
 
 // Bytes of the small tables staged at the start of a CTA's shared memory.
@@ -116,6 +121,9 @@ template <typename R> __host__ __device__ inline size_t tables_bytes(const Small
 template <typename R> struct PointState {
   R TAUW, USTAR, Z0;
   R flx[7];  // PHIOC, TAUOC_X, TAUOC_Y, PHIBOT, TAUBOT_X, TAUBOT_Y, PHIAW
+  // integer decisions of the step: JU, MIJ of the first and of the last
+  // FRCUTINDEX call, LFACTOR iterations (ST6; 0 without reduction, -1 ST4)
+  int JU = 0, MIJ1 = 0, MIJ2 = 0, LFIT = -1;
 };
 
 template <typename R> struct Src {
@@ -132,6 +140,11 @@ template <typename R> struct Src {
   R* shl = nullptr;
   // ST6: this point's WN and CG rows formed once from the depth (WAVNU2), or null.
   const R* wncg = nullptr;
+  // When set, the step copies its LLWS masks here: bin b of the first
+  // SINPUT call's mask at dll[b * dll_ld], of the last one's at
+  // dll[(NS + b) * dll_ld] (test diagnostics of the integer decisions).
+  uint8_t* dll = nullptr;
+  size_t dll_ld = 0;
   __device__ Src(const DevTables<R>& t, const STabs<R>& s, WarpWS<R>& ws, int l, int ij_, int indep, R u10, R udir,
                  R roairn, R wstar, R depth, const R* enh, int enh_ld_)
       : T(t), S(s), w(ws), lane(l), ij(ij_), INDEP(indep), U10(u10), UDIR(udir), ROAIRN(roairn), WSTAR(wstar), DEPTH(depth),
@@ -157,28 +170,59 @@ template <typename R> struct Src {
     }
   }
 
+  // Sums of up to four rows of n terms, each in index order on its own lane
+  // (lane q sums rows[q] starting from init[q]), broadcast to every lane.
+  // The reference sums its spectral integrals in frequency order, and these
+  // sums decide the cut-off index, so they are not formed as tree reductions.
+  template <int NQ> __device__ void ordered_sums(R* const (&rows)[NQ], const R (&init)[NQ], int n, R (&out)[NQ]) const {
+    __syncwarp();
+    R acc = R(0);
+    const R* row = rows[0];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q)
+      if (lane == q) { acc = init[q]; row = rows[q]; }
+    if (lane < NQ)
+      for (int i = 0; i < n; ++i) acc = radd(acc, row[i]);
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) out[q] = __shfl_sync(0xffffffffu, acc, q);
+    __syncwarp();
+  }
+
   // TOTAL_ENERGY + FEMEAN (+ WM1 for AKMEAN); masked when mask != null.
+  // Each frequency's direction sum comes from one lane; the frequency sums run
+  // in order, with the reference's operations (interface:1342-1410, 207-286,
+  // 1591-1716), on the scratch rows 5-7 (free wherever the step calls this).
   __device__ void integrals(const uint8_t* mask, R& emean, R& fmean, R* akmean) const {
     const int kl = KL(), ml = ML(), ld = w.ld;
-    R pe = 0, pf = 0, pa = 0, tail = 0;
+    R tail = 0;
     const R DEL2 = dsqrt(P_::G) / P_::ZPI;
+    R* TE = w.t(5); R* TF = w.t(6); R* TW = w.t(7);
     for (int m = lane; m < ml; m += 32) {
       R t = 0;
       const R* f = w.F + ld * m;
       if (mask) { const uint8_t* mk = mask + ld * m; for (int k = 0; k < kl; ++k) t = t + (mk[k] ? f[k] : R(0)); }
       else for (int k = 0; k < kl; ++k) t = t + f[k];
-      pe = pe + t * S.DFIM[m];
-      pf = pf + t * S.DFIMOFR[m];
-      if (akmean) pa = pa + (T.shallow ? t / dsqrt(tfak(m)) * S.DFIM[m] : t * S.DFIMOFR[m] * DEL2);
+      TE[m] = rmul(t, S.DFIM[m]);
+      TF[m] = rmul(t, S.DFIMOFR[m]);
+      if (akmean) TW[m] = T.shallow ? rmul(t / dsqrt(tfak(m)), S.DFIM[m]) : rmul(rmul(t, S.DFIMOFR[m]), DEL2);
       if (m == ml - 1) tail = t;
     }
-    pe = warp_sum(pe); pf = warp_sum(pf);
     tail = __shfl_sync(0xffffffffu, tail, (ml - 1) & 31);
-    emean = dmax(T.MO_TAIL * tail + pe, R(1.0E-12));
-    fmean = emean / dmax(T.MM1_TAIL * tail + pf, R(1.0E-12));
+    R* rows[3] = {TE, TF, TW};
+    const R init[3] = {rmul(T.MO_TAIL, tail), rmul(T.MM1_TAIL, tail), rmul(rmul(T.MM1_TAIL, DEL2), tail)};
+    R sum[3];
+    if (akmean) ordered_sums<3>(rows, init, ml, sum);
+    else {
+      R* rows2[2] = {TE, TF};
+      const R init2[2] = {init[0], init[1]};
+      R sum2[2];
+      ordered_sums<2>(rows2, init2, ml, sum2);
+      sum[0] = sum2[0]; sum[1] = sum2[1]; sum[2] = R(0);
+    }
+    emean = dmax(sum[0], R(1.0E-12));
+    fmean = emean / dmax(sum[1], R(1.0E-12));
     if (akmean) {
-      pa = warp_sum(pa);
-      R wm = T.MM1_TAIL * DEL2 * tail + pa;
+      const R wm = sum[2];
       *akmean = (emean > R(1.0E-12)) ? (emean / wm) * (emean / wm) : R(1.);
     }
   }
@@ -210,10 +254,14 @@ template <typename R> struct Src {
     Z0 = z0ch;
   }
 
+  // (the drag law's sums are rounded separately: u* decides the ST6 cut-off)
   __device__ void w3flx4(R& UST, R& Z0) const {
     R cd;
     if (U10 >= R(50.33)) { UST = R(2.026) * dsqrt(T.CDFAC); cd = (UST / U10) * (UST / U10); }
-    else { cd = T.CDFAC * (R(8.058) + R(0.967) * U10 - R(0.016) * (U10 * U10)) * R(1E-4); UST = U10 * dsqrt(cd); }
+    else {
+      cd = T.CDFAC * rsub(radd(R(8.058), rmul(R(0.967), U10)), rmul(R(0.016), U10 * U10)) * R(1E-4);
+      UST = U10 * dsqrt(cd);
+    }
     Z0 = P_::XNLEV * dexp(-R(0.4) / dsqrt(cd));
   }
 
@@ -416,23 +464,25 @@ template <typename R> struct Src {
     stresso_finish(USTAR, Z0, mij, pphi, px, py, TAUW, PHIAW);
   }
 
+  // FRCUTINDEX with the logarithms correctly rounded and the sums of the
+  // ST6 form rounded separately: equal inputs give the oracle's MIJ.
   __device__ int frcutindex(R fm, R fmws, R ustar) const {
     R fpmh = R(2.5) / S.FR[0];
     R fppm = R(3.0) * P_::G / (R(28.0) * P_::ZPI * S.FR[0]);
     R fpm4 = dmax(dmax(fmws, fm) * fpmh, fppm / dmax(ustar, R(1.0E-6)));
-    int mij = (int)lround((double)(dlog10(fpm4) * T.INV_LOG_CO)) + 1;
+    int mij = (int)lround((double)(crlog10(fpm4) * T.INV_LOG_CO)) + 1;
     return min(max(1, mij), ML());
   }
   __device__ int frcutindex_st6(R fmean, R ustar) const {
     const int nk = ML();
     R fxfm = R(6.) * P_::ZPI, fxpm = R(4.0) * P_::G / R(28.);
     R signk = P_::ZPI * S.FR[nk - 1];
-    R facti1 = R(1.) / dlog(P_::CO), facti2 = R(1.) - dlog(P_::ZPI * S.FR[0]) * facti1;
+    R facti1 = R(1.) / crlog(P_::CO), facti2 = rsub(R(1.), rmul(crlog(P_::ZPI * S.FR[0]), facti1));
     R fhigh = dmax(fxfm * fmean, fxpm / ustar);
-    int nkh = min(nk, (int)(facti2 + facti1 * dlog(dmax(R(1.E-7), fhigh))));
+    int nkh = min(nk, (int)radd(facti2, rmul(facti1, crlog(dmax(R(1.E-7), fhigh)))));
     int nkh1 = min(nk, nkh + 1);
     fhigh = dmin(signk, fhigh);
-    return max(2, min(nkh1, (int)(facti2 + facti1 * dlog(dmax(R(1.E-7), fhigh)))));
+    return max(2, min(nkh1, (int)radd(facti2, rmul(facti1, crlog(dmax(R(1.E-7), fhigh))))));
   }
 
   // IMPHFTAIL: diagnostic tail above MIJ.
@@ -717,26 +767,36 @@ template <typename R> struct Src {
     __syncwarp();
   }
 
-  // SINPUT_ST6 with LFACTOR: writes SL, FL, LL (and SP when kept); TAUW out.
+  // SINPUT_ST6 with LFACTOR: writes SL, FL, LL (and SP when kept); TAUW out;
+  // nit: the LFACTOR iterations run (0 when the stress needs no reduction).
   // The positive growth rate D1 and the negative-input term D2 of every bin
   // are formed once (kept in SL and FL until the final pass).
-  __device__ void sinput_st6(R USTAR, R& TAUW) const {
+  //
+  // LFACTOR ends its iteration on |ERR| < 1.54E-4 (:4647-4672), so a last-bit
+  // difference in the stress sums can change its iteration count and with it
+  // every high-frequency growth rate.  Everything that enters those sums
+  // follows the reference's operations: A = F*CGG/(ZPI*SIG) and
+  // SDENSIG = S*SIG/CGG with the reference's divisions, sums rounded
+  // separately (no FMA contraction), the TAUWINDS sums (:5555-5587) and the
+  // sum of the LFACT in order, and the exponentials and wind-direction
+  // cosines correctly rounded.  Equal inputs then give the oracle's
+  // iteration count unless a per-bin TANH differs by an ulp.
+  __device__ void sinput_st6(R USTAR, R& TAUW, int& nit) const {
     const int kl = KL(), nk = ML(), nk10 = T.NK10, ld = w.ld;
     const R* WN = w.t(0); const R* CG = w.t(1);
     R* SQB = w.t(2); R* LF = w.t(3); R* SDX = w.t(4); R* SDY = w.t(5); R* CI10 = w.t(6);
-    const R cu = dcos(UDIR), su = dsin(UDIR), uproxy = R(32.) * USTAR;
+    const R cu = crcos(UDIR), su = crsin(UDIR), uproxy = R(32.) * USTAR;
     const R raw = ROAIRN / P_::ROWATER;
     // directional narrowness and saturation per frequency; CI10 = k/sigma
-    // (the per-frequency factors of the direction loops are formed once)
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m];
       const R* fm = w.F + ld * m;
-      const R cgs = CG[m] / (P_::ZPI * sig);
+      const R zs = P_::ZPI * sig;
       R s = 0, mx = 0;
-      for (int k = 0; k < kl; ++k) { R a = fm[k] * cgs; s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
+      for (int k = 0; k < kl; ++k) { R a = (fm[k] * CG[m]) / zs; s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
       R s2 = 0;
       if (mx < R(1.0E-34)) s2 = R(kl);
-      else { const R rmx = R(1.) / mx; for (int k = 0; k < kl; ++k) s2 = s2 + (fm[k] * cgs) * rmx; }
+      else for (int k = 0; k < kl; ++k) s2 = s2 + ((fm[k] * CG[m]) / zs) / mx;
       R adensig = s * sig * T.DELTH, anar = R(1.0) / (s2 * T.DELTH);
       SQB[m] = dsqrt(anar * adensig * (WN[m] * WN[m] * WN[m]));
       CI10[m] = WN[m] / sig;
@@ -747,11 +807,11 @@ template <typename R> struct Src {
     // term is +0 whatever its tanh, so one tanh per bin gives the same D1, D2.
     for_bins(nk, [&](int m, int k) {
       R sig = P_::ZPI * S.FR[m], sqb = SQB[m];
-      R proj = uproxy * CI10[m] * (S.COSTH[k] * cu + S.SINTH[k] * su) - R(1.);
+      R proj = rsub(rmul(uproxy * CI10[m], radd(rmul(S.COSTH[k], cu), rmul(S.SINTH[k], su))), R(1.));
       R w1 = dmax(R(0.), proj); w1 = w1 * w1;
       R w2 = dmin(R(0.), proj); w2 = w2 * w2;
       const bool up = proj > R(0.);
-      const R g = R(2.8) - (R(1.) + dtanh(R(10.) * sqb * (up ? w1 : w2) - R(11.)));
+      const R g = R(2.8) - (R(1.) + dtanh(rsub(rmul(R(10.) * sqb, up ? w1 : w2), R(11.))));
       R d1 = up ? raw * sig * g * sqb * w1 : R(0.);
       R d2 = up ? R(0.) : raw * sig * R(0.09) * g * sqb * w2;
       w.SF[k + ld * m] = r2(d1, d2);
@@ -761,12 +821,12 @@ template <typename R> struct Src {
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m], bx = 0, by = 0;
       const R* fm = w.F + ld * m; const R2* d1 = w.SF + ld * m;
-      const R cgs = CG[m] / (P_::ZPI * sig), scg = sig / CG[m];
+      const R zs = P_::ZPI * sig;
       for (int k = 0; k < kl; ++k) {
-        R a = fm[k] * cgs;
-        R sd = d1[k].x * a * scg;
-        bx = bx + dmax(R(0.), sd) * S.COSTH[k];
-        by = by + dmax(R(0.), sd) * S.SINTH[k];
+        const R a = (fm[k] * CG[m]) / zs;
+        const R sd = ((d1[k].x * a) * sig) / CG[m];
+        bx = radd(bx, rmul(dmax(R(0.), sd), S.COSTH[k]));
+        by = radd(by, rmul(dmax(R(0.), sd), S.SINTH[k]));
       }
       SDX[m] = bx * T.DELTH; SDY[m] = by * T.DELTH;
     }
@@ -782,18 +842,33 @@ template <typename R> struct Src {
     }
     __syncwarp();
     const R* DS10 = S.DSII10;
-    // LFACTOR: shrink the high-frequency input until the total stress matches u*^2
+    // TAUWINDS: the terms of both components go to rows 2 (SQB, done with)
+    // and 7, and lanes 0 and 1 sum them in order
+    R* TX = w.t(2); R* TY = w.t(7);
     const R gro = P_::G * P_::ROWATER;
+    auto tauwinds = [&](R& tx, R& ty) {
+      R* rows[2] = {TX, TY};
+      const R init[2] = {R(0), R(0)};
+      R sum[2];
+      ordered_sums<2>(rows, init, nk10, sum);
+      tx = gro * sum[0]; ty = gro * sum[1];
+    };
+    // LFACTOR: shrink the high-frequency input until the total stress matches u*^2
     R tau_tot = USTAR * USTAR * ROAIRN;
-    R tau_vis = dmax(R(0.0), -(R(5.0E-5) * U10) + R(1.1E-3)) * (U10 * U10) * ROAIRN;
+    R tau_vis = dmax(R(0.0), radd(-rmul(R(5.0E-5), U10), R(1.1E-3))) * (U10 * U10) * ROAIRN;
     tau_vis = dmin(R(0.95) * tau_tot, tau_vis);
-    R tvx = tau_vis * dcos(UDIR), tvy = tau_vis * dsin(UDIR);
-    R px = 0, py = 0;
-    for (int i = lane; i < nk10; i += 32) { px = px + SDX[i] * CI10[i] * DS10[i]; py = py + SDY[i] * CI10[i] * DS10[i]; }
-    R tauwx = gro * warp_sum(px), tauwy = gro * warp_sum(py);
-    R tau = dsqrt((tvx + tauwx) * (tvx + tauwx) + (tvy + tauwy) * (tvy + tauwy));
+    R tvx = tau_vis * cu, tvy = tau_vis * su;
+    for (int i = lane; i < nk10; i += 32) { TX[i] = SDX[i] * CI10[i] * DS10[i]; TY[i] = SDY[i] * CI10[i] * DS10[i]; }
+    R tauwx, tauwy;
+    tauwinds(tauwx, tauwy);
+    auto total = [&]() {
+      const R ax = radd(tvx, tauwx), ay = radd(tvy, tauwy);
+      return dsqrt(radd(rmul(ax, ax), rmul(ay, ay)));
+    };
+    R tau = total();
     R err = (tau - tau_tot) / tau_tot;
     for (int i = lane; i < nk; i += 32) LF[i] = R(1.0);
+    nit = 0;
     if (tau > tau_tot) {
       bool over = false;
       R rtau = err / R(90.), drtau = R(2.0);
@@ -807,21 +882,22 @@ template <typename R> struct Src {
         const int i = lane + 32 * q;
         const bool in = i < nk10;
         qx[q] = in ? SDX[i] : R(0); qy[q] = in ? SDY[i] : R(0); qc[q] = in ? CI10[i] : R(0);
-        qd[q] = in ? DS10[i] : R(0); qa[q] = R(1.0) - uproxy * qc[q]; qf[q] = R(1.0);
+        qd[q] = in ? DS10[i] : R(0); qa[q] = rsub(R(1.0), rmul(uproxy, qc[q])); qf[q] = R(1.0);
       }
       for (int it = 0; it < 80; ++it) {
-        px = 0; py = 0;
+        nit = it + 1;
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
-          if (lane + 32 * q < nk10) {
-            const R lf = dmin(R(1.0), dexp(qa[q] * rtau));
+          const int i = lane + 32 * q;
+          if (i < nk10) {
+            const R lf = dmin(R(1.0), crexp(rmul(qa[q], rtau)));
             qf[q] = lf;
-            px = px + (qx[q] * lf) * qc[q] * qd[q];
-            py = py + (qy[q] * lf) * qc[q] * qd[q];
+            TX[i] = (qx[q] * lf) * qc[q] * qd[q];
+            TY[i] = (qy[q] * lf) * qc[q] * qd[q];
           }
         }
-        tauwx = gro * warp_sum(px); tauwy = gro * warp_sum(py);
-        tau = dsqrt((tvx + tauwx) * (tvx + tauwx) + (tvy + tauwy) * (tvy + tauwy));
+        tauwinds(tauwx, tauwy);
+        tau = total();
         err = (tau - tau_tot) / tau_tot;
         int sold = sgn;
         sgn = (err >= R(0)) ? 1 : -1;
@@ -835,10 +911,15 @@ template <typename R> struct Src {
         if (lane + 32 * q < nk) LF[lane + 32 * q] = qf[q];
     }
     __syncwarp();
-    R sumlf = 0;
-    for (int m = lane; m < nk; m += 32) sumlf = sumlf + LF[m];
-    const bool reduce = warp_sum(sumlf) < R(nk);
-    TAUW = dsqrt(tauwx * tauwx + tauwy * tauwy);
+    bool reduce;
+    {
+      R* rows[1] = {LF};
+      const R init[1] = {R(0)};
+      R sum[1];
+      ordered_sums<1>(rows, init, nk, sum);
+      reduce = sum[0] < R(nk);
+    }
+    TAUW = dsqrt(radd(rmul(tauwx, tauwx), rmul(tauwy, tauwy)));
     for_bins(nk, [&](int m, int k) {
       const int p = k + ld * m;
       const R2 v = w.SF[p];
@@ -937,14 +1018,17 @@ template <typename R> struct Src {
     R TAUW = ps.TAUW, USTAR, Z0;
     R emean, fmean, akmean = 0, emeanws, fmeanws, phiaw = 0;
     const int ju = min(300, max((int)lround((double)(U10 / T.DELU)), 1));
+    ps.JU = ju;
     integrals(nullptr, emean, fmean, (T.shallow && T.isnonlin == 0) ? &akmean : nullptr);
     if (T.iphys == 2) { wavnu2(); w3flx4(USTAR, Z0); }
     else airsea(TAUW, USTAR, Z0);
     if (T.iphys == 1) sinput_ard(USTAR, Z0);
-    else sinput_st6(USTAR, TAUW);
+    else sinput_st6(USTAR, TAUW, ps.LFIT);
     phase();
+    if (dll) copy_mask(0);
     integrals(w.LL, emeanws, fmeanws, nullptr);
     int mij = (T.iphys == 2) ? frcutindex_st6(fmean, USTAR) : frcutindex(fmean, fmeanws, USTAR);
+    ps.MIJ1 = mij;
     if (T.iphys == 2) { w3flx4(USTAR, Z0); }
     else { stresso_sums(USTAR, Z0, mij, TAUW, phiaw); airsea(TAUW, USTAR, Z0); }
     imphftail(mij);
@@ -1020,8 +1104,16 @@ template <typename R> struct Src {
     integrals(nullptr, emean, fmean, nullptr);
     integrals(w.LL, emeanws, fmeanws, nullptr);
     mij = (T.iphys == 2) ? frcutindex_st6(fmean, USTAR) : frcutindex(fmean, fmeanws, USTAR);
+    ps.MIJ2 = mij;
+    if (dll) copy_mask(1);
     imphftail(mij);
     ps.TAUW = TAUW; ps.USTAR = USTAR; ps.Z0 = Z0;
+  }
+
+  // LLWS mask of this point to plane q of the diagnostics
+  __device__ void copy_mask(int q) const {
+    const int ns = KL() * ML();
+    for_bins(ML(), [&](int m, int k) { dll[((size_t)q * ns + k + KL() * m) * dll_ld] = w.LL[k + w.ld * m]; });
   }
 };
 

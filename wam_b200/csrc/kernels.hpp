@@ -28,6 +28,12 @@ template <typename R> struct ImplArgs {
   int enh_ld;
   const R* wncg;  // ST6: WN then CG (ML values each) per point [ij * 2*ML], or null (formed in the step)
   int* status; // bit 0: non-finite output
+  // test diagnostics of the integer decisions (null: off): diag[ij + diag_ld*q]
+  // for q = JU, MIJ first, MIJ last, LFACTOR iterations; diag_ll[ij +
+  // diag_ld*(b + NS*q)] the LLWS masks of the first and of the last SINPUT call
+  int* diag = nullptr;
+  uint8_t* diag_ll = nullptr;
+  int diag_ld = 0;
 };
 
 template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const ImplArgs<R>& a, int points_per_cta, cudaStream_t s);
@@ -90,6 +96,31 @@ template <typename R> struct DerivArgs {
   R *fl3_out, *dfl3_out, *tauw_out, *dtauw_out, *ustar_out, *z0_out;
 };
 template <typename R> size_t deriv_work_bytes(int KL, int ML);
+
+// Arguments of the integrated-output kernel (COMPUTE_OUTPUT_PARAMETER,
+// wam_output_module.f90:481-640): one thread per sea point.  block receives
+// parameter IP (the reference's numbering) at block[ij + block_ld*(IP-1)].
+template <typename R> struct OutArgs {
+  int nsea, ld, KL, ML, NDEPTH, shallow, from;
+  const R* fl3;
+  const R *u10, *udir, *tauw, *depth, *u, *v;  // u, v: currents or null
+  R *ustar, *z0;                               // written by AIRSEA when USTAR is zero everywhere
+  const int* indep;
+  R* block;
+  int block_ld;
+  const R *FR, *DFIM, *DFIMOFR, *DFIM_FR, *DFIM_FR2, *MSSFD, *SINTH, *COSTH, *TFAK;
+  R MO_TAIL, MM1_TAIL, MP1_TAIL, MP2_TAIL;
+  adj::ATabs<R> A;
+  const unsigned long long* ustar_max;  // set by the launcher
+};
+// PUT_ICE_SPEC / PUT_DRY_SPEC and PUT_ICE_PAR / PUT_DRY_PAR: data[(ij-1) +
+// ld*row] = value for rows 0..nrows-1 and the 1-based sea points ij of the
+// list that lie in lo..hi.
+template <typename R>
+cudaError_t launch_put_points(R* data, size_t ld, int nrows, const int* points, int n, int lo, int hi, R value,
+                              cudaStream_t s);
+// ustar_max: device word for MAXVAL(USTAR), or null to skip the AIRSEA check.
+template <typename R> cudaError_t launch_output(const OutArgs<R>& a, unsigned long long* ustar_max, cudaStream_t s);
 template <typename R> cudaError_t launch_implsch_adj(const DevTables<R>& T, const DerivArgs<R>& a, cudaStream_t s);
 template <typename R> cudaError_t launch_implsch_tl(const DerivArgs<R>& a, cudaStream_t s);
 // Transpose of one PROPAGS sub-step: lam_old (zeroed by the caller) +=

@@ -153,7 +153,8 @@ template <typename R> struct TableSet {
   int KL = 0, ML = 0;
   // wam_fre_dir_module.f90:297-459
   std::vector<R> FR, DF, DFIM, DFIMOFR, FR5, FRM5, RHOWG_DFIM, GOM, C, TH, COSTH, SINTH;
-  R DELTH = 0, DELTR = 0, INV_LOG_CO = 0, MO_TAIL = 0, MM1_TAIL = 0, MP1_TAIL = 0;
+  std::vector<R> DFIM_FR, DFIM_FR2;  // DF*FR*DELTH, DF*FR**2*DELTH (fre_dir:392-393)
+  R DELTH = 0, DELTR = 0, INV_LOG_CO = 0, MO_TAIL = 0, MM1_TAIL = 0, MP1_TAIL = 0, MP2_TAIL = 0;
   // wam_tables_module.f90:388-464 ([(jd-1) + NDEPTH*m])
   int NDEPTH = 0; R DEPTHA = 0, DEPTHD = 0;
   std::vector<R> TFAK, TCGOND, TSIHKD;
@@ -217,6 +218,13 @@ template <typename R> struct TableSet {
     MO_TAIL = -(DELTH / R(ex_tail + 1) * FR[ML - 1]);
     MM1_TAIL = -(DELTH / R(ex_tail));
     MP1_TAIL = -(DELTH / R(ex_tail + 2) * powi(FR[ML - 1], 2));
+    MP2_TAIL = -(DELTH / R(ex_tail + 3) * powi(FR[ML - 1], 3));
+    DFIM_FR.resize(ML); DFIM_FR2.resize(ML);
+    for (int m = 0; m < ML; ++m) {
+      const R df_fr = DF[m] * FR[m], df_fr2 = df_fr * FR[m];
+      DFIM_FR[m] = df_fr * DELTH;
+      DFIM_FR2[m] = df_fr2 * DELTH;
+    }
   }
 
   void build_shallow(const Config& c) {

@@ -23,6 +23,7 @@ import numpy as np
 from ._lib import WamgpuConfig, WamgpuError, load
 
 _PF = ctypes.POINTER(ctypes.c_float)
+OUT_NPARAM = 40  # WAMGPU_OUT_NPARAM
 _PI = ctypes.POINTER(ctypes.c_int)
 
 
@@ -161,6 +162,38 @@ class WamModel:
         self._check(self.L.wamgpu_implsch_host(self.h, *args), "implsch")
         self._kept = []
 
+    def set_diagnostics(self, decisions=None, llws=None, ld=None):
+        """Test diagnostics of IMPLSCH's integer decisions (wamgpu_set_diagnostics):
+        decisions an int32 CUDA tensor (4, ld), llws None or a uint8 CUDA
+        tensor (2, ML, KL, ld); decisions=None switches them off."""
+        if decisions is None:
+            self._check(self.L.wamgpu_set_diagnostics(self.h, None, None, 0), "set_diagnostics")
+            return
+        ld = decisions.shape[-1] if ld is None else ld
+        self._check(self.L.wamgpu_set_diagnostics(self.h, decisions.data_ptr(),
+                                                  None if llws is None else llws.data_ptr(), int(ld)),
+                    "set_diagnostics")
+
+    def implsch_decisions(self, fl3, u10, udir, tauw, ustar, z0, roairn, wstar):
+        """implsch() that also returns the step's integer decisions: JU, MIJ1,
+        MIJ2 (first and last FRCUTINDEX), LFIT (LFACTOR iterations, -1 for
+        ST4) as int arrays of NSEA, and the LLWS masks of the first and the
+        last SINPUT call (LLWS1, LLWS2, uint8 shaped like FL3)."""
+        import torch
+        dev = torch.device("cuda", int(self.cfg.get("device", 0)))
+        n = self.nsea
+        dg = torch.full((4, n), -99, dtype=torch.int32, device=dev)
+        ll = torch.full((2, self.ml, self.kl, n), 7, dtype=torch.uint8, device=dev)
+        torch.cuda.synchronize(dev)
+        self.set_diagnostics(dg, ll, n)
+        try:
+            self.implsch(fl3, u10, udir, tauw, ustar, z0, roairn, wstar)
+        finally:
+            self.set_diagnostics(None)
+        d, m = dg.cpu().numpy(), ll.cpu().numpy()
+        return dict(JU=d[0], MIJ1=d[1], MIJ2=d[2], LFIT=d[3], LLWS1=np.asfortranarray(m[0].transpose(2, 1, 0)),
+                    LLWS2=np.asfortranarray(m[1].transpose(2, 1, 0)))
+
     def propags(self, f3):
         if not (f3.dtype == np.float32 and f3.flags.f_contiguous):
             raise WamgpuError("PROPAGS array must be float32 and Fortran-contiguous")
@@ -185,6 +218,34 @@ class WamModel:
         s = None if stream is None else ctypes.c_void_p(stream)
         sc = None if scratch is None else ctypes.c_void_p(scratch.data_ptr())
         self._check(self.L.wamgpu_propags_dev(self.h, f3.data_ptr(), ld, sc, s), "propags_dev")
+
+    def output_parameters_dev(self, fl3, u10, udir, tauw, ustar, z0, block=None, from_=True, ld=None, stream=None):
+        """COMPUTE_OUTPUT_PARAMETER on the device: returns block, a tensor
+        (WAMGPU_OUT_NPARAM, ld) whose row IP-1 holds the reference's output
+        parameter IP (9 Hs, 11 mean period, 12 TM1, 13 TM2, 10 peak period,
+        14 mean direction, ...); USTAR and Z0 are set by AIRSEA when USTAR is
+        zero everywhere."""
+        import torch
+        ld = fl3.shape[-1] if ld is None else ld
+        if block is None:
+            block = torch.empty((OUT_NPARAM, ld), dtype=fl3.dtype, device=fl3.device)
+        s = None if stream is None else ctypes.c_void_p(stream)
+        p = lambda t: t.data_ptr()
+        self._check(self.L.wamgpu_output_parameters_dev(self.h, p(fl3), ld, p(u10), p(udir), p(tauw), p(ustar), p(z0),
+                                                        int(bool(from_)), p(block), block.shape[-1], s),
+                    "output_parameters_dev")
+        return block
+
+    def put_points_dev(self, data, points, value=0.0, ld=None, stream=None):
+        """PUT_ICE / PUT_DRY on a device tensor shaped (..., ld) with the sea
+        point fastest (a spectrum (ML, KL, ld) or a parameter block): every
+        row at the 1-based sea points `points` (an int32 CUDA tensor) becomes
+        `value`; points outside the owned range are skipped."""
+        ld = data.shape[-1] if ld is None else ld
+        nrows = data.numel() // data.shape[-1]
+        s = None if stream is None else ctypes.c_void_p(stream)
+        self._check(self.L.wamgpu_put_points_dev(self.h, data.data_ptr(), ld, nrows, points.data_ptr(),
+                                                 int(points.numel()), float(value), s), "put_points_dev")
 
     def propags_dev_static(self, f3, ld=None, stream=None):
         """PROPAGS through the fixed per-device scratch (no allocation; calls

@@ -122,6 +122,22 @@ def _finish(name, cfg, g, depth_grid, u_grid, v_grid, rng, seed_fn=None, **kw):
     return Workload(name, cfg, g, depth, u10, udir, e_fm, d_fk, **kw)
 
 
+def vary_sea_state(w, seed=99, fp_range=(0.07, 0.25), wstar_range=(0.0, 1.5)):
+    """Start spectra with a per-point peak frequency drawn from fp_range and
+    a per-point convective velocity scale WSTAR from wstar_range (the gust
+    branch of WSIGSTAR, wam_source_module.f90:4250-4339), so that the
+    cut-off index, the wind-sea mask and the gustiness vary over the grid.
+    Modifies w in place and returns it."""
+    rng = np.random.default_rng(seed)
+    cfg = w.cfg
+    fr = cfg["fr1"] * 1.1 ** np.arange(cfg["ml"])
+    th = (np.arange(cfg["kl"]) + 0.5) * (2 * math.pi / cfg["kl"])
+    fp = rng.uniform(fp_range[0], fp_range[1], w.nsea)
+    w.e_fm, w.d_fk = jonswap_factors(fr, th, fp, 0.018, 3.3, 0.07, 0.09, w.udir)
+    w.wstar = rng.uniform(wstar_range[0], wstar_range[1], w.nsea).astype(np.float32)
+    return w
+
+
 def make_direction_variant(kl, iphys, seed=1234, scale=0.25, precision=4, device=0):
     """The small open-ocean grid of "c0" with KL directions and ST4 (iphys=1)
     or ST6 (iphys=2) source terms.  The direction count decides how the source
