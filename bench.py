@@ -118,6 +118,31 @@ class ClockSampler:
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # nominal: SMs x FP32 lanes x 2 (FMA) x max SM clock
+
+
+def fp32_roofline(workload, kernels, bins):
+    """FP32 roofline of IMPLSCH: the algorithm's floating-point operations per
+    bin (the oracle run with a counting number type, profiles/op_counts.json
+    written by oracle/count_ops.py) times the bins of one launch, over the
+    launch's CUDA-event time, against the nominal FP32 peak."""
+    path = os.path.join(ROOT, "profiles", "op_counts.json")
+    key = f"implsch_{workload}"
+    if "implsch" not in kernels or not os.path.exists(path):
+        return None
+    with open(path) as f:
+        ops = json.load(f)
+    if key not in ops:
+        return None
+    fpb = ops[key]["flops_per_bin"]
+    ach = fpb * bins / (kernels["implsch"]["avg_ms"] / 1e3) / 1e12
+    return {"kernel": "implsch", "achieved": ach, "peak": FP32_PEAK_TFLOPS, "unit": "TFLOP/s",
+            "frac": ach / FP32_PEAK_TFLOPS, "flops_per_bin": fpb,
+            "transcendentals_per_bin": ops[key]["per_bin"]["trans"],
+            "peak_kind": "nominal (148 SMs x 128 FP32 lanes x 2 x 1965 MHz)",
+            "counts": "profiles/op_counts.json (oracle/count_ops.py)"}
+
+
 def workload_config(name, scale, nsea, kl, ml):
     """The `config` of both arms: the workload, its sea points and bins per point."""
     if name == "c1" and scale == 1.0:
@@ -543,6 +568,9 @@ def main():
     roof = {"bound": "hbm", "achieved": kernels[dom]["achieved_gbs"], "peak": hbm, "unit": "GB/s",
             "frac": kernels[dom]["achieved_gbs"] / hbm, "traffic": traffic, "kernel": dom,
             "peak_kind": f"{hbm_kind} (MEASURED_PEAKS.json hbm_gbs)" if hbm_kind == "measured" else "fallback"}
+    fp32 = fp32_roofline(args.workload, kernels, bins)
+    if fp32:
+        roof["fp32"] = fp32
     # end to end through the C ABI with host buffers (pinned): FL3 and the point fields in, results back
     e2e = None
     if not args.no_e2e and rank == 0:

@@ -211,6 +211,16 @@ WAMGPU_API int wamgpu_get_timing(wamgpu_ctx* ctx, float* ms, int* count);
 WAMGPU_API int wamgpu_set_owned(wamgpu_ctx* ctx, int i0, int i1);
 WAMGPU_API int wamgpu_set_counter(wamgpu_ctx* ctx, int counter);
 WAMGPU_API int wamgpu_propags_substep_dev(wamgpu_ctx* ctx, const void* src, void* dst, int ld, void* stream);
+/* The same sub-step over the sea points i0..i1-1 only (0-based, inside the
+ * owned range).  A point further than the halo width from both ends of the
+ * owned range reads no halo point, so a band driver sub-steps those interior
+ * points while its halo exchange (mpi_exchng, wam_mpi_comp_module.f90:
+ * 1466-1626) is in flight and the points near the band edges after it.
+ * wamgpu_get_halo_width returns that width: the largest |neighbour - point|
+ * over KLAT/KLON, in sea points (or a negative code without a grid). */
+WAMGPU_API int wamgpu_propags_substep_range_dev(wamgpu_ctx* ctx, const void* src, void* dst, int ld, int i0, int i1,
+                                                void* stream);
+WAMGPU_API int wamgpu_get_halo_width(const wamgpu_ctx* ctx);
 
 /* Batched ensembles.  No single counterpart in the reference, where each
  * member is a separate WAMODEL run calling PROPAGS (propagation:635-829) and

@@ -62,6 +62,7 @@ def lib():
                                           ctypes.c_int, ip, dp, ctypes.POINTER(ctypes.c_ubyte)]
         L.oracle_propags.argtypes = [vp, dp]
         L.oracle_resident_set.argtypes = [vp] + [dp] * 9
+        L.oracle_count_implsch.argtypes = [ctypes.POINTER(OracleConfig), ctypes.c_int] + [dp] * 9 + [ip, dp]
         L.oracle_output_params.argtypes = [vp, ctypes.c_int] + [dp] * 9 + [ip, ctypes.c_int, dp]
         L.oracle_resident_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.oracle_resident_get.argtypes = [vp, dp, dp, dp, dp]
@@ -214,6 +215,21 @@ class Oracle:
                     LF_MARGIN=fdg[3], LLWS1=np.asfortranarray(ll[0].transpose(2, 1, 0)),
                     LLWS2=np.asfortranarray(ll[1].transpose(2, 1, 0)))
         return f, tw, us, zz, (fl.reshape(7, nsea) if fl is not None else None), diag
+
+    def count_implsch(self, fl3, u10, udir, tauw, ustar, z0, roairn, wstar, depth, indep):
+        """Floating-point operation counts of IMPLSCH on these points (the
+        restatement run with a counting number type): dict of additions,
+        multiplications, divisions, square roots, transcendental functions and
+        comparisons, summed over the points."""
+        fields = {f for f, _ in OracleConfig._fields_}
+        c = OracleConfig(**{k: v for k, v in self.cfg.items() if k in fields})
+        nsea = fl3.shape[0]
+        cnt = np.zeros(6)
+        a = lambda x: np.ascontiguousarray(x, float)
+        self.L.oracle_count_implsch(ctypes.byref(c), nsea, _d(np.asfortranarray(fl3, float)), _d(a(u10)), _d(a(udir)),
+                                    _d(a(tauw)), _d(a(ustar)), _d(a(z0)), _d(a(roairn)), _d(a(wstar)), _d(a(depth)),
+                                    _i(np.ascontiguousarray(indep, np.int32)), _d(cnt))
+        return dict(zip(("add", "mul", "div", "sqrt", "trans", "cmp"), cnt.astype(np.int64).tolist()))
 
     def output_params(self, fl3, u10, udir, ustar, tauw, z0, depth, u=None, v=None, indep=None, from_=True):
         """COMPUTE_OUTPUT_PARAMETER: returns (block[40, nsea] with row IP-1 = parameter IP, ustar, z0)."""

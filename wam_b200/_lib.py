@@ -60,6 +60,8 @@ SIGNATURES = {
     "wamgpu_step_ckpt_dev": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_int] + [c_void_p] * 8),
     "wamgpu_step_adj_dev": (c_int, [c_void_p, c_int, c_int, c_void_p, c_int] + [c_void_p] * 7),
     "wamgpu_propags_substep_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
+    "wamgpu_propags_substep_range_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_int, c_int, c_void_p]),
+    "wamgpu_get_halo_width": (c_int, [c_void_p]),
     "wamgpu_batch_create": (c_int, [ctypes.POINTER(c_void_p), c_int, ctypes.POINTER(c_void_p)]),
     "wamgpu_batch_destroy": (c_int, [c_void_p]),
     "wamgpu_batch_last_error": (c_char_p, [c_void_p]),

@@ -687,6 +687,20 @@ template <typename R> int propags_substep_t(wamgpu_ctx* ctx, Impl<R>& I, const v
   return WAMGPU_OK;
 }
 
+// The same over the points [i0, i1) of the owned range only.
+template <typename R>
+int propags_range_t(wamgpu_ctx* ctx, Impl<R>& I, const void* src, void* dst, int ld, int i0, int i1, cudaStream_t s) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  if (src == dst) return fail(ctx, WAMGPU_E_ARG, "a sub-step needs distinct source and destination spectra");
+  const int o0 = ctx->own0, o1 = ctx->own1 < 0 ? ctx->nsea : ctx->own1;
+  if (i0 < o0 || i1 > o1 || i0 > i1) return fail(ctx, WAMGPU_E_ARG, "point range outside the owned range");
+  PropArgs<R> A = I.pa;
+  A.i0 = i0; A.i1 = i1;
+  { TimedLaunch tl(ctx, 0, s); CK(launch_propags<R>(A, (const R*)src, ld, (R*)dst, ld, s), "propags launch"); }
+  return WAMGPU_OK;
+}
+
 template <typename R> int set_counter_t(wamgpu_ctx* ctx, Impl<R>& I, int counter) {
   if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
   if (counter < ctx->counter)
@@ -1915,6 +1929,18 @@ int wamgpu_set_owned(wamgpu_ctx* ctx, int i0, int i1) {
 int wamgpu_set_counter(wamgpu_ctx* ctx, int counter) {
   if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
   return DISPATCH_CTX(ctx, set_counter_t, counter);
+}
+
+int wamgpu_propags_substep_range_dev(wamgpu_ctx* ctx, const void* src, void* dst, int ld, int i0, int i1,
+                                     void* stream) {
+  if (!ctx || !ctx->impl || !src || !dst) return WAMGPU_E_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, propags_range_t, src, dst, ld, i0, i1, s);
+}
+
+int wamgpu_get_halo_width(const wamgpu_ctx* ctx) {
+  if (!ctx || !ctx->have_grid) return WAMGPU_E_STATE;
+  return ctx->halo;
 }
 
 int wamgpu_propags_substep_dev(wamgpu_ctx* ctx, const void* src, void* dst, int ld, void* stream) {

@@ -107,35 +107,58 @@ def exchange_plan(parts, me):
 
 class HaloExchange:
     """Refreshes the halo of a band's spectrum (a tensor shaped (ML, KL, ld)
-    over the band's extended range) from the owning ranks."""
+    over the band's extended range) from the owning ranks.
+
+    The send and receive strips are allocated once per spectrum shape.  With
+    NCCL they stay on the device and the P2P operations are ordered on the
+    stream passed (torch's NCCL work waits for that stream, and the stream
+    waits for it).  With gloo and a CUDA spectrum the strips are staged
+    through pinned host buffers: the host waits only for the strip copies of
+    that stream, sends and receives, and queues the halo writes on it.  With
+    CPU tensors there is no stream."""
 
     def __init__(self, parts, me, group=None):
         self.parts, self.me, self.group = parts, me, group
         self.sends, self.recvs = exchange_plan(parts, me)
         self.base = parts[me]["ninf"]
+        self._key = None
 
-    def __call__(self, f):
+    def _alloc(self, f):
         import torch
         import torch.distributed as dist
-        ops, bufs = [], []
-        for q, lo, hi in self.sends:
-            buf = f[:, :, lo - self.base:hi - self.base].contiguous()
-            bufs.append(buf)
-            ops.append(dist.P2POp(dist.isend, buf, q, group=self.group))
-        rbufs = []
-        for q, lo, hi in self.recvs:
-            buf = torch.empty((f.shape[0], f.shape[1], hi - lo), dtype=f.dtype, device=f.device)
-            rbufs.append((buf, lo, hi))
-            ops.append(dist.P2POp(dist.irecv, buf, q, group=self.group))
-        if ops:
-            if dist.get_backend(self.group) == "nccl":
-                reqs = dist.batch_isend_irecv(ops)
-            else:  # one request per strip
-                reqs = [op.op(op.tensor, op.peer, group=self.group) for op in ops]
-            for req in reqs:
-                req.wait()
-        for buf, lo, hi in rbufs:
-            f[:, :, lo - self.base:hi - self.base] = buf
+        self._staged = f.is_cuda and dist.get_backend(self.group) != "nccl"
+        dev = torch.device("cpu") if self._staged else f.device
+
+        def strip(n):
+            return torch.empty((f.shape[0], f.shape[1], n), dtype=f.dtype, device=dev, pin_memory=self._staged)
+        self._send = [strip(hi - lo) for _, lo, hi in self.sends]
+        self._recv = [strip(hi - lo) for _, lo, hi in self.recvs]
+        self._key = (tuple(f.shape), f.dtype, str(f.device))
+
+    def __call__(self, f, stream=None):
+        import contextlib
+        import torch
+        import torch.distributed as dist
+        if self._key != (tuple(f.shape), f.dtype, str(f.device)):
+            self._alloc(f)
+        b = self.base
+        ctx = torch.cuda.stream(stream) if (f.is_cuda and stream is not None) else contextlib.nullcontext()
+        with ctx:
+            for buf, (q, lo, hi) in zip(self._send, self.sends):
+                buf.copy_(f[:, :, lo - b:hi - b], non_blocking=True)
+            if self._staged:
+                torch.cuda.current_stream(f.device).synchronize()  # the strips are on the host
+            ops = [dist.P2POp(dist.isend, buf, q, group=self.group) for buf, (q, _, _) in zip(self._send, self.sends)]
+            ops += [dist.P2POp(dist.irecv, buf, q, group=self.group) for buf, (q, _, _) in zip(self._recv, self.recvs)]
+            if ops:
+                if dist.get_backend(self.group) == "nccl":
+                    reqs = dist.batch_isend_irecv(ops)
+                else:  # one request per strip
+                    reqs = [op.op(op.tensor, op.peer, group=self.group) for op in ops]
+                for req in reqs:
+                    req.wait()
+            for buf, (q, lo, hi) in zip(self._recv, self.recvs):
+                f[:, :, lo - b:hi - b].copy_(buf, non_blocking=True)
         return f
 
 
@@ -184,14 +207,46 @@ class BandModel:
         self.m.prepare_source()
         self.exchange = HaloExchange(parts, me, group)
         self.nprop = cfg["idelt"] // cfg["idelpro"]
+        self.halo = self.m.halo_width()
+        self._xs = None
 
-    def step(self, f, scratch, u10, udir, tauw, ustar, z0, roairn, wstar, stream=None):
-        """One WAMODEL pass; returns the tensor that holds the new spectrum
-        (f or scratch: the sub-steps ping-pong between them)."""
+    def step(self, f, scratch, u10, udir, tauw, ustar, z0, roairn, wstar, stream=None, overlap=True):
+        """One WAMODEL pass on `stream` (a torch.cuda.Stream; default: the
+        current stream); returns the tensor that holds the new spectrum (f or
+        scratch: the sub-steps ping-pong between them).
+
+        With overlap, each sub-step first runs the interior owned points (more
+        than the halo width from the band's ends, so they read no halo point)
+        on `stream` while the halo exchange runs on a second stream (NCCL) or
+        on the host (gloo), and then the points near the band's ends once the
+        halo has arrived.  Every kernel computes the same elements from the
+        same inputs as the unsplit sub-step."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream(f.device)
+        h = s.cuda_stream
+        o0, o1 = self.part["lo"] - self.part["ninf"], self.part["hi"] - self.part["ninf"]
+        i0, i1 = o0 + self.halo, o1 - self.halo
+        split = overlap and i0 < i1
+        if split and self._xs is None:
+            self._xs = torch.cuda.Stream(f.device)
+            self._ev = (torch.cuda.Event(), torch.cuda.Event())
         src, dst = f, scratch
         for _ in range(self.nprop * self.counter):
-            self.exchange(src)
-            self.m.propags_substep_dev(src, dst, stream=stream)
+            if split:
+                ready, halo = self._ev
+                ready.record(s)                                     # src complete
+                self.m.propags_substep_range_dev(src, dst, i0, i1, stream=h)
+                self._xs.wait_event(ready)
+                self.exchange(src, stream=self._xs)                 # halo of src, beside the interior
+                halo.record(self._xs)
+                s.wait_event(halo)
+                if o0 < i0:
+                    self.m.propags_substep_range_dev(src, dst, o0, i0, stream=h)
+                if i1 < o1:
+                    self.m.propags_substep_range_dev(src, dst, i1, o1, stream=h)
+            else:
+                self.exchange(src, stream=s)
+                self.m.propags_substep_dev(src, dst, stream=h)
             src, dst = dst, src
-        self.m.implsch_dev(src, u10, udir, tauw, ustar, z0, roairn, wstar, stream=stream)
+        self.m.implsch_dev(src, u10, udir, tauw, ustar, z0, roairn, wstar, stream=h)
         return src

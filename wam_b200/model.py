@@ -290,6 +290,19 @@ class WamModel:
         s = None if stream is None else ctypes.c_void_p(stream)
         self._check(self.L.wamgpu_propags_substep_dev(self.h, src.data_ptr(), dst.data_ptr(), ld, s), "propags_substep")
 
+    def propags_substep_range_dev(self, src, dst, i0, i1, ld=None, stream=None):
+        """One PROPAGS sub-step over the points i0..i1-1 of the owned range."""
+        ld = src.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        self._check(self.L.wamgpu_propags_substep_range_dev(self.h, src.data_ptr(), dst.data_ptr(), ld, int(i0), int(i1),
+                                                            s), "propags_substep_range")
+
+    def halo_width(self):
+        """Largest |neighbour - point| over KLAT/KLON, in sea points."""
+        w = self.L.wamgpu_get_halo_width(self.h)
+        self._check(0 if w >= 0 else w, "get_halo_width")
+        return w
+
     # ---- derivatives (ST4) ---------------------------------------------------
     def implsch_tl_dev(self, fl3, dfl3, tauw, dtauw, u10, du10, udir, roairn, wstar,
                        fl3_out, dfl3_out, tauw_out, dtauw_out, ld=None, stream=None):
