@@ -333,6 +333,58 @@ WAMGPU_API int wamgpu_step_adj_dev(wamgpu_ctx* ctx, int slot, int nprop, void* l
  * writes none of this. */
 WAMGPU_API int wamgpu_set_diagnostics(wamgpu_ctx* ctx, int* decisions, unsigned char* llws, int ld);
 
+/* Restart files from and to device buffers: SAVE_RESTART_FILE
+ * (wam_restart_module.f90:414-591) and CONNECT_RESTART (:109-327) in the
+ * reference's sequential unformatted layout (4-byte record lengths around
+ * each record; REAL = 4-byte float on file whatever the context's
+ * precision):
+ *   record 1   NSEA, CDTPRO, CDTSOU, CDA, CDTA, CDCA (CHARACTER(14) each)
+ *   records    U10, UDIR, TAUW (NSEA values each), FL3 (NSEA x KL x ML)
+ *   then       DEPTH if CDTA is not blank, U and V (one record) if CDCA is
+ *              not blank.
+ * ij2newij (host, NSEA 1-based) renumbers as the reference does without the
+ * spatial decomposition: file position p holds model point ij2newij[p-1];
+ * NULL is the identity (L_DECOMP).  The spectrum moves through a pinned
+ * staging buffer in chunks, gathered / scattered on the device, so it is
+ * never held whole on the host.  Device buffers in the context's precision;
+ * fl3 with leading dimension ld; depth, u, v may be NULL when their dates are
+ * blank.  The context must cover the whole grid (no owned range), and the
+ * spectrum record must stay below 2 GiB (NSEA*KL*ML*4 bytes).  Reading
+ * checks NSEA and every record length against the model grid and returns
+ * WAMGPU_E_ARG where the reference calls ABORT1.  Both calls synchronise
+ * the context stream; make the buffers' producers finish first. */
+typedef struct wamgpu_restart_dates {
+  char cdtpro[14], cdtsou[14], cda[14], cdta[14], cdca[14];  /* blank-padded, no terminator */
+} wamgpu_restart_dates;
+WAMGPU_API int wamgpu_restart_write(wamgpu_ctx* ctx, const char* path, const void* fl3, int ld, const void* u10,
+                                    const void* udir, const void* tauw, const void* depth, const void* u,
+                                    const void* v, const wamgpu_restart_dates* dates, const int* ij2newij);
+WAMGPU_API int wamgpu_restart_read(wamgpu_ctx* ctx, const char* path, void* fl3, int ld, void* u10, void* udir,
+                                   void* tauw, void* depth, void* u, void* v, wamgpu_restart_dates* dates,
+                                   const int* ij2newij);
+
+/* New wind fields on the device: GET_WIND's conversion of an input field
+ * to the sea points (WAM_WIND, wam_wind_module.f90:1063-1216), so that a
+ * pass with hourly winds keeps U10 and UDIR resident.
+ *  - wamgpu_set_wind_grid: INITIALIZE of INTERPOLATION_TO_GRID (:1296-1375)
+ *    for the input grid of nx_in x ny_in points with west/south corner and
+ *    steps in the reference's integer units (1/100 arc-second, M_SEC),
+ *    periodic in longitude or not, from the model grid's AMOWEP, AMOSOP,
+ *    XDELLA, ZDELLO (one per latitude row) and IFROMIJ (one per sea point;
+ *    KFROMIJ is the context's).  equal_grid != 0: the input grid is the
+ *    model grid (EQUAL_GRID), and point (IFROMIJ, KFROMIJ) is copied.  A sea
+ *    point outside the input grid is WAMGPU_E_ARG, where the reference calls
+ *    ABORT1.
+ *  - wamgpu_wind_dev: u_in, v_in (device, nx_in x ny_in, longitude fastest)
+ *    of WIND CODE code_in (1 friction velocity, 2 surface stress, 3 U10) to
+ *    U10 >= 2 m/s and UDIR = ATAN2(U,V) in [0, 2*pi) at every sea point of the
+ *    context, in its precision. */
+WAMGPU_API int wamgpu_set_wind_grid(wamgpu_ctx* ctx, int nx_in, int ny_in, int west_in, int south_in, int dx_in,
+                                    int dy_in, int periodic, int equal_grid, int amowep, int amosop, int xdella,
+                                    const int* zdello, const int* ifromij);
+WAMGPU_API int wamgpu_wind_dev(wamgpu_ctx* ctx, const void* u_in, const void* v_in, int code_in, void* u10, void* udir,
+                               void* stream);
+
 /* PUT_ICE (FL3, INDICATOR) and PUT_DRY (FL3, INDICATOR) on device data
  * (PUT_ICE_SPEC wam_ice_module.f90:312-324, PUT_DRY_SPEC
  * wam_topo_module.f90:557-569; called by WAMODEL at wamodel.f90:380-397),

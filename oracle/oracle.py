@@ -281,3 +281,128 @@ def put_points(data, points, value, nijs=1, nijl=None):
         if nijs <= ij <= nijl:
             out[ij - 1, ...] = value
     return out
+
+
+M_S_PER = 360 * 360000
+
+
+def wind_tables(grid, nx_in, ny_in, west_in, south_in, dx_in, dy_in, periodic=False, equal_grid=False):
+    """INITIALIZE of INTERPOLATION_TO_GRID (wam_wind_module.f90:1296-1375):
+    per sea point the input cell I1, I2, K1, K2 (1-based) and the weights DI,
+    DK, in the reference's integer units and REAL (float32) arithmetic.
+    Raises where the reference calls ABORT1 (a point outside the input grid)."""
+    f32 = np.float32
+    ifr = np.asarray(grid["ixlg"], np.int64)
+    kfr = np.asarray(grid["kfromij"], np.int64)
+    if equal_grid:
+        z = np.zeros(ifr.size, f32)
+        return ifr, ifr.copy(), kfr, kfr.copy(), z, z.copy()
+    zdello = np.broadcast_to(np.asarray(grid.get("zdello", grid["xdello"]), np.int64), (int(grid["ny"]),))
+    i1 = grid["amowep"] + (ifr - 1) * zdello[kfr - 1] - west_in
+    i1 = np.mod(i1 + 2 * M_S_PER, M_S_PER)
+    di = i1.astype(f32) / f32(dx_in)
+    k1 = grid["amosop"] + (kfr - 1) * grid["xdella"] - south_in
+    dk = k1.astype(f32) / f32(dy_in)
+    i1 = di.astype(np.int64) + 1
+    k1 = dk.astype(np.int64) + 1
+    k2 = np.minimum(ny_in, k1 + 1)
+    i2 = i1 + 1
+    di = (di - i1.astype(f32)) + f32(1.)
+    dk = (dk - k1.astype(f32)) + f32(1.)
+    if periodic:
+        i2 = np.where(i1 == nx_in, 1, i2)
+        i1 = np.where(i1 == 0, nx_in, i1)
+    else:
+        i2 = np.where(i1 == nx_in, nx_in, i2)
+    if i1.min() < 1 or i1.max() > nx_in or k1.min() < 1 or k1.max() > ny_in:
+        raise ValueError("point is outside of input grid")
+    return i1, i2, k1, k2, di.astype(f32), dk.astype(f32)
+
+
+def wam_wind(u_in, v_in, tables, code_in=3, equal_grid=False):
+    """WAM_WIND (wam_wind_module.f90:1063-1216) in float32: the input
+    components u_in, v_in [ny_in, nx_in] at the sea points (bilinear, or a
+    copy on the model's own grid), speed, direction ATAN2(U,V) in [0, 2 pi),
+    the friction-velocity (1) or stress (2) input turned into U10, U10 >= 2."""
+    f32 = np.float32
+    i1, i2, k1, k2, di, dk = tables
+    U = np.asarray(u_in, f32)
+    V = np.asarray(v_in, f32)
+    at = lambda F, i, k: F[k - 1, i - 1]
+    if equal_grid:
+        uu, vv = at(U, i1, k1), at(V, i1, k1)
+    else:
+        one = f32(1.)
+        uu = (at(U, i1, k1) * (one - di) + at(U, i2, k1) * di) * (one - dk) + \
+             (at(U, i1, k2) * (one - di) + at(U, i2, k2) * di) * dk
+        vv = (at(V, i1, k1) * (one - di) + at(V, i2, k1) * di) * (one - dk) + \
+             (at(V, i1, k2) * (one - di) + at(V, i2, k2) * di) * dk
+    us = np.sqrt(uu * uu + vv * vv).astype(f32)
+    ds = np.where(us != 0, np.arctan2(uu, vv), f32(0.)).astype(f32)
+    ds = np.where(ds < 0, ds + f32(2.) * f32(3.1415927), ds).astype(f32)
+    if code_in in (1, 2):
+        ust = np.maximum(f32(0.01), us) if code_in == 1 else np.maximum(f32(0.01), np.sqrt(us / f32(1.225)))
+        z0 = f32(0.0185) / f32(9.806) * (ust * ust)
+        cd = f32(0.40) / np.log(f32(10.) / z0)
+        us = (ust / cd).astype(f32)
+    return np.maximum(us, f32(2.0)).astype(f32), ds
+
+
+def write_restart(path, nsea, dates, u10, udir, tauw, fl3, depth=None, u=None, v=None, ij2newij=None):
+    """SAVE_RESTART_FILE's records (wam_restart_module.f90:414-591) as a
+    Fortran sequential unformatted file: record lengths around every record,
+    REAL as float32.  fl3 is (NSEA, KL, ML); with ij2newij file position p
+    holds model point ij2newij[p-1]."""
+    perm = np.arange(nsea) if ij2newij is None else np.asarray(ij2newij) - 1
+
+    def rec(fh, payload):
+        m = np.int32(len(payload)).tobytes()
+        fh.write(m + payload + m)
+
+    with open(path, "wb") as fh:
+        head = np.int32(nsea).tobytes() + b"".join(str(dates.get(k, "")).ljust(14)[:14].encode()
+                                                     for k in ("CDTPRO", "CDTSOU", "CDA", "CDTA", "CDCA"))
+        rec(fh, head)
+        for a in (u10, udir, tauw):
+            rec(fh, np.asarray(a, np.float32)[perm].tobytes())
+        rec(fh, np.asarray(fl3, np.float32)[perm].tobytes(order="F"))
+        if str(dates.get("CDTA", "")).strip():
+            rec(fh, np.asarray(depth, np.float32)[perm].tobytes())
+        if str(dates.get("CDCA", "")).strip():
+            rec(fh, np.asarray(u, np.float32)[perm].tobytes() + np.asarray(v, np.float32)[perm].tobytes())
+
+
+def read_restart(path, kl, ml, ij2newij=None):
+    """CONNECT_RESTART's records (wam_restart_module.f90:109-327): returns a
+    dict of NSEA, the dates, U10, UDIR, TAUW, FL3 (NSEA, KL, ML) in model
+    order, and DEPTH / U / V when their dates are not blank."""
+    with open(path, "rb") as fh:
+        data = fh.read()
+    recs, pos = [], 0
+    while pos < len(data):
+        n = int(np.frombuffer(data, np.int32, 1, pos)[0])
+        recs.append(data[pos + 4:pos + 4 + n])
+        assert int(np.frombuffer(data, np.int32, 1, pos + 4 + n)[0]) == n, "record length markers differ"
+        pos += n + 8
+    head = recs[0]
+    nsea = int(np.frombuffer(head, np.int32, 1, 0)[0])
+    out = {"NSEA": nsea}
+    for i, k in enumerate(("CDTPRO", "CDTSOU", "CDA", "CDTA", "CDCA")):
+        out[k] = head[4 + 14 * i:18 + 14 * i].decode()
+    perm = np.arange(nsea) if ij2newij is None else np.asarray(ij2newij) - 1
+
+    def model(x):
+        y = np.empty_like(x)
+        y[perm] = x
+        return y
+    f = lambda r: np.frombuffer(r, np.float32)
+    out["U10"], out["UDIR"], out["TAUW"] = (model(f(recs[i])) for i in (1, 2, 3))
+    spec = f(recs[4]).reshape((nsea, kl, ml), order="F")
+    out["FL3"] = np.asfortranarray(model(spec))
+    i = 5
+    if out["CDTA"].strip():
+        out["DEPTH"] = model(f(recs[i])); i += 1
+    if out["CDCA"].strip():
+        uv = f(recs[i])
+        out["U"], out["V"] = model(uv[:nsea]), model(uv[nsea:])
+    return out

@@ -21,6 +21,12 @@ class WamgpuConfig(ctypes.Structure):
                 ("delphi", ctypes.c_double), ("precision", c_int), ("device", c_int)]
 
 
+class RestartDates(ctypes.Structure):
+    """struct wamgpu_restart_dates: CHARACTER(14) dates, blank-padded."""
+    _fields_ = [("cdtpro", ctypes.c_char * 14), ("cdtsou", ctypes.c_char * 14), ("cda", ctypes.c_char * 14),
+                ("cdta", ctypes.c_char * 14), ("cdca", ctypes.c_char * 14)]
+
+
 SIGNATURES = {
     "wamgpu_create": (c_int, [ctypes.POINTER(WamgpuConfig), ctypes.POINTER(c_void_p)]),
     "wamgpu_destroy": (c_int, [c_void_p]),
@@ -46,6 +52,12 @@ SIGNATURES = {
     "wamgpu_get_fluxes": (c_int, [c_void_p, PF]),
     "wamgpu_sync": (c_int, [c_void_p]),
     "wamgpu_set_diagnostics": (c_int, [c_void_p, c_void_p, c_void_p, c_int]),
+    "wamgpu_restart_write": (c_int, [c_void_p, c_char_p, c_void_p, c_int] + [c_void_p] * 6 +
+                             [ctypes.POINTER(RestartDates), PI]),
+    "wamgpu_restart_read": (c_int, [c_void_p, c_char_p, c_void_p, c_int] + [c_void_p] * 6 +
+                            [ctypes.POINTER(RestartDates), PI]),
+    "wamgpu_set_wind_grid": (c_int, [c_void_p] + [c_int] * 11 + [PI, PI]),
+    "wamgpu_wind_dev": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
     "wamgpu_put_points_dev": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, ctypes.c_double, c_void_p]),
     "wamgpu_output_parameters_dev": (c_int, [c_void_p, c_void_p, c_int] + [c_void_p] * 5 + [c_int, c_void_p, c_int,
                                                                                              c_void_p]),

@@ -73,6 +73,7 @@ struct wamgpu_ctx {
   int* diag = nullptr;
   unsigned char* diag_ll = nullptr;
   int diag_ld = 0;
+  int wind_nx = 0, wind_ny = 0, wind_equal = 0;  // wind input grid (wamgpu_set_wind_grid)
   std::unique_ptr<ImplBase> impl;
   // opt-in kernel timing: event pairs per kernel class (0 = PROPAGS, 1 = IMPLSCH)
   bool timing = false;
@@ -96,6 +97,8 @@ template <typename R> struct Impl : ImplBase {
   DevBuf small, ismall, tfak, tcgond, tsihkd, flminfr, enh, gom, fr, sinth, costh;
   DevBuf outtab;         // integrated output: DFIM_FR, DFIM_FR2, MEANSQS deep-water weights (ML each)
   DevBuf ustar_max;      // MAXVAL(USTAR) word of the output step
+  DevBuf wind_tab, wind_w;  // INTERPOLATION_TO_GRID tables (I1, I2, K1, K2; DI, DK) of the sea points
+  DevBuf rst_stage, rst_perm;  // restart records: REAL staging chunk, IJ2NEWIJ
   DevBuf diamc;          // per-MC DIA rows and write masks (DevTables::diamc)
   DevBuf dslot;          // DIA batch slot entries (DevTables::dslot)
   // per-point metadata
@@ -1004,6 +1007,224 @@ int put_points_t(wamgpu_ctx* ctx, Impl<R>& I, void* data, int ld, int nrows, con
   return WAMGPU_OK;
 }
 
+// INITIALIZE of INTERPOLATION_TO_GRID (wam_wind_module.f90:1296-1375): per
+// sea point the input-grid cell (I1, I2, K1, K2) and the weights DI, DK, in
+// the reference's integer 1/100 arc-second units and REAL arithmetic.
+template <typename R>
+int set_wind_grid_t(wamgpu_ctx* ctx, Impl<R>& I, int nx_in, int ny_in, int west_in, int south_in, int dx_in, int dy_in,
+                    int per, int equal, int amowep, int amosop, int xdella, const int* zdello, const int* ifromij) {
+  if (!ctx->have_grid) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_set_grid first");
+  if (nx_in < 1 || ny_in < 1 || !ifromij || (!equal && (!zdello || dx_in == 0 || dy_in == 0)))
+    return fail(ctx, WAMGPU_E_ARG, "wind grid: bad dimensions or missing tables");
+  const int n = ctx->nsea;
+  const long long M_S_PER = 360LL * 360000LL;
+  std::vector<int> tab(4 * (size_t)n);
+  std::vector<R> w(2 * (size_t)n, R(0));
+  for (int ij = 0; ij < n; ++ij) {
+    const int kf = ctx->kfromij[ij], ifr = ifromij[ij];
+    int i1, i2, k1, k2;
+    if (equal) {
+      i1 = i2 = ifr; k1 = k2 = kf;
+    } else {
+      if (kf < 1 || kf > ctx->ny) return fail(ctx, WAMGPU_E_ARG, "KFROMIJ outside the grid rows");
+      long long li = (long long)amowep + (long long)(ifr - 1) * zdello[kf - 1] - west_in;
+      li = (li + 2 * M_S_PER) % M_S_PER;
+      R di = R((int)li) / R(dx_in);
+      const long long lk = (long long)amosop + (long long)(kf - 1) * xdella - south_in;
+      R dk = R((int)lk) / R(dy_in);
+      i1 = (int)di + 1; k1 = (int)dk + 1;
+      k2 = std::min(ny_in, k1 + 1);
+      i2 = i1 + 1;
+      di = di - R(i1) + R(1.);
+      dk = dk - R(k1) + R(1.);
+      if (per) { if (i1 == nx_in) i2 = 1; if (i1 == 0) i1 = nx_in; }
+      else if (i1 == nx_in) i2 = nx_in;
+      w[ij] = di; w[ij + n] = dk;
+    }
+    if (i1 < 1 || i1 > nx_in || k1 < 1 || k1 > ny_in)
+      return fail(ctx, WAMGPU_E_ARG, "sea point " + std::to_string(ij + 1) + " lies outside the wind input grid");
+    tab[ij] = i1; tab[ij + n] = i2; tab[ij + 2 * (size_t)n] = k1; tab[ij + 3 * (size_t)n] = k2;
+  }
+  CK(upload(I.wind_tab, tab, ctx->stream), "upload wind tables");
+  CK(upload(I.wind_w, w, ctx->stream), "upload wind tables");
+  CK(cudaStreamSynchronize(ctx->stream), "wind tables");
+  ctx->wind_nx = nx_in; ctx->wind_ny = ny_in; ctx->wind_equal = equal ? 1 : 0;
+  return WAMGPU_OK;
+}
+
+template <typename R>
+int wind_dev_t(wamgpu_ctx* ctx, Impl<R>& I, const void* u_in, const void* v_in, int code_in, void* u10, void* udir,
+               cudaStream_t s) {
+  if (ctx->wind_nx <= 0) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_set_wind_grid first");
+  if (code_in < 1 || code_in > 3) return fail(ctx, WAMGPU_E_ARG, "wind code must be 1 (USTAR), 2 (stress) or 3 (U10)");
+  if (!u_in || !v_in || !u10 || !udir) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  CK(launch_wind<R>((const R*)u_in, (const R*)v_in, ctx->wind_nx, ctx->nsea, I.wind_tab.template as<int>(),
+                    I.wind_w.template as<R>(), ctx->wind_equal, code_in, (R*)u10, (R*)udir, s), "wind launch");
+  return WAMGPU_OK;
+}
+
+// ---- restart files (wam_restart_module.f90) ---------------------------------
+// The reference writes them as Fortran sequential unformatted records: a
+// 4-byte length, the payload, the length again (the layout of gfortran and
+// ifort for records below 2 GiB).  Record 1 holds NSEA and the dates CDTPRO,
+// CDTSOU, CDA, CDTA, CDCA (CHARACTER(14)); then U10, UDIR, TAUW, FL3 and,
+// when their dates are not blank, DEPTH and U with V (one record).  Without
+// the spatial decomposition (L_DECOMP false) file position p holds model
+// point IJ2NEWIJ(p) (:198-211, :540-559).
+constexpr size_t kRestartChunkFloats = size_t(8) << 20;  // 32 MiB staging per copy
+
+bool blank14(const char* c) {
+  for (int i = 0; i < 14; ++i) if (c[i] != ' ' && c[i] != 0) return false;
+  return true;
+}
+
+template <typename R>
+int restart_setup(wamgpu_ctx* ctx, Impl<R>& I, int ld, const int* ij2newij, const int** perm_dev) {
+  if (!ctx->have_grid) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_set_grid first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  if (ctx->own0 != 0 || (ctx->own1 >= 0 && ctx->own1 != ctx->nsea))
+    return fail(ctx, WAMGPU_E_ARG, "restart files hold the whole grid; this context has an owned range");
+  const size_t rec = (size_t)ctx->nsea * ctx->cfg.kl * ctx->cfg.ml * 4;
+  if (rec > (size_t)INT_MAX)
+    return fail(ctx, WAMGPU_E_ARG, "spectrum record of " + std::to_string(rec) + " bytes exceeds the 2 GiB of one "
+                                   "unformatted record");
+  *perm_dev = nullptr;
+  if (ij2newij) {
+    std::vector<char> seen(ctx->nsea + 1, 0);
+    for (int p = 0; p < ctx->nsea; ++p) {
+      const int q = ij2newij[p];
+      if (q < 1 || q > ctx->nsea || seen[q]) return fail(ctx, WAMGPU_E_ARG, "IJ2NEWIJ is not a permutation of 1..NSEA");
+      seen[q] = 1;
+    }
+    std::vector<int> v(ij2newij, ij2newij + ctx->nsea);
+    CK(upload(I.rst_perm, v, ctx->stream), "upload IJ2NEWIJ");
+    *perm_dev = I.rst_perm.template as<int>();
+  }
+  CK(I.rst_stage.ensure(kRestartChunkFloats * 4), "alloc restart staging");
+  return WAMGPU_OK;
+}
+
+template <typename R>
+int restart_write_t(wamgpu_ctx* ctx, Impl<R>& I, const char* path, const void* fl3, int ld, const void* u10,
+                    const void* udir, const void* tauw, const void* depth, const void* cu, const void* cv,
+                    const wamgpu_restart_dates* dates, const int* ij2newij) {
+  if (!path || !fl3 || !u10 || !udir || !tauw || !dates) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  const bool has_d = !blank14(dates->cdta), has_c = !blank14(dates->cdca);
+  if ((has_d && !depth) || (has_c && (!cu || !cv)))
+    return fail(ctx, WAMGPU_E_ARG, "CDTA / CDCA set without the depth / current fields");
+  const int* perm = nullptr;
+  int rc = restart_setup(ctx, I, ld, ij2newij, &perm);
+  if (rc) return rc;
+  const int n = ctx->nsea;
+  cudaStream_t s = ctx->stream;
+  CK(cudaStreamSynchronize(s), "restart: pending work");
+  float* host = nullptr;
+  CK(cudaMallocHost(&host, kRestartChunkFloats * 4), "restart: pinned staging");
+  std::unique_ptr<float, cudaError_t (*)(void*)> hold(host, cudaFreeHost);
+  std::unique_ptr<FILE, int (*)(FILE*)> f(std::fopen(path, "wb"), std::fclose);
+  if (!f) return fail(ctx, WAMGPU_E_ARG, std::string("cannot open ") + path + " for writing");
+  auto raw = [&](const void* p, size_t bytes) { return std::fwrite(p, 1, bytes, f.get()) == bytes; };
+  auto marker = [&](size_t bytes) { const int32_t m = (int32_t)bytes; return raw(&m, 4); };
+  // rows of a device array, gathered into file order in chunks
+  auto rows = [&](const void* src, size_t sld, int nrows) -> int {
+    const int per = (int)std::max<size_t>(1, kRestartChunkFloats / (size_t)n);
+    for (int b0 = 0; b0 < nrows; b0 += per) {
+      const int nb = std::min(per, nrows - b0);
+      CK(launch_restart_gather<R>((const R*)src, sld, n, perm, b0, nb, I.rst_stage.template as<float>(), s),
+         "restart gather");
+      CK(cudaMemcpyAsync(host, I.rst_stage.p, (size_t)n * nb * 4, cudaMemcpyDeviceToHost, s), "restart D2H");
+      CK(cudaStreamSynchronize(s), "restart D2H");
+      if (!raw(host, (size_t)n * nb * 4)) return fail(ctx, WAMGPU_E_ARG, std::string("write error on ") + path);
+    }
+    return WAMGPU_OK;
+  };
+  auto record = [&](std::initializer_list<std::pair<const void*, std::pair<size_t, int>>> parts) -> int {
+    size_t bytes = 0;
+    for (auto& q : parts) bytes += (size_t)n * q.second.second * 4;
+    if (!marker(bytes)) return fail(ctx, WAMGPU_E_ARG, std::string("write error on ") + path);
+    for (auto& q : parts) { const int r = rows(q.first, q.second.first, q.second.second); if (r) return r; }
+    if (!marker(bytes)) return fail(ctx, WAMGPU_E_ARG, std::string("write error on ") + path);
+    return WAMGPU_OK;
+  };
+  {
+    char head[74];
+    const int32_t nn = n;
+    std::memcpy(head, &nn, 4);
+    std::memcpy(head + 4, dates->cdtpro, 14); std::memcpy(head + 18, dates->cdtsou, 14);
+    std::memcpy(head + 32, dates->cda, 14); std::memcpy(head + 46, dates->cdta, 14); std::memcpy(head + 60, dates->cdca, 14);
+    if (!marker(74) || !raw(head, 74) || !marker(74)) return fail(ctx, WAMGPU_E_ARG, std::string("write error on ") + path);
+  }
+  const size_t one = (size_t)n;
+  if ((rc = record({{u10, {one, 1}}}))) return rc;
+  if ((rc = record({{udir, {one, 1}}}))) return rc;
+  if ((rc = record({{tauw, {one, 1}}}))) return rc;
+  if ((rc = record({{fl3, {(size_t)ld, ctx->cfg.kl * ctx->cfg.ml}}}))) return rc;
+  if (has_d && (rc = record({{depth, {one, 1}}}))) return rc;
+  if (has_c && (rc = record({{cu, {one, 1}}, {cv, {one, 1}}}))) return rc;
+  if (std::fflush(f.get()) != 0) return fail(ctx, WAMGPU_E_ARG, std::string("write error on ") + path);
+  return WAMGPU_OK;
+}
+
+template <typename R>
+int restart_read_t(wamgpu_ctx* ctx, Impl<R>& I, const char* path, void* fl3, int ld, void* u10, void* udir, void* tauw,
+                   void* depth, void* cu, void* cv, wamgpu_restart_dates* dates, const int* ij2newij) {
+  if (!path || !fl3 || !u10 || !udir || !tauw) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  const int* perm = nullptr;
+  int rc = restart_setup(ctx, I, ld, ij2newij, &perm);
+  if (rc) return rc;
+  const int n = ctx->nsea;
+  cudaStream_t s = ctx->stream;
+  std::unique_ptr<FILE, int (*)(FILE*)> f(std::fopen(path, "rb"), std::fclose);
+  if (!f) return fail(ctx, WAMGPU_E_ARG, std::string("cannot open ") + path);
+  float* host = nullptr;
+  CK(cudaMallocHost(&host, kRestartChunkFloats * 4), "restart: pinned staging");
+  std::unique_ptr<float, cudaError_t (*)(void*)> hold(host, cudaFreeHost);
+  auto raw = [&](void* p, size_t bytes) { return std::fread(p, 1, bytes, f.get()) == bytes; };
+  auto bad = [&](const std::string& what) { return fail(ctx, WAMGPU_E_ARG, std::string("restart file ") + path + ": " + what); };
+  auto marker = [&](size_t want) -> bool { int32_t m = -1; return raw(&m, 4) && (size_t)m == want; };
+  auto rows = [&](void* dst, size_t dld, int nrows) -> int {
+    const int per = (int)std::max<size_t>(1, kRestartChunkFloats / (size_t)n);
+    for (int b0 = 0; b0 < nrows; b0 += per) {
+      const int nb = std::min(per, nrows - b0);
+      if (!raw(host, (size_t)n * nb * 4)) return bad("short record");
+      CK(cudaMemcpyAsync(I.rst_stage.p, host, (size_t)n * nb * 4, cudaMemcpyHostToDevice, s), "restart H2D");
+      CK(launch_restart_scatter<R>(I.rst_stage.template as<float>(), n, perm, b0, nb, (R*)dst, dld, s), "restart scatter");
+      CK(cudaStreamSynchronize(s), "restart H2D");
+    }
+    return WAMGPU_OK;
+  };
+  auto record = [&](std::initializer_list<std::pair<void*, std::pair<size_t, int>>> parts) -> int {
+    size_t bytes = 0;
+    for (auto& q : parts) bytes += (size_t)n * q.second.second * 4;
+    if (!marker(bytes)) return bad("record length differs from the model grid's");
+    for (auto& q : parts) {
+      if (q.first) { const int r = rows(q.first, q.second.first, q.second.second); if (r) return r; }
+      else if (std::fseek(f.get(), (long)((size_t)n * q.second.second * 4), SEEK_CUR) != 0) return bad("short record");
+    }
+    if (!marker(bytes)) return bad("record length differs from the model grid's");
+    return WAMGPU_OK;
+  };
+  char head[74];
+  if (!marker(74) || !raw(head, 74) || !marker(74)) return bad("no header record");
+  int32_t nsea_r;
+  std::memcpy(&nsea_r, head, 4);
+  if (nsea_r != n)
+    return bad("NSEA " + std::to_string(nsea_r) + " in the file, " + std::to_string(n) + " in the model grid");
+  wamgpu_restart_dates dt;
+  std::memcpy(dt.cdtpro, head + 4, 14); std::memcpy(dt.cdtsou, head + 18, 14); std::memcpy(dt.cda, head + 32, 14);
+  std::memcpy(dt.cdta, head + 46, 14); std::memcpy(dt.cdca, head + 60, 14);
+  if (dates) *dates = dt;
+  CK(cudaStreamSynchronize(s), "restart: pending work");
+  const size_t one = (size_t)n;
+  if ((rc = record({{u10, {one, 1}}}))) return rc;
+  if ((rc = record({{udir, {one, 1}}}))) return rc;
+  if ((rc = record({{tauw, {one, 1}}}))) return rc;
+  if ((rc = record({{fl3, {(size_t)ld, ctx->cfg.kl * ctx->cfg.ml}}}))) return rc;
+  if (!blank14(dt.cdta) && (rc = record({{depth, {one, 1}}}))) return rc;
+  if (!blank14(dt.cdca) && (rc = record({{cu, {one, 1}}, {cv, {one, 1}}}))) return rc;
+  return WAMGPU_OK;
+}
+
 template <typename R> std::vector<R> to_r(const float* p, size_t n) {
   std::vector<R> v(n);
   for (size_t i = 0; i < n; ++i) v[i] = R(p[i]);
@@ -1779,6 +2000,34 @@ int wamgpu_output_parameters_dev(wamgpu_ctx* ctx, const void* fl3, int ld, const
   if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   return DISPATCH_CTX(ctx, output_params_t, fl3, ld, u10, udir, tauw, ustar, z0, from, block, block_ld, s);
+}
+
+int wamgpu_restart_write(wamgpu_ctx* ctx, const char* path, const void* fl3, int ld, const void* u10, const void* udir,
+                         const void* tauw, const void* depth, const void* u, const void* v,
+                         const wamgpu_restart_dates* dates, const int* ij2newij) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  return DISPATCH_CTX(ctx, restart_write_t, path, fl3, ld, u10, udir, tauw, depth, u, v, dates, ij2newij);
+}
+
+int wamgpu_restart_read(wamgpu_ctx* ctx, const char* path, void* fl3, int ld, void* u10, void* udir, void* tauw,
+                        void* depth, void* u, void* v, wamgpu_restart_dates* dates, const int* ij2newij) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  return DISPATCH_CTX(ctx, restart_read_t, path, fl3, ld, u10, udir, tauw, depth, u, v, dates, ij2newij);
+}
+
+int wamgpu_set_wind_grid(wamgpu_ctx* ctx, int nx_in, int ny_in, int west_in, int south_in, int dx_in, int dy_in,
+                         int periodic, int equal_grid, int amowep, int amosop, int xdella, const int* zdello,
+                         const int* ifromij) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  return DISPATCH_CTX(ctx, set_wind_grid_t, nx_in, ny_in, west_in, south_in, dx_in, dy_in, periodic, equal_grid, amowep,
+                      amosop, xdella, zdello, ifromij);
+}
+
+int wamgpu_wind_dev(wamgpu_ctx* ctx, const void* u_in, const void* v_in, int code_in, void* u10, void* udir,
+                    void* stream) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, wind_dev_t, u_in, v_in, code_in, u10, udir, s);
 }
 
 int wamgpu_put_points_dev(wamgpu_ctx* ctx, void* data, int ld, int nrows, const int* points, int n, double value,

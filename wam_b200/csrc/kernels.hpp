@@ -119,6 +119,21 @@ template <typename R> struct OutArgs {
 template <typename R>
 cudaError_t launch_put_points(R* data, size_t ld, int nrows, const int* points, int n, int lo, int hi, R value,
                               cudaStream_t s);
+// WAM_WIND: input wind components u_in, v_in [(i-1) + nx_in*(k-1)] to U10
+// and UDIR of n sea points; tab holds I1, I2, K1, K2 (1-based, 4 blocks of
+// n), w the weights DI, DK (2 blocks of n); equal != 0 copies point (I1, K1).
+template <typename R>
+cudaError_t launch_wind(const R* u_in, const R* v_in, int nx_in, int n, const int* tab, const R* w, int equal,
+                        int code_in, R* us, R* ds, cudaStream_t s);
+// Restart records (REAL, file order: position p holds point perm[p], 1-based,
+// or p without perm) from rows b0..b0+nb-1 of a device array with the sea
+// point fastest, and back.
+template <typename R>
+cudaError_t launch_restart_gather(const R* src, size_t ld, int nsea, const int* perm, int b0, int nb, float* out,
+                                  cudaStream_t s);
+template <typename R>
+cudaError_t launch_restart_scatter(const float* in, int nsea, const int* perm, int b0, int nb, R* dst, size_t ld,
+                                   cudaStream_t s);
 // ustar_max: device word for MAXVAL(USTAR), or null to skip the AIRSEA check.
 template <typename R> cudaError_t launch_output(const OutArgs<R>& a, unsigned long long* ustar_max, cudaStream_t s);
 template <typename R> cudaError_t launch_implsch_adj(const DevTables<R>& T, const DerivArgs<R>& a, cudaStream_t s);

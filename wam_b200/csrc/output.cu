@@ -180,6 +180,103 @@ cudaError_t launch_put_points(R* data, size_t ld, int nrows, const int* points, 
 template cudaError_t launch_put_points<float>(float*, size_t, int, const int*, int, int, int, float, cudaStream_t);
 template cudaError_t launch_put_points<double>(double*, size_t, int, const int*, int, int, int, double, cudaStream_t);
 
+// WAM_WIND (wam_wind_module.f90:1063-1216): one input wind field to the sea
+// points.  Bilinear interpolation with the tables of INTERPOLATION_TO_GRID
+// (:1224-1377; a plain copy on the model's own grid, EQUAL_GRID), then speed
+// and direction ATAN2(U,V) in [0, 2*pi), the friction-velocity (CODE_IN 1)
+// or surface-stress (2) input turned into U10 through a Charnock drag, and
+// U10 >= 2 m/s.  One thread per sea point; the unit rounds every operation
+// separately, as the reference does.
+template <typename R>
+__global__ void __launch_bounds__(256) wind_kernel(const R* __restrict__ u_in, const R* __restrict__ v_in, int nx_in,
+                                                   int n, const int* __restrict__ tab, const R* __restrict__ w, int equal,
+                                                   int code_in, R* __restrict__ us, R* __restrict__ ds) {
+  const int ij = blockIdx.x * blockDim.x + threadIdx.x;
+  if (ij >= n) return;
+  const int i1 = tab[ij] - 1, i2 = tab[ij + n] - 1, k1 = tab[ij + 2 * n] - 1, k2 = tab[ij + 3 * n] - 1;
+  auto at = [&](const R* f, int i, int k) { return __ldg(&f[i + (size_t)nx_in * k]); };
+  R uu, vv;
+  if (equal) {
+    uu = at(u_in, i1, k1);
+    vv = at(v_in, i1, k1);
+  } else {
+    const R di = w[ij], dk = w[ij + n];
+    uu = (at(u_in, i1, k1) * (R(1.) - di) + at(u_in, i2, k1) * di) * (R(1.) - dk) +
+         (at(u_in, i1, k2) * (R(1.) - di) + at(u_in, i2, k2) * di) * dk;
+    vv = (at(v_in, i1, k1) * (R(1.) - di) + at(v_in, i2, k1) * di) * (R(1.) - dk) +
+         (at(v_in, i1, k2) * (R(1.) - di) + at(v_in, i2, k2) * di) * dk;
+  }
+  R s = sqrt(uu * uu + vv * vv);
+  R d = (s != R(0.)) ? atan2(uu, vv) : R(0.);
+  if (d < R(0.)) d = d + Phys<R>::ZPI;
+  if (code_in == 1 || code_in == 2) {
+    const R alphach = R(0.0185);
+    const R ust = code_in == 1 ? dmax(R(0.01), s) : dmax(R(0.01), sqrt(s / Phys<R>::ROAIR));
+    const R z0 = alphach / Phys<R>::G * (ust * ust);
+    const R cd = Phys<R>::XKAPPA / log(R(10.) / z0);
+    s = ust / cd;
+  }
+  us[ij] = dmax(s, R(2.0));
+  ds[ij] = d;
+}
+
+template <typename R>
+cudaError_t launch_wind(const R* u_in, const R* v_in, int nx_in, int n, const int* tab, const R* w, int equal,
+                        int code_in, R* us, R* ds, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  wind_kernel<R><<<(n + 255) / 256, 256, 0, s>>>(u_in, v_in, nx_in, n, tab, w, equal, code_in, us, ds);
+  return cudaGetLastError();
+}
+template cudaError_t launch_wind<float>(const float*, const float*, int, int, const int*, const float*, int, int, float*,
+                                        float*, cudaStream_t);
+template cudaError_t launch_wind<double>(const double*, const double*, int, int, const int*, const double*, int, int,
+                                         double*, double*, cudaStream_t);
+
+// Restart records: rows b0..b0+nb-1 of a sea-point-fastest device array
+// gathered into REAL file order (file position p holds model point perm[p],
+// 1-based; perm null = the identity) and scattered back.
+template <typename R>
+__global__ void __launch_bounds__(256) restart_gather_kernel(const R* __restrict__ src, size_t ld, int nsea,
+                                                             const int* __restrict__ perm, int b0, int nb,
+                                                             float* __restrict__ out) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)nsea * nb) return;
+  const int p = (int)(t % nsea), b = b0 + (int)(t / nsea);
+  const int ij = perm ? perm[p] - 1 : p;
+  out[t] = (float)src[ij + ld * b];
+}
+template <typename R>
+__global__ void __launch_bounds__(256) restart_scatter_kernel(const float* __restrict__ in, int nsea,
+                                                              const int* __restrict__ perm, int b0, int nb,
+                                                              R* __restrict__ dst, size_t ld) {
+  const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (t >= (size_t)nsea * nb) return;
+  const int p = (int)(t % nsea), b = b0 + (int)(t / nsea);
+  const int ij = perm ? perm[p] - 1 : p;
+  dst[ij + ld * b] = (R)in[t];
+}
+template <typename R>
+cudaError_t launch_restart_gather(const R* src, size_t ld, int nsea, const int* perm, int b0, int nb, float* out,
+                                  cudaStream_t s) {
+  const size_t n = (size_t)nsea * nb;
+  if (n == 0) return cudaSuccess;
+  restart_gather_kernel<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(src, ld, nsea, perm, b0, nb, out);
+  return cudaGetLastError();
+}
+template <typename R>
+cudaError_t launch_restart_scatter(const float* in, int nsea, const int* perm, int b0, int nb, R* dst, size_t ld,
+                                   cudaStream_t s) {
+  const size_t n = (size_t)nsea * nb;
+  if (n == 0) return cudaSuccess;
+  restart_scatter_kernel<R><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, nsea, perm, b0, nb, dst, ld);
+  return cudaGetLastError();
+}
+template cudaError_t launch_restart_gather<float>(const float*, size_t, int, const int*, int, int, float*, cudaStream_t);
+template cudaError_t launch_restart_gather<double>(const double*, size_t, int, const int*, int, int, float*, cudaStream_t);
+template cudaError_t launch_restart_scatter<float>(const float*, int, const int*, int, int, float*, size_t, cudaStream_t);
+template cudaError_t launch_restart_scatter<double>(const float*, int, const int*, int, int, double*, size_t,
+                                                    cudaStream_t);
+
 template <typename R> size_t output_smem_bytes(int KL, int ML) { return (size_t)kOutThreads * (KL + ML) * sizeof(R); }
 
 template <typename R> cudaError_t launch_output(const OutArgs<R>& a, unsigned long long* ustar_max, cudaStream_t s) {

@@ -50,6 +50,65 @@ __global__ void __launch_bounds__(128) propags_kernel(const __grid_constant__ Pr
   propags_point<R, VAR, RED, REFRD>(A, f1, ld1, f3, ld3, i, m0 + blockIdx.y);
 }
 
+// Two frequencies m, m+1 of one sea point per thread, for the variants
+// without currents (a sub-step of plane m then reads plane m only).  The
+// direction-dependent work that does not depend on the frequency (direction
+// tables, upwind neighbour choice and addresses, |SIN|, |COS| and the metric
+// products, the depth-gradient part of THDD) is the same expression for both
+// frequencies and is formed once; every coefficient still gets the
+// reference's operations, so the result equals the one-frequency kernel's.
+// With mb beyond the planes (odd count) the second frequency repeats the
+// first and is not stored.
+template <typename R, int VAR, bool RED, bool REFRD>
+__device__ __forceinline__ void propags_point2(const PropArgs<R>& A, const R* __restrict__ f1, int ld1,
+                                               R* __restrict__ f3, int ld3, int i, int m, bool two) {
+  using S = Site<R, VAR, RED, REFRD>;
+  static_assert(!S::CUR, "two-frequency PROPAGS is for the variants without currents");
+  const int mb = two ? m + 1 : m;
+  const S sa(A, i, m), sb(A, i, mb);
+  const int KL = A.KL;
+  const size_t plane = (size_t)ld1 * KL;
+  const R* fa = f1 + plane * m;
+  const R* fb = f1 + plane * mb;
+  const bool theta = REFRD || S::SPH;
+  auto at = [&](const R* fm, int p1, int k) -> R { return p1 == 0 ? R(0) : __ldg(&fm[(p1 - 1) + (size_t)ld1 * k]); };
+  R fkm_a = at(fa, i + 1, KL - 1), fk_a = at(fa, i + 1, 0);
+  R fkm_b = at(fb, i + 1, KL - 1), fk_b = at(fb, i + 1, 0);
+  R* outa = f3 + i + (size_t)ld3 * KL * m;
+  R* outb = f3 + i + (size_t)ld3 * KL * mb;
+  typename S::Win Wa = sa.window(0), Wb = sb.window(0);
+  for (int k = 0; k < KL; ++k) {
+    const int kp = (k + 1 == KL) ? 0 : k + 1;
+    const R fkp_a = at(fa, i + 1, kp), fkp_b = at(fb, i + 1, kp);
+    const Coefs<R> ca = sa.coef_w(Wa), cb = sb.coef_w(Wb);
+    const bool ic0 = Wa.cs >= R(0.), is0 = Wa.sn >= R(0.);
+    const int pl = ic0 ? sa.s0 : sa.n0, pw = is0 ? sa.w0 : sa.e0;
+    R va = ca.sum * fk_a + ca.lat11 * at(fa, pl, k) + ca.lon1 * at(fa, pw, k);
+    R vb = cb.sum * fk_b + cb.lat11 * at(fb, pl, k) + cb.lon1 * at(fb, pw, k);
+    if (theta) { va = va + ca.th1 * fkp_a + ca.th2 * fkm_a; vb = vb + cb.th1 * fkp_b + cb.th2 * fkm_b; }
+    if (RED) {
+      const int p2 = ic0 ? sa.s1 : sa.n1;
+      va = va + ca.lat12 * at(fa, p2, k);
+      vb = vb + cb.lat12 * at(fb, p2, k);
+    }
+    outa[(size_t)ld3 * k] = va;
+    if (two) outb[(size_t)ld3 * k] = vb;
+    fkm_a = fk_a; fk_a = fkp_a; fkm_b = fk_b; fk_b = fkp_b;
+    sa.advance(Wa, k);
+    sb.advance(Wb, k);
+  }
+}
+
+// Frequencies m0 + 2*blockIdx.y and the next one (if below m0 + mcount).
+template <typename R, int VAR, bool RED, bool REFRD>
+__global__ void __launch_bounds__(128) propags2_kernel(const __grid_constant__ PropArgs<R> A, const R* __restrict__ f1,
+                                                       int ld1, R* __restrict__ f3, int ld3, int m0, int mcount) {
+  const int i = A.i0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.i1) return;
+  const int q = 2 * blockIdx.y;
+  propags_point2<R, VAR, RED, REFRD>(A, f1, ld1, f3, ld3, i, m0 + q, q + 1 < mcount);
+}
+
 // Batched form: every member of an ensemble (one coefficient family) in one
 // launch of BS-point CTAs.  CTA b belongs to member g with first[g] <= b <
 // first[g + 1] and covers frequency m and points ib*BS .. of that member; the
@@ -193,6 +252,13 @@ cudaError_t dispatch(const PropArgs<R>& A, Args&&... args) {
 
 template <typename R, int V, bool RED, bool RD> struct PropLaunch {
   static cudaError_t run(const PropArgs<R>& A, const R* f1, int ld1, R* f3, int ld3, int m0, int mcount, cudaStream_t s) {
+    if constexpr (!var_current(V)) {
+      if (mcount >= 2) {
+        dim3 grid((A.i1 - A.i0 + 127) / 128, (mcount + 1) / 2);
+        propags2_kernel<R, V, RED, RD><<<grid, 128, 0, s>>>(A, f1, ld1, f3, ld3, m0, mcount);
+        return cudaGetLastError();
+      }
+    }
     dim3 grid((A.i1 - A.i0 + 127) / 128, mcount);
     propags_kernel<R, V, RED, RD><<<grid, 128, 0, s>>>(A, f1, ld1, f3, ld3, m0);
     return cudaGetLastError();

@@ -20,7 +20,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import WamgpuConfig, WamgpuError, load
+from ._lib import RestartDates, WamgpuConfig, WamgpuError, load
 
 _PF = ctypes.POINTER(ctypes.c_float)
 OUT_NPARAM = 40  # WAMGPU_OUT_NPARAM
@@ -235,6 +235,47 @@ class WamModel:
                                                         int(bool(from_)), p(block), block.shape[-1], s),
                     "output_parameters_dev")
         return block
+
+    def restart_write(self, path, fl3, u10, udir, tauw, dates, depth=None, u=None, v=None, ij2newij=None, ld=None):
+        """SAVE_RESTART_FILE from device tensors; dates: dict of CDTPRO, CDTSOU,
+        CDA, CDTA, CDCA strings (blank = not stored)."""
+        d = RestartDates(**{k.lower(): str(dates.get(k, "")).ljust(14)[:14].encode() for k in
+                            ("CDTPRO", "CDTSOU", "CDA", "CDTA", "CDCA")})
+        ld = fl3.shape[-1] if ld is None else ld
+        p = lambda t: None if t is None else t.data_ptr()
+        perm = None if ij2newij is None else np.ascontiguousarray(ij2newij, np.int32)
+        self._check(self.L.wamgpu_restart_write(self.h, str(path).encode(), p(fl3), ld, p(u10), p(udir), p(tauw),
+                                                p(depth), p(u), p(v), ctypes.byref(d),
+                                                None if perm is None else _ip(perm)), "restart_write")
+
+    def restart_read(self, path, fl3, u10, udir, tauw, depth=None, u=None, v=None, ij2newij=None, ld=None):
+        """CONNECT_RESTART into device tensors; returns the dates."""
+        d = RestartDates()
+        ld = fl3.shape[-1] if ld is None else ld
+        p = lambda t: None if t is None else t.data_ptr()
+        perm = None if ij2newij is None else np.ascontiguousarray(ij2newij, np.int32)
+        self._check(self.L.wamgpu_restart_read(self.h, str(path).encode(), p(fl3), ld, p(u10), p(udir), p(tauw),
+                                               p(depth), p(u), p(v), ctypes.byref(d),
+                                               None if perm is None else _ip(perm)), "restart_read")
+        return {k.upper(): getattr(d, k).decode() for k in ("cdtpro", "cdtsou", "cda", "cdta", "cdca")}
+
+    def set_wind_grid(self, grid, nx_in, ny_in, west_in, south_in, dx_in, dy_in, periodic=False, equal_grid=False):
+        """Interpolation tables from a wind input grid (integer 1/100 arc-second
+        units) to the sea points of `grid` (wamgpu_set_wind_grid)."""
+        ny = int(grid["ny"])
+        zdello = np.ascontiguousarray(np.broadcast_to(np.asarray(grid.get("zdello", grid["xdello"])), (ny,)), np.int32)
+        ifromij = np.ascontiguousarray(grid["ixlg"], np.int32)
+        self._check(self.L.wamgpu_set_wind_grid(self.h, int(nx_in), int(ny_in), int(west_in), int(south_in), int(dx_in),
+                                                int(dy_in), int(bool(periodic)), int(bool(equal_grid)),
+                                                int(grid["amowep"]), int(grid["amosop"]), int(grid["xdella"]),
+                                                _ip(zdello), _ip(ifromij)), "set_wind_grid")
+
+    def wind_dev(self, u_in, v_in, u10, udir, code_in=3, stream=None):
+        """WAM_WIND on the device: input components (tensors (ny_in, nx_in),
+        longitude fastest) to U10 and UDIR of every sea point."""
+        s = None if stream is None else ctypes.c_void_p(stream)
+        self._check(self.L.wamgpu_wind_dev(self.h, u_in.data_ptr(), v_in.data_ptr(), int(code_in), u10.data_ptr(),
+                                           udir.data_ptr(), s), "wind_dev")
 
     def put_points_dev(self, data, points, value=0.0, ld=None, stream=None):
         """PUT_ICE / PUT_DRY on a device tensor shaped (..., ld) with the sea
