@@ -1,6 +1,6 @@
-// Adjoint (one sea point per warp, work arrays in shared memory) and
-// tangent-linear (one sea point per thread, work arrays in global memory with
-// the sea point fastest) kernels of IMPLSCH (ST4).
+// Adjoint (one sea point per warp, work arrays in shared memory; ST4 and ST6)
+// and tangent-linear (one sea point per thread, work arrays in global memory
+// with the sea point fastest; ST4) kernels of IMPLSCH.
 #include <mutex>
 #include "adjoint_warp.cuh"
 #include "kernels.hpp"
@@ -85,9 +85,14 @@ __global__ void __launch_bounds__(P * 32) implsch_adj_kernel(const __grid_consta
     AdjW<R> g(src, A, pin, a.fl3_in + ij, ld, reinterpret_cast<R*>(base + loff),
               reinterpret_cast<R*>(base + adjw_at_offset<R>(LD, ML, T.scr)), base + adjw_ll1_offset<R>(LD, ML, T.scr));
     const R tw0 = a.tauw_in[ij], ltw = a.lam_tauw[ij];
-    g.forward(tw0);
     R lT0 = 0, lU = 0;
-    g.reverse(tw0, ltw, lT0, lU);
+    if (T.iphys == 2) {
+      g.forward6();
+      g.reverse6(ltw, lT0, lU);
+    } else {
+      g.forward(tw0);
+      g.reverse(tw0, ltw, lT0, lU);
+    }
     if (lane == 0 && ij0 + warp < a.nsea) { a.lam_tauw[ij] = lT0; a.lam_u10[ij] = lU; }
   }
   __syncthreads();

@@ -168,7 +168,7 @@ template <typename R> struct AdjW {
     s.template ordered_sums<4>(rows, init, ml, sum);
     const R e = dmax(sum[0], R(1.0E-12)), fm = e / dmax(sum[1], R(1.0E-12));
     const R ew = dmax(sum[2], R(1.0E-12)), fmw = ew / dmax(sum[3], R(1.0E-12));
-    return s.frcutindex(fm, fmw, us2);
+    return T.iphys == 2 ? s.frcutindex_st6(fm, us2) : s.frcutindex(fm, fmw, us2);
   }
 
   // ---- reverse sweep ---------------------------------------------------------------
@@ -853,6 +853,402 @@ template <typename R> struct AdjW {
     const int kl = KL(), ld = w.ld;
     s.for_bins(ML(), [&](int m, int k) { w.F[k + ld * m] = __ldg(&F0g[ldg * (size_t)(k + kl * m)]); });
     __syncwarp();
+  }
+
+  // ---- ST6 (IPHYS = 2) ---------------------------------------------------------
+  // Record of the LFACTOR iteration, at the end of the tape rows.
+  __device__ R* lfrec() const { return AT + 14 * ML() - 16; }
+  // dUSTAR/dU10 of W3FLX4 (:5372-5443); Z0 does not enter the step.
+  __device__ R w3flx4_dus(R U) const {
+    if (U >= R(50.33)) return R(0);
+    const R cd = T.CDFAC * (R(8.058) + R(0.967) * U - R(0.016) * (U * U)) * R(1E-4);
+    const R dcd = T.CDFAC * (R(0.967) - R(0.032) * U) * R(1E-4);
+    const R sq = dsqrt(cd);
+    return sq + U * dcd / (R(2) * sq);
+  }
+
+  // Forward ST6 step with recording (the forward kernel's statement order).
+  __device__ void forward6() {
+    const int ml = ML(), ld = w.ld;
+    ju = min(300, max((int)lround((double)(s.U10 / T.DELU)), 1));
+    R emean, emeanws;
+    akmean = 0;
+    const bool need_ak = T.shallow && T.isnonlin == 0;
+    s.integrals(nullptr, emean, fmean, need_ak ? &akmean : nullptr);
+    s.wavnu2();
+    s.w3flx4(us1, z01);
+    s.lfrec = lfrec();
+    int nit = 0;
+    s.sinput_st6(us1, tauw1, nit);
+    s.lfrec = nullptr;
+    phase();
+    s.for_bins(ml, [&](int m, int k) { LL1[k + ld * m] = w.LL[k + ld * m]; });
+    __syncwarp();
+    s.integrals(w.LL, emeanws, fmeanws, nullptr);
+    mij = s.frcutindex_st6(fmean, us1);
+    us2 = us1; z02 = z01;
+    s.imphftail(mij);  // F = F1 from here on
+    phase();
+    s.sdissip_st6();
+    phase();
+    s.snonlin(akmean);
+    phase();
+    fmx = dmax(fmeanws, fmean);
+    update_rows();
+    mij2 = cutoff_after_update();
+  }
+
+  // SDISSIP_ST6^T and W3SWL6^T on F1 (:4929-5252): SL += (T12 + AB) F and
+  // FL += T12 + AB per frequency row.  T12 = -(T1 + 7E-5 P) with P the prefix
+  // sum over frequency (transposed: a suffix sum), AB = -2/3 b1 sig sqrt(BN)
+  // with BN = sig WN^3 (row sum / narrowness sum) = sig WN^3 max_k a_k and b1
+  // from the frequency-weighted total and the frozen MAXLOC row.
+  __device__ void sdissip_st6_adj() const {
+    const int kl = KL(), nk = ML(), ld = w.ld;
+    s.wavnu2();
+    const R* WN = w.t(0); const R* CG = w.t(1);
+    R *T12 = w.t(2), *ABV = w.t(3), *LR = w.t(4), *LS = w.t(5), *LQ = w.t(6), *LADF = w.t(7);
+    R *NEX = AT, *ADF = AT + nk, *SA = AT + 2 * nk, *KX = AT + 3 * nk, *BN = AT + 4 * nk, *ET = AT + 5 * nk;
+    const R bnt = R(0.035) * R(0.035);
+    const R xfac = (R(1.0) - R(1.0) / P_::CO) / (P_::CO - R(1.0) / P_::CO);
+    R ps = 0, amax = -R(1);
+    int imax = 0;
+    for (int m = lane; m < nk; m += 32) {
+      const R sig = P_::ZPI * S.FR[m];
+      const R* fm = w.F + ld * m;
+      const R2* lv = w.SF + ld * m;
+      const R et = (P_::ZPI * bnt) / (CG[m] * (WN[m] * WN[m] * WN[m]));
+      R sm = 0, lr = 0;
+      for (int k = 0; k < kl; ++k) { sm = sm + fm[k]; lr = lr + (lv[k].x * fm[k] + lv[k].y); }
+      LR[m] = lr;
+      const R nex = dmax(R(0.0), sm * T.DELTH - et) / et;
+      const R nex4 = (nex * nex) * (nex * nex);
+      NEX[m] = nex; ET[m] = et;
+      T12[m] = R(4.75E-6) * S.FR[m] * nex4;  // T1 until the scan
+      const R dfii = (m > 0 && m < nk - 1) ? S.DF[m] * xfac : S.DF[m];
+      ADF[m] = nex4 * dfii;
+      const R cgs = CG[m] / (P_::ZPI * sig);
+      R sa = 0, mx = 0;
+      int kx = 0;
+      for (int k = 0; k < kl; ++k) {
+        const R a = fm[k] * cgs;
+        sa = sa + a;
+        if (k == 0 || mx < a) { mx = a; kx = k; }
+      }
+      R s2 = 0;
+      if (mx < R(1.0E-34)) { s2 = R(kl); kx = -1; }
+      else { const R rmx = R(1.) / mx; for (int k = 0; k < kl; ++k) s2 = s2 + (fm[k] * cgs) * rmx; }
+      const R anar = R(1.0) / (s2 * T.DELTH);
+      SA[m] = sa; KX[m] = R(kx);
+      BN[m] = anar * (sa * sig * T.DELTH) * (WN[m] * WN[m] * WN[m]);
+      ps = ps + sa * (P_::ZPI * S.DFIM[m] * sig) / CG[m];
+      if (sa > amax) { amax = sa; imax = m; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const R oa = __shfl_xor_sync(0xffffffffu, amax, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, imax, o);
+      if (oa > amax || (oa == amax && oi < imax)) { amax = oa; imax = oi; }
+    }
+    ps = warp_sum(ps);
+    __syncwarp();
+    const R b1 = R(0.0041) * (R(2.) * dsqrt(ps) * WN[imax]);
+    // T2 prefix sum as the forward forms it, then the suffix sum of the
+    // adjoints of P
+    R carry = 0;
+    for (int base = 0; base < nk; base += 32) {
+      const int m = base + lane;
+      R v = (m < nk) ? ADF[m] : R(0);
+      for (int o = 1; o < 32; o <<= 1) { const R u = __shfl_up_sync(0xffffffffu, v, o); if (lane >= o) v = v + u; }
+      v = v + carry;
+      if (m < nk) {
+        const R t1 = T12[m], p = R(7.00E-5) * v;
+        T12[m] = R(-1.0) * (dmax(R(0.0), t1) + dmax(R(0.0), p));
+        LADF[m] = (R(0.0) < p) ? -R(7.00E-5) * LR[m] : R(0);  // adjoint of P(m), before the suffix sum
+      }
+      carry = __shfl_sync(0xffffffffu, v, 31);
+    }
+    __syncwarp();
+    R lb1 = 0;
+    for (int m = lane; m < nk; m += 32) {
+      const R sig = P_::ZPI * S.FR[m];
+      R ab = 0;
+      if (SA[m] > R(1.E-30)) {
+        const R sb = dsqrt(BN[m]);
+        ab = -(R(2.) / R(3.) * b1 * sig * sb);
+        lb1 = lb1 + LR[m] * (-(R(2.) / R(3.)) * sig * sb);
+        const R lbn = sb > R(0) ? LR[m] * (-(R(2.) / R(3.)) * b1 * sig) / (R(2) * sb) : R(0);
+        LQ[m] = lbn * sig * (WN[m] * WN[m] * WN[m]);  // adjoint of sa/s2 (= max_k a_k)
+      } else LQ[m] = R(0);
+      ABV[m] = ab;
+    }
+    lb1 = warp_sum(lb1);
+    const R lps = ps > R(0) ? lb1 * R(0.0041) * WN[imax] / dsqrt(ps) : R(0);
+    __syncwarp();
+    // suffix sums of the P adjoints (chunks from the top)
+    R scarry = 0;
+    for (int top = ((nk - 1) / 32) * 32; top >= 0; top -= 32) {
+      const int m = top + lane;
+      R v = (m < nk) ? LADF[m] : R(0);
+      for (int o = 1; o < 32; o <<= 1) { const R u = __shfl_down_sync(0xffffffffu, v, o); if (lane + o < 32) v = v + u; }
+      v = v + scarry;
+      scarry = __shfl_sync(0xffffffffu, v, 0);
+      __syncwarp();
+      if (m < nk) LADF[m] = v;
+    }
+    __syncwarp();
+    for (int m = lane; m < nk; m += 32) {
+      const R sig = P_::ZPI * S.FR[m];
+      const R dfii = (m > 0 && m < nk - 1) ? S.DF[m] * xfac : S.DF[m];
+      const R lt1 = -LR[m];
+      const R lnex4 = lt1 * R(4.75E-6) * S.FR[m] + LADF[m] * dfii;
+      const R nex = NEX[m];
+      LS[m] = nex > R(0) ? lnex4 * R(4) * (nex * nex * nex) * T.DELTH / ET[m] : R(0);
+      // adjoint of the row sum sa: the frequency weights of b1, and the
+      // narrowness factor when the row has no maximum
+      R lsa = lps * (P_::ZPI * S.DFIM[m] * sig) / CG[m];
+      if (KX[m] < R(0)) lsa = lsa + LQ[m] / R(kl);
+      SA[m] = lsa;  // reused: adjoint of the row sum
+    }
+    __syncwarp();
+    s.for_bins(nk, [&](int m, int k) {
+      const int b = k + ld * m;
+      const R sig = P_::ZPI * S.FR[m], cgs = CG[m] / (P_::ZPI * sig);
+      R l = w.SF[b].x * (T12[m] + ABV[m]) + LS[m] + cgs * SA[m];
+      if (KX[m] >= R(0) && k == (int)KX[m]) l = l + cgs * LQ[m];
+      LAM[b] = LAM[b] + l;
+    });
+    __syncwarp();
+  }
+
+  // SINPUT_ST6^T with LFACTOR^T (:4465-4925) on F0.  The iteration's
+  // decisions (its count, the sign sequence that fixes every DRTAU, the
+  // MIN(1, EXP) branches, the reduce flag) are those of the forward pass, so
+  // the final RTAU is the first one, ERR/90, times a constant, and LFACT
+  // depends on the spectrum and u* through the first stress sums and through
+  // its exponent.  In: SF = {lambda_SL, lambda_FL}, lTAUW.  Adds to LAM, lus
+  // (adjoint of USTAR) and lU10 (tau_vis).
+  __device__ void sinput_st6_adj(R lTAUW, R& lus, R& lU10) const {
+    const int kl = KL(), nk = ML(), nk10 = T.NK10, ld = w.ld;
+    s.wavnu2();
+    const R* WN = w.t(0); const R* CG = w.t(1);
+    R *SQB = w.t(2), *CI10 = w.t(3), *SDX = w.t(4), *SDY = w.t(5), *LF = w.t(6), *LLF = w.t(7);
+    R *LSDX = AT, *LSDY = AT + nk10, *KXR = AT + 2 * nk10;
+    const R* rec = lfrec();
+    const R USTAR = us1, U10 = s.U10, ROAIRN = s.ROAIRN;
+    const R cu = crcos(s.UDIR), su = crsin(s.UDIR), uproxy = R(32.) * USTAR;
+    const R raw = ROAIRN / P_::ROWATER, gro = P_::G * P_::ROWATER;
+    const int nit = (int)rec[LF_NIT];
+    const bool reduce = rec[LF_REDUCE] != R(0);
+    const R rl = rec[LF_RLAST];
+    // growth rate of bin (m, k) and its parts
+    struct Bin { R proj, w, th, g, d1, d2; bool up; };
+    auto bin = [&](int m, int k) {
+      Bin q;
+      const R sig = P_::ZPI * S.FR[m], sqb = SQB[m];
+      q.proj = rsub(rmul(uproxy * CI10[m], radd(rmul(S.COSTH[k], cu), rmul(S.SINTH[k], su))), R(1.));
+      const R w1 = dmax(R(0.), q.proj), w2 = dmin(R(0.), q.proj);
+      q.up = q.proj > R(0.);
+      q.w = q.up ? w1 * w1 : w2 * w2;
+      q.th = dtanh(rsub(rmul(R(10.) * sqb, q.w), R(11.)));
+      q.g = R(2.8) - (R(1.) + q.th);
+      q.d1 = q.up ? raw * sig * q.g * sqb * q.w : R(0.);
+      q.d2 = q.up ? R(0.) : raw * sig * R(0.09) * q.g * sqb * q.w;
+      return q;
+    };
+    // forward quantities per frequency (lane = m): SQB, CI10, the first
+    // maximum of the row, and the directional stress sums
+    for (int m = lane; m < nk; m += 32) {
+      const R sig = P_::ZPI * S.FR[m];
+      const R* fm = w.F + ld * m;
+      const R zs = P_::ZPI * sig;
+      R sm = 0, mx = 0;
+      int kx = 0;
+      for (int k = 0; k < kl; ++k) {
+        const R a = (fm[k] * CG[m]) / zs;
+        sm = sm + a;
+        if (k == 0 || mx < a) { mx = a; kx = k; }
+      }
+      R s2 = 0;
+      if (mx < R(1.0E-34)) { s2 = R(kl); kx = -1; }
+      else for (int k = 0; k < kl; ++k) s2 = s2 + ((fm[k] * CG[m]) / zs) / mx;
+      const R adensig = sm * sig * T.DELTH, anar = R(1.0) / (s2 * T.DELTH);
+      SQB[m] = dsqrt(anar * adensig * (WN[m] * WN[m] * WN[m]));
+      CI10[m] = WN[m] / sig;
+      KXR[m] = R(kx);
+    }
+    __syncwarp();
+    for (int m = lane; m < nk; m += 32) {
+      const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig;
+      const R* fm = w.F + ld * m;
+      R bx = 0, by = 0;
+      for (int k = 0; k < kl; ++k) {
+        const Bin q = bin(m, k);
+        const R a = (fm[k] * CG[m]) / zs;
+        const R sd = ((q.d1 * a) * sig) / CG[m];
+        bx = radd(bx, rmul(dmax(R(0.), sd), S.COSTH[k]));
+        by = radd(by, rmul(dmax(R(0.), sd), S.SINTH[k]));
+      }
+      SDX[m] = bx * T.DELTH; SDY[m] = by * T.DELTH;
+    }
+    __syncwarp();
+    if (nk < nk10) {
+      const R signk = S.SIG10[nk - 1];
+      for (int i = nk + lane; i < nk10; i += 32) {
+        const R r = (signk / S.SIG10[i]) * (signk / S.SIG10[i]);
+        SDX[i] = SDX[nk - 1] * r; SDY[i] = SDY[nk - 1] * r;
+        CI10[i] = S.SIG10[i] * R(0.101978);
+      }
+    }
+    for (int i = lane; i < nk10; i += 32) {
+      LF[i] = nit > 0 ? dmin(R(1.0), crexp(rmul(rsub(R(1.0), rmul(uproxy, CI10[i])), rl))) : R(1.0);
+      LLF[i] = R(0);
+    }
+    __syncwarp();
+    // 1. the bins: lambda of the total rate, of D1 and D2; LFACT's row adjoint
+    for (int m = 0; m < nk; ++m) {
+      R llf = 0;
+      for (int k = lane; k < kl; k += 32) {
+        const int b = k + ld * m;
+        const Bin q = bin(m, k);
+        const R lfr = reduce ? LF[m] : R(1);
+        const R dtot = q.d1 * lfr - q.d2;
+        const R2 v = w.SF[b];
+        const R f = w.F[b];
+        const R ld_ = v.x * f + v.y;
+        LAM[b] = LAM[b] + v.x * dtot;
+        if (reduce) llf = llf + ld_ * q.d1;
+        w.SF[b] = r2(ld_ * lfr, -ld_);  // {lambda_D1, lambda_D2}
+      }
+      llf = warp_sum(llf);
+      if (lane == 0) LLF[m] = llf;
+    }
+    __syncwarp();
+    // 2. the stress sums: final (after the iteration) and first
+    const R tx = rec[LF_TX], ty = rec[LF_TY], tw = dsqrt(tx * tx + ty * ty);
+    const R ltx = tw > R(0) ? lTAUW * tx / tw : R(0), lty = tw > R(0) ? lTAUW * ty / tw : R(0);
+    const R* DS10 = S.DSII10;
+    R ltx0 = 0, lty0 = 0, lustar = 0;
+    if (nit > 0) {
+      R lrl = 0, luq = 0;
+      for (int i = lane; i < nk10; i += 32) {
+        const R cd = gro * CI10[i] * DS10[i];
+        const R llfi = LLF[i] + cd * (ltx * SDX[i] + lty * SDY[i]);
+        LSDX[i] = cd * ltx * LF[i]; LSDY[i] = cd * lty * LF[i];
+        const R qa = rsub(R(1.0), rmul(uproxy, CI10[i]));
+        if (LF[i] < R(1.0)) {  // EXP branch of MIN(1, EXP(qa*rl))
+          lrl = lrl + llfi * LF[i] * qa;
+          luq = luq + llfi * LF[i] * rl * (-R(32.) * CI10[i]);
+        }
+      }
+      lrl = warp_sum(lrl);
+      lustar = lustar + warp_sum(luq);
+      const R r0 = rec[LF_RTAU0], tau0 = rec[LF_TAU0], tt = rec[LF_TTOT];
+      const R lr0 = r0 != R(0) ? lrl * (rl / r0) : R(0);
+      const R lerr = lr0 / R(90.);
+      const R ltau0 = lerr / tt;
+      R ltt = -lerr * tau0 / (tt * tt);
+      const R tvr = dmax(R(0.0), radd(-rmul(R(5.0E-5), U10), R(1.1E-3))) * (U10 * U10) * ROAIRN;
+      const R tv = dmin(R(0.95) * tt, tvr);
+      const R ax = radd(tv * cu, rec[LF_TX0]), ay = radd(tv * su, rec[LF_TY0]);
+      const R lax = tau0 > R(0) ? ltau0 * ax / tau0 : R(0), lay = tau0 > R(0) ? ltau0 * ay / tau0 : R(0);
+      ltx0 = lax; lty0 = lay;
+      const R ltv = lax * cu + lay * su;
+      if (tvr < R(0.95) * tt) {
+        const R inner = radd(-rmul(R(5.0E-5), U10), R(1.1E-3));
+        if (inner > R(0)) lU10 = lU10 + ltv * (-R(5.0E-5) * (U10 * U10) * ROAIRN + inner * R(2) * U10 * ROAIRN);
+      } else ltt = ltt + R(0.95) * ltv;
+      lustar = lustar + ltt * R(2) * USTAR * ROAIRN;
+    } else {
+      for (int i = lane; i < nk10; i += 32) { LSDX[i] = R(0); LSDY[i] = R(0); }
+      ltx0 = ltx; lty0 = lty;
+    }
+    __syncwarp();
+    for (int i = lane; i < nk10; i += 32) {
+      const R cd = gro * CI10[i] * DS10[i];
+      LSDX[i] = LSDX[i] + cd * ltx0; LSDY[i] = LSDY[i] + cd * lty0;
+    }
+    __syncwarp();
+    if (nk < nk10) {  // the f^-2 extension carries SDX(NK) to 10 Hz
+      const R signk = S.SIG10[nk - 1];
+      R ex = 0, ey = 0;
+      for (int i = nk + lane; i < nk10; i += 32) {
+        const R r = (signk / S.SIG10[i]) * (signk / S.SIG10[i]);
+        ex = ex + LSDX[i] * r; ey = ey + LSDY[i] * r;
+      }
+      ex = warp_sum(ex); ey = warp_sum(ey);
+      if (lane == 0) { LSDX[nk - 1] = LSDX[nk - 1] + ex; LSDY[nk - 1] = LSDY[nk - 1] + ey; }
+    }
+    __syncwarp();
+    // 3. the bins again: stress sums, growth-rate chain, narrowness
+    R luprox = 0;
+    for (int m = 0; m < nk; ++m) {
+      const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig, sqb = SQB[m];
+      const R c1 = raw * sig;
+      R lsqb = 0;
+      for (int k = lane; k < kl; k += 32) {
+        const int b = k + ld * m;
+        const Bin q = bin(m, k);
+        const R f = w.F[b];
+        const R a = (f * CG[m]) / zs;
+        const R sd = ((q.d1 * a) * sig) / CG[m];
+        const R lsd = (R(0.) < sd) ? T.DELTH * (LSDX[m] * S.COSTH[k] + LSDY[m] * S.SINTH[k]) : R(0);
+        const R2 v = w.SF[b];
+        R ld1 = v.x + lsd * a * sig / CG[m];
+        const R la = lsd * q.d1 * sig / CG[m];
+        R lw = 0, lg = 0;
+        if (q.up) {
+          lg = ld1 * c1 * sqb * q.w;
+          lsqb = lsqb + ld1 * c1 * q.g * q.w;
+          lw = ld1 * c1 * q.g * sqb;
+        } else {
+          const R c2 = c1 * R(0.09);
+          lg = v.y * c2 * sqb * q.w;
+          lsqb = lsqb + v.y * c2 * q.g * q.w;
+          lw = v.y * c2 * q.g * sqb;
+        }
+        const R lx = -lg * (R(1) - q.th * q.th);
+        lsqb = lsqb + lx * R(10.) * q.w;
+        lw = lw + lx * R(10.) * sqb;
+        const R lproj = lw * R(2) * q.proj;
+        luprox = luprox + lproj * CI10[m] * radd(rmul(S.COSTH[k], cu), rmul(S.SINTH[k], su));
+        LAM[b] = LAM[b] + la * CG[m] / zs;
+      }
+      lsqb = warp_sum(lsqb);
+      // SQB = sqrt(sig WN^3 q) with q = row sum / narrowness sum (= the row's
+      // first maximum of a, or the row sum / KL for an empty row)
+      const R lq = sqb > R(0) ? lsqb * sig * (WN[m] * WN[m] * WN[m]) / (R(2) * sqb) : R(0);
+      const int kx = (int)KXR[m];
+      for (int k = lane; k < kl; k += 32) {
+        const int b = k + ld * m;
+        if (kx < 0) LAM[b] = LAM[b] + (lq / R(kl)) * CG[m] / zs;
+        else if (k == kx) LAM[b] = LAM[b] + lq * CG[m] / zs;
+      }
+    }
+    lustar = lustar + R(32.) * warp_sum(luprox);
+    lus = lus + lustar;
+    __syncwarp();
+  }
+
+  __device__ void reverse6(R lTAUW, R& lTAUW0, R& lU10) {
+    imphftail_adj(mij2);
+    R lus = 0, lfmx = 0;
+    update_adj(lus, lfmx);
+    phase();
+    const R lak = snonlin_adj();
+    phase();
+    sdissip_st6_adj();
+    phase();
+    imphftail_adj(mij);
+    reload_f0();
+    lU10 = 0;
+    sinput_st6_adj(lTAUW, lus, lU10);
+    phase();
+    R lfmean = 0, lfmeanws = 0;
+    if (fmeanws < fmean) lfmean = lfmx; else lfmeanws = lfmx;
+    integrals_adj(w.F, nullptr, lfmean, lak, T.shallow && T.isnonlin == 0);
+    integrals_adj(w.F, LL1, lfmeanws, R(0), false);
+    lU10 = lU10 + w3flx4_dus(s.U10) * lus;
+    lTAUW0 = R(0);  // ST6 overwrites TAUW: the input does not enter the step
   }
 
   // The whole reverse sweep.  In: LAM = adjoint of the output spectrum, lTAUW =

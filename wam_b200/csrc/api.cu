@@ -738,7 +738,14 @@ template <typename R> adj::ATabs<R> atabs_of(const DevTables<R>& d) {
 
 template <typename R>
 int deriv_setup(wamgpu_ctx* ctx, Impl<R>& I, int ld, bool tl, DerivArgs<R>& a) {
-  if (ctx->cfg.iphys != 1) return fail(ctx, WAMGPU_E_ARG, "IMPLSCH derivatives are implemented for ST4 (IPHYS=1)");
+  if (tl && ctx->cfg.iphys != 1)
+    return fail(ctx, WAMGPU_E_ARG, "the IMPLSCH tangent-linear is implemented for ST4 (IPHYS=1)");
+  if (ctx->cfg.iphys == 2) {
+    // the ST6 adjoint keeps its LFACTOR record and row adjoints in the tape rows
+    const int ml = ctx->cfg.ml, nk10 = I.dt.NK10;
+    if (14 * ml - 16 < std::max(6 * ml, 2 * nk10 + ml))
+      return fail(ctx, WAMGPU_E_ARG, "ST6 adjoint: frequency grid too short for the 10 Hz extension's tape rows");
+  }
   if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first (INDEP)");
   if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
   if (ctx->own0 != 0 || (ctx->own1 >= 0 && ctx->own1 != ctx->nsea))
@@ -748,10 +755,10 @@ int deriv_setup(wamgpu_ctx* ctx, Impl<R>& I, int ld, bool tl, DerivArgs<R>& a) {
   if (ctx->cfg.kl > 64) return fail(ctx, WAMGPU_E_ARG, "IMPLSCH derivatives support at most 64 directions");
   {
     // the adjoint gathers the transposed saturation window per direction
-    // column: INDICESSAT(K, J) must be the rotation K + J - NSDSNTH
+    // column: INDICESSAT(K, J) must be the rotation K + J - NSDSNTH (ST4)
     const TableSet<R>& t = I.tab;
     const int KL = t.KL, ns = t.NSDSNTH;
-    for (int j = 0; j < 2 * ns + 1; ++j)
+    for (int j = 0; ctx->cfg.iphys == 1 && j < 2 * ns + 1; ++j)
       for (int k = 0; k < KL; ++k)
         if (t.INDICESSAT[k + KL * j] - 1 != ((k + j - ns) % KL + KL) % KL)
           return fail(ctx, WAMGPU_E_ARG, "saturation window is not a rotation of the directions");

@@ -126,6 +126,9 @@ template <typename R> struct PointState {
   int JU = 0, MIJ1 = 0, MIJ2 = 0, LFIT = -1;
 };
 
+// Slots of the LFACTOR record (Src::lfrec).
+enum LfRec { LF_TX0 = 0, LF_TY0, LF_TAU0, LF_TTOT, LF_RTAU0, LF_RLAST, LF_NIT, LF_REDUCE, LF_TX, LF_TY, LFREC_N };
+
 template <typename R> struct Src {
   using P_ = Phys<R>;
   const DevTables<R>& T;
@@ -140,6 +143,11 @@ template <typename R> struct Src {
   R* shl = nullptr;
   // ST6: this point's WN and CG rows formed once from the depth (WAVNU2), or null.
   const R* wncg = nullptr;
+  // When set, SINPUT_ST6 records what the adjoint of LFACTOR needs (lane 0
+  // writes LFREC_N values): the first stress sums, |tau|, tau_tot, tau_vis
+  // before its cap, RTAU after the first error and at the last iteration, the
+  // iteration count, the reduce flag and the final stress sums.
+  R* lfrec = nullptr;
   // When set, the step copies its LLWS masks here: bin b of the first
   // SINPUT call's mask at dll[b * dll_ld], of the last one's at
   // dll[(NS + b) * dll_ld] (test diagnostics of the integer decisions).
@@ -867,6 +875,10 @@ template <typename R> struct Src {
     };
     R tau = total();
     R err = (tau - tau_tot) / tau_tot;
+    if (lfrec && lane == 0) {
+      lfrec[LF_TX0] = tauwx; lfrec[LF_TY0] = tauwy; lfrec[LF_TAU0] = tau; lfrec[LF_TTOT] = tau_tot;
+      lfrec[LF_RTAU0] = err / R(90.); lfrec[LF_RLAST] = R(0); lfrec[LF_NIT] = R(0);
+    }
     for (int i = lane; i < nk; i += 32) LF[i] = R(1.0);
     nit = 0;
     if (tau > tau_tot) {
@@ -886,6 +898,7 @@ template <typename R> struct Src {
       }
       for (int it = 0; it < 80; ++it) {
         nit = it + 1;
+        if (lfrec && lane == 0) lfrec[LF_RLAST] = rtau;
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
           const int i = lane + 32 * q;
@@ -920,6 +933,9 @@ template <typename R> struct Src {
       reduce = sum[0] < R(nk);
     }
     TAUW = dsqrt(radd(rmul(tauwx, tauwx), rmul(tauwy, tauwy)));
+    if (lfrec && lane == 0) {
+      lfrec[LF_NIT] = R(nit); lfrec[LF_REDUCE] = reduce ? R(1) : R(0); lfrec[LF_TX] = tauwx; lfrec[LF_TY] = tauwy;
+    }
     for_bins(nk, [&](int m, int k) {
       const int p = k + ld * m;
       const R2 v = w.SF[p];
