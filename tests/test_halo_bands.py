@@ -94,3 +94,83 @@ def test_bands_match_global_propagation_gloo(tmp_path):
     for r, p in enumerate(partition(w.grid, world)):
         got = np.load(tmp_path / f"band{r}.npy")
         assert np.array_equal(got, ref[:, :, p["lo"]:p["hi"]]), r
+
+
+def _counter_rank(rank, world, port, failing, out_dir):
+    import datetime
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=20))
+    try:
+        from wam_b200.halo import global_counter
+        # COUNTER is the largest of the ranks' values; a CHECK_CFL failure on
+        # one rank raises on every rank after the same collective.
+        res = []
+        res.append(str(global_counter(rank + 1)))
+        try:
+            global_counter(2, failed=(rank == failing))
+            res.append("no error")
+        except RuntimeError as e:
+            res.append("raised: " + str(e).split(":")[0])
+        # the group stays usable after the reported failure
+        res.append(str(global_counter(5 - rank)))
+        with open(os.path.join(out_dir, f"counter{rank}.txt"), "w") as f:
+            f.write("\n".join(res))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("failing", [0, 1])
+def test_check_cfl_failure_raises_on_every_rank(tmp_path, failing):
+    import torch.multiprocessing as mp
+    world = 2
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mp.start_processes(_counter_rank, args=(world, port, failing, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    for r in range(world):
+        lines = (tmp_path / f"counter{r}.txt").read_text().splitlines()
+        assert lines == [str(world), "raised: CHECK_CFL failed on a rank", "5"], (r, lines)
+
+
+def _absent_peer_rank(rank, world, port, out_dir):
+    import datetime
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=3))
+    msg = "completed"
+    try:
+        from wam_b200.halo import HaloExchange, partition
+        w = _workload()
+        parts = partition(w.grid, world)
+        p = parts[rank]
+        dist.barrier()
+        if rank == 1:
+            return           # leaves between steps, with nothing in flight
+        t = torch.zeros((w.cfg["ml"], w.cfg["kl"], p["nsup"] - p["ninf"]), dtype=torch.float64)
+        try:
+            HaloExchange(parts, rank)(t)
+        except Exception as e:    # the short process-group timeout ends the exchange
+            msg = "error: " + type(e).__name__
+        with open(os.path.join(out_dir, f"absent{rank}.txt"), "w") as f:
+            f.write(msg)
+    finally:
+        if rank == 0:
+            dist.destroy_process_group()
+
+
+def test_halo_exchange_with_an_absent_rank_ends_in_error(tmp_path):
+    """A rank that leaves between sub-steps: the other rank's next exchange
+    ends with an error from the process group's timeout instead of waiting."""
+    import torch.multiprocessing as mp
+    world = 2
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    mp.start_processes(_absent_peer_rank, args=(world, port, str(tmp_path)), nprocs=world, join=True,
+                       start_method="spawn")
+    assert (tmp_path / "absent0.txt").read_text().startswith("error: ")

@@ -1060,17 +1060,20 @@ template <typename R> struct AdjW {
     for (int m = lane; m < nk; m += 32) {
       const R sig = P_::ZPI * S.FR[m];
       const R* fm = w.F + ld * m;
-      const R zs = P_::ZPI * sig;
+      const R zs = P_::ZPI * sig, yzs = R(1) / zs, cg = CG[m];
       R sm = 0, mx = 0;
       int kx = 0;
       for (int k = 0; k < kl; ++k) {
-        const R a = (fm[k] * CG[m]) / zs;
+        const R a = rdiv(rmul(fm[k], cg), zs, yzs);
         sm = sm + a;
         if (k == 0 || mx < a) { mx = a; kx = k; }
       }
       R s2 = 0;
       if (mx < R(1.0E-34)) { s2 = R(kl); kx = -1; }
-      else for (int k = 0; k < kl; ++k) s2 = s2 + ((fm[k] * CG[m]) / zs) / mx;
+      else {
+        const R ymx = R(1) / mx;
+        for (int k = 0; k < kl; ++k) s2 = s2 + rdiv(rdiv(rmul(fm[k], cg), zs, yzs), mx, ymx);
+      }
       const R adensig = sm * sig * T.DELTH, anar = R(1.0) / (s2 * T.DELTH);
       SQB[m] = dsqrt(anar * adensig * (WN[m] * WN[m] * WN[m]));
       CI10[m] = WN[m] / sig;
@@ -1078,13 +1081,13 @@ template <typename R> struct AdjW {
     }
     __syncwarp();
     for (int m = lane; m < nk; m += 32) {
-      const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig;
+      const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig, yzs = R(1) / zs, cg = CG[m], ycg = R(1) / cg;
       const R* fm = w.F + ld * m;
       R bx = 0, by = 0;
       for (int k = 0; k < kl; ++k) {
         const Bin q = bin(m, k);
-        const R a = (fm[k] * CG[m]) / zs;
-        const R sd = ((q.d1 * a) * sig) / CG[m];
+        const R a = rdiv(rmul(fm[k], cg), zs, yzs);
+        const R sd = rdiv(rmul(rmul(q.d1, a), sig), cg, ycg);
         bx = radd(bx, rmul(dmax(R(0.), sd), S.COSTH[k]));
         by = radd(by, rmul(dmax(R(0.), sd), S.SINTH[k]));
       }
@@ -1183,18 +1186,19 @@ template <typename R> struct AdjW {
     R luprox = 0;
     for (int m = 0; m < nk; ++m) {
       const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig, sqb = SQB[m];
+      const R cg = CG[m], yzs = R(1) / zs, ycg = R(1) / cg, cgzs = cg * yzs, sgcg = sig * ycg;
       const R c1 = raw * sig;
       R lsqb = 0;
       for (int k = lane; k < kl; k += 32) {
         const int b = k + ld * m;
         const Bin q = bin(m, k);
         const R f = w.F[b];
-        const R a = (f * CG[m]) / zs;
-        const R sd = ((q.d1 * a) * sig) / CG[m];
+        const R a = rdiv(rmul(f, cg), zs, yzs);
+        const R sd = rdiv(rmul(rmul(q.d1, a), sig), cg, ycg);
         const R lsd = (R(0.) < sd) ? T.DELTH * (LSDX[m] * S.COSTH[k] + LSDY[m] * S.SINTH[k]) : R(0);
         const R2 v = w.SF[b];
-        R ld1 = v.x + lsd * a * sig / CG[m];
-        const R la = lsd * q.d1 * sig / CG[m];
+        R ld1 = v.x + lsd * a * sgcg;
+        const R la = lsd * q.d1 * sgcg;
         R lw = 0, lg = 0;
         if (q.up) {
           lg = ld1 * c1 * sqb * q.w;
@@ -1211,7 +1215,7 @@ template <typename R> struct AdjW {
         lw = lw + lx * R(10.) * sqb;
         const R lproj = lw * R(2) * q.proj;
         luprox = luprox + lproj * CI10[m] * radd(rmul(S.COSTH[k], cu), rmul(S.SINTH[k], su));
-        LAM[b] = LAM[b] + la * CG[m] / zs;
+        LAM[b] = LAM[b] + la * cgzs;
       }
       lsqb = warp_sum(lsqb);
       // SQB = sqrt(sig WN^3 q) with q = row sum / narrowness sum (= the row's
@@ -1220,8 +1224,8 @@ template <typename R> struct AdjW {
       const int kx = (int)KXR[m];
       for (int k = lane; k < kl; k += 32) {
         const int b = k + ld * m;
-        if (kx < 0) LAM[b] = LAM[b] + (lq / R(kl)) * CG[m] / zs;
-        else if (k == kx) LAM[b] = LAM[b] + lq * CG[m] / zs;
+        if (kx < 0) LAM[b] = LAM[b] + (lq / R(kl)) * cgzs;
+        else if (k == kx) LAM[b] = LAM[b] + lq * cgzs;
       }
     }
     lustar = lustar + R(32.) * warp_sum(luprox);

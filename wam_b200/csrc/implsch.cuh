@@ -799,12 +799,15 @@ template <typename R> struct Src {
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m];
       const R* fm = w.F + ld * m;
-      const R zs = P_::ZPI * sig;
+      const R zs = P_::ZPI * sig, yzs = R(1) / zs, cg = CG[m];
       R s = 0, mx = 0;
-      for (int k = 0; k < kl; ++k) { R a = (fm[k] * CG[m]) / zs; s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
+      for (int k = 0; k < kl; ++k) { R a = rdiv(rmul(fm[k], cg), zs, yzs); s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
       R s2 = 0;
       if (mx < R(1.0E-34)) s2 = R(kl);
-      else for (int k = 0; k < kl; ++k) s2 = s2 + ((fm[k] * CG[m]) / zs) / mx;
+      else {
+        const R ymx = R(1) / mx;
+        for (int k = 0; k < kl; ++k) s2 = s2 + rdiv(rdiv(rmul(fm[k], cg), zs, yzs), mx, ymx);
+      }
       R adensig = s * sig * T.DELTH, anar = R(1.0) / (s2 * T.DELTH);
       SQB[m] = dsqrt(anar * adensig * (WN[m] * WN[m] * WN[m]));
       CI10[m] = WN[m] / sig;
@@ -829,10 +832,10 @@ template <typename R> struct Src {
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m], bx = 0, by = 0;
       const R* fm = w.F + ld * m; const R2* d1 = w.SF + ld * m;
-      const R zs = P_::ZPI * sig;
+      const R zs = P_::ZPI * sig, yzs = R(1) / zs, cg = CG[m], ycg = R(1) / cg;
       for (int k = 0; k < kl; ++k) {
-        const R a = (fm[k] * CG[m]) / zs;
-        const R sd = ((d1[k].x * a) * sig) / CG[m];
+        const R a = rdiv(rmul(fm[k], cg), zs, yzs);
+        const R sd = rdiv(rmul(rmul(d1[k].x, a), sig), cg, ycg);
         bx = radd(bx, rmul(dmax(R(0.), sd), S.COSTH[k]));
         by = radd(by, rmul(dmax(R(0.), sd), S.SINTH[k]));
       }
