@@ -27,7 +27,8 @@ Bars:
     the full 60x40 1-degree grid and sampled larger grids: 1e-4 relative at
     the maximum against the FP32 oracle; against the FP64 GPU run the FP32
     error stays within twice that of the FP32 oracle itself, and the FP64 GPU
-    run stays within 1e-7 of the FP64 oracle.
+    run stays within 1e-8 of the FP64 oracle at the median and 1e-5 at the
+    maximum (an FP64 threshold decision can flip at a point).
 """
 import numpy as np
 import pytest
@@ -147,6 +148,10 @@ def test_implsch_fp32_one_step(case):
     assert np.max(np.abs(zg - zo)[ok] / zo[ok]) <= 1e-4
     tscale = np.maximum(np.abs(two), 1e-3 * np.abs(two).max())
     assert np.max((np.abs(tg - two) / tscale)[ok]) <= 1e-5
+    lf = gd["LFIT"][gd["LFIT"] >= 0]
+    print(f"\n{name}@{w.nsea}: max point error {err.max():.2e}, decision flips {int(flipped.sum())} of {w.nsea}, "
+          f"MIJ1 range {gd['MIJ1'].min()}-{gd['MIJ1'].max()}, LFACTOR iterations "
+          f"{'-' if lf.size == 0 else f'{lf.min()}-{lf.max()} (mean {lf.mean():.1f})'}")
 
 
 def test_implsch_fp64_matches_fp64_oracle(case, oracle_mod):

@@ -1060,19 +1060,20 @@ template <typename R> struct AdjW {
     for (int m = lane; m < nk; m += 32) {
       const R sig = P_::ZPI * S.FR[m];
       const R* fm = w.F + ld * m;
-      const R zs = P_::ZPI * sig, yzs = R(1) / zs, cg = CG[m];
+      const R zs = P_::ZPI * sig, cg = CG[m];
+      const RecipDiv<R> qzs(zs);
       R sm = 0, mx = 0;
       int kx = 0;
       for (int k = 0; k < kl; ++k) {
-        const R a = rdiv(rmul(fm[k], cg), zs, yzs);
+        const R a = qzs(rmul(fm[k], cg));
         sm = sm + a;
         if (k == 0 || mx < a) { mx = a; kx = k; }
       }
       R s2 = 0;
       if (mx < R(1.0E-34)) { s2 = R(kl); kx = -1; }
       else {
-        const R ymx = R(1) / mx;
-        for (int k = 0; k < kl; ++k) s2 = s2 + rdiv(rdiv(rmul(fm[k], cg), zs, yzs), mx, ymx);
+        const RecipDiv<R> qmx(mx);
+        for (int k = 0; k < kl; ++k) s2 = s2 + qmx(qzs(rmul(fm[k], cg)));
       }
       const R adensig = sm * sig * T.DELTH, anar = R(1.0) / (s2 * T.DELTH);
       SQB[m] = dsqrt(anar * adensig * (WN[m] * WN[m] * WN[m]));
@@ -1081,13 +1082,14 @@ template <typename R> struct AdjW {
     }
     __syncwarp();
     for (int m = lane; m < nk; m += 32) {
-      const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig, yzs = R(1) / zs, cg = CG[m], ycg = R(1) / cg;
+      const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig, cg = CG[m];
+      const RecipDiv<R> qzs(zs), qcg(cg);
       const R* fm = w.F + ld * m;
       R bx = 0, by = 0;
       for (int k = 0; k < kl; ++k) {
         const Bin q = bin(m, k);
-        const R a = rdiv(rmul(fm[k], cg), zs, yzs);
-        const R sd = rdiv(rmul(rmul(q.d1, a), sig), cg, ycg);
+        const R a = qzs(rmul(fm[k], cg));
+        const R sd = qcg(rmul(rmul(q.d1, a), sig));
         bx = radd(bx, rmul(dmax(R(0.), sd), S.COSTH[k]));
         by = radd(by, rmul(dmax(R(0.), sd), S.SINTH[k]));
       }
@@ -1186,15 +1188,16 @@ template <typename R> struct AdjW {
     R luprox = 0;
     for (int m = 0; m < nk; ++m) {
       const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig, sqb = SQB[m];
-      const R cg = CG[m], yzs = R(1) / zs, ycg = R(1) / cg, cgzs = cg * yzs, sgcg = sig * ycg;
+      const R cg = CG[m], cgzs = cg / zs, sgcg = sig / cg;
+      const RecipDiv<R> qzs(zs), qcg(cg);
       const R c1 = raw * sig;
       R lsqb = 0;
       for (int k = lane; k < kl; k += 32) {
         const int b = k + ld * m;
         const Bin q = bin(m, k);
         const R f = w.F[b];
-        const R a = rdiv(rmul(f, cg), zs, yzs);
-        const R sd = rdiv(rmul(rmul(q.d1, a), sig), cg, ycg);
+        const R a = qzs(rmul(f, cg));
+        const R sd = qcg(rmul(rmul(q.d1, a), sig));
         const R lsd = (R(0.) < sd) ? T.DELTH * (LSDX[m] * S.COSTH[k] + LSDY[m] * S.SINTH[k]) : R(0);
         const R2 v = w.SF[b];
         R ld1 = v.x + lsd * a * sgcg;

@@ -47,21 +47,25 @@ __device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
-// a / b rounded as the IEEE division rounds it, given y = 1/b (itself a
-// correctly rounded quotient, formed once for a row of equal divisors):
-// Markstein's correction of q = a*y by the residual a - b*q, which one FMA
-// forms exactly (P. Markstein, IBM J. Res. Develop. 34(1), 1990, 111-119).
-// The correction is the IEEE quotient while a, b and the quotient stay far
-// from the ends of the exponent range; other operands take the division.
-__device__ __forceinline__ float rdiv(float a, float b, float y) {
-  const float q = __fmul_rn(a, y);
-  const float aa = fabsf(a), ab = fabsf(b);
-  if (aa == 0.f) return q;
-  if (aa >= 0x1p-100f && aa <= 0x1p100f && ab >= 0x1p-100f && ab <= 0x1p100f)
-    return __fmaf_rn(__fmaf_rn(-q, b, a), y, q);
-  return __fdiv_rn(a, b);
-}
-__device__ __forceinline__ double rdiv(double a, double b, double) { return a / b; }
+// Quotients a / b for one divisor b, each rounded as the IEEE division
+// rounds it, without a division per quotient.  In single precision the
+// quotient is the float rounding of a times the double reciprocal of b.  That
+// product is within 2^-52 (relative) of a/b, while a/b lies more than 2^-49
+// (relative) from every midpoint between two floats: a midpoint m has an odd
+// 25-bit significand, so a - m*b is a nonzero multiple of 2^-25 ulp(a).  Both
+// therefore round to the same float.  Branch-free, unlike the division's
+// special-operand paths.  In double precision it is the division itself.
+template <typename R> struct RecipDiv;
+template <> struct RecipDiv<float> {
+  double y;
+  __device__ explicit RecipDiv(float b) : y(1.0 / (double)b) {}
+  __device__ float operator()(float a) const { return __double2float_rn(__dmul_rn((double)a, y)); }
+};
+template <> struct RecipDiv<double> {
+  double b;
+  __device__ explicit RecipDiv(double b_) : b(b_) {}
+  __device__ double operator()(double a) const { return a / b; }
+};
 // Correctly rounded single-precision transcendentals (evaluated in double,
 // rounded once) for the same per-point values: the cut-off index's LOG10 /
 // LOG, the LFACTOR exponentials and wind-direction cosines, and WAVNU2's

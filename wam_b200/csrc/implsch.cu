@@ -11,19 +11,33 @@ __device__ __forceinline__ void implsch_cta(const DevTables<R>& T, const ImplArg
   R* sR = reinterpret_cast<R*>(smem);
   int* sI = reinterpret_cast<int*>(sR + T.lay.nreal);
   const int tid = threadIdx.x, nthr = blockDim.x;
-  for (int i = tid; i < T.lay.nreal; i += nthr) sR[i] = T.small[i];
-  for (int i = tid; i < T.lay.nint; i += nthr) sI[i] = T.ismall[i];
   const int NS = T.NS, KL = T.KL, LD = T.ld;
   const size_t wsb = warp_ws_bytes<R>(LD, T.ML, T.need_sp, T.scr);
   unsigned char* ws0 = smem + tables_bytes<R>(T.lay);
   const size_t foff = ws_f_offset<R>(LD, T.ML);  // F follows the interleaved {SL, FL} block
   const int ij0 = blk * P;
-  // stage the P spectra: consecutive threads take consecutive points of one bin
-  for (int idx = tid; idx < P * NS; idx += nthr) {
-    int p = idx % P, b = idx / P, ij = min(ij0 + p, a.nsea - 1);
-    int m = b / KL, k = b - m * KL;
-    reinterpret_cast<R*>(ws0 + p * wsb + foff)[k + LD * m] = a.fl3_in[ij + (size_t)a.ld * b];
+  // stage the P spectra: consecutive threads take consecutive points of one
+  // bin.  With 32*P threads, thread t always takes point t mod P and the bins
+  // t div P + 32 j, whose (m, k) advance by a carry instead of a division.
+  const int tp = tid % P, tb = tid / P, dq = 32 / KL, dr = 32 - dq * KL;
+  {
+    const int ij = min(ij0 + tp, a.nsea - 1);
+    R* dstF = reinterpret_cast<R*>(ws0 + tp * wsb + foff);
+    const R* src = a.fl3_in + ij;
+    int m = tb / KL, k = tb - m * KL;
+    for (int b = tb; b < NS; b += 32) {
+      const unsigned sa = (unsigned)__cvta_generic_to_shared(dstF + k + LD * m);
+      const R* g = src + (size_t)a.ld * b;
+      if (sizeof(R) == 4) asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(g) : "memory");
+      else asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+      k += dr; m += dq;
+      if (k >= KL) { k -= KL; ++m; }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
   }
+  for (int i = tid; i < T.lay.nreal; i += nthr) sR[i] = T.small[i];
+  for (int i = tid; i < T.lay.nint; i += nthr) sI[i] = T.ismall[i];
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
   __syncthreads();
   // every warp runs the step (its phases end in CTA barriers); a warp past the
   // last sea point repeats the last point and writes nothing
@@ -60,14 +74,19 @@ __device__ __forceinline__ void implsch_cta(const DevTables<R>& T, const ImplArg
     }
   }
   __syncthreads();
-  for (int idx = tid; idx < P * NS; idx += nthr) {
-    int p = idx % P, b = idx / P, ijs = ij0 + p;
-    int m = b / KL, k = b - m * KL;
-    if (ijs < a.nsea) {
-      R v = reinterpret_cast<R*>(ws0 + p * wsb + foff)[k + LD * m];
-      a.fl3[ijs + (size_t)a.ld * b] = v;
-      if (!isfinite(v)) atomicOr(a.status, 1);
+  if (ij0 + tp < a.nsea) {
+    const R* srcF = reinterpret_cast<const R*>(ws0 + tp * wsb + foff);
+    R* dst = a.fl3 + ij0 + tp;
+    bool finite = true;
+    int m = tb / KL, k = tb - m * KL;
+    for (int b = tb; b < NS; b += 32) {
+      const R v = srcF[k + LD * m];
+      dst[(size_t)a.ld * b] = v;
+      finite = finite && isfinite(v);
+      k += dr; m += dq;
+      if (k >= KL) { k -= KL; ++m; }
     }
+    if (!finite) atomicOr(a.status, 1);
   }
 }
 

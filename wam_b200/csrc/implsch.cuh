@@ -799,14 +799,15 @@ template <typename R> struct Src {
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m];
       const R* fm = w.F + ld * m;
-      const R zs = P_::ZPI * sig, yzs = R(1) / zs, cg = CG[m];
+      const R zs = P_::ZPI * sig, cg = CG[m];
+      const RecipDiv<R> qzs(zs);
       R s = 0, mx = 0;
-      for (int k = 0; k < kl; ++k) { R a = rdiv(rmul(fm[k], cg), zs, yzs); s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
+      for (int k = 0; k < kl; ++k) { R a = qzs(rmul(fm[k], cg)); s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
       R s2 = 0;
       if (mx < R(1.0E-34)) s2 = R(kl);
       else {
-        const R ymx = R(1) / mx;
-        for (int k = 0; k < kl; ++k) s2 = s2 + rdiv(rdiv(rmul(fm[k], cg), zs, yzs), mx, ymx);
+        const RecipDiv<R> qmx(mx);
+        for (int k = 0; k < kl; ++k) s2 = s2 + qmx(qzs(rmul(fm[k], cg)));
       }
       R adensig = s * sig * T.DELTH, anar = R(1.0) / (s2 * T.DELTH);
       SQB[m] = dsqrt(anar * adensig * (WN[m] * WN[m] * WN[m]));
@@ -832,10 +833,11 @@ template <typename R> struct Src {
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m], bx = 0, by = 0;
       const R* fm = w.F + ld * m; const R2* d1 = w.SF + ld * m;
-      const R zs = P_::ZPI * sig, yzs = R(1) / zs, cg = CG[m], ycg = R(1) / cg;
+      const R zs = P_::ZPI * sig, cg = CG[m];
+      const RecipDiv<R> qzs(zs), qcg(cg);
       for (int k = 0; k < kl; ++k) {
-        const R a = rdiv(rmul(fm[k], cg), zs, yzs);
-        const R sd = rdiv(rmul(rmul(d1[k].x, a), sig), cg, ycg);
+        const R a = qzs(rmul(fm[k], cg));
+        const R sd = qcg(rmul(rmul(d1[k].x, a), sig));
         bx = radd(bx, rmul(dmax(R(0.), sd), S.COSTH[k]));
         by = radd(by, rmul(dmax(R(0.), sd), S.SINTH[k]));
       }
