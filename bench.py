@@ -380,10 +380,11 @@ def batched_ensemble(dev, steps, warmup, n_members=32):
     return out
 
 
-def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242, scale=1.0):
+def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242, scale=1.0, name="c2"):
     """Adjoint of one assimilation window on the 400x300 regional grid
     (KL=36, ML=30, ST4, IDELPRO=120 s, IDELT=600 s), FP32, through the C ABI
-    an assimilation driver calls.
+    an assimilation driver calls.  name="c1" with scale=1/3 is the same grid
+    size on the ST6 regional recipe.
 
     The forward sweep runs `passes` WAMODEL passes with wamgpu_step_ckpt_dev,
     one checkpoint per pass (the spectrum entering IMPLSCH, TAUW, U10).  The
@@ -399,7 +400,7 @@ def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242, scale=1.0):
     from wam_b200 import WamModel
     from wam_b200.adjoint import significant_wave_height
     from wam_b200.synth import make_workload
-    w = make_workload("c2", scale=scale, device=dev.index)
+    w = make_workload(name, scale=scale, device=dev.index)
     n_obs = min(n_obs, w.nsea)
     m = WamModel(w.cfg)
     m.set_grid(w.grid)
@@ -470,8 +471,12 @@ def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242, scale=1.0):
     J, lam_f, lam_t, lam_u, ms_fwd, ms_adj = window(passes)
     finite = bool(torch.isfinite(lam_f).all()) and all(bool(torch.isfinite(u).all()) for u in lam_u)
     bins = w.nsea * w.cfg["kl"] * w.cfg["ml"]
-    grid = "400x300 regional" if scale == 1.0 else f"400x300 regional recipe at scale {scale}"
-    out = {"workload": f"c2: {grid}, {w.nsea} sea points, ST4, KL=36 ML=30, IDELPRO=120 s IDELT=600 s, "
+    if name == "c2":
+        grid = "c2: 400x300 regional" if scale == 1.0 else f"c2: 400x300 regional recipe at scale {scale}"
+    else:
+        grid = f"{name} regional recipe at scale {scale:.4g}"
+    phys = "ST4" if w.cfg["iphys"] == 1 else "ST6"
+    out = {"workload": f"{grid}, {w.nsea} sea points, {phys}, KL=36 ML=30, IDELPRO=120 s IDELT=600 s, "
                        f"{passes}-pass window, {n_obs} Hs observations",
            "value": bins / (ms_adj / 1e3), "unit": UNIT + " (adjoint pass)", "ms_per_adjoint_pass": ms_adj,
            "ms_per_forward_pass": ms_plain, "ms_per_checkpointed_forward_pass": ms_fwd,
@@ -625,6 +630,8 @@ def main():
             line["batched"] = batched_ensemble(dev, max(3, min(args.steps, 10)), max(3, args.warmup))
         if not args.no_adjoint and world == 1:
             line["adjoint"] = adjoint_window(dev, max(3, args.warmup))
+            # the same window size on the ST6 recipe (1200x900 / 3 = 400x300)
+            line["adjoint_st6"] = adjoint_window(dev, max(3, args.warmup), passes=12, scale=1.0 / 3.0, name="c1")
         print(json.dumps(line), flush=True)
     m.close()
     if world > 1:

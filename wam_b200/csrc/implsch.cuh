@@ -901,20 +901,47 @@ template <typename R> struct Src {
         qx[q] = in ? SDX[i] : R(0); qy[q] = in ? SDY[i] : R(0); qc[q] = in ? CI10[i] : R(0);
         qd[q] = in ? DS10[i] : R(0); qa[q] = rsub(R(1.0), rmul(uproxy, qc[q])); qf[q] = R(1.0);
       }
+      // Terms before the first negative exponent factor keep LFACT = 1 in
+      // every iteration (RTAU stays positive), so their in-order partial sums
+      // are formed once and each iteration continues from them.
+      int L = nk10;
+#pragma unroll
+      for (int q = NQ - 1; q >= 0; --q) {
+        const unsigned neg = __ballot_sync(0xffffffffu, lane + 32 * q < nk10 && qa[q] < R(0));
+        if (neg) L = 32 * q + __ffs(neg) - 1;
+      }
+      R prex, prey;
+      {
+        __syncwarp();
+        R acc = R(0);
+        const R* row = lane == 0 ? TX : TY;
+        if (lane < 2)
+          for (int i = 0; i < L; ++i) acc = radd(acc, row[i]);
+        prex = __shfl_sync(0xffffffffu, acc, 0); prey = __shfl_sync(0xffffffffu, acc, 1);
+        __syncwarp();
+      }
       for (int it = 0; it < 80; ++it) {
         nit = it + 1;
         if (lfrec && lane == 0) lfrec[LF_RLAST] = rtau;
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
           const int i = lane + 32 * q;
-          if (i < nk10) {
+          if (i >= L && i < nk10) {
             const R lf = dmin(R(1.0), crexp(rmul(qa[q], rtau)));
             qf[q] = lf;
             TX[i] = (qx[q] * lf) * qc[q] * qd[q];
             TY[i] = (qy[q] * lf) * qc[q] * qd[q];
           }
         }
-        tauwinds(tauwx, tauwy);
+        {
+          __syncwarp();
+          R acc = lane == 0 ? prex : prey;
+          const R* row = lane == 0 ? TX : TY;
+          if (lane < 2)
+            for (int i = L; i < nk10; ++i) acc = radd(acc, row[i]);
+          tauwx = gro * __shfl_sync(0xffffffffu, acc, 0); tauwy = gro * __shfl_sync(0xffffffffu, acc, 1);
+          __syncwarp();
+        }
         tau = total();
         err = (tau - tau_tot) / tau_tot;
         int sold = sgn;
