@@ -413,8 +413,9 @@ WAMGPU_API int wamgpu_put_points_dev(wamgpu_ctx* ctx, void* data, int ld, int nr
  *   (TM1_TM2_PERIODS :1152), 14 mean direction and 15 directional spread
  *   [deg] (MEAN_DIRECTION :412), 16 normalised wave stress, 32 Z0 [m],
  *   40 mean square slope (MEANSQS :639).
- * The other parameters up to WAMGPU_OUT_NPARAM (swell separation, kurtosis,
- * radiation stress, Stokes drift) are not computed and are set to 0.
+ * The other parameters up to WAMGPU_OUT_NPARAM are set to 0: the wind-sea
+ * and swell parameters 17-23 and 25-31 come from wamgpu_output_swell_dev;
+ * kurtosis (33-39) is not computed.
  * from != 0 gives directions the waves and wind come from (the reference's
  * default orientation_of_directions), 0 directions they go to.  When USTAR
  * is zero at every point, AIRSEA (wam_source_module.f90:868-971) first sets
@@ -425,6 +426,17 @@ WAMGPU_API int wamgpu_put_points_dev(wamgpu_ctx* ctx, void* data, int ld, int nr
 WAMGPU_API int wamgpu_output_parameters_dev(wamgpu_ctx* ctx, const void* fl3, int ld, const void* u10,
                                             const void* udir, const void* tauw, void* ustar, void* z0, int from,
                                             void* block, int block_ld, void* stream);
+
+/* SWELL_SEPARATION (wam_swell_module.f90:106-350, called by
+ * COMPUTE_OUTPUT_PARAMETER at wam_output_module.f90:637) on the device: the
+ * wind-sea parameters 17-23 and the swell parameters 25-31 of the block
+ * (significant wave height, peak period, mean period, TM1, TM2, mean
+ * direction, directional spread), the other rows untouched.  A bin is swell
+ * where 28/C(M) * 1.2*USTAR*COS(TH(K)-UDIR) < 1.  The swell partitioning
+ * (parameters 41-49) is not computed.  ustar is the USTAR of the step (after
+ * wamgpu_output_parameters_dev when that set it); from as there. */
+WAMGPU_API int wamgpu_output_swell_dev(wamgpu_ctx* ctx, const void* fl3, int ld, const void* udir, const void* ustar,
+                                       int from, void* block, int block_ld, void* stream);
 
 /* Synchronises the context stream; returns WAMGPU_E_NUMERIC if a kernel
  * reported non-finite output since the last call. */

@@ -64,6 +64,7 @@ def lib():
         L.oracle_resident_set.argtypes = [vp] + [dp] * 9
         L.oracle_count_implsch.argtypes = [ctypes.POINTER(OracleConfig), ctypes.c_int] + [dp] * 9 + [ip, dp]
         L.oracle_output_params.argtypes = [vp, ctypes.c_int] + [dp] * 9 + [ip, ctypes.c_int, dp]
+        L.oracle_output_swell.argtypes = [vp, ctypes.c_int, dp, dp, dp, ctypes.c_int, dp]
         L.oracle_resident_step.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.oracle_resident_get.argtypes = [vp, dp, dp, dp, dp]
         L.oracle_grid_create.restype = vp
@@ -242,6 +243,17 @@ class Oracle:
         self.L.oracle_output_params(self.h, nsea, _d(f), _d(c(u10)), _d(c(udir)), _d(us), _d(c(tauw)), _d(zz),
                                     _d(c(depth)), _d(c(u)), _d(c(v)), _i(ind), int(bool(from_)), _d(out))
         return out.reshape(40, nsea), us, zz
+
+    def output_swell(self, fl3, udir, ustar, from_=True, block=None):
+        """SWELL_SEPARATION: rows 16..22 and 24..30 (parameters 17-23, 25-31)
+        of block[40, nsea] (zeros when not given) filled."""
+        nsea = fl3.shape[0]
+        f = np.asfortranarray(fl3, float)
+        out = np.zeros((40, nsea)) if block is None else np.array(block, float)
+        c = lambda a: np.ascontiguousarray(a, float)
+        o = np.ascontiguousarray(out).ravel()
+        self.L.oracle_output_swell(self.h, nsea, _d(f), _d(c(udir)), _d(c(ustar)), int(bool(from_)), _d(o))
+        return o.reshape(40, nsea)
 
     def resident_set(self, fl3, u10, udir, tauw, ustar, z0, roairn, wstar, depth):
         """Keep a model state inside the oracle in its own precision (the timed CPU baseline)."""

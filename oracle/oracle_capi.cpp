@@ -228,6 +228,27 @@ int oracle_output_params(void* h, int nsea, const double* fl3, const double* u10
   return DISPATCH(h, f);
 }
 
+// SWELL_SEPARATION (wam_swell_module.f90:106-350) for nsea points:
+// out[ij + nsea*(IP-1)] for IP = 17..23 and 25..31 (the other rows untouched).
+int oracle_output_swell(void* h, int nsea, const double* fl3, const double* udir, const double* ustar, int from,
+                        double* out) {
+  auto f = [&](auto* o) {
+    using RR = typename std::decay<decltype(o->fd.FR[0])>::type;
+    const int kl = o->fd.KL, ml = o->fd.ML;
+    o->outm.from = from != 0;
+    std::vector<RR> F((size_t)kl * ml), P(OUT_NPARAM, RR(0));
+    for (int ij = 0; ij < nsea; ++ij) {
+      for (int m = 0; m < ml; ++m)
+        for (int k = 0; k < kl; ++k) F[k + kl * m] = RR(fl3[ij + (size_t)nsea * (k + (size_t)kl * m)]);
+      o->outm.swell(F.data(), RR(udir[ij]), RR(ustar[ij]), P.data());
+      for (int p = 17; p <= 31; ++p)
+        if (p != 24) out[ij + (size_t)nsea * (p - 1)] = (double)P[p - 1];
+    }
+    return 0;
+  };
+  return DISPATCH(h, f);
+}
+
 int oracle_get_table(void* h, const char* name, double* out) {
   std::string n(name);
   auto f = [&](auto* o) { return get_table_t(o, n, out); };

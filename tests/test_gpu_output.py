@@ -112,3 +112,49 @@ def test_output_parameters_going_to_and_airsea(oracle_mod):
             d = np.abs(g - r) / np.maximum(np.abs(r), 1e-30)
         assert np.max(d) <= tol, f"parameter {p}: {np.max(d):.3e}"
     m.close()
+
+
+SWELL = [17, 18, 19, 20, 21, 22, 23, 25, 26, 27, 28, 29, 30, 31]
+SWELL_ANGLES = {22, 30}
+
+
+@pytest.mark.parametrize("precision", [4, 8])
+@pytest.mark.parametrize("name,scale,from_", [("c0", 0.5, True), ("c2", 0.05, False)])
+def test_swell_separation_matches_oracle(oracle_mod, name, scale, from_, precision):
+    """SWELL_SEPARATION (wam_swell_module.f90:106-350) through
+    wamgpu_output_swell_dev: wind-sea parameters 17-23 and swell parameters
+    25-31 against the oracle.  The split of every bin uses the correctly
+    rounded cosine on both sides, so FP32 values are bit-identical except
+    the two mean directions (ATAN2 of the device library); FP64 to 1e-12.
+    The other rows of the block are left as they were."""
+    import torch
+    w, o, m, f, tw, us, zz, u, v = _case(oracle_mod, name, scale, precision, False)
+    ref = o.output_swell(f, w.udir, us, from_=from_)
+    dt = torch.float64 if precision == 8 else torch.float32
+    t = lambda a: torch.tensor(np.asarray(a), dtype=dt, device="cuda")
+    F = t(np.ascontiguousarray(np.asarray(f).transpose(2, 1, 0)))
+    blk = torch.full((40, w.nsea), 7.0, dtype=dt, device="cuda")
+    m.output_swell_dev(F, t(w.udir), t(us), blk, from_=from_)
+    m.sync()
+    got = blk.cpu().numpy()
+    for p in SWELL:
+        g, r = got[p - 1], ref[p - 1]
+        if precision == 8:
+            err = np.max(np.abs(g - r) / np.maximum(np.abs(r), 1e-30))
+            assert err <= 1e-12, f"{name} fp64 parameter {p}: {err:.2e}"
+        elif p in SWELL_ANGLES:
+            d = np.abs(g - r)
+            d = np.minimum(d, 360.0 - d)
+            assert np.max(d / 360.0) <= 2e-6, f"{name} parameter {p}: {np.max(d):.3e} deg"
+        else:
+            bad = np.nonzero(g.astype(np.float32) != r.astype(np.float32))[0]
+            assert bad.size == 0, f"{name} parameter {p}: {bad.size} points differ, e.g. {g[bad[0]]!r} vs {r[bad[0]]!r}"
+    others = [p for p in range(1, 41) if p not in SWELL]
+    assert np.all(got[[p - 1 for p in others]] == 7.0)
+    # both parts present on these sea states, and the wind-sea and swell
+    # energies add up to the total (the bins below EPSMIN aside)
+    hs_ws, hs_sw = got[16].astype(float), got[24].astype(float)
+    assert (hs_sw > 0).any() and (hs_ws > 0.01).any()
+    tot = o.output_params(f, w.u10, w.udir, us, tw, zz, w.depth)[0][8].astype(float)
+    assert np.allclose((hs_ws ** 2 + hs_sw ** 2) / 16.0, tot ** 2 / 16.0, rtol=1e-4, atol=1e-10)
+    m.close()

@@ -61,6 +61,7 @@ SIGNATURES = {
     "wamgpu_put_points_dev": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, ctypes.c_double, c_void_p]),
     "wamgpu_output_parameters_dev": (c_int, [c_void_p, c_void_p, c_int] + [c_void_p] * 5 + [c_int, c_void_p, c_int,
                                                                                              c_void_p]),
+    "wamgpu_output_swell_dev": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p]),
     "wamgpu_set_timing": (c_int, [c_void_p, c_int]),
     "wamgpu_get_timing": (c_int, [c_void_p, PF, PI]),
     "wamgpu_set_owned": (c_int, [c_void_p, c_int, c_int]),

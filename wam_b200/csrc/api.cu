@@ -95,7 +95,7 @@ template <typename R> struct Impl : ImplBase {
   DevBuf wncg;           // ST6: WN and CG per (sea point, frequency), formed by wamgpu_prepare_source
   int nckpt = 0, ckpt_ld = 0;
   DevBuf small, ismall, tfak, tcgond, tsihkd, flminfr, enh, gom, fr, sinth, costh;
-  DevBuf outtab;         // integrated output: DFIM_FR, DFIM_FR2, MEANSQS deep-water weights (ML each)
+  DevBuf outtab;         // integrated output: DFIM_FR, DFIM_FR2, MEANSQS deep-water weights, C (ML each)
   DevBuf ustar_max;      // MAXVAL(USTAR) word of the output step
   DevBuf wind_tab, wind_w;  // INTERPOLATION_TO_GRID tables (I1, I2, K1, K2; DI, DK) of the sea points
   DevBuf rst_stage, rst_perm;  // restart records: REAL staging chunk, IJ2NEWIJ
@@ -212,6 +212,7 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
     ot.insert(ot.end(), t.DFIM_FR2.begin(), t.DFIM_FR2.end());
     for (int m = 0; m < t.ML; ++m)
       ot.push_back(t.DFIM[m] * powi(Phys<R>::ZPI * t.FR[m], 4) / powi(Phys<R>::G, 2));
+    ot.insert(ot.end(), t.C.begin(), t.C.end());  // deep-water phase speeds (swell separation)
     CK(upload(I.outtab, ot, s), "upload tables");
   }
   DevTables<R>& d = I.dt;
@@ -995,6 +996,35 @@ int output_params_t(wamgpu_ctx* ctx, Impl<R>& I, const void* fl3, int ld, const 
   for (int p = 0; p < WAMGPU_OUT_NPARAM; ++p)
     CK(cudaMemsetAsync((R*)block + p0 + (size_t)block_ld * p, 0, (size_t)(p1 - p0) * sizeof(R), s), "memset block");
   CK(launch_output<R>(a, I.ustar_max.template as<unsigned long long>(), s), "output launch");
+  return WAMGPU_OK;
+}
+
+// SWELL_SEPARATION (wam_swell_module.f90:106-350) without the partitioning:
+// parameters 17-23 (wind sea) and 25-31 (swell) of the output block.
+template <typename R>
+int output_swell_t(wamgpu_ctx* ctx, Impl<R>& I, const void* fl3, int ld, const void* udir, const void* ustar, int from,
+                   void* block, int block_ld, cudaStream_t s) {
+  if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first");
+  if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
+  if (block_ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "block_ld < nsea");
+  if (!fl3 || !udir || !ustar || !block) return fail(ctx, WAMGPU_E_ARG, "null argument");
+  const int p0 = ctx->own0, p1 = ctx->own1 < 0 ? ctx->nsea : ctx->own1;
+  const DevTables<R>& d = I.dt;
+  OutArgs<R> a;
+  a.nsea = p1 - p0; a.ld = ld; a.KL = d.KL; a.ML = d.ML; a.NDEPTH = d.NDEPTH; a.shallow = d.shallow;
+  a.from = from ? 1 : 0;
+  a.fl3 = (const R*)fl3 + p0;
+  a.udir = (const R*)udir + p0;
+  a.ustar = const_cast<R*>((const R*)ustar) + p0;
+  a.block = (R*)block + p0; a.block_ld = block_ld;
+  const R* r = d.small;
+  a.FR = r + d.lay.FR; a.DFIM = r + d.lay.DFIM; a.DFIMOFR = r + d.lay.DFIMOFR;
+  a.SINTH = r + d.lay.SINTH; a.COSTH = r + d.lay.COSTH; a.TH = r + d.lay.TH;
+  const R* ot = I.outtab.template as<R>();
+  a.DFIM_FR = ot; a.DFIM_FR2 = ot + d.ML; a.MSSFD = ot + 2 * d.ML; a.C = ot + 3 * d.ML;
+  a.MO_TAIL = d.MO_TAIL; a.MM1_TAIL = d.MM1_TAIL;
+  a.MP1_TAIL = R(I.tab.MP1_TAIL); a.MP2_TAIL = R(I.tab.MP2_TAIL);
+  CK(launch_swell<R>(a, s), "swell launch");
   return WAMGPU_OK;
 }
 
@@ -2007,6 +2037,13 @@ int wamgpu_output_parameters_dev(wamgpu_ctx* ctx, const void* fl3, int ld, const
   if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
   cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
   return DISPATCH_CTX(ctx, output_params_t, fl3, ld, u10, udir, tauw, ustar, z0, from, block, block_ld, s);
+}
+
+int wamgpu_output_swell_dev(wamgpu_ctx* ctx, const void* fl3, int ld, const void* udir, const void* ustar, int from,
+                            void* block, int block_ld, void* stream) {
+  if (!ctx || !ctx->impl) return WAMGPU_E_ARG;
+  cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+  return DISPATCH_CTX(ctx, output_swell_t, fl3, ld, udir, ustar, from, block, block_ld, s);
 }
 
 int wamgpu_restart_write(wamgpu_ctx* ctx, const char* path, const void* fl3, int ld, const void* u10, const void* udir,

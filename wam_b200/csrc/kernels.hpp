@@ -109,10 +109,14 @@ template <typename R> struct OutArgs {
   R* block;
   int block_ld;
   const R *FR, *DFIM, *DFIMOFR, *DFIM_FR, *DFIM_FR2, *MSSFD, *SINTH, *COSTH, *TFAK;
+  const R *TH = nullptr, *C = nullptr;  // directions and deep-water phase speeds (swell separation)
   R MO_TAIL, MM1_TAIL, MP1_TAIL, MP2_TAIL;
   adj::ATabs<R> A;
   const unsigned long long* ustar_max;  // set by the launcher
 };
+// SWELL_SEPARATION without the partitioning: parameters 17-23 and 25-31 of
+// a.block from the spectrum, UDIR and USTAR.
+template <typename R> cudaError_t launch_swell(const OutArgs<R>& a, cudaStream_t s);
 // PUT_ICE_SPEC / PUT_DRY_SPEC and PUT_ICE_PAR / PUT_DRY_PAR: data[(ij-1) +
 // ld*row] = value for rows 0..nrows-1 and the 1-based sea points ij of the
 // list that lie in lo..hi.

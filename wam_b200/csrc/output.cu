@@ -153,7 +153,135 @@ __global__ void __launch_bounds__(kOutThreads) output_kernel(const __grid_consta
   put(32, Z0);
 }
 
+// The integrals COMPUTE_OUTPUT_PARAMETER and SWELL_SEPARATION take of one
+// spectrum, from its frequency sums Tm[m * st] (directions summed in order)
+// and direction sums Tk[k * st] (DFIM-weighted, frequencies in order):
+// TOTAL_ENERGY, FEMEAN, TM1_TM2_PERIODS, PEAK_PERIOD, MEAN_DIRECTION, in the
+// statement order of the parameters 9-15 above.
+template <typename R> struct SpecInt { R E, TM, TM1, TM2, TP, THQ, SPREAD; };
+template <typename R>
+__device__ SpecInt<R> spec_integrals(const OutArgs<R>& a, const R* Tk, const R* Tm, int st) {
+  using P_ = Phys<R>;
+  const int kl = a.KL, ml = a.ML;
+  const R DEG = OutConst<R>::DEG;
+  SpecInt<R> o;
+  const R tail = Tm[(ml - 1) * st];
+  R E = a.MO_TAIL * tail, FM = a.MM1_TAIL * tail, TM1 = a.MP1_TAIL * tail, TM2 = a.MP2_TAIL * tail;
+  for (int m = 0; m < ml; ++m) {
+    const R t = Tm[m * st];
+    E = E + t * a.DFIM[m];
+    FM = FM + t * a.DFIMOFR[m];
+    TM1 = TM1 + t * a.DFIM_FR[m];
+    TM2 = TM2 + t * a.DFIM_FR2[m];
+  }
+  E = dmax(E, R(1.0E-12));
+  FM = E / dmax(FM, R(1.0E-12));
+  o.E = E;
+  o.TM = R(1.) / FM;
+  o.TM1 = (E > R(1.0E-12)) ? E / TM1 : R(1.);
+  o.TM2 = (E > R(1.0E-12)) ? sqrt(E / TM2) : R(1.);
+  int ip = 0;
+  R best = Tm[0];
+  for (int m = 1; m < ml; ++m) {
+    const R t = Tm[m * st];
+    if (t > best) { best = t; ip = m; }
+  }
+  o.TP = ip == 0 ? R(1.) : R(1.) / a.FR[ip];
+  R SI = 0, CI = 0, SP = 0;
+  for (int k = 0; k < kl; ++k) {
+    const R t = Tk[k * st];
+    SI = SI + a.SINTH[k] * t;
+    CI = CI + a.COSTH[k] * t;
+    SP = SP + t;
+  }
+  {
+    const R ci = (CI == R(0.)) ? R(0.1E-30) : CI;
+    R thq = atan2(SI, ci);
+    if (thq < R(0.)) thq = thq + P_::ZPI;
+    if (thq > P_::ZPI - R(0.001)) thq = R(0.);
+    o.THQ = orient(thq * DEG, a.from);
+  }
+  {
+    const R lim = R(0.1E-15);
+    const R ci = (dabs(CI) < lim) ? copysign(lim, CI) : CI;
+    const R si = (dabs(SI) < lim) ? copysign(lim, SI) : SI;
+    R sp = (dabs(SP) < lim) ? copysign(lim, SP) : SP;
+    sp = R(2.) * (R(1.) - sqrt(si * si + ci * ci) / sp);
+    sp = (sp <= R(0)) ? (sizeof(R) == 4 ? R(FLT_MIN) : R(DBL_MIN)) : sqrt(sp);  // TINY(1.)
+    o.SPREAD = sp * DEG;
+  }
+  return o;
+}
+
+constexpr int kSwThreads = 64;
+
+// SWELL_SEPARATION (wam_swell_module.f90:106-350) without the partitioning
+// (parameters 41-49).  One thread per sea point walks the directions: a bin
+// is swell where FRIC/C(M) * 1.2*USTAR*COS(TH(K)-UDIR) < 1, its swell value
+// MAX(F, EPSMIN) there and 0 elsewhere, its wind-sea value F minus that.
+// The cosine is the correctly rounded single-precision value (the oracle
+// forms it the same way, so both split every bin alike).  The frequency sums
+// of both spectra still add their directions in order, the direction sums
+// their frequencies in order.  Parameters 17-23 (wind sea) and 25-31 (swell):
+// Hs, peak period, mean period, TM1, TM2, mean direction, spread.
+template <typename R>
+__global__ void __launch_bounds__(kSwThreads) swell_kernel(const __grid_constant__ OutArgs<R> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  R* sm = reinterpret_cast<R*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int ij = blockIdx.x * kSwThreads + tid;
+  if (ij >= a.nsea) return;
+  const int kl = a.KL, ml = a.ML, st = kSwThreads;
+  R* Tk1 = sm + tid;                      // swell direction sums
+  R* Tk4 = Tk1 + kl * st;                 // wind-sea direction sums
+  R* Tm1 = Tk4 + kl * st;                 // swell frequency sums
+  R* Tm4 = Tm1 + ml * st;                 // wind-sea frequency sums
+  for (int m = 0; m < ml; ++m) { Tm1[m * st] = R(0); Tm4[m * st] = R(0); }
+  const R FRIC = R(28.), EPSMIN = R(0.1E-32);
+  const R us = a.ustar[ij], ud = a.udir[ij];
+  const R* f = a.fl3 + ij;
+  for (int k = 0; k < kl; ++k) {
+    const R flpp = R(1.2) * us * crcos(a.TH[k] - ud);
+    R t1 = R(0), t4 = R(0);
+    for (int m = 0; m < ml; ++m) {
+      const R v = __ldg(f + (size_t)a.ld * (k + (size_t)kl * m));
+      const R cm = FRIC / a.C[m];
+      const R f1 = (cm * flpp < R(1.0)) ? dmax(v, EPSMIN) : R(0.);
+      const R f4 = v - f1;
+      Tm1[m * st] = Tm1[m * st] + f1;
+      Tm4[m * st] = Tm4[m * st] + f4;
+      t1 = t1 + f1 * a.DFIM[m];
+      t4 = t4 + f4 * a.DFIM[m];
+    }
+    Tk1[k * st] = t1;
+    Tk4[k * st] = t4;
+  }
+  R* out = a.block + ij;
+  auto put = [&](int p, R v) { out[(size_t)a.block_ld * (p - 1)] = v; };
+  const SpecInt<R> ws = spec_integrals(a, Tk4, Tm4, st), sw = spec_integrals(a, Tk1, Tm1, st);
+  put(17, R(4.) * sqrt(ws.E)); put(18, ws.TP); put(19, ws.TM); put(20, ws.TM1); put(21, ws.TM2);
+  put(22, ws.THQ); put(23, ws.SPREAD);
+  put(25, R(4.) * sqrt(sw.E)); put(26, sw.TP); put(27, sw.TM); put(28, sw.TM1); put(29, sw.TM2);
+  put(30, sw.THQ); put(31, sw.SPREAD);
+}
+
 }  // namespace
+
+template <typename R> cudaError_t launch_swell(const OutArgs<R>& a, cudaStream_t s) {
+  if (a.nsea == 0) return cudaSuccess;
+  const size_t smem = (size_t)kSwThreads * 2 * (a.KL + a.ML) * sizeof(R);
+  static bool raised[2] = {false, false};
+  if (smem > 48 * 1024 && !raised[sizeof(R) == 8]) {
+    cudaError_t e = cudaFuncSetAttribute(swell_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)((size_t)kSwThreads * 2 * (MAX_KL + MAX_ML) * sizeof(R)));
+    if (e != cudaSuccess) return e;
+    raised[sizeof(R) == 8] = true;
+  }
+  swell_kernel<R><<<(a.nsea + kSwThreads - 1) / kSwThreads, kSwThreads, smem, s>>>(a);
+  return cudaGetLastError();
+}
+template cudaError_t launch_swell<float>(const OutArgs<float>&, cudaStream_t);
+template cudaError_t launch_swell<double>(const OutArgs<double>&, cudaStream_t);
 
 // PUT_ICE / PUT_DRY: rows of the listed sea points set to a value.  One
 // thread per (row, listed point): the list is short and scattered, each

@@ -118,6 +118,12 @@ MODULE WAMGPU_BINDING
          TYPE(C_PTR), VALUE    :: ctx, fl3, u10, udir, tauw, ustar, z0, block, stream
          INTEGER(C_INT), VALUE :: ld, from, block_ld
       END FUNCTION
+      INTEGER(C_INT) FUNCTION wamgpu_output_swell_dev(ctx, fl3, ld, udir, ustar, from, block, block_ld, stream) &
+&                    BIND(C, NAME='wamgpu_output_swell_dev')
+         IMPORT :: C_INT, C_PTR
+         TYPE(C_PTR), VALUE    :: ctx, fl3, udir, ustar, block, stream
+         INTEGER(C_INT), VALUE :: ld, from, block_ld
+      END FUNCTION
       INTEGER(C_INT) FUNCTION wamgpu_get_fluxes(ctx, out7) BIND(C, NAME='wamgpu_get_fluxes')
          IMPORT :: C_INT, C_FLOAT, C_PTR
          TYPE(C_PTR), VALUE :: ctx
@@ -259,6 +265,8 @@ CONTAINS
       IF (FROM) IFROM = 1
       CALL WAMGPU_CHECK (wamgpu_output_parameters_dev(CTX, S%FL3, INT(S%LD, C_INT), S%U10, S%UDIR, S%TAUW,  &
 &                        S%USTAR, S%Z0, IFROM, S%BLOCK, INT(S%LD, C_INT), C_NULL_PTR), 'COMPUTE_OUTPUT_PARAMETER')
+      CALL WAMGPU_CHECK (wamgpu_output_swell_dev(CTX, S%FL3, INT(S%LD, C_INT), S%UDIR, S%USTAR, IFROM,      &
+&                        S%BLOCK, INT(S%LD, C_INT), C_NULL_PTR), 'SWELL_SEPARATION')
       CALL WAMGPU_CHECK (wamgpu_sync(CTX), 'SYNC')
    END SUBROUTINE WAMGPU_OUTPUT
 END MODULE WAM_GPU_DRIVER

@@ -236,6 +236,16 @@ class WamModel:
                     "output_parameters_dev")
         return block
 
+    def output_swell_dev(self, fl3, udir, ustar, block, from_=True, ld=None, stream=None):
+        """SWELL_SEPARATION on the device: rows 16..22 and 24..30 of block
+        (wind-sea and swell parameters 17-23, 25-31); returns block."""
+        ld = fl3.shape[-1] if ld is None else ld
+        s = None if stream is None else ctypes.c_void_p(stream)
+        self._check(self.L.wamgpu_output_swell_dev(self.h, fl3.data_ptr(), ld, udir.data_ptr(), ustar.data_ptr(),
+                                                   int(bool(from_)), block.data_ptr(), block.shape[-1], s),
+                    "output_swell_dev")
+        return block
+
     def restart_write(self, path, fl3, u10, udir, tauw, dates, depth=None, u=None, v=None, ij2newij=None, ld=None):
         """SAVE_RESTART_FILE from device tensors; dates: dict of CDTPRO, CDTSOU,
         CDA, CDTA, CDCA strings (blank = not stored)."""
