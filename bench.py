@@ -49,7 +49,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-batched", action="store_true")
     p.add_argument("--no-adjoint", action="store_true")
-    p.add_argument("--only", choices=["batched", "adjoint"], default=None,
+    p.add_argument("--only", choices=["batched", "adjoint", "adjoint_st6"], default=None,
                    help="run only the batched-ensemble or the adjoint-window section and print its object "
                         "(for profiling those kernels; not a bench line)")
     return p.parse_args()
@@ -508,8 +508,10 @@ def main():
         dev = torch.device("cuda", local)
         if args.only == "batched":
             out = batched_ensemble(dev, max(3, min(args.steps, 10)), max(3, args.warmup))
-        else:
+        elif args.only == "adjoint":
             out = adjoint_window(dev, max(3, args.warmup), scale=args.scale)
+        else:
+            out = adjoint_window(dev, max(3, args.warmup), passes=12, scale=args.scale / 3.0, name="c1")
         print(json.dumps({"section": args.only, **out}), flush=True)
         return
     if world > 1:
