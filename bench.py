@@ -481,7 +481,7 @@ def adjoint_window(dev, warmup, passes=24, n_obs=2000, seed=4242, scale=1.0, nam
            "value": bins / (ms_adj / 1e3), "unit": UNIT + " (adjoint pass)", "ms_per_adjoint_pass": ms_adj,
            "ms_per_forward_pass": ms_plain, "ms_per_checkpointed_forward_pass": ms_fwd,
            "adjoint_over_forward": ms_adj / ms_plain, "counter": counter, "cost": J, "gradients_finite": finite,
-           "checkpoint_bytes": passes * (bins + 2 * w.nsea) * 4,
+           "checkpoint_bytes": passes * (bins + 3 * w.nsea) * 4,
            "how": "C ABI: forward = wamgpu_step_ckpt_dev per pass; backward = the misfit adjoint at the observed "
                   "points, then wamgpu_step_adj_dev per pass (IMPLSCH adjoint recomputing the source terms from "
                   "the checkpoint, then IDELT/IDELPRO PROPAGS transposes); plain forward = wamgpu_step_dev"}

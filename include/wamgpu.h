@@ -297,8 +297,9 @@ WAMGPU_API int wamgpu_propags_adj_dev(wamgpu_ctx* ctx, void* lam_f3, int ld, voi
  * observation terms to lam_fl3 between steps.
  *  - wamgpu_checkpoint_reserve keeps room on the device for n checkpoints of
  *    spectra with leading dimension ld (n = 0 releases it).  A checkpoint is
- *    the spectrum entering IMPLSCH, and TAUW and U10 before it:
- *    ld*KL*ML + 2*NSEA values.
+ *    the spectrum entering IMPLSCH, TAUW and U10 before it, and for ST6 the
+ *    RTAU of LFACTOR's last round (the adjoint repeats that round only):
+ *    ld*KL*ML + 3*NSEA values.
  *  - wamgpu_step_ckpt_dev is wamgpu_step_dev (WAMODEL's PROP/PHYSICS pass,
  *    wamodel.f90:286-360) that also stores checkpoint `slot`.
  *  - wamgpu_step_adj_dev is the adjoint of that step: wamgpu_implsch_adj_dev

@@ -54,12 +54,32 @@ __global__ void __launch_bounds__(P * 32) implsch_adj_kernel(const __grid_consta
   const size_t foff = ws_f_offset<R>(LD, ML), loff = adjw_lam_offset<R>(LD, ML, T.scr);
   const int ij0 = blockIdx.x * P;
   const size_t ld = (size_t)a.ld;
-  for (int idx = tid; idx < P * NS; idx += nthr) {
-    const int p = idx % P, b = idx / P, ij = min(ij0 + p, a.nsea - 1);
-    const int m = b / KL, k = b - m * KL;
-    unsigned char* base = ws0 + p * wsb;
-    reinterpret_cast<R*>(base + foff)[k + LD * m] = a.fl3_in[ij + ld * b];
-    reinterpret_cast<R*>(base + loff)[k + LD * m] = a.lam_fl3[ij + ld * b];
+  // stage F and its adjoint with cp.async: thread t takes point t mod P and
+  // bins t div P + 32 j, whose (m, k) advance by a carry
+  const int tp = tid % P, tb = tid / P, dq = 32 / KL, dr = 32 - dq * KL;
+  {
+    const int ij = min(ij0 + tp, a.nsea - 1);
+    unsigned char* base = ws0 + tp * wsb;
+    R* dF = reinterpret_cast<R*>(base + foff);
+    R* dL = reinterpret_cast<R*>(base + loff);
+    int m = tb / KL, k = tb - m * KL;
+    for (int b = tb; b < NS; b += 32) {
+      const unsigned sf = (unsigned)__cvta_generic_to_shared(dF + k + LD * m);
+      const unsigned sl = (unsigned)__cvta_generic_to_shared(dL + k + LD * m);
+      const R* gf = a.fl3_in + ij + ld * b;
+      const R* gl = a.lam_fl3 + ij + ld * b;
+      if (sizeof(R) == 4) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sf), "l"(gf) : "memory");
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sl), "l"(gl) : "memory");
+      } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sf), "l"(gf) : "memory");
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sl), "l"(gl) : "memory");
+      }
+      k += dr; m += dq;
+      if (k >= KL) { k -= KL; ++m; }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
   }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, ij = min(ij0 + warp, a.nsea - 1);
@@ -76,6 +96,7 @@ __global__ void __launch_bounds__(P * 32) implsch_adj_kernel(const __grid_consta
     w.LL = reinterpret_cast<uint8_t*>(w.T + 8 * T.scr);
     Src<R> src(T, S, w, lane, ij, a.indep[ij], a.u10[ij], a.udir[ij], a.roairn[ij], a.wstar[ij], a.depth[ij], a.enh,
                a.enh_ld);
+    if (a.lfin) src.lfreplay = a.lfin + ij;
     const adj::ATabs<R> A = atabs_view(T, S);
     adj::PointIn<R> pin;
     pin.INDEP = a.indep[ij]; pin.DEPTH = a.depth[ij]; pin.UDIR = a.udir[ij]; pin.ROAIRN = a.roairn[ij];
@@ -97,10 +118,15 @@ __global__ void __launch_bounds__(P * 32) implsch_adj_kernel(const __grid_consta
   }
   __syncthreads();
   R* lout = a.lam_out ? a.lam_out : a.lam_fl3;
-  for (int idx = tid; idx < P * NS; idx += nthr) {
-    const int p = idx % P, b = idx / P, ijs = ij0 + p;
-    const int m = b / KL, k = b - m * KL;
-    if (ijs < a.nsea) lout[ijs + ld * b] = reinterpret_cast<R*>(ws0 + p * wsb + loff)[k + LD * m];
+  if (ij0 + tp < a.nsea) {
+    const R* sL = reinterpret_cast<const R*>(ws0 + tp * wsb + loff);
+    R* dst = lout + ij0 + tp;
+    int m = tb / KL, k = tb - m * KL;
+    for (int b = tb; b < NS; b += 32) {
+      dst[ld * b] = sL[k + LD * m];
+      k += dr; m += dq;
+      if (k >= KL) { k -= KL; ++m; }
+    }
   }
 }
 

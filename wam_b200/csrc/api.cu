@@ -229,11 +229,15 @@ template <typename R> int build_tables(wamgpu_ctx* ctx, Impl<R>& I) {
   // MP1) at a time, so the rows that one kind writes must be distinct within
   // a batch: strictly increasing in MC.  Otherwise the batch is one MC.
   d.dia_batch = 1;
+  // Scratch rows 4 reals longer than a multiple of 32: the rows that lanes
+  // read side by side in the ordered sums (the spectral integrals, TAUWINDS)
+  // then start in different shared-memory banks.
+  d.scr += 4;
   if (t.KL > 32) {
     const int nx = t.KL - 32, ML = t.ML, mfr1 = -t.MFRSTLW + 1, mfrl = ML - t.KFRH + mfr1;
     int b = 32 / nx;
     while (b > 1 && 8 * t.KL + 8 * nx * b > 8 * d.scr) --b;
-    if (8 * t.KL + 8 * nx * b > 8 * d.scr) d.scr = ((8 * t.KL + 8 * nx * b + 7) / 8 + 31) / 32 * 32;
+    if (8 * t.KL + 8 * nx * b > 8 * d.scr) d.scr = ((8 * t.KL + 8 * nx * b + 7) / 8 + 31) / 32 * 32 + 4;
     int last[5] = {INT_MIN, INT_MIN, INT_MIN, INT_MIN, INT_MIN};
     bool mono = true;
     for (int mc = 1; mc <= t.MLSTHG; ++mc) {
@@ -605,7 +609,8 @@ template <typename R> int prepare_source_t(wamgpu_ctx* ctx, Impl<R>& I) {
 
 template <typename R>
 int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u10, const void* udir, void* tauw,
-                  void* ustar, void* z0, const void* roairn, const void* wstar, cudaStream_t s, const void* fl3_in = nullptr) {
+                  void* ustar, void* z0, const void* roairn, const void* wstar, cudaStream_t s, const void* fl3_in = nullptr,
+                  R* lfout = nullptr) {
   if (!ctx->prepared) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_prepare_propagation first (INDEP)");
   if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
   if (ctx->cfg.shallow_run && ctx->cfg.isnonlin != 0 && !I.has_enh)
@@ -625,6 +630,7 @@ int implsch_dev_t(wamgpu_ctx* ctx, Impl<R>& I, void* fl3, int ld, const void* u1
   a.enh = I.has_enh ? I.enh.template as<R>() + p0 : nullptr; a.enh_ld = ctx->nsea;
   a.wncg = ctx->wncg_valid ? I.wncg.template as<R>() + (size_t)p0 * 2 * ctx->cfg.ml : nullptr;
   a.status = I.status.template as<int>();
+  a.lfout = lfout ? lfout + p0 : nullptr;
   if (ctx->diag) {
     a.diag = ctx->diag + p0;
     a.diag_ll = ctx->diag_ll ? ctx->diag_ll + p0 : nullptr;
@@ -781,11 +787,12 @@ int deriv_setup(wamgpu_ctx* ctx, Impl<R>& I, int ld, bool tl, DerivArgs<R>& a) {
 template <typename R>
 int implsch_adj_t(wamgpu_ctx* ctx, Impl<R>& I, const void* fl3_in, int ld, const void* tauw_in, const void* u10,
                   const void* udir, const void* roairn, const void* wstar, void* lam_fl3, void* lam_tauw, void* lam_u10,
-                  cudaStream_t s, void* lam_out = nullptr) {
+                  cudaStream_t s, void* lam_out = nullptr, const R* lfin = nullptr) {
   DerivArgs<R> a;
   int rc = deriv_setup<R>(ctx, I, ld, false, a);
   if (rc) return rc;
   a.lam_out = (R*)lam_out;
+  a.lfin = lfin;
   a.fl3_in = (const R*)fl3_in; a.tauw_in = (const R*)tauw_in; a.u10 = (const R*)u10; a.udir = (const R*)udir;
   a.roairn = (const R*)roairn; a.wstar = (const R*)wstar;
   a.lam_fl3 = (R*)lam_fl3; a.lam_tauw = (R*)lam_tauw; a.lam_u10 = (R*)lam_u10;
@@ -829,9 +836,11 @@ template <typename R> int propags_adj_t(wamgpu_ctx* ctx, Impl<R>& I, void* lam, 
 // ---- checkpointed assimilation windows ------------------------------------------
 
 // Slot q of the checkpoint store: the spectrum entering IMPLSCH (pitch
-// ckpt_ld), then TAUW before IMPLSCH and U10 (NSEA values each).
+// ckpt_ld), then TAUW before IMPLSCH, U10 and, for ST6, the RTAU of
+// LFACTOR's last round (NSEA values each), so that the adjoint repeats only
+// that round.
 template <typename R> R* ckpt_slot(const wamgpu_ctx* ctx, Impl<R>& I, int q) {
-  const size_t per = (size_t)I.ckpt_ld * ctx->cfg.kl * ctx->cfg.ml + 2 * (size_t)ctx->nsea;
+  const size_t per = (size_t)I.ckpt_ld * ctx->cfg.kl * ctx->cfg.ml + 3 * (size_t)ctx->nsea;
   return I.ckpt.template as<R>() + per * q;
 }
 
@@ -840,7 +849,7 @@ template <typename R> int checkpoint_reserve_t(wamgpu_ctx* ctx, Impl<R>& I, int 
   if (n == 0) { I.ckpt = DevBuf(); I.nckpt = 0; I.ckpt_ld = 0; return WAMGPU_OK; }
   if (!ctx->have_grid) return fail(ctx, WAMGPU_E_STATE, "call wamgpu_set_grid first");
   if (ld < ctx->nsea) return fail(ctx, WAMGPU_E_ARG, "ld < nsea");
-  const size_t per = (size_t)ld * ctx->cfg.kl * ctx->cfg.ml + 2 * (size_t)ctx->nsea;
+  const size_t per = (size_t)ld * ctx->cfg.kl * ctx->cfg.ml + 3 * (size_t)ctx->nsea;
   CK(I.ckpt.ensure(per * n * sizeof(R)), "alloc checkpoints");
   I.nckpt = n; I.ckpt_ld = ld;
   return WAMGPU_OK;
@@ -875,7 +884,8 @@ int step_ckpt_dev_t(wamgpu_ctx* ctx, Impl<R>& I, int slot, void* f3v, int ld, vo
   CK(cudaMemcpyAsync(c, src, bytes, cudaMemcpyDeviceToDevice, s), "checkpoint spectrum");
   CK(cudaMemcpyAsync(c + (size_t)ld * nb, tauw, n * sizeof(R), cudaMemcpyDeviceToDevice, s), "checkpoint TAUW");
   CK(cudaMemcpyAsync(c + (size_t)ld * nb + n, u10, n * sizeof(R), cudaMemcpyDeviceToDevice, s), "checkpoint U10");
-  return implsch_dev_t<R>(ctx, I, f3, ld, u10, udir, tauw, ustar, z0, roairn, wstar, s, src);
+  return implsch_dev_t<R>(ctx, I, f3, ld, u10, udir, tauw, ustar, z0, roairn, wstar, s, src,
+                          ctx->cfg.iphys == 2 ? c + (size_t)ld * nb + 2 * n : nullptr);
 }
 
 // The adjoint of the step stored in `slot`: IMPLSCH's adjoint at the
@@ -896,7 +906,8 @@ int step_adj_dev_t(wamgpu_ctx* ctx, Impl<R>& I, int slot, int nprop, void* lam_f
   const int nsub = nprop * ctx->counter;
   R* src = (nsub % 2) ? sc : lam;
   rc = implsch_adj_t<R>(ctx, I, c, ld, c + (size_t)ld * nb, c + (size_t)ld * nb + ctx->nsea, udir, roairn, wstar, lam,
-                        lam_tauw, lam_u10, s, src == lam ? nullptr : src);
+                        lam_tauw, lam_u10, s, src == lam ? nullptr : src,
+                        ctx->cfg.iphys == 2 ? c + (size_t)ld * nb + 2 * (size_t)ctx->nsea : nullptr);
   if (rc) return rc;
   R* dst = src == lam ? sc : lam;
   for (int it = 0; it < nsub; ++it) {

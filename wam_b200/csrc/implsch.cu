@@ -59,6 +59,7 @@ __device__ __forceinline__ void implsch_cta(const DevTables<R>& T, const ImplArg
                a.enh_ld);
     src.wncg = a.wncg ? a.wncg + (size_t)ij * 2 * T.ML : nullptr;
     if (a.diag_ll && real) { src.dll = a.diag_ll + ij; src.dll_ld = (size_t)a.diag_ld; }
+    if (a.lfout && real) src.lfout = a.lfout + ij;
     PointState<R> ps;
     ps.TAUW = a.tauw[ij];
     src.run(ps);

@@ -153,6 +153,13 @@ template <typename R> struct Src {
   // dll[(NS + b) * dll_ld] (test diagnostics of the integer decisions).
   uint8_t* dll = nullptr;
   size_t dll_ld = 0;
+  // ST6 LFACTOR: when lfout is set, lane 0 stores the RTAU of the last
+  // iteration (0 when LFACTOR does not iterate); when lfreplay is set, the
+  // step takes that value instead of iterating and repeats only the last
+  // round, which gives the same LFACT and stress sums (the adjoint's
+  // recomputation from a checkpoint).
+  R* lfout = nullptr;
+  const R* lfreplay = nullptr;
   __device__ Src(const DevTables<R>& t, const STabs<R>& s, WarpWS<R>& ws, int l, int ij_, int indep, R u10, R udir,
                  R roairn, R wstar, R depth, const R* enh, int enh_ld_)
       : T(t), S(s), w(ws), lane(l), ij(ij_), INDEP(indep), U10(u10), UDIR(udir), ROAIRN(roairn), WSTAR(wstar), DEPTH(depth),
@@ -920,28 +927,32 @@ template <typename R> struct Src {
         prex = __shfl_sync(0xffffffffu, acc, 0); prey = __shfl_sync(0xffffffffu, acc, 1);
         __syncwarp();
       }
-      for (int it = 0; it < 80; ++it) {
-        nit = it + 1;
-        if (lfrec && lane == 0) lfrec[LF_RLAST] = rtau;
+      // one round: LFACT of the 10 Hz axis at RTAU r and the stress sums
+      auto round = [&](R r) {
+        if (lfrec && lane == 0) lfrec[LF_RLAST] = r;
 #pragma unroll
         for (int q = 0; q < NQ; ++q) {
           const int i = lane + 32 * q;
           if (i >= L && i < nk10) {
-            const R lf = dmin(R(1.0), crexp(rmul(qa[q], rtau)));
+            const R lf = dmin(R(1.0), crexp(rmul(qa[q], r)));
             qf[q] = lf;
             TX[i] = (qx[q] * lf) * qc[q] * qd[q];
             TY[i] = (qy[q] * lf) * qc[q] * qd[q];
           }
         }
-        {
-          __syncwarp();
-          R acc = lane == 0 ? prex : prey;
-          const R* row = lane == 0 ? TX : TY;
-          if (lane < 2)
-            for (int i = L; i < nk10; ++i) acc = radd(acc, row[i]);
-          tauwx = gro * __shfl_sync(0xffffffffu, acc, 0); tauwy = gro * __shfl_sync(0xffffffffu, acc, 1);
-          __syncwarp();
-        }
+        __syncwarp();
+        R acc = lane == 0 ? prex : prey;
+        const R* row = lane == 0 ? TX : TY;
+        if (lane < 2)
+          for (int i = L; i < nk10; ++i) acc = radd(acc, row[i]);
+        tauwx = gro * __shfl_sync(0xffffffffu, acc, 0); tauwy = gro * __shfl_sync(0xffffffffu, acc, 1);
+        __syncwarp();
+      };
+      R rlast = rtau;
+      for (int it = 0; it < (lfreplay ? 0 : 80); ++it) {
+        nit = it + 1;
+        rlast = rtau;
+        round(rtau);
         tau = total();
         err = (tau - tau_tot) / tau_tot;
         int sold = sgn;
@@ -951,9 +962,17 @@ template <typename R> struct Src {
         rtau = (sgn > 0) ? rtau * drtau : rtau * (R(1) / drtau);
         if (dabs(err) < R(1.54E-4)) break;
       }
+      if (lfreplay) {
+        rlast = *lfreplay;
+        nit = 1;
+        round(rlast);
+      }
+      if (lfout && lane == 0) *lfout = rlast;
 #pragma unroll
       for (int q = 0; q < NQ; ++q)
         if (lane + 32 * q < nk) LF[lane + 32 * q] = qf[q];
+    } else if (lfout && lane == 0) {
+      *lfout = R(0);
     }
     __syncwarp();
     bool reduce;

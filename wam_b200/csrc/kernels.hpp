@@ -34,6 +34,7 @@ template <typename R> struct ImplArgs {
   int* diag = nullptr;
   uint8_t* diag_ll = nullptr;
   int diag_ld = 0;
+  R* lfout = nullptr;  // ST6: per point the RTAU of LFACTOR's last round (0 without one), or null
 };
 
 template <typename R> cudaError_t launch_implsch(const DevTables<R>& T, const ImplArgs<R>& a, int points_per_cta, cudaStream_t s);
@@ -91,6 +92,7 @@ template <typename R> struct DerivArgs {
   // adjoint: in = adjoints of the outputs, out = adjoints of the inputs
   R *lam_fl3, *lam_tauw, *lam_u10;
   R* lam_out;  // where the adjoint kernel writes the input spectrum's adjoint (null: lam_fl3)
+  const R* lfin;  // ST6: per point the RTAU of LFACTOR's last round of the forward step (null: iterate again)
   // tangent-linear
   const R *dfl3_in, *dtauw_in, *du10;
   R *fl3_out, *dfl3_out, *tauw_out, *dtauw_out, *ustar_out, *z0_out;
