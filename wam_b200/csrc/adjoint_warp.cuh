@@ -1109,23 +1109,36 @@ template <typename R> struct AdjW {
       LLF[i] = R(0);
     }
     __syncwarp();
-    // 1. the bins: lambda of the total rate, of D1 and D2; LFACT's row adjoint
+    // 1. the bins: lambda of the total rate, of D1 and D2; LFACT's row adjoint.
+    // Directions 0..31 go one frequency at a time; the directions beyond 32
+    // of all frequencies in one pass, one lane per (frequency, direction),
+    // their row-sum terms through XC (tape space free here).
+    const int kmain = kl < 32 ? kl : 32, nx = kl - kmain;
+    R* XC = AT + 3 * nk10;
+    const bool bx = nx > 0 && 3 * nk10 + nk * nx <= 14 * nk - 16;
+    auto body1 = [&](int m, int k) -> R {
+      const int b = k + ld * m;
+      const Bin q = bin(m, k);
+      const R lfr = reduce ? LF[m] : R(1);
+      const R dtot = q.d1 * lfr - q.d2;
+      const R2 v = w.SF[b];
+      const R f = w.F[b];
+      const R ld_ = v.x * f + v.y;
+      LAM[b] = LAM[b] + v.x * dtot;
+      w.SF[b] = r2(ld_ * lfr, -ld_);  // {lambda_D1, lambda_D2}
+      return reduce ? ld_ * q.d1 : R(0);
+    };
     for (int m = 0; m < nk; ++m) {
       R llf = 0;
-      for (int k = lane; k < kl; k += 32) {
-        const int b = k + ld * m;
-        const Bin q = bin(m, k);
-        const R lfr = reduce ? LF[m] : R(1);
-        const R dtot = q.d1 * lfr - q.d2;
-        const R2 v = w.SF[b];
-        const R f = w.F[b];
-        const R ld_ = v.x * f + v.y;
-        LAM[b] = LAM[b] + v.x * dtot;
-        if (reduce) llf = llf + ld_ * q.d1;
-        w.SF[b] = r2(ld_ * lfr, -ld_);  // {lambda_D1, lambda_D2}
-      }
+      if (bx) { if (lane < kmain) llf = body1(m, lane); }
+      else for (int k = lane; k < kl; k += 32) llf = llf + body1(m, k);
       llf = warp_sum(llf);
       if (lane == 0) LLF[m] = llf;
+    }
+    if (bx) {
+      for (int it = lane; it < nk * nx; it += 32) { const int m = it / nx; XC[it] = body1(m, kmain + it - m * nx); }
+      __syncwarp();
+      for (int m = lane; m < nk; m += 32) { R t = LLF[m]; for (int x = 0; x < nx; ++x) t = t + XC[m * nx + x]; LLF[m] = t; }
     }
     __syncwarp();
     // 2. the stress sums: final (after the iteration) and first
@@ -1184,15 +1197,17 @@ template <typename R> struct AdjW {
       if (lane == 0) { LSDX[nk - 1] = LSDX[nk - 1] + ex; LSDY[nk - 1] = LSDY[nk - 1] + ey; }
     }
     __syncwarp();
-    // 3. the bins again: stress sums, growth-rate chain, narrowness
+    // 3. the bins again: stress sums, growth-rate chain, narrowness (row sums
+    // of the directions beyond 32 as in 1., in LSQ = the LLF row, free now)
     R luprox = 0;
-    for (int m = 0; m < nk; ++m) {
+    R* LSQ = LLF;
+    auto body3 = [&](int m, int k) -> R {
       const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig, sqb = SQB[m];
       const R cg = CG[m], cgzs = cg / zs, sgcg = sig / cg;
       const RecipDiv<R> qzs(zs), qcg(cg);
       const R c1 = raw * sig;
       R lsqb = 0;
-      for (int k = lane; k < kl; k += 32) {
+      {
         const int b = k + ld * m;
         const Bin q = bin(m, k);
         const R f = w.F[b];
@@ -1220,7 +1235,25 @@ template <typename R> struct AdjW {
         luprox = luprox + lproj * CI10[m] * radd(rmul(S.COSTH[k], cu), rmul(S.SINTH[k], su));
         LAM[b] = LAM[b] + la * cgzs;
       }
+      return lsqb;
+    };
+    for (int m = 0; m < nk; ++m) {
+      R lsqb = 0;
+      if (bx) { if (lane < kmain) lsqb = body3(m, lane); }
+      else for (int k = lane; k < kl; k += 32) lsqb = lsqb + body3(m, k);
       lsqb = warp_sum(lsqb);
+      if (lane == 0) LSQ[m] = lsqb;
+    }
+    if (bx) {
+      for (int it = lane; it < nk * nx; it += 32) { const int m = it / nx; XC[it] = body3(m, kmain + it - m * nx); }
+      __syncwarp();
+      for (int m = lane; m < nk; m += 32) { R t = LSQ[m]; for (int x = 0; x < nx; ++x) t = t + XC[m * nx + x]; LSQ[m] = t; }
+    }
+    __syncwarp();
+    for (int m = 0; m < nk; ++m) {
+      const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig, sqb = SQB[m];
+      const R cgzs = CG[m] / zs;
+      const R lsqb = LSQ[m];
       // SQB = sqrt(sig WN^3 q) with q = row sum / narrowness sum (= the row's
       // first maximum of a, or the row sum / KL for an empty row)
       const R lq = sqb > R(0) ? lsqb * sig * (WN[m] * WN[m] * WN[m]) / (R(2) * sqb) : R(0);
