@@ -1250,7 +1250,9 @@ template <typename R> struct AdjW {
       for (int m = lane; m < nk; m += 32) { R t = LSQ[m]; for (int x = 0; x < nx; ++x) t = t + XC[m * nx + x]; LSQ[m] = t; }
     }
     __syncwarp();
-    for (int m = 0; m < nk; ++m) {
+    // one lane per frequency: only the row's maximum bin (every bin of a row
+    // without maximum) takes the narrowness term
+    for (int m = lane; m < nk; m += 32) {
       const R sig = P_::ZPI * S.FR[m], zs = P_::ZPI * sig, sqb = SQB[m];
       const R cgzs = CG[m] / zs;
       const R lsqb = LSQ[m];
@@ -1258,11 +1260,9 @@ template <typename R> struct AdjW {
       // first maximum of a, or the row sum / KL for an empty row)
       const R lq = sqb > R(0) ? lsqb * sig * (WN[m] * WN[m] * WN[m]) / (R(2) * sqb) : R(0);
       const int kx = (int)KXR[m];
-      for (int k = lane; k < kl; k += 32) {
-        const int b = k + ld * m;
-        if (kx < 0) LAM[b] = LAM[b] + (lq / R(kl)) * cgzs;
-        else if (k == kx) LAM[b] = LAM[b] + lq * cgzs;
-      }
+      if (kx >= 0) LAM[kx + ld * m] = LAM[kx + ld * m] + lq * cgzs;
+      else
+        for (int k = 0; k < kl; ++k) LAM[k + ld * m] = LAM[k + ld * m] + (lq / R(kl)) * cgzs;
     }
     lustar = lustar + R(32.) * warp_sum(luprox);
     lus = lus + lustar;
