@@ -83,7 +83,6 @@ template <typename R> struct AdjW {
     R emean, emeanws;
     akmean = 0;
     const bool need_ak = T.shallow && T.isnonlin == 0;
-    s.integrals(nullptr, emean, fmean, need_ak ? &akmean : nullptr);
     s.airsea(TAUW0, us1, z01);
     s.shl = shl_rows(0);
     s.template sinput_ard<true>(us1, z01);
@@ -91,7 +90,7 @@ template <typename R> struct AdjW {
     s.for_bins(ml, [&](int m, int k) { LL1[k + ld * m] = w.LL[k + ld * m]; });
     for (int m = lane; m < ml; m += 32) { sx_row(0)[m] = w.t(1)[m]; sy_row(0)[m] = w.t(2)[m]; }
     __syncwarp();
-    s.integrals(w.LL, emeanws, fmeanws, nullptr);
+    s.integrals(w.LL, emean, fmean, need_ak ? &akmean : nullptr, emeanws, fmeanws);
     mij = s.frcutindex(fmean, fmeanws, us1);
     R phiaw;
     s.stresso_sums(us1, z01, mij, tauw1, phiaw);
@@ -874,7 +873,6 @@ template <typename R> struct AdjW {
     R emean, emeanws;
     akmean = 0;
     const bool need_ak = T.shallow && T.isnonlin == 0;
-    s.integrals(nullptr, emean, fmean, need_ak ? &akmean : nullptr);
     s.wavnu2();
     s.w3flx4(us1, z01);
     s.lfrec = lfrec();
@@ -884,7 +882,7 @@ template <typename R> struct AdjW {
     phase();
     s.for_bins(ml, [&](int m, int k) { LL1[k + ld * m] = w.LL[k + ld * m]; });
     __syncwarp();
-    s.integrals(w.LL, emeanws, fmeanws, nullptr);
+    s.integrals(w.LL, emean, fmean, need_ak ? &akmean : nullptr, emeanws, fmeanws);
     mij = s.frcutindex_st6(fmean, us1);
     us2 = us1; z02 = z01;
     s.imphftail(mij);  // F = F1 from here on

@@ -203,41 +203,50 @@ template <typename R> struct Src {
     __syncwarp();
   }
 
-  // TOTAL_ENERGY + FEMEAN (+ WM1 for AKMEAN); masked when mask != null.
-  // Each frequency's direction sum comes from one lane; the frequency sums run
-  // in order, with the reference's operations (interface:1342-1410, 207-286,
-  // 1591-1716), on the scratch rows 5-7 (free wherever the step calls this).
-  __device__ void integrals(const uint8_t* mask, R& emean, R& fmean, R* akmean) const {
+  // TOTAL_ENERGY + FEMEAN (+ WM1 for AKMEAN) of the spectrum, and the same
+  // masked by the wind-sea mask LLWS, in one pass (interface:1342-1410,
+  // 207-286, 1591-1716): EMEAN, FMEAN, AKMEAN when asked, EMEANWS, FMEANWS.
+  // Each frequency's two direction sums run on one lane; the frequency sums
+  // run in order, with the reference's operations, on four or five lanes at
+  // once (scratch rows 3-7, free wherever the step calls this).
+  __device__ void integrals(const uint8_t* mask, R& emean, R& fmean, R* akmean, R& emeanws, R& fmeanws) const {
     const int kl = KL(), ml = ML(), ld = w.ld;
-    R tail = 0;
+    R tail = 0, tailw = 0;
     const R DEL2 = dsqrt(P_::G) / P_::ZPI;
-    R* TE = w.t(5); R* TF = w.t(6); R* TW = w.t(7);
+    R* TE = w.t(3); R* TF = w.t(4); R* TEW = w.t(5); R* TFW = w.t(6); R* TW = w.t(7);
     for (int m = lane; m < ml; m += 32) {
-      R t = 0;
+      R t = 0, tw = 0;
       const R* f = w.F + ld * m;
-      if (mask) { const uint8_t* mk = mask + ld * m; for (int k = 0; k < kl; ++k) t = t + (mk[k] ? f[k] : R(0)); }
-      else for (int k = 0; k < kl; ++k) t = t + f[k];
+      const uint8_t* mk = mask + ld * m;
+      for (int k = 0; k < kl; ++k) { const R v = f[k]; t = t + v; tw = tw + (mk[k] ? v : R(0)); }
       TE[m] = rmul(t, S.DFIM[m]);
       TF[m] = rmul(t, S.DFIMOFR[m]);
+      TEW[m] = rmul(tw, S.DFIM[m]);
+      TFW[m] = rmul(tw, S.DFIMOFR[m]);
       if (akmean) TW[m] = T.shallow ? rmul(t / dsqrt(tfak(m)), S.DFIM[m]) : rmul(rmul(t, S.DFIMOFR[m]), DEL2);
-      if (m == ml - 1) tail = t;
+      if (m == ml - 1) { tail = t; tailw = tw; }
     }
     tail = __shfl_sync(0xffffffffu, tail, (ml - 1) & 31);
-    R* rows[3] = {TE, TF, TW};
-    const R init[3] = {rmul(T.MO_TAIL, tail), rmul(T.MM1_TAIL, tail), rmul(rmul(T.MM1_TAIL, DEL2), tail)};
-    R sum[3];
-    if (akmean) ordered_sums<3>(rows, init, ml, sum);
+    tailw = __shfl_sync(0xffffffffu, tailw, (ml - 1) & 31);
+    R* rows[5] = {TE, TF, TEW, TFW, TW};
+    const R init[5] = {rmul(T.MO_TAIL, tail), rmul(T.MM1_TAIL, tail), rmul(T.MO_TAIL, tailw), rmul(T.MM1_TAIL, tailw),
+                       rmul(rmul(T.MM1_TAIL, DEL2), tail)};
+    R sum[5];
+    if (akmean) ordered_sums<5>(rows, init, ml, sum);
     else {
-      R* rows2[2] = {TE, TF};
-      const R init2[2] = {init[0], init[1]};
-      R sum2[2];
-      ordered_sums<2>(rows2, init2, ml, sum2);
-      sum[0] = sum2[0]; sum[1] = sum2[1]; sum[2] = R(0);
+      R* rows4[4] = {TE, TF, TEW, TFW};
+      const R init4[4] = {init[0], init[1], init[2], init[3]};
+      R sum4[4];
+      ordered_sums<4>(rows4, init4, ml, sum4);
+      for (int q = 0; q < 4; ++q) sum[q] = sum4[q];
+      sum[4] = R(0);
     }
     emean = dmax(sum[0], R(1.0E-12));
     fmean = emean / dmax(sum[1], R(1.0E-12));
+    emeanws = dmax(sum[2], R(1.0E-12));
+    fmeanws = emeanws / dmax(sum[3], R(1.0E-12));
     if (akmean) {
-      const R wm = sum[2];
+      const R wm = sum[4];
       *akmean = (emean > R(1.0E-12)) ? (emean / wm) * (emean / wm) : R(1.);
     }
   }
@@ -1086,14 +1095,15 @@ template <typename R> struct Src {
     R emean, fmean, akmean = 0, emeanws, fmeanws, phiaw = 0;
     const int ju = min(300, max((int)lround((double)(U10 / T.DELU)), 1));
     ps.JU = ju;
-    integrals(nullptr, emean, fmean, (T.shallow && T.isnonlin == 0) ? &akmean : nullptr);
+    // the first spectral integrals come with the masked ones after SINPUT
+    // (neither SINPUT nor AIRSEA / W3FLX4 reads them, and F is unchanged)
     if (T.iphys == 2) { wavnu2(); w3flx4(USTAR, Z0); }
     else airsea(TAUW, USTAR, Z0);
     if (T.iphys == 1) sinput_ard(USTAR, Z0);
     else sinput_st6(USTAR, TAUW, ps.LFIT);
     phase();
     if (dll) copy_mask(0);
-    integrals(w.LL, emeanws, fmeanws, nullptr);
+    integrals(w.LL, emean, fmean, (T.shallow && T.isnonlin == 0) ? &akmean : nullptr, emeanws, fmeanws);
     int mij = (T.iphys == 2) ? frcutindex_st6(fmean, USTAR) : frcutindex(fmean, fmeanws, USTAR);
     ps.MIJ1 = mij;
     if (T.iphys == 2) { w3flx4(USTAR, Z0); }
@@ -1168,8 +1178,7 @@ template <typename R> struct Src {
       w.F[p] = dmax(f, FMIN[m] * C2[k]);
     });
     __syncwarp();
-    integrals(nullptr, emean, fmean, nullptr);
-    integrals(w.LL, emeanws, fmeanws, nullptr);
+    integrals(w.LL, emean, fmean, nullptr, emeanws, fmeanws);
     mij = (T.iphys == 2) ? frcutindex_st6(fmean, USTAR) : frcutindex(fmean, fmeanws, USTAR);
     ps.MIJ2 = mij;
     if (dll) copy_mask(1);
