@@ -1017,16 +1017,36 @@ template <typename R> struct Src {
     R* ADF = w.t(2); R* T12 = w.t(3);
     const R bnt = R(0.035) * R(0.035);
     const R xfac = (R(1.0) - R(1.0) / P_::CO) / (P_::CO - R(1.0) / P_::CO);
+    // per frequency: T1 and the T2 increment, and W3SWL6's row sum, first
+    // maximum and narrowness (one pass over the row for the two sums)
+    R* BN = w.t(4); R* AB = w.t(5);
+    R ps = 0, amax = -R(1);
+    int imax = 0;
     for (int m = lane; m < nk; m += 32) {
       R et = (P_::ZPI * bnt) / (CG[m] * (WN[m] * WN[m] * WN[m]));
-      R s = 0;
+      const R sig = P_::ZPI * S.FR[m];
       const R* fm = w.F + ld * m;
-      for (int k = 0; k < kl; ++k) s = s + fm[k];
+      const R cgs = CG[m] / (P_::ZPI * sig);
+      R s = 0, sa = 0, mx = 0;
+      for (int k = 0; k < kl; ++k) {
+        const R f = fm[k], a = f * cgs;
+        s = s + f;
+        sa = sa + a;
+        mx = (k == 0) ? a : dmax(mx, a);
+      }
       R nex = dmax(R(0.0), s * T.DELTH - et) / et;
       R nex4 = (nex * nex) * (nex * nex);
       T12[m] = R(4.75E-6) * S.FR[m] * nex4;  // T1
       R dfii = (m > 0 && m < nk - 1) ? S.DF[m] * xfac : S.DF[m];
       ADF[m] = nex4 * dfii;
+      R s2 = 0;
+      if (mx < R(1.0E-34)) s2 = R(kl);
+      else { const R rmx = R(1.) / mx; for (int k = 0; k < kl; ++k) s2 = s2 + (fm[k] * cgs) * rmx; }
+      R anar = R(1.0) / (s2 * T.DELTH);
+      AB[m] = sa;
+      BN[m] = anar * (sa * sig * T.DELTH) * (WN[m] * WN[m] * WN[m]);
+      ps = ps + sa * (P_::ZPI * S.DFIM[m] * sig) / CG[m];
+      if (sa > amax) { amax = sa; imax = m; }
     }
     __syncwarp();
     // T2 is a cumulative sum over frequency: inclusive warp scan in chunks of 32
@@ -1040,25 +1060,6 @@ template <typename R> struct Src {
       carry = __shfl_sync(0xffffffffu, v, 31);
     }
     __syncwarp();
-    // W3SWL6 per-frequency quantities
-    R* BN = w.t(4); R* AB = w.t(5);
-    R ps = 0, amax = -R(1);
-    int imax = 0;
-    for (int m = lane; m < nk; m += 32) {
-      R sig = P_::ZPI * S.FR[m];
-      const R* fm = w.F + ld * m;
-      const R cgs = CG[m] / (P_::ZPI * sig);
-      R s = 0, mx = 0;
-      for (int k = 0; k < kl; ++k) { R a = fm[k] * cgs; s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
-      R s2 = 0;
-      if (mx < R(1.0E-34)) s2 = R(kl);
-      else { const R rmx = R(1.) / mx; for (int k = 0; k < kl; ++k) s2 = s2 + (fm[k] * cgs) * rmx; }
-      R anar = R(1.0) / (s2 * T.DELTH);
-      AB[m] = s;
-      BN[m] = anar * (s * sig * T.DELTH) * (WN[m] * WN[m] * WN[m]);
-      ps = ps + s * (P_::ZPI * S.DFIM[m] * sig) / CG[m];
-      if (s > amax) { amax = s; imax = m; }
-    }
     // first maximum over frequency (MAXLOC)
     for (int o = 16; o > 0; o >>= 1) {
       R oa = __shfl_xor_sync(0xffffffffu, amax, o);
