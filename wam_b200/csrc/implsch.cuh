@@ -936,7 +936,8 @@ template <typename R> struct Src {
         prex = __shfl_sync(0xffffffffu, acc, 0); prey = __shfl_sync(0xffffffffu, acc, 1);
         __syncwarp();
       }
-      // one round: LFACT of the 10 Hz axis at RTAU r and the stress sums
+      // LFACT of the 10 Hz axis at RTAU r and the stress sums (the replay of a
+      // stored RTAU)
       auto round = [&](R r) {
         if (lfrec && lane == 0) lfrec[LF_RLAST] = r;
 #pragma unroll
@@ -958,10 +959,19 @@ template <typename R> struct Src {
         __syncwarp();
       };
       R rlast = rtau;
-      for (int it = 0; it < (lfreplay ? 0 : 80); ++it) {
-        nit = it + 1;
-        rlast = rtau;
-        round(rtau);
+      // Two iterations per round: with the sums at RTAU r the round also forms
+      // those at the two RTAU the next iteration can take (one per sign of
+      // ERR, from the same state update); the second iteration of the round
+      // then takes the one its sign selects.  Rows 3-6 (LF, SDX, SDY, CI10)
+      // are free here: their values are in the q registers, and LF is
+      // stored after the loop.
+      R* UX = w.t(3); R* UY = w.t(4); R* DX = w.t(5); R* DY = w.t(6);
+      auto next_r = [&](int s_, R r) -> R {
+        const bool ov = over || (s_ != sgn);
+        const R d = ov ? dmax(R(0.5) * (R(1.0) + drtau), R(1.00010)) : drtau;
+        return (s_ > 0) ? r * d : r * (R(1) / d);
+      };
+      auto step_state = [&]() {
         tau = total();
         err = (tau - tau_tot) / tau_tot;
         int sold = sgn;
@@ -969,6 +979,49 @@ template <typename R> struct Src {
         if (sgn != sold) over = true;
         if (over) drtau = dmax(R(0.5) * (R(1.0) + drtau), R(1.00010));
         rtau = (sgn > 0) ? rtau * drtau : rtau * (R(1) / drtau);
+      };
+      while (!lfreplay && nit < 80) {
+        const R rA = rtau, rU = next_r(1, rA), rD = next_r(-1, rA);
+        R qfU[NQ], qfD[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+          const int i = lane + 32 * q;
+          qfU[q] = qf[q]; qfD[q] = qf[q];
+          if (i >= L && i < nk10) {
+            const R la = dmin(R(1.0), crexp(rmul(qa[q], rA)));
+            const R lu = dmin(R(1.0), crexp(rmul(qa[q], rU)));
+            const R lb = dmin(R(1.0), crexp(rmul(qa[q], rD)));
+            qf[q] = la; qfU[q] = lu; qfD[q] = lb;
+            TX[i] = (qx[q] * la) * qc[q] * qd[q]; TY[i] = (qy[q] * la) * qc[q] * qd[q];
+            UX[i] = (qx[q] * lu) * qc[q] * qd[q]; UY[i] = (qy[q] * lu) * qc[q] * qd[q];
+            DX[i] = (qx[q] * lb) * qc[q] * qd[q]; DY[i] = (qy[q] * lb) * qc[q] * qd[q];
+          }
+        }
+        __syncwarp();
+        R acc = (lane & 1) ? prey : prex;
+        const R* row = lane == 0 ? TX : lane == 1 ? TY : lane == 2 ? UX : lane == 3 ? UY : lane == 4 ? DX : DY;
+        if (lane < 6)
+          for (int i = L; i < nk10; ++i) acc = radd(acc, row[i]);
+        R sm[6];
+#pragma unroll
+        for (int q = 0; q < 6; ++q) sm[q] = __shfl_sync(0xffffffffu, acc, q);
+        __syncwarp();
+        // the iteration at rA
+        nit = nit + 1;
+        rlast = rA;
+        if (lfrec && lane == 0) lfrec[LF_RLAST] = rA;
+        tauwx = gro * sm[0]; tauwy = gro * sm[1];
+        step_state();
+        if (dabs(err) < R(1.54E-4) || nit >= 80) break;
+        // the iteration at the RTAU its sign selected (rtau equals rU or rD)
+        const bool up = sgn > 0;
+        nit = nit + 1;
+        rlast = rtau;
+        if (lfrec && lane == 0) lfrec[LF_RLAST] = rtau;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) qf[q] = up ? qfU[q] : qfD[q];
+        tauwx = gro * (up ? sm[2] : sm[4]); tauwy = gro * (up ? sm[3] : sm[5]);
+        step_state();
         if (dabs(err) < R(1.54E-4)) break;
       }
       if (lfreplay) {
