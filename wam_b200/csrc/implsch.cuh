@@ -830,30 +830,28 @@ template <typename R> struct Src {
       CI10[m] = WN[m] / sig;
     }
     __syncwarp();
-    // growth rates per bin: D1 in SF.x, D2 in SF.y
-    // Only one of W1 (proj > 0) and W2 (proj < 0) is nonzero, and the other
-    // term is +0 whatever its tanh, so one tanh per bin gives the same D1, D2.
-    for_bins(nk, [&](int m, int k) {
-      R sig = P_::ZPI * S.FR[m], sqb = SQB[m];
-      R proj = rsub(rmul(uproxy * CI10[m], radd(rmul(S.COSTH[k], cu), rmul(S.SINTH[k], su))), R(1.));
-      R w1 = dmax(R(0.), proj); w1 = w1 * w1;
-      R w2 = dmin(R(0.), proj); w2 = w2 * w2;
-      const bool up = proj > R(0.);
-      const R g = R(2.8) - (R(1.) + dtanh(rsub(rmul(R(10.) * sqb, up ? w1 : w2), R(11.))));
-      R d1 = up ? raw * sig * g * sqb * w1 : R(0.);
-      R d2 = up ? R(0.) : raw * sig * R(0.09) * g * sqb * w2;
-      w.SF[k + ld * m] = r2(d1, d2);
-    });
-    __syncwarp();
-    // directional sums of the positive stress spectrum (LFACTOR :4580-4595)
+    // growth rates per bin, D1 to SF.x and D2 to SF.y, and the directional
+    // sums of the positive stress spectrum (LFACTOR :4580-4595) in one pass
+    // over each frequency row.  Only one of W1 (proj > 0) and W2 (proj < 0) is
+    // nonzero, and the other term is +0 whatever its tanh, so one tanh per bin
+    // gives the same D1, D2.
     for (int m = lane; m < nk; m += 32) {
-      R sig = P_::ZPI * S.FR[m], bx = 0, by = 0;
-      const R* fm = w.F + ld * m; const R2* d1 = w.SF + ld * m;
+      const R sig = P_::ZPI * S.FR[m], sqb = SQB[m], uci = uproxy * CI10[m];
+      R bx = 0, by = 0;
+      const R* fm = w.F + ld * m; R2* sfm = w.SF + ld * m;
       const R zs = P_::ZPI * sig, cg = CG[m];
       const RecipDiv<R> qzs(zs), qcg(cg);
       for (int k = 0; k < kl; ++k) {
+        R proj = rsub(rmul(uci, radd(rmul(S.COSTH[k], cu), rmul(S.SINTH[k], su))), R(1.));
+        R w1 = dmax(R(0.), proj); w1 = w1 * w1;
+        R w2 = dmin(R(0.), proj); w2 = w2 * w2;
+        const bool up = proj > R(0.);
+        const R g = R(2.8) - (R(1.) + dtanh(rsub(rmul(R(10.) * sqb, up ? w1 : w2), R(11.))));
+        const R d1 = up ? raw * sig * g * sqb * w1 : R(0.);
+        const R d2 = up ? R(0.) : raw * sig * R(0.09) * g * sqb * w2;
+        sfm[k] = r2(d1, d2);
         const R a = qzs(rmul(fm[k], cg));
-        const R sd = qcg(rmul(rmul(d1[k].x, a), sig));
+        const R sd = qcg(rmul(rmul(d1, a), sig));
         bx = radd(bx, rmul(dmax(R(0.), sd), S.COSTH[k]));
         by = radd(by, rmul(dmax(R(0.), sd), S.SINTH[k]));
       }
