@@ -815,15 +815,20 @@ template <typename R> struct Src {
     for (int m = lane; m < nk; m += 32) {
       R sig = P_::ZPI * S.FR[m];
       const R* fm = w.F + ld * m;
+      R2* sfm = w.SF + ld * m;  // SF.x keeps F*CG/ZS per bin until the growth rates replace it
       const R zs = P_::ZPI * sig, cg = CG[m];
       const RecipDiv<R> qzs(zs);
       R s = 0, mx = 0;
-      for (int k = 0; k < kl; ++k) { R a = qzs(rmul(fm[k], cg)); s = s + a; mx = (k == 0) ? a : dmax(mx, a); }
+      for (int k = 0; k < kl; ++k) {
+        const R a = qzs(rmul(fm[k], cg));
+        sfm[k].x = a;
+        s = s + a; mx = (k == 0) ? a : dmax(mx, a);
+      }
       R s2 = 0;
       if (mx < R(1.0E-34)) s2 = R(kl);
       else {
         const RecipDiv<R> qmx(mx);
-        for (int k = 0; k < kl; ++k) s2 = s2 + qmx(qzs(rmul(fm[k], cg)));
+        for (int k = 0; k < kl; ++k) s2 = s2 + qmx(sfm[k].x);
       }
       R adensig = s * sig * T.DELTH, anar = R(1.0) / (s2 * T.DELTH);
       SQB[m] = dsqrt(anar * adensig * (WN[m] * WN[m] * WN[m]));
@@ -838,10 +843,10 @@ template <typename R> struct Src {
     for (int m = lane; m < nk; m += 32) {
       const R sig = P_::ZPI * S.FR[m], sqb = SQB[m], uci = uproxy * CI10[m];
       R bx = 0, by = 0;
-      const R* fm = w.F + ld * m; R2* sfm = w.SF + ld * m;
-      const R zs = P_::ZPI * sig, cg = CG[m];
-      const RecipDiv<R> qzs(zs), qcg(cg);
+      R2* sfm = w.SF + ld * m;
+      const RecipDiv<R> qcg(CG[m]);
       for (int k = 0; k < kl; ++k) {
+        const R a = sfm[k].x;  // F*CG/ZS, from the first pass
         R proj = rsub(rmul(uci, radd(rmul(S.COSTH[k], cu), rmul(S.SINTH[k], su))), R(1.));
         R w1 = dmax(R(0.), proj); w1 = w1 * w1;
         R w2 = dmin(R(0.), proj); w2 = w2 * w2;
@@ -850,7 +855,6 @@ template <typename R> struct Src {
         const R d1 = up ? raw * sig * g * sqb * w1 : R(0.);
         const R d2 = up ? R(0.) : raw * sig * R(0.09) * g * sqb * w2;
         sfm[k] = r2(d1, d2);
-        const R a = qzs(rmul(fm[k], cg));
         const R sd = qcg(rmul(rmul(d1, a), sig));
         bx = radd(bx, rmul(dmax(R(0.), sd), S.COSTH[k]));
         by = radd(by, rmul(dmax(R(0.), sd), S.SINTH[k]));
