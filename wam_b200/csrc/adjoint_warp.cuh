@@ -877,12 +877,13 @@ template <typename R> struct AdjW {
     s.w3flx4(us1, z01);
     s.lfrec = lfrec();
     int nit = 0;
-    s.sinput_st6(us1, tauw1, nit);
+    R tail = 0, tailw = 0;
+    s.sinput_st6(us1, tauw1, nit, tail, tailw, need_ak);
     s.lfrec = nullptr;
     phase();
     s.for_bins(ml, [&](int m, int k) { LL1[k + ld * m] = w.LL[k + ld * m]; });
     __syncwarp();
-    s.integrals(w.LL, emean, fmean, need_ak ? &akmean : nullptr, emeanws, fmeanws);
+    s.integral_sums(tail, tailw, emean, fmean, need_ak ? &akmean : nullptr, emeanws, fmeanws);
     mij = s.frcutindex_st6(fmean, us1);
     us2 = us1; z02 = z01;
     s.imphftail(mij);  // F = F1 from here on

@@ -212,20 +212,31 @@ template <typename R> struct Src {
   __device__ void integrals(const uint8_t* mask, R& emean, R& fmean, R* akmean, R& emeanws, R& fmeanws) const {
     const int kl = KL(), ml = ML(), ld = w.ld;
     R tail = 0, tailw = 0;
-    const R DEL2 = dsqrt(P_::G) / P_::ZPI;
-    R* TE = w.t(3); R* TF = w.t(4); R* TEW = w.t(5); R* TFW = w.t(6); R* TW = w.t(7);
     for (int m = lane; m < ml; m += 32) {
       R t = 0, tw = 0;
       const R* f = w.F + ld * m;
       const uint8_t* mk = mask + ld * m;
       for (int k = 0; k < kl; ++k) { const R v = f[k]; t = t + v; tw = tw + (mk[k] ? v : R(0)); }
-      TE[m] = rmul(t, S.DFIM[m]);
-      TF[m] = rmul(t, S.DFIMOFR[m]);
-      TEW[m] = rmul(tw, S.DFIM[m]);
-      TFW[m] = rmul(tw, S.DFIMOFR[m]);
-      if (akmean) TW[m] = T.shallow ? rmul(t / dsqrt(tfak(m)), S.DFIM[m]) : rmul(rmul(t, S.DFIMOFR[m]), DEL2);
-      if (m == ml - 1) { tail = t; tailw = tw; }
+      integral_rows(m, t, tw, akmean != nullptr, tail, tailw);
     }
+    integral_sums(tail, tailw, emean, fmean, akmean, emeanws, fmeanws);
+  }
+  // The row terms of frequency m from its direction sums t (all bins) and tw
+  // (bins of the mask); lane (ML-1) mod 32 keeps the last row's sums as tails.
+  __device__ __forceinline__ void integral_rows(int m, R t, R tw, bool ak, R& tail, R& tailw) const {
+    const R DEL2 = dsqrt(P_::G) / P_::ZPI;
+    w.t(3)[m] = rmul(t, S.DFIM[m]);
+    w.t(4)[m] = rmul(t, S.DFIMOFR[m]);
+    w.t(5)[m] = rmul(tw, S.DFIM[m]);
+    w.t(6)[m] = rmul(tw, S.DFIMOFR[m]);
+    if (ak) w.t(7)[m] = T.shallow ? rmul(t / dsqrt(tfak(m)), S.DFIM[m]) : rmul(rmul(t, S.DFIMOFR[m]), DEL2);
+    if (m == ML() - 1) { tail = t; tailw = tw; }
+  }
+  // The frequency sums of the row terms in order, and the integrals.
+  __device__ void integral_sums(R tail, R tailw, R& emean, R& fmean, R* akmean, R& emeanws, R& fmeanws) const {
+    const int ml = ML();
+    const R DEL2 = dsqrt(P_::G) / P_::ZPI;
+    R* TE = w.t(3); R* TF = w.t(4); R* TEW = w.t(5); R* TFW = w.t(6); R* TW = w.t(7);
     tail = __shfl_sync(0xffffffffu, tail, (ml - 1) & 31);
     tailw = __shfl_sync(0xffffffffu, tailw, (ml - 1) & 31);
     R* rows[5] = {TE, TF, TEW, TFW, TW};
@@ -805,7 +816,7 @@ template <typename R> struct Src {
   // sum of the LFACT in order, and the exponentials and wind-direction
   // cosines correctly rounded.  Equal inputs then give the oracle's
   // iteration count unless a per-bin TANH differs by an ulp.
-  __device__ void sinput_st6(R USTAR, R& TAUW, int& nit) const {
+  __device__ void sinput_st6(R USTAR, R& TAUW, int& nit, R& tail, R& tailw, bool ak) const {
     const int kl = KL(), nk = ML(), nk10 = T.NK10, ld = w.ld;
     const R* WN = w.t(0); const R* CG = w.t(1);
     R* SQB = w.t(2); R* LF = w.t(3); R* SDX = w.t(4); R* SDY = w.t(5); R* CI10 = w.t(6);
@@ -1051,17 +1062,29 @@ template <typename R> struct Src {
     if (lfrec && lane == 0) {
       lfrec[LF_NIT] = R(nit); lfrec[LF_REDUCE] = reduce ? R(1) : R(0); lfrec[LF_TX] = tauwx; lfrec[LF_TY] = tauwy;
     }
-    for_bins(nk, [&](int m, int k) {
-      const int p = k + ld * m;
-      const R2 v = w.SF[p];
-      R d = v.x;
-      if (reduce) d = d * LF[m];
-      R dtot = d - v.y;
-      R f = w.F[p];
-      w.SF[p] = r2(dtot * f, dtot);
-      if (w.SP) w.SP[p] = d * f;
-      w.LL[p] = (d * f > R(0));
-    });
+    // The source terms and the wind-sea mask per frequency row, and with them
+    // the row sums of the (unchanged) spectrum, all bins and the mask's, that
+    // the spectral integrals after SINPUT take: their row terms replace LF
+    // (row 3, read first) and fill rows 4-7.
+    tail = R(0); tailw = R(0);
+    for (int m = lane; m < nk; m += 32) {
+      const R lfm = LF[m];
+      R t = 0, tw = 0;
+      for (int k = 0; k < kl; ++k) {
+        const int p = k + ld * m;
+        const R2 v = w.SF[p];
+        R d = v.x;
+        if (reduce) d = d * lfm;
+        R dtot = d - v.y;
+        R f = w.F[p];
+        w.SF[p] = r2(dtot * f, dtot);
+        if (w.SP) w.SP[p] = d * f;
+        const bool ll = d * f > R(0);
+        w.LL[p] = ll;
+        t = t + f; tw = tw + (ll ? f : R(0));
+      }
+      integral_rows(m, t, tw, ak, tail, tailw);
+    }
     __syncwarp();
   }
 
@@ -1156,10 +1179,12 @@ template <typename R> struct Src {
     if (T.iphys == 2) { wavnu2(); w3flx4(USTAR, Z0); }
     else airsea(TAUW, USTAR, Z0);
     if (T.iphys == 1) sinput_ard(USTAR, Z0);
-    else sinput_st6(USTAR, TAUW, ps.LFIT);
+    R tail6 = 0, tailw6 = 0;
+    if (T.iphys == 2) sinput_st6(USTAR, TAUW, ps.LFIT, tail6, tailw6, T.shallow && T.isnonlin == 0);
     phase();
     if (dll) copy_mask(0);
-    integrals(w.LL, emean, fmean, (T.shallow && T.isnonlin == 0) ? &akmean : nullptr, emeanws, fmeanws);
+    if (T.iphys == 2) integral_sums(tail6, tailw6, emean, fmean, (T.shallow && T.isnonlin == 0) ? &akmean : nullptr, emeanws, fmeanws);
+    else integrals(w.LL, emean, fmean, (T.shallow && T.isnonlin == 0) ? &akmean : nullptr, emeanws, fmeanws);
     int mij = (T.iphys == 2) ? frcutindex_st6(fmean, USTAR) : frcutindex(fmean, fmeanws, USTAR);
     ps.MIJ1 = mij;
     if (T.iphys == 2) { w3flx4(USTAR, Z0); }
@@ -1222,19 +1247,33 @@ template <typename R> struct Src {
       FMIN[m] = __ldg(&T.FLMINFR[(ju - 1) + 300 * m]);
     }
     __syncwarp();
-    for_bins(ml, [&](int m, int k) {
-      const int p = k + ld * m;
-      R f0 = w.F[p];
-      const R2 v = w.SF[p];
-      R sl = v.x, fl = v.y;
-      if (T.shallow) { sl = sl + SBO[m] * f0; fl = fl + SBO[m]; }
-      R t1 = fdiv(delt * sl, dmax(R(1.), R(1.) - delt * fl));  // divisor >= 1
-      R t3 = dmin(dabs(t1), LIM[m]);
-      R f = f0 + ((t1 >= R(0)) ? t3 : -t3);
-      w.F[p] = dmax(f, FMIN[m] * C2[k]);
-    });
-    __syncwarp();
-    integrals(w.LL, emean, fmean, nullptr, emeanws, fmeanws);
+    // one frequency row per lane: the update of its bins and, with it, the
+    // row sums of the updated spectrum (all bins and the mask's) that the
+    // spectral integrals take; their row terms replace LIM, FMIN and SBO
+    // (rows 3, 4 and 6, read first) and fill row 5
+    {
+      R tail = 0, tailw = 0;
+      for (int m = lane; m < ml; m += 32) {
+        const R lim = LIM[m], fmin = FMIN[m], sbo = T.shallow ? SBO[m] : R(0);
+        R t = 0, tw = 0;
+        for (int k = 0; k < kl; ++k) {
+          const int p = k + ld * m;
+          R f0 = w.F[p];
+          const R2 v = w.SF[p];
+          R sl = v.x, fl = v.y;
+          if (T.shallow) { sl = sl + sbo * f0; fl = fl + sbo; }
+          R t1 = fdiv(delt * sl, dmax(R(1.), R(1.) - delt * fl));  // divisor >= 1
+          R t3 = dmin(dabs(t1), lim);
+          R f = f0 + ((t1 >= R(0)) ? t3 : -t3);
+          f = dmax(f, fmin * C2[k]);
+          w.F[p] = f;
+          t = t + f; tw = tw + (w.LL[p] ? f : R(0));
+        }
+        integral_rows(m, t, tw, false, tail, tailw);
+      }
+      __syncwarp();
+      integral_sums(tail, tailw, emean, fmean, nullptr, emeanws, fmeanws);
+    }
     mij = (T.iphys == 2) ? frcutindex_st6(fmean, USTAR) : frcutindex(fmean, fmeanws, USTAR);
     ps.MIJ2 = mij;
     if (dll) copy_mask(1);
