@@ -807,25 +807,60 @@ template <typename R> struct AdjW {
     __syncwarp();
   }
 
-  // Adjoint of the spectral integrals of Fs (masked by `mask` when set) with
-  // respect to the spectrum, given the adjoints of FMEAN and AKMEAN.
-  __device__ void integrals_adj(const R* Fs, const uint8_t* mask, R lfm, R lak, bool with_ak) const {
+  // The adjoints of both integral groups of one spectrum, unmasked (FMEAN,
+  // AKMEAN) and masked by `mask` (FMEANWS), in one pass: the same sums and
+  // terms as the two groups one after the other, LAM getting the unmasked
+  // group's term first.
+  __device__ void integrals_adj2(const R* Fs, const uint8_t* mask, R lfm, R lak, bool with_ak, R lfmw) const {
     const int kl = KL(), ml = ML(), ld = w.ld;
     const R DEL2 = dsqrt(P_::G) / P_::ZPI;
-    R pe = 0, pf = 0, pa = 0, tail = 0;
+    R pe = 0, pf = 0, pa = 0, tail = 0, pe2 = 0, pf2 = 0, tail2 = 0;
     for (int m = lane; m < ml; m += 32) {
-      R t = 0;
-      for (int k = 0; k < kl; ++k) { const int b = k + ld * m; if (!mask || mask[b]) t = t + Fs[b]; }
+      R t = 0, t2 = 0;
+      for (int k = 0; k < kl; ++k) {
+        const int b = k + ld * m;
+        const R v = Fs[b];
+        t = t + v;
+        if (mask[b]) t2 = t2 + v;
+      }
       pe = pe + t * S.DFIM[m];
       pf = pf + t * S.DFIMOFR[m];
       if (with_ak) pa = pa + (T.shallow ? t / dsqrt(s.tfak(m)) * S.DFIM[m] : t * S.DFIMOFR[m] * DEL2);
-      if (m == ml - 1) tail = t;
+      pe2 = pe2 + t2 * S.DFIM[m];
+      pf2 = pf2 + t2 * S.DFIMOFR[m];
+      if (m == ml - 1) { tail = t; tail2 = t2; }
     }
     pe = warp_sum(pe); pf = warp_sum(pf); pa = warp_sum(pa);
+    pe2 = warp_sum(pe2); pf2 = warp_sum(pf2);
     tail = __shfl_sync(0xffffffffu, tail, (ml - 1) & 31);
+    tail2 = __shfl_sync(0xffffffffu, tail2, (ml - 1) & 31);
+    R lpe, lpf, lpa, ltail, lpe2, lpf2, lpa2, ltail2;
+    integral_adj_terms(pe, pf, pa, tail, lfm, lak, with_ak, lpe, lpf, lpa, ltail);
+    integral_adj_terms(pe2, pf2, R(0), tail2, lfmw, R(0), false, lpe2, lpf2, lpa2, ltail2);
+    s.for_bins(ml, [&](int m, int k) {
+      const int b = k + ld * m;
+      R lt = lpe * S.DFIM[m] + lpf * S.DFIMOFR[m];
+      if (with_ak) lt = lt + lpa * (T.shallow ? S.DFIM[m] / dsqrt(s.tfak(m)) : S.DFIMOFR[m] * DEL2);
+      if (m == ml - 1) lt = lt + ltail;
+      R v = LAM[b] + lt;
+      if (mask[b]) {
+        R lt2 = lpe2 * S.DFIM[m] + lpf2 * S.DFIMOFR[m];
+        if (m == ml - 1) lt2 = lt2 + ltail2;
+        v = v + lt2;
+      }
+      LAM[b] = v;
+    });
+    __syncwarp();
+  }
+  // The adjoints of the row-sum totals pe, pf, pa and of the tail row from
+  // those of FMEAN (lfm) and AKMEAN (lak).
+  __device__ void integral_adj_terms(R pe, R pf, R pa, R tail, R lfm, R lak, bool with_ak, R& lpe, R& lpf, R& lpa,
+                                     R& ltail) const {
+    const R DEL2 = dsqrt(P_::G) / P_::ZPI;
     const R e_raw = T.MO_TAIL * tail + pe, emean = dmax(e_raw, R(1.0E-12));
     const R den_raw = T.MM1_TAIL * tail + pf, den = dmax(den_raw, R(1.0E-12));
-    R lpe = 0, lpf = 0, lpa = 0, ltail = 0, le = 0;
+    R le = 0;
+    lpe = 0; lpf = 0; lpa = 0; ltail = 0;
     if (with_ak && emean > R(1.0E-12)) {
       const R wm = T.MM1_TAIL * DEL2 * tail + pa, qv = emean / wm;
       const R lq = lak * R(2) * qv;
@@ -837,14 +872,6 @@ template <typename R> struct AdjW {
     const R lden = -lfm * emean / (den * den);
     if (den_raw >= R(1.0E-12)) { lpf = lden; ltail = ltail + lden * T.MM1_TAIL; }
     if (e_raw >= R(1.0E-12)) { lpe = le; ltail = ltail + le * T.MO_TAIL; }
-    s.for_bins(ml, [&](int m, int k) {
-      const int b = k + ld * m;
-      R lt = lpe * S.DFIM[m] + lpf * S.DFIMOFR[m];
-      if (with_ak) lt = lt + lpa * (T.shallow ? S.DFIM[m] / dsqrt(s.tfak(m)) : S.DFIMOFR[m] * DEL2);
-      if (m == ml - 1) lt = lt + ltail;
-      if (!mask || mask[b]) LAM[b] = LAM[b] + lt;
-    });
-    __syncwarp();
   }
 
   // F <- F0 (the input spectrum), read back from global memory.
@@ -1284,8 +1311,7 @@ template <typename R> struct AdjW {
     phase();
     R lfmean = 0, lfmeanws = 0;
     if (fmeanws < fmean) lfmean = lfmx; else lfmeanws = lfmx;
-    integrals_adj(w.F, nullptr, lfmean, lak, T.shallow && T.isnonlin == 0);
-    integrals_adj(w.F, LL1, lfmeanws, R(0), false);
+    integrals_adj2(w.F, LL1, lfmean, lak, T.shallow && T.isnonlin == 0, lfmeanws);
     lU10 = lU10 + w3flx4_dus(s.U10) * lus;
     lTAUW0 = R(0);  // ST6 overwrites TAUW: the input does not enter the step
   }
@@ -1317,8 +1343,7 @@ template <typename R> struct AdjW {
     phase();
     R lfmean = 0, lfmeanws = 0;
     if (fmeanws < fmean) lfmean = lfmx; else lfmeanws = lfmx;
-    integrals_adj(w.F, nullptr, lfmean, lak, T.shallow && T.isnonlin == 0);
-    integrals_adj(w.F, LL1, lfmeanws, R(0), false);
+    integrals_adj2(w.F, LL1, lfmean, lak, T.shallow && T.isnonlin == 0, lfmeanws);
     const adj::Jac2<R> J1 = airsea_jac(s.U10, TAUW0);
     lU10 = lU10 + J1.d00 * lus1 + J1.d10 * lz01;
     lTAUW0 = J1.d01 * lus1 + J1.d11 * lz01;
