@@ -905,11 +905,11 @@ template <typename R> struct AdjW {
     s.lfrec = lfrec();
     int nit = 0;
     R tail = 0, tailw = 0;
+    s.llcopy = LL1;  // the first LLWS mask, kept for the reverse sweep
     s.sinput_st6(us1, tauw1, nit, tail, tailw, need_ak);
     s.lfrec = nullptr;
+    s.llcopy = nullptr;
     phase();
-    s.for_bins(ml, [&](int m, int k) { LL1[k + ld * m] = w.LL[k + ld * m]; });
-    __syncwarp();
     s.integral_sums(tail, tailw, emean, fmean, need_ak ? &akmean : nullptr, emeanws, fmeanws);
     mij = s.frcutindex_st6(fmean, us1);
     us2 = us1; z02 = z01;

@@ -152,6 +152,7 @@ template <typename R> struct Src {
   // SINPUT call's mask at dll[b * dll_ld], of the last one's at
   // dll[(NS + b) * dll_ld] (test diagnostics of the integer decisions).
   uint8_t* dll = nullptr;
+  uint8_t* llcopy = nullptr;  // when set, SINPUT_ST6 also writes its LLWS mask here (same layout)
   size_t dll_ld = 0;
   // ST6 LFACTOR: when lfout is set, lane 0 stores the RTAU of the last
   // iteration (0 when LFACTOR does not iterate); when lfreplay is set, the
@@ -1081,6 +1082,7 @@ template <typename R> struct Src {
         if (w.SP) w.SP[p] = d * f;
         const bool ll = d * f > R(0);
         w.LL[p] = ll;
+        if (llcopy) llcopy[p] = ll;
         t = t + f; tw = tw + (ll ? f : R(0));
       }
       integral_rows(m, t, tw, ak, tail, tailw);
